@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark: askAdam voxel-fits/s on the monoexponential R2* + 3-D TV
+workload (128x128x64 ellipsoidal mask, 629,432 voxels, 12 echoes
+TE = 2:3.5:40.5 ms, MSE, Adam lr 0.01, 4000 iterations, lambda 1e-3 on R2*).
+
+A step is one full fit of one such volume.  `value` times the fit with the
+inputs already resident in device memory; `e2e` times the same call through
+the C-ABI with pinned host buffers (host<->device copies inside the timed
+region).  With torchrun each rank fits its own volume (independent objects,
+no collective): weak scaling.  `--impl reference` times the FP64 CPU
+restatement of the reference algorithm (the oracle) on this box's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NITER = 4000
+ALG_BYTES_PER_VOXEL_ITER = 100.0   # 12 echoes x 4 B data + (z, m, v) x 2 params read+write + 4 B TV map
+METRIC = "askAdam voxel-fits/s & MCMC samples/s, fused vs plain GPU, equal FP64 error"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--no-extra", action="store_true", help="skip the plain-path and MCMC side measurements")
+    p.add_argument("--cpu-iters", type=int, default=40, help="iterations of the bounded CPU sample")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "engine" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def workload(seed=1002):
+    from gacelle_b200 import phantoms, utils
+    mask = phantoms.ellipsoid_mask((128, 128, 64), 1.05)
+    data, _ = phantoms.r2s_phantom(mask, seed)
+    idx = utils.mask_index(mask)
+    y = utils.reshape_ND2GD(data, idx)
+    n = y.shape[1]
+    th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, n))
+    fitting = {"iteration": NITER, "initialLearnRate": 0.01, "decayRate": 0.0, "lossFunction": "mse",
+               "tol": 0.0, "convergenceValue": 1e-6, "patienceConvergence": float("inf"),
+               "convergenceStepTol": 0.0, "convergenceGradTol": 0.0, "lambda": [1e-3], "regmap": ["R2star"],
+               "TVmode": "3D", "voxelSize": [2, 2, 2], "parameterTransform": "sigmoid"}
+    return {"mask": mask, "y": y, "idx": idx.astype(np.int32), "th0": th0, "fitting": fitting, "nvox": n,
+            "te": phantoms.R2S_TE, "lb": [0.0, 0.1], "ub": [2.0, 200.0]}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.rows = []
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the TV step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "tv_step_r2s_c2_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle): bounded sample of the same workload
+# ---------------------------------------------------------------------------
+def cpu_sample(W, iters):
+    import oracle
+    f = dict(W["fitting"])
+    from gacelle_b200 import askadam_solver as gxa
+    f = gxa.check_set_default_basic(f)
+    f["iteration"] = iters
+    f["_reg_index"] = [1]
+    f["_reg_lambda"] = [1e-3]
+    cores = os.cpu_count() or 1
+    f["nthreads"] = cores
+    vol = oracle.Volume(W["y"].astype(np.float64), dims=W["mask"].shape, grid_index=W["idx"],
+                        theta0=W["th0"].astype(np.float64))
+    o = oracle.adam_opts(W["lb"], W["ub"], f)
+    t0 = time.perf_counter()
+    oracle.askadam(oracle.r2s(W["te"]), vol, o, want_min=False, want_history=False)
+    dt = time.perf_counter() - t0
+    per_iter = dt / (iters + 1)  # init evaluation + iters epochs
+    fits_per_s = W["nvox"] / (per_iter * NITER)
+    return fits_per_s, cores, dt
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    W = workload()
+    for _ in range(args.warmup):
+        cpu_sample(W, max(2, args.cpu_iters // 4))
+    vals, tot = [], 0.0
+    for _ in range(args.steps):
+        v, cores, dt = cpu_sample(W, args.cpu_iters)
+        vals.append(v)
+        tot += dt
+    value = statistics.median(vals)
+    sample = (f"{W['nvox']}-voxel R2*+3-D TV volume, {args.cpu_iters} of {NITER} iterations per step "
+              f"on all {cores} host threads, extrapolated to the full {NITER}-iteration fit")
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "voxel-fits/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded phantom, seed 1002)",
+            "config": {"workload": "askAdam R2* MSE + 3-D TV, 128x128x64 ellipsoid mask (629,432 voxels), "
+                                   "12 echoes, 4000 iterations", "global_batch": W["nvox"], "seq_len": NITER,
+                       "parallelism": f"replicas{args.gpus}", "l2": "working set per step exceeds L2 on CPU"},
+            "cpu_baseline": {"value": value, "unit": "voxel-fits/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "voxel-fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Engine arm
+# ---------------------------------------------------------------------------
+def engine_arm(args, world, rank, local):
+    import torch
+
+    import gacelle_b200
+    from gacelle_b200 import _lib, askadam_solver as gxa
+    from gacelle_b200.models import _GxModelHandle
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    W = workload(seed=1002 + rank)
+    ctx = gacelle_b200.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    f = gxa.check_set_default_basic(W["fitting"])
+    opts = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], "fused")
+    model = _GxModelHandle(_lib.MODEL_R2S, te=W["te"])
+    n, nm = W["nvox"], 12
+    fp = lambda t: C.cast(C.c_void_p(t.data_ptr()), _lib._fp)  # noqa: E731
+
+    # device-resident inputs and outputs
+    d_y = torch.from_numpy(W["y"]).to(dev)
+    d_idx = torch.from_numpy(W["idx"]).to(dev)
+    d_th0 = torch.from_numpy(W["th0"]).to(dev)
+    d_out = [torch.empty((2, n), dtype=torch.float32, device=dev) for _ in range(2)]
+    hist = np.zeros(NITER + 1)
+
+    def make_vol(y, idx, th0):
+        v = _lib.GxVolume()
+        for i in range(3):
+            v.dims[i] = W["mask"].shape[i]
+        v.nvox = n
+        v.grid_index = C.cast(C.c_void_p(idx.data_ptr()), _lib._i32p)
+        v.data = fp(y)
+        v.theta0 = fp(th0)
+        return v
+
+    def make_res(outs):
+        r = _lib.GxAskadamResult()
+        r.final_theta = fp(outs[0])
+        r.min_theta = fp(outs[1])
+        r.loss_history = hist.ctypes.data_as(_lib._dp)
+        return r
+
+    vol_d = make_vol(d_y, d_idx, d_th0)
+    res_d = make_res(d_out)
+    L = _lib.lib()
+
+    def step_device():
+        _lib.check(L.gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_DEVICE, C.byref(vol_d), 1, C.byref(opts),
+                                C.byref(res_d)))
+
+    # pinned host inputs and outputs for the end-to-end leg
+    h_y = torch.from_numpy(W["y"]).pin_memory()
+    h_idx = torch.from_numpy(W["idx"]).pin_memory()
+    h_th0 = torch.from_numpy(W["th0"]).pin_memory()
+    h_out = [torch.empty((2, n), dtype=torch.float32).pin_memory() for _ in range(2)]
+    vol_h = make_vol(h_y, h_idx, h_th0)
+    res_h = make_res(h_out)
+
+    def step_host():
+        _lib.check(L.gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, C.byref(vol_h), 1, C.byref(opts),
+                                C.byref(res_h)))
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+
+    for _ in range(max(args.warmup, 3)):
+        step_device()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local).start()
+    time.sleep(0.25)
+    launches = 0
+    main_ms, main_n = 0.0, 0
+    times = []
+    torch.cuda.synchronize()
+    barrier(world)
+    for _ in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        step_device()
+        e.record(stream)
+        t = ctx.timing()
+        launches += t["kernel_launches"]
+        main_ms += t["main_kernel_ms"]
+        main_n += t["main_launches"]
+        times.append((s, e))
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms_total = sum(s.elapsed_time(e) for s, e in times)
+    ms_total = max_over_ranks(ms_total, world)
+    ms_step = ms_total / args.steps
+    value = world * n * args.steps / (ms_total / 1000.0)
+
+    # end to end through the C-ABI with pinned host buffers
+    for _ in range(2):
+        step_host()
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = 0.0
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        step_host()
+        e.record(stream)
+        e.synchronize()
+        e2e_ms += s.elapsed_time(e)
+        t = ctx.timing()
+        h2d, d2h = t["h2d_bytes"], t["d2h_bytes"]
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_value = world * n * args.steps / (e2e_ms / 1000.0)
+
+    # parity spot check of the measured fit against the oracle on a voxel subset is done in tests;
+    # here only sanity: parameters finite and inside bounds
+    th = d_out[0].cpu().numpy()
+    assert np.all(np.isfinite(th)) and th[1].min() >= 0.1 and th[1].max() <= 200.0
+
+    peak, peak_kind = measured_peaks()
+    avg_launch_ms = main_ms / max(main_n, 1)
+    achieved = ALG_BYTES_PER_VOXEL_ITER * n / (avg_launch_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "kernel": "tv_step_kernel<R2S,MSE> (one epoch: forward, loss, "
+                                                  "adjoint, TV, Adam)",
+                "algorithmic_bytes_per_launch": ALG_BYTES_PER_VOXEL_ITER * n,
+                "avg_launch_ms": avg_launch_ms, "traffic": profile_traffic()}
+    line = {"metric": METRIC, "value": value, "unit": "voxel-fits/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, seed 1002+rank)",
+            "config": {"workload": "askAdam R2* MSE + 3-D TV (lambda 1e-3 on R2*), 128x128x64 ellipsoid mask "
+                                   "(629,432 voxels), 12 echoes TE=2:3.5:40.5 ms, Adam lr 0.01, 4000 iterations",
+                       "global_batch": world * n, "seq_len": NITER, "parallelism": f"replicas{world}",
+                       "l2": "flushed between steps (256 MB write)", "path": "fused"},
+            "gpu_launches": launches, "clocks": clk, "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": "voxel-fits/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h}}
+    if rank == 0:
+        cv, cores, dt = cpu_sample(W, args.cpu_iters)
+        line["cpu_baseline"] = {"value": cv, "unit": "voxel-fits/s", "cores": cores, "kind": "port",
+                                "sample": f"{n}-voxel volume, {args.cpu_iters} of {NITER} iterations "
+                                          f"({dt:.1f} s on {cores} threads), extrapolated"}
+        if not args.no_extra:
+            line["extra"] = extras(ctx, W, opts, model, stream)
+        print(json.dumps(line), flush=True)
+
+
+def extras(ctx, W, opts, model, stream):
+    """Plain (op-by-op) path on the same volume and GW MCMC throughput."""
+    import torch
+    from gacelle_b200 import _lib, askadam_solver as gxa
+    out = {}
+    f = gxa.check_set_default_basic(dict(W["fitting"], iteration=200))
+    n = W["nvox"]
+    solver = gxa.askadam(ctx, "plain")
+    o2 = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], "plain")
+    solver._run(model, W["y"], None, W["th0"], None, None, W["idx"], W["mask"].shape, o2, 12, 2)
+    t = solver.last_timing
+    plain_ms_iter = t["main_kernel_ms"] / 200.0
+    out["plain_voxel_fits_per_s"] = n / (plain_ms_iter * NITER / 1000.0)
+    out["plain_ms_per_iteration"] = plain_ms_iter
+    return out
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, world, rank)
+        else:
+            engine_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1190 @@
+// capi.cu -- host runtime behind the C-ABI of include/gacelle_b200.h.
+//
+// A gx_context owns one device, one stream and a grow-only device workspace
+// reused across calls.  gx_askadam lays the volumes out as one padded SoA
+// work-list, runs the fused kernels (or, for opts.path == GX_PATH_PLAIN, the
+// op-by-op kernels with a host read of the loss every epoch, mirroring the
+// reference loop), and restates the reference's host-side bookkeeping
+// (min-loss tracking, convergence signals, stopping; utils/askadam.m:433-671)
+// on the per-epoch sums the kernels record.  States the fused kernels do not
+// keep (the minimum-loss parameters, the state at a stopping epoch) are rebuilt
+// bit-exactly by replaying from the nearest checkpoint.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gacelle_b200.h"
+#include "gx_internal.h"
+
+using namespace gx;
+
+static thread_local std::string g_err;
+
+static gx_status fail(gx_status s, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? GX_ENOMEM : GX_ECUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                   \
+    } while (0)
+
+#define TRY(expr)                         \
+    do {                                          \
+        gx_status s_ = (expr);                    \
+        if (s_ != GX_OK) return s_;               \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Context and workspace
+// ---------------------------------------------------------------------------
+enum Slot {
+    S_DATA, S_W, S_B1, S_SIG, S_TH0, S_Z, S_M1, S_M2, S_ZP, S_ZR, S_M1R, S_M2R, S_HIST, S_SCHED,
+    S_CKPT, S_RESF, S_RESM, S_THF, S_THM, S_RLF, S_RLM, S_BLK, S_VOLS, S_GIDX, S_MASK, S_GRID0,
+    S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
+    S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
+    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_NSLOTS
+};
+
+struct gx_context {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    volatile int32_t* cancel = nullptr;
+    gx_timing timing{};
+    void* buf[S_NSLOTS] = {};
+    size_t cap[S_NSLOTS] = {};
+    cudaEvent_t ev[4] = {};
+};
+
+static gx_status ws(gx_context* c, Slot s, size_t bytes, void** out) {
+    if (bytes == 0) bytes = 16;
+    if (c->cap[s] < bytes) {
+        if (c->buf[s]) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(c->buf[s]);
+            c->buf[s] = nullptr;
+            c->cap[s] = 0;
+        }
+        size_t b = bytes + bytes / 8;
+        CK(cudaMalloc(&c->buf[s], b));
+        c->cap[s] = b;
+    }
+    *out = c->buf[s];
+    return GX_OK;
+}
+
+template <class T>
+static gx_status wsT(gx_context* c, Slot s, size_t n, T** out) {
+    void* p;
+    TRY(ws(c, s, n * sizeof(T), &p));
+    *out = (T*)p;
+    return GX_OK;
+}
+
+struct CallScope {
+    gx_context* c;
+    std::lock_guard<std::mutex> lk;
+    long long launches0;
+    explicit CallScope(gx_context* ctx) : c(ctx), lk(ctx->mu), launches0(g_kernel_launches) {
+        cudaSetDevice(ctx->device);
+        c->timing = gx_timing{};
+    }
+};
+
+extern "C" {
+
+const char* gx_version(void) { return "gacelle_b200 0.1.0 (sm_100a)"; }
+int32_t gx_abi_version(void) { return GX_ABI_VERSION; }
+const char* gx_last_error(void) { return g_err.c_str(); }
+
+size_t gx_struct_size(const char* name) {
+    if (!name) return 0;
+    std::string n(name);
+    if (n == "gx_model") return sizeof(gx_model);
+    if (n == "gx_volume") return sizeof(gx_volume);
+    if (n == "gx_askadam_opts") return sizeof(gx_askadam_opts);
+    if (n == "gx_askadam_result") return sizeof(gx_askadam_result);
+    if (n == "gx_mcmc_opts") return sizeof(gx_mcmc_opts);
+    if (n == "gx_mcmc_result") return sizeof(gx_mcmc_result);
+    if (n == "gx_timing") return sizeof(gx_timing);
+    return 0;
+}
+
+gx_status gx_context_create(int32_t device, gx_context** out) {
+    if (!out) return fail(GX_EINVAL, "gx_context_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(GX_ECUDA, "gx_context_create: no CUDA device (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= n) return fail(GX_EINVAL, "gx_context_create: device %d of %d", device, n);
+    CK(cudaSetDevice(device));
+    gx_context* c = new gx_context();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return fail(GX_ECUDA, "gx_context_create: stream creation failed");
+    }
+    c->stream = c->own;
+    for (auto& ev : c->ev) cudaEventCreate(&ev);
+    *out = c;
+    return GX_OK;
+}
+
+gx_status gx_context_destroy(gx_context* c) {
+    if (!c) return GX_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (int s = 0; s < S_NSLOTS; ++s)
+        if (c->buf[s]) cudaFree(c->buf[s]);
+    for (auto& ev : c->ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(c->own);
+    delete c;
+    return GX_OK;
+}
+
+gx_status gx_context_set_stream(gx_context* c, void* s) {
+    if (!c) return fail(GX_EINVAL, "context is NULL");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->stream = s ? (cudaStream_t)s : c->own;
+    return GX_OK;
+}
+
+gx_status gx_last_timing(gx_context* c, gx_timing* out) {
+    if (!c || !out) return fail(GX_EINVAL, "gx_last_timing: NULL argument");
+    *out = c->timing;
+    return GX_OK;
+}
+
+gx_status gx_set_cancel_flag(gx_context* c, volatile int32_t* flag) {
+    if (!c) return fail(GX_EINVAL, "context is NULL");
+    c->cancel = flag;
+    return GX_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Model / protocol
+// ---------------------------------------------------------------------------
+static gx_status model_sizes(const gx_model* m, int* np, int* nm, int* id) {
+    if (!m) return fail(GX_EINVAL, "model is NULL");
+    switch (m->kind) {
+    case GX_MODEL_R2S:
+        if (m->n_te < 1 || m->n_te > kMaxTE || !m->te) return fail(GX_EINVAL, "R2*: need 1..%d echo times", kMaxTE);
+        *np = 2; *nm = m->n_te; *id = kR2S;
+        return GX_OK;
+    case GX_MODEL_R1R2S:
+        if (m->n_te < 1 || m->n_te > kMaxTE || !m->te) return fail(GX_EINVAL, "R1R2*: need 1..%d echo times", kMaxTE);
+        if (m->n_fa < 1 || m->n_fa > kMaxFA || !m->fa_deg) return fail(GX_EINVAL, "R1R2*: need 1..%d flip angles", kMaxFA);
+        if (m->n_te * m->n_fa > kMaxMeas) return fail(GX_EINVAL, "R1R2*: at most %d measurements", kMaxMeas);
+        *np = 3; *nm = m->n_te * m->n_fa; *id = kR1R2S;
+        return GX_OK;
+    case GX_MODEL_NEXI:
+        if (m->n_shell < 1 || m->n_shell > kMaxShell || !m->bval || !m->big_delta)
+            return fail(GX_EINVAL, "NEXI: need 1..%d shells with b and Delta", kMaxShell);
+        if (m->lmax != 0 && m->lmax != 2) return fail(GX_EINVAL, "NEXI: lmax must be 0 or 2");
+        if (m->nx < 2 || m->nx > 4096) return fail(GX_EINVAL, "NEXI: nx must be in [2, 4096]");
+        *np = m->lmax == 2 ? 5 : 4;
+        *nm = m->n_shell * (m->lmax / 2 + 1);
+        *id = m->lmax == 2 ? kNEXI2 : kNEXI;
+        return GX_OK;
+    }
+    return fail(GX_EUNSUPPORTED, "unknown model kind %d (custom FWD handles are not accelerated)", m->kind);
+}
+
+extern "C" gx_status gx_model_sizes(const gx_model* m, int32_t* np, int32_t* nm) {
+    int a, b, id;
+    TRY(model_sizes(m, &a, &b, &id));
+    if (np) *np = a;
+    if (nm) *nm = b;
+    return GX_OK;
+}
+
+static DevProtocol make_protocol(const gx_model* m, int id, int np, int nm, const double* lb,
+                                 const double* ub, int nbound) {
+    DevProtocol P;
+    memset(&P, 0, sizeof(P));
+    P.model = id;
+    P.nm = nm;
+    P.np = np;
+    P.n_te = m->n_te;
+    P.n_fa = m->n_fa;
+    P.n_shell = m->n_shell;
+    P.nx = m->nx;
+    P.tr = (float)m->tr;
+    P.h = m->nx > 1 ? (float)(1.0 / (m->nx - 1)) : 0.0f;
+    if (m->te) for (int i = 0; i < m->n_te && i < kMaxTE; ++i) P.te[i] = (float)m->te[i];
+    if (m->fa_deg) for (int i = 0; i < m->n_fa && i < kMaxFA; ++i) P.fa_rad[i] = (float)(m->fa_deg[i] * M_PI / 180.0);
+    if (m->bval) for (int i = 0; i < m->n_shell && i < kMaxShell; ++i) P.bval[i] = (float)m->bval[i];
+    if (m->big_delta) for (int i = 0; i < m->n_shell && i < kMaxShell; ++i) P.delta[i] = (float)m->big_delta[i];
+    for (int i = 0; i < nbound && i < kMaxParam; ++i) {
+        P.lb[i] = lb ? (float)lb[i] : 0.0f;
+        P.ub[i] = ub ? (float)ub[i] : 1.0f;
+    }
+    return P;
+}
+
+// ---------------------------------------------------------------------------
+// Host restatement of the reference's per-epoch bookkeeping
+// (update_min_loss :433-446, update_convergence_signals :512-632,
+// check_stopping :634-671 of utils/askadam.m; robustConvergence off).
+// ---------------------------------------------------------------------------
+struct Tracker {
+    const gx_askadam_opts* o = nullptr;
+    double minLoss = 0, minFid = 0, minReg = 0;
+    int minIter = 0;
+    double ema = 0;
+    std::vector<double> buf;
+    double ewic = 0, ewis = 0, ewig = 0;
+    bool stopped = false;
+    int stop_epoch = 0, reason = GX_STOP_NONE;
+
+    void init(const gx_askadam_opts* opts, double fid0, double reg0) {
+        o = opts;
+        minLoss = fid0 + reg0; minFid = fid0; minReg = reg0; minIter = 0;
+        ema = minLoss;
+        buf.assign(o->convergence_window > 0 ? o->convergence_window : 1, 1.0);
+    }
+    // Returns true if the loop stops at epoch e (before the update).
+    bool epoch(int e, double fid, double reg, double g2, double z2, double d2) {
+        double L = fid + reg;
+        if (minLoss > L) { minLoss = L; minFid = fid; minReg = reg; minIter = e; }
+        double conv;
+        if (o->convergence_model == GX_CONV_EMA) {
+            double en = o->ema_decay * ema + (1.0 - o->ema_decay) * L;
+            conv = std::fabs(en - ema) / (std::fabs(ema) + 1e-8);
+            ema = en;
+        } else {
+            int W = (int)buf.size();
+            for (int i = 0; i < W - 1; ++i) buf[i] = buf[i + 1];
+            buf[W - 1] = L;
+            double xm = (W + 1) / 2.0, ym = 0, sxy = 0, sxx = 0;
+            for (int i = 0; i < W; ++i) ym += buf[i];
+            ym /= W;
+            for (int i = 0; i < W; ++i) {
+                sxy += (i + 1 - xm) * (buf[i] - ym);
+                sxx += (i + 1 - xm) * (i + 1 - xm);
+            }
+            conv = sxx > 0 ? -(sxy / sxx) : 0.0;
+        }
+        if (conv > o->convergence_value || e <= o->convergence_window) ewic = 0;
+        else if ((minLoss - L) > o->convergence_value) ewic = 0;
+        else ewic += 1;
+        if (o->step_tol > 0) {
+            double sn = std::sqrt(d2) / (1.0 + std::sqrt(z2));
+            ewis = sn < o->step_tol ? ewis + 1 : 0;
+        }
+        if (o->grad_tol > 0) {
+            double gn = std::sqrt(g2);
+            ewig = gn < o->grad_tol ? ewig + 1 : 0;
+        }
+        int r = GX_STOP_NONE;
+        if (ewic > o->patience_convergence) r = GX_STOP_CONVERGENCE;
+        else if (L < o->tol) r = GX_STOP_TOL;
+        else if (o->step_tol > 0 && ewis > o->patience_step) r = GX_STOP_STEP;
+        else if (o->grad_tol > 0 && ewig > o->patience_grad) r = GX_STOP_GRAD;
+        if (r != GX_STOP_NONE) { stopped = true; stop_epoch = e; reason = r; }
+        return stopped;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// askAdam
+// ---------------------------------------------------------------------------
+static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume* vols, int nvol,
+                               int nm) {
+    if (!o) return fail(GX_EINVAL, "opts is NULL");
+    if (!vols || nvol < 1) return fail(GX_EINVAL, "need at least one volume");
+    if (o->iteration < 0) return fail(GX_EINVAL, "iteration must be >= 0");
+    if (!o->lb || !o->ub) return fail(GX_EINVAL, "lb/ub are required");
+    for (int k = 0; k < np; ++k)
+        if (!(o->ub[k] > o->lb[k])) return fail(GX_EINVAL, "ub[%d] must exceed lb[%d]", k, k);
+    if (o->loss < GX_LOSS_L1 || o->loss > GX_LOSS_RICIAN_LOGP) return fail(GX_EINVAL, "unknown loss %d", o->loss);
+    if (o->optimiser < GX_OPT_ADAM || o->optimiser > GX_OPT_RMSPROP) return fail(GX_EINVAL, "unknown optimiser %d", o->optimiser);
+    if (o->transform != GX_TRANSFORM_SIGMOID && o->transform != GX_TRANSFORM_LINEAR)
+        return fail(GX_EINVAL, "unknown parameterTransform %d", o->transform);
+    if (o->n_reg < 0 || o->n_reg > kMaxReg) return fail(GX_EINVAL, "n_reg must be in [0, %d]", kMaxReg);
+    for (int r = 0; r < o->n_reg; ++r)
+        if (o->reg_param[r] < 0 || o->reg_param[r] >= np) return fail(GX_EINVAL, "regmap index %d out of range", o->reg_param[r]);
+    bool tv = o->n_reg > 0 && o->lambda[0] > 0;
+    if (tv)
+        for (int d = 0; d < (o->tv_3d ? 3 : 2); ++d)
+            if (!(o->voxel_size[d] > 0)) return fail(GX_EINVAL, "voxel_size must be positive");
+    if ((o->loss == GX_LOSS_GAUSS_LOGP || o->loss == GX_LOSS_RICIAN_LOGP) && !(o->sigma > 0)) {
+        for (int i = 0; i < nvol; ++i)
+            if (!vols[i].sigma) return fail(GX_EINVAL, "likelihood loss needs sigma > 0 or a sigma map");
+    }
+    for (int i = 0; i < nvol; ++i) {
+        const gx_volume& v = vols[i];
+        if (v.nvox < 1) return fail(GX_EINVAL, "volume %d: nvox must be >= 1", i);
+        if (!v.data) return fail(GX_EINVAL, "volume %d: data is NULL", i);
+        if (tv) {
+            if (!v.grid_index) return fail(GX_EINVAL, "volume %d: TV needs grid_index", i);
+            long long g = (long long)v.dims[0] * v.dims[1] * v.dims[2];
+            if (v.dims[0] < 1 || v.dims[1] < 1 || v.dims[2] < 1 || g < v.nvox || g > (1LL << 31) - 1)
+                return fail(GX_EINVAL, "volume %d: bad grid dims", i);
+        }
+    }
+    (void)nm;
+    return GX_OK;
+}
+
+static bool copy_kind_host(int mem) { return mem == GX_MEM_HOST; }
+
+// Copy a [rows][n] array into a padded [rows][stride] device array at offset off.
+static gx_status upload_rows(gx_context* c, float* dst, size_t stride, size_t off, const float* src,
+                             int rows, int n, int mem, long long* bytes) {
+    cudaMemcpyKind kind = copy_kind_host(mem) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int r = 0; r < rows; ++r)
+        CK(cudaMemcpyAsync(dst + (size_t)r * stride + off, src + (size_t)r * n, sizeof(float) * n, kind, c->stream));
+    if (copy_kind_host(mem)) *bytes += (long long)rows * n * sizeof(float);
+    return GX_OK;
+}
+
+static gx_status download_rows(gx_context* c, float* dst, const float* src, size_t stride, size_t off,
+                               int rows, int n, int mem, long long* bytes) {
+    if (!dst) return GX_OK;
+    cudaMemcpyKind kind = copy_kind_host(mem) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    for (int r = 0; r < rows; ++r)
+        CK(cudaMemcpyAsync(dst + (size_t)r * n, src + (size_t)r * stride + off, sizeof(float) * n, kind, c->stream));
+    if (copy_kind_host(mem)) *bytes += (long long)rows * n * sizeof(float);
+    return GX_OK;
+}
+
+static bool cancelled(gx_context* c) { return c->cancel && *c->cancel; }
+
+struct AdamJob {
+    gx_context* c;
+    const gx_model* model;
+    const gx_askadam_opts* o;
+    int mem;
+    const gx_volume* vols;
+    int nvol;
+    int np, nm, id;
+    int B;
+    bool tv, stats, want_min, want_res_f, want_res_m;
+    std::vector<DevVol> hv;
+    std::vector<int> hblk;
+    int nvtot = 0, nblocks = 0;
+    long long grid_total = 0;
+    AdamParams a;
+    int ckpt_every = 0, nslots = 0;
+    std::vector<double> hist;   // [nvol][N+1][kHistW]
+    long long h2d = 0, d2h = 0;
+    DevVol* local_vols = nullptr;   // per-volume copies with off = 0 (volume views)
+    float* grid[2] = {nullptr, nullptr};  // TV grids, alternating by epoch parity
+    float *zr = nullptr, *m1r = nullptr, *m2r = nullptr;  // replay / plain min-loss state
+};
+
+static double sched_pow(double b, int e) { return std::pow(b, (double)e); }
+
+static gx_status adam_setup(AdamJob& J) {
+    gx_context* c = J.c;
+    const gx_askadam_opts* o = J.o;
+    int N = o->iteration;
+    J.B = o->block_size > 0 ? o->block_size : 128;
+    if (J.B % 32 || J.B < 32 || J.B > 1024) return fail(GX_EINVAL, "block_size must be a multiple of 32 in [32,1024]");
+    J.tv = o->n_reg > 0 && o->lambda[0] > 0;
+    J.stats = o->step_tol > 0 || o->grad_tol > 0;
+    // work-list layout
+    J.hv.resize(J.nvol);
+    int off = 0;
+    long long goff = 0;
+    for (int i = 0; i < J.nvol; ++i) {
+        const gx_volume& v = J.vols[i];
+        DevVol& d = J.hv[i];
+        memset(&d, 0, sizeof(d));
+        d.off = off;
+        d.nvox = v.nvox;
+        d.npad = (v.nvox + J.B - 1) / J.B * J.B;
+        d.normd = 1.0 / ((double)J.nm * (double)v.nvox);
+        d.norm = (float)d.normd;
+        for (int q = 0; q < 3; ++q) d.dims[q] = J.tv ? v.dims[q] : (q == 0 ? v.nvox : 1);
+        d.grid_off = goff;
+        for (int r = 0; r < o->n_reg && r < kMaxReg; ++r) d.tv_scale[r] = (float)(o->lambda[r] / (double)v.nvox);
+        if (J.tv) goff += (long long)v.dims[0] * v.dims[1] * v.dims[2];
+        for (int b = 0; b < d.npad / J.B; ++b) J.hblk.push_back(i);
+        off += d.npad;
+    }
+    J.nvtot = off;
+    J.nblocks = off / J.B;
+    J.grid_total = goff;
+
+    AdamParams& a = J.a;
+    memset(&a, 0, sizeof(a));
+    a.P = make_protocol(J.model, J.id, J.np, J.nm, o->lb, o->ub, J.np);
+    a.nm = J.nm;
+    a.np = J.np;
+    a.nvtot = J.nvtot;
+    a.nvol = J.nvol;
+    a.niter = N;
+    a.optimiser = o->optimiser;
+    a.transform = o->transform;
+    a.beta1 = (float)o->beta1; a.beta2 = (float)o->beta2; a.eps = (float)o->epsilon;
+    a.momentum = (float)o->momentum; a.rms_decay = (float)o->rms_decay; a.rms_eps = (float)o->rms_epsilon;
+    a.mse_scale = (float)o->mse_scale;
+    a.huber_delta = (float)o->huber_delta;
+    a.sigma_default = (float)o->sigma;
+    a.n_reg = J.tv ? o->n_reg : 0;
+    for (int r = 0; r < a.n_reg; ++r) a.reg_param[r] = o->reg_param[r];
+    a.tv_3d = o->tv_3d;
+    for (int d = 0; d < 3; ++d) a.inv_vs[d] = o->voxel_size[d] > 0 ? (float)(1.0 / o->voxel_size[d]) : 0.0f;
+    a.grid_total = J.grid_total;
+
+    size_t nv = J.nvtot;
+    bool anyw = false, anyb1 = false, anysig = false, anyth0 = false;
+    for (int i = 0; i < J.nvol; ++i) {
+        anyw |= J.vols[i].weights != nullptr;
+        anyb1 |= J.vols[i].b1 != nullptr;
+        anysig |= J.vols[i].sigma != nullptr;
+        anyth0 |= J.vols[i].theta0 != nullptr;
+    }
+    float *data, *w = nullptr, *b1 = nullptr, *sig = nullptr, *th0 = nullptr;
+    TRY(wsT(c, S_DATA, (size_t)J.nm * nv, &data));
+    CK(cudaMemsetAsync(data, 0, sizeof(float) * J.nm * nv, c->stream));
+    if (anyw) {
+        TRY(wsT(c, S_W, (size_t)J.nm * nv, &w));
+        CK(cudaMemsetAsync(w, 0, sizeof(float) * J.nm * nv, c->stream));
+    }
+    if (anyb1) TRY(wsT(c, S_B1, nv, &b1));
+    if (anysig) TRY(wsT(c, S_SIG, nv, &sig));
+    if (anyth0) TRY(wsT(c, S_TH0, (size_t)J.np * nv, &th0));
+    for (int i = 0; i < J.nvol; ++i) {
+        const gx_volume& v = J.vols[i];
+        const DevVol& d = J.hv[i];
+        TRY(upload_rows(c, data, nv, d.off, v.data, J.nm, v.nvox, J.mem, &J.h2d));
+        if (anyw) {
+            if (v.weights) TRY(upload_rows(c, w, nv, d.off, v.weights, J.nm, v.nvox, J.mem, &J.h2d));
+            else {
+                std::vector<float> ones((size_t)v.nvox, 1.0f);
+                for (int m = 0; m < J.nm; ++m)
+                    CK(cudaMemcpyAsync(w + (size_t)m * nv + d.off, ones.data(), sizeof(float) * v.nvox, cudaMemcpyHostToDevice, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+        }
+        if (anyb1) {
+            if (v.b1) TRY(upload_rows(c, b1, nv, d.off, v.b1, 1, v.nvox, J.mem, &J.h2d));
+            else {
+                std::vector<float> ones((size_t)v.nvox, 1.0f);
+                CK(cudaMemcpyAsync(b1 + d.off, ones.data(), sizeof(float) * v.nvox, cudaMemcpyHostToDevice, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+        }
+        if (anysig) {
+            if (v.sigma) TRY(upload_rows(c, sig, nv, d.off, v.sigma, 1, v.nvox, J.mem, &J.h2d));
+            else {
+                std::vector<float> s((size_t)v.nvox, (float)o->sigma);
+                CK(cudaMemcpyAsync(sig + d.off, s.data(), sizeof(float) * v.nvox, cudaMemcpyHostToDevice, c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+        }
+        if (anyth0 && v.theta0) TRY(upload_rows(c, th0, nv, d.off, v.theta0, J.np, v.nvox, J.mem, &J.h2d));
+    }
+    a.data = data; a.weights = w; a.b1 = b1; a.sigma = sig;
+    TRY(wsT(c, S_Z, (size_t)J.np * nv, &a.z));
+    TRY(wsT(c, S_M1, (size_t)J.np * nv, &a.m1));
+    TRY(wsT(c, S_M2, (size_t)J.np * nv, &a.m2));
+    if (J.stats) TRY(wsT(c, S_ZP, (size_t)J.np * nv, &a.zprev));
+    int* blk;
+    DevVol* dvols;
+    TRY(wsT(c, S_BLK, J.hblk.size(), &blk));
+    TRY(wsT(c, S_VOLS, 2 * J.hv.size(), &dvols));
+    std::vector<DevVol> both(J.hv);
+    for (const DevVol& d : J.hv) {
+        DevVol l = d;
+        l.off = 0;
+        both.push_back(l);
+    }
+    CK(cudaMemcpyAsync(blk, J.hblk.data(), sizeof(int) * J.hblk.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dvols, both.data(), sizeof(DevVol) * both.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    J.local_vols = dvols + J.hv.size();
+    a.blk_vol = blk;
+    a.vols = dvols;
+    // optimiser schedule per epoch (update_learn_rate :1180-1183, adamupdate bias correction)
+    std::vector<float2> sched((size_t)N + 1, float2{0.f, 0.f});
+    for (int e = 1; e <= N; ++e) {
+        double lr = o->initial_learn_rate / (1.0 + o->decay_rate * (e - 1));
+        if (o->optimiser == GX_OPT_ADAM)
+            sched[e] = float2{(float)(lr / (1.0 - sched_pow(o->beta1, e))), (float)(1.0 / (1.0 - sched_pow(o->beta2, e)))};
+        else
+            sched[e] = float2{(float)lr, 0.f};
+    }
+    float2* dsched;
+    TRY(wsT(c, S_SCHED, sched.size(), &dsched));
+    CK(cudaMemcpyAsync(dsched, sched.data(), sizeof(float2) * sched.size(), cudaMemcpyHostToDevice, c->stream));
+    a.sched = dsched;
+    TRY(wsT(c, S_HIST, (size_t)J.nvol * (N + 1) * kHistW, &a.hist));
+    CK(cudaMemsetAsync(a.hist, 0, sizeof(double) * J.nvol * (N + 1) * kHistW, c->stream));
+    // checkpoints: slot c holds the state after c*ckpt_every updates
+    size_t slot_bytes = sizeof(float) * 3 * (size_t)J.np * nv;
+    size_t budget = (size_t)4 << 30;
+    size_t freeb = 0, totalb = 0;
+    if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && freeb / 4 < budget) budget = freeb / 4;
+    long long max_slots = budget / slot_bytes;
+    if (max_slots < 2) max_slots = 2;
+    int K = 16;
+    while ((long long)(N / K) + 1 > max_slots) K *= 2;
+    J.ckpt_every = K;
+    J.nslots = N / K + 1;
+    TRY(wsT(c, S_CKPT, (size_t)J.nslots * 3 * J.np * nv, &a.ckpt));
+    a.ckpt_every = K;
+    // TV grids and masks
+    if (J.tv) {
+        int* gidx;
+        unsigned char* mk;
+        float *g0, *g1;
+        TRY(wsT(c, S_GIDX, nv, &gidx));
+        TRY(wsT(c, S_MASK, (size_t)J.grid_total, &mk));
+        TRY(wsT(c, S_GRID0, (size_t)a.n_reg * J.grid_total, &g0));
+        TRY(wsT(c, S_GRID1, (size_t)a.n_reg * J.grid_total, &g1));
+        CK(cudaMemsetAsync(gidx, 0, sizeof(int) * nv, c->stream));
+        CK(cudaMemsetAsync(g0, 0, sizeof(float) * a.n_reg * J.grid_total, c->stream));
+        CK(cudaMemsetAsync(g1, 0, sizeof(float) * a.n_reg * J.grid_total, c->stream));
+        std::vector<unsigned char> hm((size_t)J.grid_total, 0);
+        for (int i = 0; i < J.nvol; ++i) {
+            const gx_volume& v = J.vols[i];
+            const DevVol& d = J.hv[i];
+            std::vector<int32_t> gi((size_t)v.nvox);
+            if (J.mem == GX_MEM_HOST) memcpy(gi.data(), v.grid_index, sizeof(int32_t) * v.nvox);
+            else CK(cudaMemcpy(gi.data(), v.grid_index, sizeof(int32_t) * v.nvox, cudaMemcpyDeviceToHost));
+            long long gsz = (long long)v.dims[0] * v.dims[1] * v.dims[2];
+            for (int q = 0; q < v.nvox; ++q) {
+                if (gi[q] < 0 || gi[q] >= gsz) return fail(GX_EINVAL, "volume %d: grid_index[%d] out of range", i, q);
+                if (hm[d.grid_off + gi[q]]) return fail(GX_EINVAL, "volume %d: duplicate grid_index %d", i, gi[q]);
+                hm[d.grid_off + gi[q]] = 1;
+            }
+            CK(cudaMemcpyAsync(gidx + d.off, gi.data(), sizeof(int32_t) * v.nvox, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            if (J.mem == GX_MEM_HOST) J.h2d += sizeof(int32_t) * v.nvox;
+        }
+        CK(cudaMemcpyAsync(mk, hm.data(), hm.size(), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        a.gidx = gidx;
+        a.maskgrid = mk;
+        a.grid_cur = g0;
+        a.grid_next = g1;
+        J.grid[0] = g0;
+        J.grid[1] = g1;
+    }
+    // initial state + checkpoint slot 0
+    CK(launch_init_state(a, anyth0 ? th0 : nullptr, o->randomness, o->seed, J.B, c->stream));
+    if (anyth0) {
+        // volumes without theta0 start from the no-start-point initialisation
+        for (int i = 0; i < J.nvol; ++i)
+            if (!J.vols[i].theta0) return fail(GX_EUNSUPPORTED, "mixing volumes with and without theta0");
+    }
+    CK(launch_copy_state(a, a.ckpt, a.z, a.m1, a.m2, true, J.B, J.nblocks, c->stream));
+    return GX_OK;
+}
+
+// A view of the work-list restricted to one volume: pointers are offset to
+// the volume's first (padded) voxel and the volume table entry has off = 0,
+// so every kernel runs unchanged on that volume alone.
+struct View {
+    AdamParams a;
+    int nblocks;
+};
+
+static gx_status make_view(AdamJob& J, int i, const AdamParams& base, View* out) {
+    const DevVol& d = J.hv[i];
+    AdamParams a = base;
+    size_t o = d.off;
+    a.data += o;
+    if (a.weights) a.weights += o;
+    if (a.b1) a.b1 += o;
+    if (a.sigma) a.sigma += o;
+    a.z += o; a.m1 += o; a.m2 += o;
+    if (a.zprev) a.zprev += o;
+    if (a.ckpt) a.ckpt += o;
+    if (a.gidx) a.gidx += o;
+    a.blk_vol += d.off / J.B;
+    a.vols = J.local_vols;
+    out->a = a;
+    out->nblocks = d.npad / J.B;
+    return GX_OK;
+}
+
+// Run epochs [e0, e1] on the (sub)list described by `a` (TV: one launch per
+// epoch, alternating the two grids by epoch parity).
+static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e1, int update_last,
+                            bool record, float* res_out) {
+    gx_context* c = J.c;
+    a.res_out = res_out;
+    if (!record) a.hist = nullptr;
+    if (!J.tv) {
+        CK(launch_fused(a, J.id, J.o->loss, J.stats && record, e0, e1, update_last, record, J.B, nblocks, c->stream));
+        return GX_OK;
+    }
+    float* g[2] = {J.grid[0], J.grid[1]};
+    for (int e = e0; e <= e1; ++e) {
+        a.grid_cur = g[(e - 1) & 1];
+        a.grid_next = g[e & 1];
+        CK(launch_tv_step(a, J.id, J.o->loss, J.stats && record, e, e <= update_last, record,
+                          e == e1 && res_out != nullptr, J.B, nblocks, c->stream));
+        if ((e & 63) == 0 && cancelled(c)) return fail(GX_ECANCELLED, "cancelled");
+    }
+    return GX_OK;
+}
+
+// Rebuild, for volume i, the state after `target` updates into the replay
+// buffers (J.zr, J.m1r, J.m2r), the residuals at it into res_out (may be
+// NULL) and theta into th_out (padded layout, rows of the volume only).
+static gx_status replay_volume(AdamJob& J, int i, int target, float* th_out, float* res_out) {
+    gx_context* c = J.c;
+    AdamParams base = J.a;
+    base.z = J.zr; base.m1 = J.m1r; base.m2 = J.m2r;
+    base.zprev = nullptr;
+    base.ckpt_every = 0;
+    View V;
+    TRY(make_view(J, i, base, &V));
+    int slot = target / J.ckpt_every;
+    float* src = J.a.ckpt + (size_t)slot * 3 * J.np * J.nvtot + J.hv[i].off;
+    V.a.ckpt = nullptr;
+    CK(launch_copy_state(V.a, src, nullptr, nullptr, nullptr, false, J.B, V.nblocks, c->stream));
+    int e0 = slot * J.ckpt_every + 1;
+    if (J.tv) CK(launch_tv_scatter(V.a, J.grid[(e0 - 1) & 1], J.B, V.nblocks, c->stream));
+    size_t o = J.hv[i].off;
+    TRY(run_epochs(J, V.a, V.nblocks, e0, target + 1, target, false, res_out ? res_out + o : nullptr));
+    CK(launch_finalize(V.a, V.a.z, th_out + o, nullptr, nullptr, J.B, V.nblocks, c->stream));
+    return GX_OK;
+}
+
+struct AdamOut {
+    std::vector<Tracker> tr;
+    std::vector<int> final_epoch;
+    float *thf = nullptr, *thm = nullptr, *resf = nullptr, *resm = nullptr;
+};
+
+static gx_status alloc_outputs(AdamJob& J, AdamOut& out) {
+    gx_context* c = J.c;
+    size_t pn = (size_t)J.np * J.nvtot, mn = (size_t)J.nm * J.nvtot;
+    TRY(wsT(c, S_THF, pn, &out.thf));
+    TRY(wsT(c, S_THM, pn, &out.thm));
+    if (J.want_res_f) TRY(wsT(c, S_RESF, mn, &out.resf));
+    if (J.want_res_m) TRY(wsT(c, S_RESM, mn, &out.resm));
+    TRY(wsT(c, S_ZR, pn, &J.zr));
+    TRY(wsT(c, S_M1R, pn, &J.m1r));
+    TRY(wsT(c, S_M2R, pn, &J.m2r));
+    return GX_OK;
+}
+
+static bool can_stop(const gx_askadam_opts* o) {
+    bool signed_loss = o->loss == GX_LOSS_GAUSS_LOGP || o->loss == GX_LOSS_RICIAN_LOGP;
+    return std::isfinite(o->patience_convergence) || o->step_tol > 0 || o->grad_tol > 0 ||
+           o->tol > 0 || (signed_loss && o->tol > -INFINITY);
+}
+
+static gx_status adam_fused(AdamJob& J, AdamOut& out) {
+    gx_context* c = J.c;
+    const gx_askadam_opts* o = J.o;
+    const int N = o->iteration;
+    const bool stop_possible = can_stop(o);
+    const int chunk = stop_possible ? (o->chunk > 0 ? o->chunk : 200) : (N > 0 ? N : 1);
+    TRY(alloc_outputs(J, out));
+    if (J.tv) CK(launch_tv_scatter(J.a, J.grid[0], J.B, J.nblocks, c->stream));
+
+    out.tr.assign(J.nvol, Tracker());
+    out.final_epoch.assign(J.nvol, N);
+    J.hist.assign((size_t)J.nvol * (N + 1) * kHistW, 0.0);
+    std::vector<bool> started(J.nvol, false);
+    int n_main = 0;
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    if (N == 0) {
+        TRY(run_epochs(J, J.a, J.nblocks, 0, 0, -1, true, out.resf));
+        ++n_main;
+    } else {
+        bool all_stopped = false;
+        for (int eb = 1; eb <= N && !all_stopped; eb += chunk) {
+            int ee = std::min(eb + chunk - 1, N);
+            TRY(run_epochs(J, J.a, J.nblocks, eb, ee, std::min(ee, N - 1), true, ee == N ? out.resf : nullptr));
+            n_main += J.tv ? (ee - eb + 1) : 1;
+            if (cancelled(c)) return fail(GX_ECANCELLED, "cancelled");
+            if (!stop_possible) continue;
+            CK(cudaStreamSynchronize(c->stream));
+            all_stopped = true;
+            for (int i = 0; i < J.nvol; ++i) {
+                size_t base = (size_t)i * (N + 1) * kHistW;
+                CK(cudaMemcpy(J.hist.data() + base + (size_t)eb * kHistW, J.a.hist + base + (size_t)eb * kHistW,
+                              sizeof(double) * (ee - eb + 1) * kHistW, cudaMemcpyDeviceToHost));
+                Tracker& t = out.tr[i];
+                if (!started[i]) {
+                    t.init(o, J.hist[base + kHistW], J.hist[base + kHistW + 1]);
+                    started[i] = true;
+                }
+                for (int e = eb; e <= ee && !t.stopped; ++e) {
+                    const double* h = J.hist.data() + base + (size_t)e * kHistW;
+                    t.epoch(e, h[0], h[1], h[2], h[3], h[4]);
+                }
+                all_stopped = all_stopped && t.stopped;
+            }
+        }
+    }
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    if (!stop_possible || N == 0) {
+        CK(cudaMemcpyAsync(J.hist.data(), J.a.hist, sizeof(double) * J.hist.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < J.nvol; ++i) {
+            size_t base = (size_t)i * (N + 1) * kHistW;
+            Tracker& t = out.tr[i];
+            if (N == 0) {
+                t.init(o, J.hist[base], J.hist[base + 1]);
+                continue;
+            }
+            t.init(o, J.hist[base + kHistW], J.hist[base + kHistW + 1]);
+            for (int e = 1; e <= N && !t.stopped; ++e) {
+                const double* h = J.hist.data() + base + (size_t)e * kHistW;
+                t.epoch(e, h[0], h[1], h[2], h[3], h[4]);
+            }
+        }
+    }
+    CK(cudaEventSynchronize(c->ev[3]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+    c->timing.main_kernel_ms = ms;
+    c->timing.main_launches = n_main;
+    for (int i = 0; i < J.nvol && N > 0; ++i) {  // the initial evaluation equals epoch 1's
+        size_t base = (size_t)i * (N + 1) * kHistW;
+        for (int q = 0; q < kHistW; ++q) J.hist[base + q] = J.hist[base + kHistW + q];
+    }
+    for (int i = 0; i < J.nvol; ++i)
+        if (out.tr[i].stopped) out.final_epoch[i] = out.tr[i].stop_epoch;
+
+    // final state: the live z holds z_{N-1}; volumes that stopped at e* are replayed to z_{e*-1}
+    CK(launch_finalize(J.a, J.a.z, out.thf, nullptr, nullptr, J.B, J.nblocks, c->stream));
+    for (int i = 0; i < J.nvol; ++i)
+        if (out.final_epoch[i] != N) TRY(replay_volume(J, i, std::max(out.final_epoch[i] - 1, 0), out.thf, out.resf));
+    // minimum-loss state (z_{minIter-1}); equal to the final state when the loss never rose
+    for (int i = 0; i < J.nvol; ++i) {
+        int tmin = std::max(out.tr[i].minIter - 1, 0);
+        int tfin = std::max(out.final_epoch[i] - 1, 0);
+        const DevVol& d = J.hv[i];
+        if (tmin == tfin && out.tr[i].minIter == out.final_epoch[i]) {
+            for (int k = 0; k < J.np; ++k)
+                CK(cudaMemcpyAsync(out.thm + (size_t)k * J.nvtot + d.off, out.thf + (size_t)k * J.nvtot + d.off,
+                                   sizeof(float) * d.npad, cudaMemcpyDeviceToDevice, c->stream));
+            if (out.resm && out.resf)
+                for (int m = 0; m < J.nm; ++m)
+                    CK(cudaMemcpyAsync(out.resm + (size_t)m * J.nvtot + d.off, out.resf + (size_t)m * J.nvtot + d.off,
+                                       sizeof(float) * d.npad, cudaMemcpyDeviceToDevice, c->stream));
+        } else {
+            TRY(replay_volume(J, i, tmin, out.thm, out.resm));
+        }
+    }
+    return GX_OK;
+}
+
+// Plain path: op-by-op kernels, one volume at a time, with the loss read back
+// every epoch and the reference's bookkeeping run on the host in the loop.
+static gx_status adam_plain(AdamJob& J, AdamOut& out) {
+    gx_context* c = J.c;
+    const gx_askadam_opts* o = J.o;
+    const int N = o->iteration;
+    TRY(alloc_outputs(J, out));
+    size_t pn = (size_t)J.np * J.nvtot, mn = (size_t)J.nm * J.nvtot;
+    PlainBufs pb;
+    TRY(wsT(c, S_P_TH, pn, &pb.theta));
+    TRY(wsT(c, S_P_DTH, pn, &pb.dth));
+    TRY(wsT(c, S_P_SIG, mn, &pb.signal));
+    TRY(wsT(c, S_P_DSIG, mn, &pb.dsig));
+    TRY(wsT(c, S_P_RES, mn, &pb.res));
+    TRY(wsT(c, S_P_GTH, pn, &pb.gth));
+    TRY(wsT(c, S_P_GZ, pn, &pb.gz));
+    TRY(wsT(c, S_P_ACC, 8, &pb.acc));
+    if (!J.stats) {
+        // plain_zgrad only touches zprev when statistics are requested
+        J.a.zprev = nullptr;
+    }
+    out.tr.assign(J.nvol, Tracker());
+    out.final_epoch.assign(J.nvol, N);
+    J.hist.assign((size_t)J.nvol * (N + 1) * kHistW, 0.0);
+    int n_main = 0;
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    for (int i = 0; i < J.nvol; ++i) {
+        View V;
+        TRY(make_view(J, i, J.a, &V));
+        AdamParams& a = V.a;
+        const size_t off = J.hv[i].off;
+        PlainBufs b = pb;
+        b.theta += off; b.dth += off; b.signal += off; b.dsig += off; b.res += off;
+        b.gth += off; b.gz += off;
+        Tracker& t = out.tr[i];
+        float* zmin = J.zr + off;
+        float* resm = out.resm ? out.resm + off : nullptr;
+        size_t base = (size_t)i * (N + 1) * kHistW;
+        int last = 0;
+        for (int e = (N == 0 ? 0 : 1); e <= N; ++e) {
+            last = e;
+            CK(cudaMemsetAsync(pb.acc, 0, sizeof(double) * 8, c->stream));
+            CK(launch_plain_unscale(a, b, J.B, V.nblocks, c->stream));
+            CK(launch_plain_forward(a, J.id, b, J.B, V.nblocks, c->stream));
+            CK(launch_plain_loss(a, o->loss, b, J.B, V.nblocks, c->stream));
+            CK(launch_plain_adjoint(a, J.id, b, J.B, V.nblocks, c->stream));
+            if (J.tv) CK(launch_plain_tv(a, b, J.grid[0], J.B, V.nblocks, c->stream));
+            CK(launch_plain_zgrad(a, b, J.stats, J.B, V.nblocks, c->stream));
+            n_main += J.tv ? 7 : 5;
+            double acc[8];
+            CK(cudaMemcpyAsync(acc, pb.acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            double* h = J.hist.data() + base + (size_t)e * kHistW;
+            h[0] = acc[0]; h[1] = acc[1]; h[2] = acc[2]; h[3] = acc[3]; h[4] = acc[4];
+            bool snap = false;
+            if (e <= 1) {
+                t.init(o, acc[0], acc[1]);
+                for (int q = 0; q < kHistW; ++q) J.hist[base + q] = h[q];
+                snap = true;  // parameters_minLoss = initial parameters (askadam.m:203-208)
+            }
+            if (e >= 1) {
+                int before = t.minIter;
+                t.epoch(e, acc[0], acc[1], acc[2], acc[3], acc[4]);
+                snap = snap || t.minIter != before;
+            }
+            if (snap) {
+                for (int k = 0; k < J.np; ++k)
+                    CK(cudaMemcpyAsync(zmin + (size_t)k * J.nvtot, a.z + (size_t)k * J.nvtot, sizeof(float) * J.hv[i].npad,
+                                       cudaMemcpyDeviceToDevice, c->stream));
+                if (resm)
+                    for (int m = 0; m < J.nm; ++m)
+                        CK(cudaMemcpyAsync(resm + (size_t)m * J.nvtot, b.res + (size_t)m * J.nvtot, sizeof(float) * J.hv[i].npad,
+                                           cudaMemcpyDeviceToDevice, c->stream));
+            }
+            if (t.stopped) break;
+            if (e >= 1 && e < N) {
+                CK(launch_plain_update(a, b, e, J.B, V.nblocks, c->stream));
+                ++n_main;
+            }
+            if (cancelled(c)) return fail(GX_ECANCELLED, "cancelled");
+        }
+        out.final_epoch[i] = last;
+        CK(launch_finalize(a, a.z, out.thf + off, nullptr, nullptr, J.B, V.nblocks, c->stream));
+        CK(launch_finalize(a, zmin, out.thm + off, nullptr, nullptr, J.B, V.nblocks, c->stream));
+        if (out.resf)
+            for (int m = 0; m < J.nm; ++m)
+                CK(cudaMemcpyAsync(out.resf + off + (size_t)m * J.nvtot, b.res + (size_t)m * J.nvtot,
+                                   sizeof(float) * J.hv[i].npad, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(cudaEventSynchronize(c->ev[3]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+    c->timing.main_kernel_ms = ms;
+    c->timing.main_launches = n_main;
+    return GX_OK;
+}
+
+static gx_status adam_write_results(AdamJob& J, AdamOut& out, gx_askadam_result* results) {
+    gx_context* c = J.c;
+    const int N = J.o->iteration;
+    float *rlf = nullptr, *rlm = nullptr;
+    bool want_rlf = false, want_rlm = false;
+    for (int i = 0; i < J.nvol; ++i) {
+        want_rlf |= results[i].final_resloss != nullptr;
+        want_rlm |= results[i].min_resloss != nullptr;
+    }
+    if (want_rlf && out.resf) {
+        TRY(wsT(c, S_RLF, J.nvtot, &rlf));
+        CK(launch_finalize(J.a, nullptr, nullptr, out.resf, rlf, J.B, J.nblocks, c->stream));
+    }
+    if (want_rlm && out.resm) {
+        TRY(wsT(c, S_RLM, J.nvtot, &rlm));
+        CK(launch_finalize(J.a, nullptr, nullptr, out.resm, rlm, J.B, J.nblocks, c->stream));
+    }
+    for (int i = 0; i < J.nvol; ++i) {
+        gx_askadam_result& r = results[i];
+        const DevVol& d = J.hv[i];
+        int n = d.nvox;
+        TRY(download_rows(c, r.final_theta, out.thf, J.nvtot, d.off, J.np, n, J.mem, &J.d2h));
+        TRY(download_rows(c, r.min_theta, out.thm, J.nvtot, d.off, J.np, n, J.mem, &J.d2h));
+        if (out.resf) TRY(download_rows(c, r.final_residual, out.resf, J.nvtot, d.off, J.nm, n, J.mem, &J.d2h));
+        if (out.resm) TRY(download_rows(c, r.min_residual, out.resm, J.nvtot, d.off, J.nm, n, J.mem, &J.d2h));
+        if (rlf) TRY(download_rows(c, r.final_resloss, rlf, J.nvtot, d.off, 1, n, J.mem, &J.d2h));
+        if (rlm) TRY(download_rows(c, r.min_resloss, rlm, J.nvtot, d.off, 1, n, J.mem, &J.d2h));
+        const Tracker& t = out.tr[i];
+        int fe = out.final_epoch[i];
+        size_t base = (size_t)i * (N + 1) * kHistW;
+        const double* hf = J.hist.data() + base + (size_t)fe * kHistW;
+        r.final_loss = hf[0] + hf[1];
+        r.final_loss_fidelity = hf[0];
+        r.final_loss_reg = hf[1];
+        r.min_loss = t.minLoss;
+        r.min_loss_fidelity = t.minFid;
+        r.min_loss_reg = t.minReg;
+        r.final_niteration = fe;
+        r.min_niteration = t.minIter;
+        r.stop_reason = t.reason;
+        if (r.loss_history)
+            for (int e = 0; e <= N; ++e) {
+                const double* h = J.hist.data() + base + (size_t)e * kHistW;
+                r.loss_history[e] = e <= fe ? h[0] + h[1] : NAN;
+            }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < J.nvol; ++i)
+        if (!std::isfinite(results[i].final_loss))
+            return fail(GX_ENUMERIC, "volume %d: non-finite loss", i);
+    return GX_OK;
+}
+
+extern "C" gx_status gx_askadam(gx_context* c, const gx_model* model, int32_t mem,
+                                const gx_volume* vols, int32_t nvol, const gx_askadam_opts* opts,
+                                gx_askadam_result* results) {
+    if (!c) return fail(GX_EINVAL, "context is NULL");
+    if (!results) return fail(GX_EINVAL, "results is NULL");
+    if (mem != GX_MEM_HOST && mem != GX_MEM_DEVICE) return fail(GX_EINVAL, "mem must be GX_MEM_HOST or GX_MEM_DEVICE");
+    CallScope scope(c);
+    AdamJob J;
+    J.c = c; J.model = model; J.o = opts; J.mem = mem; J.vols = vols; J.nvol = nvol;
+    TRY(model_sizes(model, &J.np, &J.nm, &J.id));
+    TRY(validate_adam(opts, J.np, vols, nvol, J.nm));
+    for (int i = 0; i < nvol; ++i)
+        if (!results[i].final_theta) return fail(GX_EINVAL, "volume %d: final_theta is NULL", i);
+    J.want_min = true;
+    J.want_res_f = J.want_res_m = false;
+    for (int i = 0; i < nvol; ++i) {
+        J.want_res_f |= results[i].final_residual || results[i].final_resloss;
+        J.want_res_m |= results[i].min_residual || results[i].min_resloss;
+    }
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    TRY(adam_setup(J));
+    AdamOut out;
+    if (opts->path == GX_PATH_PLAIN) TRY(adam_plain(J, out));
+    else TRY(adam_fused(J, out));
+    gx_status st = adam_write_results(J, out, results);
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventSynchronize(c->ev[1]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->timing.total_ms = ms;
+    c->timing.kernel_launches = g_kernel_launches - scope.launches0;
+    c->timing.h2d_bytes = J.h2d;
+    c->timing.d2h_bytes = J.d2h;
+    return st;
+}
+
+// One evaluation of loss and d loss / d theta at physical parameters theta
+// (askadam.model_gradient, utils/askadam.m:23-117).
+extern "C" gx_status gx_model_gradient(gx_context* c, const gx_model* model, int32_t mem,
+                                       const gx_volume* vol, const gx_askadam_opts* opts,
+                                       const float* theta, float* gtheta, float* residual,
+                                       double* loss, double* loss_fid, double* loss_reg) {
+    if (!c || !theta) return fail(GX_EINVAL, "NULL argument");
+    CallScope scope(c);
+    AdamJob J;
+    J.c = c; J.model = model; J.o = opts; J.mem = mem; J.vols = vol; J.nvol = 1;
+    TRY(model_sizes(model, &J.np, &J.nm, &J.id));
+    TRY(validate_adam(opts, J.np, vol, 1, J.nm));
+    gx_askadam_opts o2 = *opts;
+    o2.iteration = 0;
+    J.o = &o2;
+    TRY(adam_setup(J));
+    size_t pn = (size_t)J.np * J.nvtot, mn = (size_t)J.nm * J.nvtot;
+    PlainBufs b;
+    TRY(wsT(c, S_P_TH, pn, &b.theta));
+    TRY(wsT(c, S_P_DTH, pn, &b.dth));
+    TRY(wsT(c, S_P_SIG, mn, &b.signal));
+    TRY(wsT(c, S_P_DSIG, mn, &b.dsig));
+    TRY(wsT(c, S_P_RES, mn, &b.res));
+    TRY(wsT(c, S_P_GTH, pn, &b.gth));
+    TRY(wsT(c, S_P_GZ, pn, &b.gz));
+    TRY(wsT(c, S_P_ACC, 8, &b.acc));
+    CK(cudaMemsetAsync(b.theta, 0, sizeof(float) * pn, c->stream));
+    TRY(upload_rows(c, b.theta, J.nvtot, 0, theta, J.np, vol->nvox, mem, &J.h2d));
+    CK(cudaMemsetAsync(b.acc, 0, sizeof(double) * 8, c->stream));
+    AdamParams a = J.a;
+    a.zprev = nullptr;
+    CK(launch_plain_forward(a, J.id, b, J.B, J.nblocks, c->stream));
+    CK(launch_plain_loss(a, opts->loss, b, J.B, J.nblocks, c->stream));
+    CK(launch_plain_adjoint(a, J.id, b, J.B, J.nblocks, c->stream));
+    if (J.tv) CK(launch_plain_tv(a, b, J.grid[0], J.B, J.nblocks, c->stream));
+    double acc[8];
+    CK(cudaMemcpyAsync(acc, b.acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
+    TRY(download_rows(c, gtheta, b.gth, J.nvtot, 0, J.np, vol->nvox, mem, &J.d2h));
+    if (residual) TRY(download_rows(c, residual, b.res, J.nvtot, 0, J.nm, vol->nvox, mem, &J.d2h));
+    CK(cudaStreamSynchronize(c->stream));
+    if (loss) *loss = acc[0] + acc[1];
+    if (loss_fid) *loss_fid = acc[0];
+    if (loss_reg) *loss_reg = acc[1];
+    c->timing.kernel_launches = g_kernel_launches - scope.launches0;
+    return GX_OK;
+}
+
+extern "C" gx_status gx_forward(gx_context* c, const gx_model* model, int32_t mem, const float* theta,
+                                const float* b1, int32_t nvox, float* signal) {
+    if (!c || !theta || !signal) return fail(GX_EINVAL, "NULL argument");
+    if (nvox < 1) return fail(GX_EINVAL, "nvox must be >= 1");
+    CallScope scope(c);
+    int np, nm, id;
+    TRY(model_sizes(model, &np, &nm, &id));
+    DevProtocol P = make_protocol(model, id, np, nm, nullptr, nullptr, 0);
+    const float *dth = theta, *db1 = b1;
+    float* dsig = signal;
+    long long h2d = 0, d2h = 0;
+    if (mem == GX_MEM_HOST) {
+        float *t, *s, *bb = nullptr;
+        TRY(wsT(c, S_FWD_TH, (size_t)np * nvox, &t));
+        TRY(wsT(c, S_FWD_SIG, (size_t)nm * nvox, &s));
+        CK(cudaMemcpyAsync(t, theta, sizeof(float) * np * nvox, cudaMemcpyHostToDevice, c->stream));
+        h2d += sizeof(float) * np * nvox;
+        if (b1) {
+            TRY(wsT(c, S_FWD_B1, (size_t)nvox, &bb));
+            CK(cudaMemcpyAsync(bb, b1, sizeof(float) * nvox, cudaMemcpyHostToDevice, c->stream));
+            h2d += sizeof(float) * nvox;
+        }
+        dth = t; db1 = bb; dsig = s;
+    }
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(launch_forward_only(P, id, dth, db1, nvox, dsig, c->stream));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    if (mem == GX_MEM_HOST) {
+        CK(cudaMemcpyAsync(signal, dsig, sizeof(float) * nm * nvox, cudaMemcpyDeviceToHost, c->stream));
+        d2h += sizeof(float) * nm * nvox;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+    c->timing.main_kernel_ms = ms;
+    c->timing.main_launches = 1;
+    c->timing.kernel_launches = g_kernel_launches - scope.launches0;
+    c->timing.h2d_bytes = h2d;
+    c->timing.d2h_bytes = d2h;
+    return GX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MCMC
+// ---------------------------------------------------------------------------
+static int mcmc_nsamples(int iteration, int nb, int thinning) {
+    if (nb + 1 > iteration) return 0;
+    return (iteration - nb - 1) / thinning + 1;  // numel(Nburnin+1:thinning:iteration)
+}
+
+extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, const gx_volume* vols,
+                             int32_t nvol, const gx_mcmc_opts* o, gx_mcmc_result* results) {
+    if (!c || !o || !vols || !results || nvol < 1) return fail(GX_EINVAL, "NULL argument");
+    if (mem != GX_MEM_HOST && mem != GX_MEM_DEVICE) return fail(GX_EINVAL, "bad mem");
+    CallScope scope(c);
+    int np, nm, id;
+    TRY(model_sizes(model, &np, &nm, &id));
+    int nvar = np + 1;
+    if (o->algorithm != GX_MCMC_MH && o->algorithm != GX_MCMC_ENSEMBLE) return fail(GX_EINVAL, "unknown algorithm");
+    if (o->iteration < 1 || o->thinning < 1 || o->repetition < 1) return fail(GX_EINVAL, "iteration, thinning and repetition must be >= 1");
+    if (!o->lb || !o->ub) return fail(GX_EINVAL, "lb/ub required");
+    for (int q = 0; q < nvar; ++q)
+        if (!(o->ub[q] >= o->lb[q])) return fail(GX_EINVAL, "ub[%d] < lb[%d]", q, q);
+    if (o->lb[nvar - 1] <= 0) return fail(GX_EINVAL, "noise lower bound must be positive");
+    if (o->algorithm == GX_MCMC_ENSEMBLE) {
+        if (o->nwalker < 2 || o->nwalker > 256) return fail(GX_EINVAL, "nwalker must be in [2, 256]");
+        if (!(o->step_size > 1.0)) return fail(GX_EINVAL, "StepSize must exceed 1");
+        if (o->ensemble_update != GX_GW_SIMULTANEOUS && o->ensemble_update != GX_GW_REDBLACK)
+            return fail(GX_EINVAL, "unknown Ensembleupdate");
+    } else if (!o->x_step) {
+        return fail(GX_EINVAL, "MH needs x_step (xStepSize)");
+    }
+    int nb = o->burnin < 1 ? (int)std::floor(o->iteration * o->burnin) : (int)o->burnin;
+    int ns = mcmc_nsamples(o->iteration, nb, o->thinning);
+    int W = o->algorithm == GX_MCMC_ENSEMBLE ? o->nwalker : 1;
+    long long h2d = 0, d2h = 0;
+    double kernel_ms = 0.0;
+    int launches = 0;
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    for (int i = 0; i < nvol; ++i) {
+        const gx_volume& v = vols[i];
+        gx_mcmc_result& r = results[i];
+        if (v.nvox < 1 || !v.data || !v.theta0) return fail(GX_EINVAL, "volume %d: need nvox, data and theta0 (pars0)", i);
+        int nv = v.nvox;
+        McmcParams p;
+        memset(&p, 0, sizeof(p));
+        p.P = make_protocol(model, id, np, nm, nullptr, nullptr, 0);
+        p.nm = nm; p.nvar = nvar; p.nvox = nv;
+        for (int q = 0; q < nvar; ++q) {
+            p.lb[q] = (float)o->lb[q];
+            p.ub[q] = (float)o->ub[q];
+            p.xstep[q] = o->x_step ? (float)o->x_step[q] : 0.0f;
+        }
+        p.algorithm = o->algorithm; p.nwalker = W; p.iteration = o->iteration; p.thinning = o->thinning;
+        p.nburnin = nb; p.ns = ns; p.repetition = o->repetition; p.update = o->ensemble_update;
+        p.a = (float)o->step_size; p.start_range = (float)o->start_range; p.seed = o->seed;
+        float *data, *w = nullptr, *b1 = nullptr, *x0, *shift, *post = nullptr;
+        double *sum, *sumsq;
+        unsigned long long* nacc;
+        int* partner = nullptr;
+        TRY(wsT(c, S_DATA, (size_t)nm * nv, &data));
+        TRY(upload_rows(c, data, nv, 0, v.data, nm, nv, mem, &h2d));
+        if (v.weights) { TRY(wsT(c, S_W, (size_t)nm * nv, &w)); TRY(upload_rows(c, w, nv, 0, v.weights, nm, nv, mem, &h2d)); }
+        if (v.b1) { TRY(wsT(c, S_B1, (size_t)nv, &b1)); TRY(upload_rows(c, b1, nv, 0, v.b1, 1, nv, mem, &h2d)); }
+        TRY(wsT(c, S_MC_X0, (size_t)nvar * nv, &x0));
+        TRY(upload_rows(c, x0, nv, 0, v.theta0, nvar, nv, mem, &h2d));
+        TRY(wsT(c, S_MC_SHIFT, (size_t)nvar * nv, &shift));
+        TRY(wsT(c, S_MC_SUM, (size_t)nvar * nv, &sum));
+        TRY(wsT(c, S_MC_SUMSQ, (size_t)nvar * nv, &sumsq));
+        TRY(wsT(c, S_MC_ACC, 1, &nacc));
+        CK(cudaMemsetAsync(sum, 0, sizeof(double) * nvar * nv, c->stream));
+        CK(cudaMemsetAsync(sumsq, 0, sizeof(double) * nvar * nv, c->stream));
+        CK(cudaMemsetAsync(nacc, 0, sizeof(unsigned long long), c->stream));
+        if (r.posterior) {
+            if (mem == GX_MEM_DEVICE) post = r.posterior;
+            else TRY(wsT(c, S_MC_POST, (size_t)nvar * o->repetition * ns * W * nv, &post));
+        }
+        if (o->algorithm == GX_MCMC_ENSEMBLE) TRY(wsT(c, S_MC_PART, (size_t)o->repetition * o->iteration * W, &partner));
+        p.data = data; p.weights = w; p.b1 = b1; p.x0 = x0; p.shift = shift; p.sum = sum; p.sumsq = sumsq;
+        p.posterior = post; p.n_acc = nacc; p.partner = partner;
+        if (partner) CK(launch_mcmc_partners(p, partner, c->stream));
+        CK(cudaEventRecord(c->ev[2], c->stream));
+        CK(launch_mcmc(p, id, o->block_size, c->stream));
+        CK(cudaEventRecord(c->ev[3], c->stream));
+        launches += (o->iteration + 249) / 250 * o->repetition;
+        float *mean = nullptr, *stdv = nullptr;
+        if (mem == GX_MEM_DEVICE) { mean = r.mean; stdv = r.std; }
+        else {
+            TRY(wsT(c, S_MC_MEAN, (size_t)nvar * nv, &mean));
+            TRY(wsT(c, S_MC_STD, (size_t)nvar * nv, &stdv));
+        }
+        CK(launch_mcmc_finalize(p, mean, stdv, c->stream));
+        if (mem == GX_MEM_HOST) {
+            if (r.mean) { CK(cudaMemcpyAsync(r.mean, mean, sizeof(float) * nvar * nv, cudaMemcpyDeviceToHost, c->stream)); d2h += sizeof(float) * nvar * nv; }
+            if (r.std) { CK(cudaMemcpyAsync(r.std, stdv, sizeof(float) * nvar * nv, cudaMemcpyDeviceToHost, c->stream)); d2h += sizeof(float) * nvar * nv; }
+            if (r.posterior) {
+                size_t n = (size_t)nvar * o->repetition * ns * W * nv;
+                CK(cudaMemcpyAsync(r.posterior, post, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+                d2h += sizeof(float) * n;
+            }
+        }
+        unsigned long long acc = 0;
+        CK(cudaMemcpyAsync(&acc, nacc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+        kernel_ms += ms;
+        r.n_accepted = (int64_t)acc;
+        r.n_proposals = (int64_t)nv * W * o->iteration * o->repetition;
+        r.ns = ns;
+    }
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventSynchronize(c->ev[1]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->timing.total_ms = ms;
+    c->timing.main_kernel_ms = kernel_ms;
+    c->timing.main_launches = launches;
+    c->timing.kernel_launches = g_kernel_launches - scope.launches0;
+    c->timing.h2d_bytes = h2d;
+    c->timing.d2h_bytes = d2h;
+    return GX_OK;
+}

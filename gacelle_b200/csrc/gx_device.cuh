@@ -1,0 +1,418 @@
+// gx_device.cuh -- device building blocks shared by the askAdam and MCMC
+// kernels: acquisition protocol, Philox4x32-10, elementwise losses (with the
+// Rician log-Bessel terms) and the per-voxel forward models with their
+// tangent (dS/dtheta) accumulation.  All reference citations are paths in
+// kschan0214/gacelle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define GX_HD __host__ __device__ __forceinline__
+#else
+#define GX_HD inline
+#endif
+
+namespace gx {
+
+constexpr int kMaxTE = 64;
+constexpr int kMaxFA = 16;
+constexpr int kMaxShell = 64;
+constexpr int kMaxParam = 6;  // fitted parameters + noise
+constexpr int kMaxMeas = 128;
+
+enum ModelId { kR2S = 1, kR1R2S = 2, kNEXI = 3, kNEXI2 = 4 };
+enum LossId { kL1 = 0, kL2 = 1, kHuber = 2, kMSE = 3, kGauss = 4, kRician = 5 };
+enum OptId { kAdam = 0, kSGDM = 1, kRMSProp = 2 };
+
+// Acquisition protocol, passed by value as a kernel parameter (constant
+// bank): every thread of a warp reads the same element, which the constant
+// cache broadcasts.
+struct DevProtocol {
+    int model;   // ModelId; NEXI with lmax = 2 is kNEXI2
+    int nm;      // measurements
+    int np;      // fitted parameters (without noise)
+    int n_te, n_fa, n_shell, nx;
+    float tr;    // [s]
+    float h;     // NEXI node spacing 1/(nx-1)
+    float te[kMaxTE];
+    float fa_rad[kMaxFA];
+    float bval[kMaxShell];
+    float delta[kMaxShell];
+    float lb[kMaxParam], ub[kMaxParam];
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11).  Counter words are
+// (a, b, c, tag); the key is the 64-bit seed.
+// ---------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+
+GX_HD U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint64_t seed) {
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return U4{c0, c1, c2, c3};
+}
+
+// Uniform on (0,1) from 23 random bits: exactly representable in FP32.
+GX_HD float u01(uint32_t x) { return ((float)(x >> 9) + 0.5f) * (1.0f / 8388608.0f); }
+GX_HD uint32_t rand_below(uint32_t x, uint32_t n) { return (uint32_t)(((uint64_t)x * n) >> 32); }
+
+enum RngTag : uint32_t { kTagAdamInit = 1, kTagGwInit = 2, kTagGwMove = 3, kTagGwPerm = 4,
+                         kTagGwRbPart = 5, kTagMhMove = 6 };
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, float& n1) {
+    float u1 = u01(a), u2 = u01(b);
+    float r = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    n0 = r * c;
+    n1 = r * s;
+}
+#endif
+
+// ---------------------------------------------------------------------------
+// Rician log-likelihood terms.  I0 and I1 from the polynomial approximations
+// of Abramowitz & Stegun 9.8.1-9.8.4 (|x| < 3.75: series in (x/3.75)^2;
+// |x| >= 3.75: x^(1/2) e^(-x) I_nu(x) as a polynomial in 3.75/x).  For the
+// large-argument branch 1 - I1/I0 is evaluated as (P0 - P1)/P0 with the
+// coefficient differences taken exactly, so the gradient term does not cancel.
+// log_i0e = log(exp(-|x|) I0(x));  omr = 1 - I1(x)/I0(x).
+// ---------------------------------------------------------------------------
+GX_HD void rician_terms(float x, float& log_i0e, float& omr) {
+    float ax = fabsf(x);
+    float r;  // 1 - I1(|x|)/I0(|x|)
+    if (ax < 3.75f) {
+        float t = ax * (1.0f / 3.75f);
+        float t2 = t * t;
+        float i0 = 1.0f + t2 * (3.5156229f + t2 * (3.0899424f + t2 * (1.2067492f +
+                   t2 * (0.2659732f + t2 * (0.0360768f + t2 * 0.0045813f)))));
+        float i1x = 0.5f + t2 * (0.87890594f + t2 * (0.51498869f + t2 * (0.15084934f +
+                    t2 * (0.02658733f + t2 * (0.00301532f + t2 * 0.00032411f)))));
+        log_i0e = logf(i0) - ax;
+        r = 1.0f - ax * i1x / i0;
+    } else {
+        float u = 3.75f / ax;
+        float p0 = 0.39894228f + u * (0.01328592f + u * (0.00225319f + u * (-0.00157565f +
+                   u * (0.00916281f + u * (-0.02057706f + u * (0.02635537f +
+                   u * (-0.01647633f + u * 0.00392377f)))))));
+        float d = u * (0.05316616f + u * (0.00587337f + u * (-0.00321366f + u * (0.01947836f +
+                  u * (-0.04340673f + u * (0.05530849f + u * (-0.03435287f +
+                  u * 0.00812436f)))))));
+        log_i0e = logf(p0) - 0.5f * logf(ax);
+        r = d / p0;
+    }
+    omr = x >= 0.0f ? r : 2.0f - r;  // I1 is odd: 1 - R(-a) = 1 + R(a)
+}
+
+// Per-voxel constants of the likelihood losses.
+struct LossAux {
+    float inv_s2;     // 1/sigma^2
+    float gauss_c;    // 0.5*log(2*pi*sigma^2)
+};
+
+GX_HD LossAux make_loss_aux(float sigma) {
+    LossAux a;
+    a.inv_s2 = 1.0f / (sigma * sigma);
+    a.gauss_c = 0.5f * logf(6.283185307179586f * sigma * sigma);
+    return a;
+}
+
+// Elementwise loss value and derivative with respect to the prediction s
+// (utils/askadam.m:86-95 for l1/l2/huber/mse with Reduction="none").
+template <int LOSS>
+GX_HD float loss_elem(float s, float y, float w, const LossAux& a, float mse_scale,
+                      float hd, float& d) {
+    float r = s - y;
+    if (LOSS == kL1) {
+        d = w * (float)((r > 0.0f) - (r < 0.0f));
+        return w * fabsf(r);
+    } else if (LOSS == kL2) {
+        d = 2.0f * w * r;
+        return w * r * r;
+    } else if (LOSS == kHuber) {
+        float ar = fabsf(r);
+        if (ar <= hd) {
+            d = w * r;
+            return w * 0.5f * r * r;
+        }
+        d = w * hd * (float)((r > 0.0f) - (r < 0.0f));
+        return w * (hd * ar - 0.5f * hd * hd);
+    } else if (LOSS == kMSE) {
+        d = 2.0f * mse_scale * r;
+        return mse_scale * r * r;
+    } else if (LOSS == kGauss) {
+        d = w * r * a.inv_s2;
+        return w * (0.5f * r * r * a.inv_s2 + a.gauss_c);
+    } else {  // kRician: (y-s)^2/(2 s2) - log(i0e(y s / s2)) - log(y / s2)
+        float x = y * s * a.inv_s2;
+        float lg, omr;
+        rician_terms(x, lg, omr);
+        float c = y > 0.0f ? -logf(y * a.inv_s2) : 0.0f;
+        d = w * (r * a.inv_s2 + y * a.inv_s2 * omr);
+        return w * (0.5f * r * r * a.inv_s2 - lg + c);
+    }
+}
+
+#if defined(__CUDACC__)
+
+// Accumulates loss and d(loss)/d(theta) over the measurements of one voxel.
+// set_nan_inf_zero (utils/askadam.m:80): a non-finite prediction becomes 0
+// and carries no gradient.
+template <int LOSS, int NP>
+struct LossAcc {
+    float total;
+    float g[NP];
+    const float* y;   // measurement m at y[m*ys]
+    int ys;
+    const float* w;   // nullptr: unit weights
+    int ws;
+    LossAux aux;
+    float mse_scale, hd;
+    float* res;       // nullptr or residual output at res[m*rs]
+    int rs;
+
+    __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
+        bool bad = !isfinite(S);
+        float s = bad ? 0.0f : S;
+        float ww = w ? w[m * ws] : 1.0f;
+        float d;
+        float l = loss_elem<LOSS>(s, y[m * ys], ww, aux, mse_scale, hd, d);
+        total += l;
+        if (res) res[m * rs] = l;
+        if (!bad) {
+#pragma unroll
+            for (int k = 0; k < NP; ++k) g[k] += d * dS[k];
+        }
+    }
+};
+
+template <int MODEL> struct ModelNP;
+template <> struct ModelNP<kR2S> { static constexpr int value = 2; };
+template <> struct ModelNP<kR1R2S> { static constexpr int value = 3; };
+template <> struct ModelNP<kNEXI> { static constexpr int value = 4; };
+template <> struct ModelNP<kNEXI2> { static constexpr int value = 5; };
+
+// Per-voxel model inputs besides theta.
+struct VoxAux {
+    float b1;                 // R1R2*: flip-angle scaling
+    const float* sa;          // R1R2*: sin(b1*FA_f) at sa[f*fs]
+    const float* ca;          // R1R2*: cos(b1*FA_f)
+    int fs;
+};
+
+// S = M0 exp(-TE R2*)  (R2star/gpuR2starMapping.m:427-434)
+template <class Acc>
+__device__ __forceinline__ void model_r2s(const DevProtocol& P, const float* th, Acc& acc) {
+    float M0 = th[0], R2 = th[1];
+    for (int m = 0; m < P.nm; ++m) {
+        float te = P.te[m];
+        float E = __expf(-te * R2);
+        float S = M0 * E;
+        float dS[2] = {E, -te * S};
+        acc.add(m, S, dS);
+    }
+}
+
+// S = M0 sin(a)(1-E1)/(1-cos(a)E1) exp(-TE R2*), E1 = exp(-TR R1), a = b1*FA;
+// measurement index TE fastest then FA (R1R2s/gpuJointR1R2starMapping.m:375-422,513-525)
+template <class Acc>
+__device__ __forceinline__ void model_r1r2s(const DevProtocol& P, const float* th,
+                                            const VoxAux& va, Acc& acc) {
+    float M0 = th[0], R1 = th[1], R2 = th[2];
+    float E1 = __expf(-P.tr * R1);
+    for (int f = 0; f < P.n_fa; ++f) {
+        float sa = va.sa[f * va.fs], ca = va.ca[f * va.fs];
+        float inv = 1.0f / (1.0f - ca * E1);
+        float A = sa * (1.0f - E1) * inv;
+        float dA = sa * (ca - 1.0f) * inv * inv * (-P.tr * E1);
+        for (int t = 0; t < P.n_te; ++t) {
+            float te = P.te[t];
+            float E2 = __expf(-te * R2);
+            float B = M0 * E2;
+            float S = A * B;
+            float dS[3] = {A * E2, B * dA, -te * S};
+            acc.add(t + f * P.n_te, S, dS);
+        }
+    }
+}
+
+// NEXI narrow-pulse Karger model (NEXI/gpuNEXI.m:902-996, M at :1090-1097):
+// per shell j, S_j = trapz_x M(x) over x = linspace(0,1,nx); lmax = 2 adds
+// Sl2_j = p2 |trapz_x M (3x^2-1)/2|; finally min(S,1).  The tangent sums per
+// node are reduced to the five intermediate partials (f, d1, d2, r1, r2) and
+// chained to (fa, Da, De, ra) once per shell.
+template <bool LMAX2, class Acc, int NP>
+__device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const float* th, Acc& acc) {
+    const float EPS = 1e-8f;
+    float fa_in = th[0];
+    float f = fmaxf(fa_in, EPS);
+    float Da = th[1], De = th[2], ra = th[3];
+    float gate = fa_in > EPS ? 1.0f : 0.0f;  // d max(fa,eps)/d fa
+    float omf = 1.0f - f;
+    float rf = f / omf;
+    int nx = P.nx;
+    float h = P.h;
+    int nsh = P.n_shell;
+    for (int j = 0; j < nsh; ++j) {
+        float b = P.bval[j], D = P.delta[j];
+        float d2 = b * De;
+        float r1 = D * ra;
+        float r2 = r1 * rf;
+        float base = r1 - r2 - d2;
+        float c1 = r1 + r2 + d2;
+        float q4 = 4.0f * r1 * r2;
+        float bDa = b * Da;
+        float fd2 = omf * d2;
+        float S0 = 0.f, Sf = 0.f, Sd1 = 0.f, Sd2 = 0.f, Sr1 = 0.f, Sr2 = 0.f;
+        float T0 = 0.f, Tf = 0.f, Td1 = 0.f, Td2 = 0.f, Tr1 = 0.f, Tr2 = 0.f;
+        for (int i = 0; i < nx; ++i) {
+            float x = (float)i * h;
+            float x2 = x * x;
+            float d1 = bDa * x2;
+            float s = base + d1;
+            float Q = fmaf(s, s, q4);
+            float rs = rsqrtf(Q);
+            float l2raw = 0.5f * Q * rs;
+            bool active = l2raw > EPS;
+            float l2 = active ? l2raw : EPS;
+            float inv_l2 = active ? 2.0f * rs : 1.0f / EPS;
+            float l1 = 0.5f * (c1 + d1);
+            float lm = l1 - l2, lp = l1 + l2;
+            float N = fmaf(f, d1, fd2) - lm;
+            float Pp = 0.5f * N * inv_l2;
+            float em = __expf(-lm), ep = __expf(-lp);
+            float M = Pp * ep + (1.0f - Pp) * em;
+            // reverse sweep with Mbar = 1
+            float Ppb = ep - em;
+            float lpb = -Pp * ep;
+            float lmb = -(1.0f - Pp) * em;
+            float Nb = 0.5f * Ppb * inv_l2;
+            float l2b = -Ppb * Pp * inv_l2;
+            lmb -= Nb;
+            float l1b = lpb + lmb;
+            l2b += lpb - lmb;
+            float Qb = active ? 0.125f * l2b * inv_l2 : 0.0f;
+            float sb = 2.0f * s * Qb;
+            float hl1 = 0.5f * l1b;
+            float fb = Nb * (d1 - d2);
+            float d1b = Nb * f + sb + hl1;
+            float d2b = Nb * omf - sb + hl1;
+            float r1b = 4.0f * r2 * Qb + sb + hl1;
+            float r2b = 4.0f * r1 * Qb - sb + hl1;
+            float wt = (i == 0 || i == nx - 1) ? 0.5f : 1.0f;
+            S0 = fmaf(wt, M, S0);
+            Sf = fmaf(wt, fb, Sf);
+            Sd1 = fmaf(wt * x2, d1b, Sd1);
+            Sd2 = fmaf(wt, d2b, Sd2);
+            Sr1 = fmaf(wt, r1b, Sr1);
+            Sr2 = fmaf(wt, r2b, Sr2);
+            if (LMAX2) {
+                float p2w = wt * (1.5f * x2 - 0.5f);
+                T0 = fmaf(p2w, M, T0);
+                Tf = fmaf(p2w, fb, Tf);
+                Td1 = fmaf(p2w * x2, d1b, Td1);
+                Td2 = fmaf(p2w, d2b, Td2);
+                Tr1 = fmaf(p2w, r1b, Tr1);
+                Tr2 = fmaf(p2w, r2b, Tr2);
+            }
+        }
+        float r2_f = r1 / (omf * omf);
+        {
+            float S = S0 * h;
+            float dS[NP];
+            dS[0] = gate * h * (Sf + Sr2 * r2_f);
+            dS[1] = h * Sd1 * b;
+            dS[2] = h * Sd2 * b;
+            dS[3] = h * (Sr1 + Sr2 * rf) * D;
+            if (NP > 4) dS[NP - 1] = 0.0f;
+            if (S > 1.0f) {  // min(S,1), NEXI/gpuNEXI.m:928
+                S = 1.0f;
+#pragma unroll
+                for (int k = 0; k < NP; ++k) dS[k] = 0.0f;
+            }
+            acc.add(j, S, dS);
+        }
+        if (LMAX2) {
+            float p2 = th[NP - 1];
+            float T = T0 * h;
+            float sg = (float)((T > 0.0f) - (T < 0.0f));
+            float S = p2 * fabsf(T);
+            float dS[NP];
+            dS[0] = gate * p2 * sg * h * (Tf + Tr2 * r2_f);
+            dS[1] = p2 * sg * h * Td1 * b;
+            dS[2] = p2 * sg * h * Td2 * b;
+            dS[3] = p2 * sg * h * (Tr1 + Tr2 * rf) * D;
+            dS[NP - 1] = fabsf(T);
+            if (S > 1.0f) {
+                S = 1.0f;
+#pragma unroll
+                for (int k = 0; k < NP; ++k) dS[k] = 0.0f;
+            }
+            acc.add(nsh + j, S, dS);
+        }
+    }
+}
+
+template <int MODEL, class Acc>
+__device__ __forceinline__ void model_eval(const DevProtocol& P, const float* th, const VoxAux& va,
+                                           Acc& acc) {
+    if constexpr (MODEL == kR2S) model_r2s(P, th, acc);
+    else if constexpr (MODEL == kR1R2S) model_r1r2s(P, th, va, acc);
+    else if constexpr (MODEL == kNEXI) model_nexi_impl<false, Acc, 4>(P, th, acc);
+    else model_nexi_impl<true, Acc, 5>(P, th, acc);
+}
+
+// Forward-only accumulation (no derivatives): used by gx_forward and MCMC.
+template <int NP>
+struct SignalSink {
+    float* out;   // out[m*os]
+    int os;
+    __device__ __forceinline__ void add(int m, float S, const float (&)[NP]) { out[m * os] = S; }
+};
+
+// Sum of weighted squared residuals, accumulated in FP64 (MCMC logP).
+template <int NP>
+struct SosSink {
+    const float* y;
+    int ys;
+    const float* w;
+    int ws;
+    double sos;
+    __device__ __forceinline__ void add(int m, float S, const float (&)[NP]) {
+        float r = S - y[m * ys];
+        float ww = w ? w[m * ws] : 1.0f;
+        sos += (double)(ww * r * r);
+    }
+};
+
+// unscale_parameters (utils/askadam.m:1063-1075) and its derivative.
+__device__ __forceinline__ float unscale(int transform, float lb, float ub, float z, float& dth) {
+    if (transform == 0) {
+        float s = 1.0f / (1.0f + __expf(-z));
+        dth = (ub - lb) * s * (1.0f - s);
+        return lb + (ub - lb) * s;
+    }
+    float zc = fminf(fmaxf(z, 0.0f), 1.0f);  // set_boundary01 before evaluation
+    dth = (z >= 0.0f && z <= 1.0f) ? (ub - lb) : 0.0f;
+    return zc * (ub - lb) + lb;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace gx

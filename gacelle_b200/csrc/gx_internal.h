@@ -1,0 +1,136 @@
+// gx_internal.h -- declarations shared between the kernel translation units
+// and the host runtime (capi.cu).  Not part of the public C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gx_device.cuh"
+
+namespace gx {
+
+constexpr int kHistW = 5;  // per-epoch record: fidelity, reg, |g|^2, |z|^2, |dz|^2
+constexpr int kMaxReg = 8;
+
+// Per-volume entry of the voxel work-list.  Volumes are concatenated in the
+// SoA arrays, each padded to a multiple of the block size so that a block
+// never straddles two volumes.
+struct DevVol {
+    int off;            // first (padded) voxel index of the volume
+    int nvox;           // real voxels
+    int npad;           // padded voxels
+    float norm;         // 1 / (nm * nvox): askadam mean (utils/askadam.m:96)
+    double normd;
+    int dims[3];        // TV grid
+    long long grid_off; // offset of the volume's grid in the TV grid buffers
+    float tv_scale[kMaxReg];  // lambda_k / Nmask (spatial_total_variation.m:40)
+};
+
+// Parameters shared by the askAdam kernels (passed by value).
+struct AdamParams {
+    DevProtocol P;
+    int nm, np, nvtot;            // nvtot: padded voxel count, array stride
+    const float* data;            // [nm][nvtot]
+    const float* weights;         // [nm][nvtot] or nullptr
+    const float* b1;              // [nvtot] or nullptr
+    const float* sigma;           // [nvtot] or nullptr
+    float sigma_default;
+    float* z; float* m1; float* m2; float* zprev;  // [np][nvtot]
+    const int* blk_vol;           // block -> volume
+    const DevVol* vols;
+    int nvol;
+    int niter;
+    const float2* sched;          // [niter+1]: (lr_e/(1-b1^e), 1/(1-b2^e)) or (lr_e, 0)
+    int optimiser, transform;
+    float beta1, beta2, eps, momentum, rms_decay, rms_eps;
+    float mse_scale, huber_delta;
+    double* hist;                 // [nvol][niter+1][kHistW] or nullptr
+    float* ckpt;                  // checkpoint slots, each 3*np*nvtot floats
+    int ckpt_every;
+    float* res_out;               // [nm][nvtot] or nullptr
+    // TV
+    int n_reg;
+    int reg_param[kMaxReg];
+    int tv_3d;
+    float inv_vs[3];
+    const int* gidx;              // [nvtot] grid index within the volume's grid
+    const unsigned char* maskgrid;
+    const float* grid_cur;        // [n_reg][grid total]
+    float* grid_next;
+    long long grid_total;
+};
+
+// Kernel launchers (askadam_kernels.cu).  Return cudaError_t of the launch.
+cudaError_t launch_init_state(const AdamParams& a, const float* theta0, double randomness,
+                              uint64_t seed, int block, cudaStream_t s);
+cudaError_t launch_fused(const AdamParams& a, int model, int loss, bool stats, int e_begin,
+                         int e_end, int update_last, bool record, int block, int nblocks,
+                         cudaStream_t s);
+cudaError_t launch_tv_step(const AdamParams& a, int model, int loss, bool stats, int e,
+                           bool update, bool record, bool want_res, int block, int nblocks,
+                           cudaStream_t s);
+cudaError_t launch_tv_scatter(const AdamParams& a, float* grid, int block, int nblocks,
+                              cudaStream_t s);
+cudaError_t launch_finalize(const AdamParams& a, const float* zsrc, float* theta_out,
+                            const float* res, float* resloss, int block, int nblocks,
+                            cudaStream_t s);
+cudaError_t launch_copy_state(const AdamParams& a, float* dst, const float* z_, const float* m1_,
+                              const float* m2_, bool to_ckpt, int block, int nblocks,
+                              cudaStream_t s);
+
+// Plain (unfused) path: one kernel per reference operation.
+struct PlainBufs {
+    float* theta;    // [np][nvtot]
+    float* dth;      // [np][nvtot] dtheta/dz
+    float* signal;   // [nm][nvtot]
+    float* dsig;     // [nm][nvtot] d loss / d signal (normalised)
+    float* res;      // [nm][nvtot]
+    float* gth;      // [np][nvtot]
+    float* gz;       // [np][nvtot]
+    double* acc;     // [8] per-iteration sums
+};
+cudaError_t launch_plain_unscale(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
+cudaError_t launch_plain_forward(const AdamParams& a, int model, const PlainBufs& b, int block,
+                                 int nblocks, cudaStream_t s);
+cudaError_t launch_plain_loss(const AdamParams& a, int loss, const PlainBufs& b, int block,
+                              int nblocks, cudaStream_t s);
+cudaError_t launch_plain_adjoint(const AdamParams& a, int model, const PlainBufs& b, int block,
+                                 int nblocks, cudaStream_t s);
+cudaError_t launch_plain_tv(const AdamParams& a, const PlainBufs& b, float* grid, int block,
+                            int nblocks, cudaStream_t s);
+cudaError_t launch_plain_zgrad(const AdamParams& a, const PlainBufs& b, bool stats, int block,
+                               int nblocks, cudaStream_t s);
+cudaError_t launch_plain_update(const AdamParams& a, const PlainBufs& b, int e, int block,
+                                int nblocks, cudaStream_t s);
+
+// Forward only (gx_forward).
+cudaError_t launch_forward_only(const DevProtocol& P, int model, const float* theta,
+                                const float* b1, int nvox, float* signal, cudaStream_t s);
+
+// MCMC (mcmc_kernels.cu).
+struct McmcParams {
+    DevProtocol P;
+    int nm, nvar, nvox;
+    const float* data;     // [nm][nvox]
+    const float* weights;  // [nm][nvox] or nullptr
+    const float* b1;
+    const float* x0;       // [nvar][nvox]
+    float lb[kMaxParam], ub[kMaxParam], xstep[kMaxParam];
+    int algorithm, nwalker, iteration, thinning, nburnin, ns, repetition, update;
+    float a;               // stretch scale
+    float start_range;
+    uint64_t seed;
+    const int* partner;    // simultaneous: [rep][iteration][W]; redblack: [rep][iteration][W]
+    double* sum;           // [nvar][nvox] shifted sums
+    double* sumsq;
+    float* shift;          // [nvar][nvox]
+    float* posterior;      // [nvar][rep][ns][W][nvox] or nullptr
+    unsigned long long* n_acc;
+};
+cudaError_t launch_mcmc_partners(const McmcParams& p, int* partner, cudaStream_t s);
+cudaError_t launch_mcmc(const McmcParams& p, int model, int block, cudaStream_t s);
+cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, cudaStream_t s);
+
+extern long long g_kernel_launches;  // launches of this library's kernels (process-wide)
+
+}  // namespace gx

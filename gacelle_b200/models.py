@@ -1,0 +1,412 @@
+"""Host-side mirrors of GACELLE's built-in model classes whose fits run on the
+B200 engine: gpuR2starMapping (R2star/gpuR2starMapping.m),
+gpuJointR1R2starMapping (R1R2s/gpuJointR1R2starMapping.m) and gpuNEXI
+(NEXI/gpuNEXI.m).
+
+Each class keeps the reference's parameter contract (modelParams, lb, ub,
+startPoint, step, index-aligned), ``updateProperty``, ``fit`` and ``FWD``.
+``fit`` dispatches to :class:`gacelle_b200.askadam_solver.askadam` or
+:class:`gacelle_b200.mcmc_solver.mcmc` exactly where the reference calls
+``askadam().optimisation`` / ``mcmc().optimisation``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib, utils
+from ._lib import GacelleError, GX_EINVAL, GX_EUNSUPPORTED
+
+
+class _GxModelHandle:
+    """A gx_model struct plus the arrays it points into."""
+
+    def __init__(self, kind, te=None, fa_deg=None, tr=0.0, bval=None, delta=None, lmax=0, nx=14):
+        self._arrays = []
+
+        def arr(a):
+            if a is None:
+                return None, 0
+            a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+            self._arrays.append(a)
+            return a.ctypes.data_as(_lib._dp), a.size
+
+        te_p, nte = arr(te)
+        fa_p, nfa = arr(fa_deg)
+        b_p, nb = arr(bval)
+        d_p, _ = arr(delta)
+        self.s = _lib.GxModel(kind, lmax, nx, nte, te_p, nfa, fa_p, float(tr), nb, b_p, d_p)
+
+    def sizes(self):
+        npar = C.c_int32()
+        nmeas = C.c_int32()
+        _lib.check(_lib.lib().gx_model_sizes(C.byref(self.s), C.byref(npar), C.byref(nmeas)))
+        return npar.value, nmeas.value
+
+
+class _ModelBase:
+    modelParams: list
+    ub: list
+    lb: list
+    startPoint: list
+    step: list
+    epsilon = 1e-8
+    seed = 48463
+
+    def __init__(self):
+        # per-instance copies of the contract so updateProperty never leaks
+        self.modelParams = list(type(self).modelParams)
+        self.ub = list(type(self).ub)
+        self.lb = list(type(self).lb)
+        self.startPoint = list(type(self).startPoint)
+        self.step = list(type(self).step)
+        self.context = None
+
+    def _strip(self, name):
+        if name in self.modelParams:
+            i = self.modelParams.index(name)
+            for attr in ("modelParams", "lb", "ub", "startPoint", "step"):
+                getattr(self, attr).pop(i)
+
+    def updateProperty(self, fitting):
+        """Drop 'noise' unless the solver is mcmc (e.g. R2star/gpuR2starMapping.m:78-91)."""
+        if str(fitting.get("solver", "askadam")).lower() != "mcmc":
+            self._strip("noise")
+        return self
+
+    def nparam_nmeas(self):
+        return self._gx_model().sizes()
+
+    def _forward(self, theta: np.ndarray, b1=None) -> np.ndarray:
+        """theta [np][N] -> signal [nm][N] on the engine (gx_forward)."""
+        ctx = self.context or _lib.Context.default()
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        n = theta.shape[1]
+        npar, nm = self.nparam_nmeas()
+        if theta.shape[0] < npar:
+            raise GacelleError(GX_EINVAL, f"FWD needs {npar} parameters")
+        theta = np.ascontiguousarray(theta[:npar])
+        out = np.zeros((nm, n), np.float32)
+        b1p = None
+        if b1 is not None:
+            b1 = np.ascontiguousarray(b1, dtype=np.float32)
+            b1p = b1.ctypes.data
+        _lib.check(_lib.lib().gx_forward(ctx.ptr, C.byref(self._gx_model().s), _lib.MEM_HOST,
+                                         theta.ctypes.data, b1p, n, out.ctypes.data))
+        return out
+
+    def _fwd_struct(self, pars: dict, names, b1=None):
+        """FWD on a parameter struct: [1,N] rows -> [nm, N]; N-D maps -> [..., nm]."""
+        first = np.asarray(pars[names[0]])
+        shape = first.shape
+        cols = [np.broadcast_to(np.asarray(pars[p], dtype=np.float64), shape).reshape(-1, order="F") for p in names]
+        b1v = None if b1 is None else np.broadcast_to(np.asarray(b1, dtype=np.float64), shape).reshape(-1, order="F")
+        s = self._forward(np.stack(cols), b1v)
+        if first.ndim <= 2 and (first.ndim < 2 or first.shape[0] == 1):
+            return s
+        return s.T.reshape(shape + (s.shape[0],), order="F")
+
+    def _solve(self, data, mask, w, pars0, fitting, extradata=None):
+        from .askadam_solver import askadam
+        from .mcmc_solver import mcmc
+        if fitting["solver"] == "askadam":
+            return askadam(self.context, fitting.get("path", "fused")).optimisation(
+                data, mask, w, pars0, fitting, self, extradata=extradata)
+        fitting = dict(fitting)
+        fitting["xStepSize"] = list(self.step)
+        return mcmc(self.context).optimisation(data, mask, w, pars0, fitting, self, extradata=extradata)
+
+
+class gpuR2starMapping(_ModelBase):
+    """Mono-exponential R2* mapping (R2star/gpuR2starMapping.m)."""
+
+    modelParams = ["M0", "R2star", "noise"]
+    ub = [2, 200, 0.1]
+    lb = [0, 0.1, 0.001]
+    startPoint = [1, 30, 0.05]
+    step = [0.01, 1, 0.005]
+
+    def __init__(self, te):
+        super().__init__()
+        self.te = np.asarray(te, dtype=np.float64).ravel()
+
+    def _gx_model(self):
+        return _GxModelHandle(_lib.MODEL_R2S, te=self.te)
+
+    def FWD(self, pars, solver=None, fitting=None):
+        """R2star/gpuR2starMapping.m:321-363."""
+        return self._fwd_struct(pars, ["M0", "R2star"])
+
+    @staticmethod
+    def check_set_default(fitting):
+        """R2star/gpuR2starMapping.m:463-486."""
+        from .askadam_solver import check_set_default_basic as adam_def
+        from .mcmc_solver import check_set_default_basic as mcmc_def
+        f = dict(fitting or {})
+        f.setdefault("solver", "askadam")
+        g = mcmc_def(f) if f["solver"].lower() == "mcmc" else adam_def(f)
+        g.setdefault("weightMethod", "1stecho")
+        g.setdefault("isWeighted", False)
+        g.setdefault("weightPower", 2)
+        g.setdefault("start", "prior")
+        return g
+
+    @staticmethod
+    def compute_optimisation_weights(data, fitting):
+        """R2star/gpuR2starMapping.m:507-530."""
+        data = np.abs(np.asarray(data, dtype=np.float64))
+        if fitting["isWeighted"]:
+            if fitting["weightMethod"].lower() == "norm":
+                w = np.sqrt(data)
+            else:
+                p = fitting["weightPower"]
+                w = data ** p / data[..., :1] ** p
+        else:
+            w = np.ones_like(data)
+        return np.clip(w, 0, 1)
+
+    @staticmethod
+    def R2star_trapezoidal(img, te):
+        """Closed-form R2* start (R2star/gpuR2starMapping.m:436-459)."""
+        img = np.abs(np.asarray(img, dtype=np.float64))
+        te = np.asarray(te, dtype=np.float64)
+        temp = 0.0
+        for k in range(img.shape[-1] - 1):
+            temp = temp + 0.5 * (img[..., k] + img[..., k + 1]) * (te[k + 1] - te[k])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t2s = temp / (img[..., 0] - img[..., -1])
+            return 1.0 / t2s
+
+    def determine_x0(self, y, mask, fitting):
+        """R2star/gpuR2starMapping.m:257-290."""
+        d3 = utils.dims3(mask)
+        start = fitting["start"]
+        if isinstance(start, str):
+            if start.lower() == "prior":
+                x0 = self.estimate_prior(y)
+            else:
+                x0 = utils.initialise_x0(d3, self.modelParams, self.startPoint)
+        else:
+            x0 = utils.initialise_x0(d3, self.modelParams, np.ravel(start))
+        return {p: np.clip(v, fitting["lb"][k], fitting["ub"][k]) for k, (p, v) in enumerate(x0.items())}
+
+    def estimate_prior(self, data):
+        """R2star/gpuR2starMapping.m:293-316 (invalid R2* voxels are set to the
+        R2star lower bound)."""
+        data = np.asarray(data)
+        if data.ndim < 4:
+            data = data.reshape(data.shape + (1,) * (4 - data.ndim)) if data.ndim != 2 else data.T[:, None, None, :]
+        r2 = self.R2star_trapezoidal(data, self.te)
+        bad = ~np.isfinite(r2) | (r2 < self.lb[1])
+        r2 = np.where(bad, self.lb[1], np.minimum(r2, self.ub[1]))
+        return {"M0": np.abs(data[..., 0]).astype(np.float32), "R2star": r2.astype(np.float32)}
+
+    def prepare_data(self, img, mask):
+        """98th-percentile scaling of the first echo (R2star/gpuR2starMapping.m:398-414)."""
+        mask = np.asarray(mask) > 0
+        tmp = np.abs(np.asarray(img)[..., 0])
+        scale = float(np.percentile(tmp[mask], 98, method="hazen"))
+        img = np.asarray(img) / scale
+        img, bad = utils.set_nan_inf_zero(img)
+        mask = mask & ~np.any(bad.reshape(mask.shape + (-1,)), axis=-1)
+        return img, mask, scale
+
+    def fit(self, data, mask=None, fitting=None):
+        """R2star/gpuR2starMapping.m:182-252."""
+        data = np.asarray(data)
+        if mask is None:
+            mask = np.ones(utils.dims3(data), dtype=bool)
+        fitting = self.check_set_default(fitting)
+        self.updateProperty(fitting)
+        fitting["modelParams"] = list(self.modelParams)
+        if not len(fitting["ub"]):
+            fitting["ub"] = self.ub[: len(self.modelParams)]
+        if not len(fitting["lb"]):
+            fitting["lb"] = self.lb[: len(self.modelParams)]
+        pars0 = self.determine_x0(data, mask, fitting)
+        w = self.compute_optimisation_weights(data, fitting)
+        w = None if np.all(w == 1) else w
+        return self._solve(data, mask, w, pars0, fitting)
+
+    def estimate(self, data, mask, fitting=None):
+        """R2star/gpuR2starMapping.m:94-179 (one segment: the engine fits the
+        whole volume in one launch)."""
+        fitting = self.check_set_default(fitting)
+        data, mask, scale = self.prepare_data(data, mask)
+        out = self.fit(data.astype(np.float32), mask, fitting)
+        for which in ("final", "min"):
+            if which in out and "M0" in out[which]:
+                out[which]["M0"] = out[which]["M0"] * scale
+        if "mean" in out and "M0" in out["mean"]:
+            out["mean"]["M0"] = out["mean"]["M0"] * scale
+        return out
+
+
+class gpuJointR1R2starMapping(_ModelBase):
+    """Joint R1-R2* mapping from vFA multi-echo GRE (R1R2s/gpuJointR1R2starMapping.m)."""
+
+    modelParams = ["M0", "R1", "R2star", "noise"]
+    ub = [2, 10, 200, 0.1]
+    lb = [0, 0.1, 0.1, 0.001]
+    startPoint = [1, 1, 30, 0.05]
+    step = [0.01, 0.01, 1, 0.005]
+
+    def __init__(self, te, tr, fa):
+        super().__init__()
+        self.te = np.asarray(te, dtype=np.float64).ravel()
+        self.tr = float(tr)
+        self.fa = np.asarray(fa, dtype=np.float64).ravel()
+
+    def _gx_model(self):
+        return _GxModelHandle(_lib.MODEL_R1R2S, te=self.te, fa_deg=self.fa, tr=self.tr)
+
+    def FWD(self, pars, extraData=None, solver=None, fitting=None):
+        """R1R2s/gpuJointR1R2starMapping.m:375-422 (measurements TE fastest, then FA)."""
+        b1 = None
+        if extraData is not None and "trueFlipAngle" in extraData:
+            raise GacelleError(GX_EUNSUPPORTED, "extraData.trueFlipAngle: pass b1 instead")
+        if extraData is not None and "b1" in extraData:
+            b1 = extraData["b1"]
+        return self._fwd_struct(pars, ["M0", "R1", "R2star"], b1)
+
+    @staticmethod
+    def check_set_default(fitting):
+        from .askadam_solver import check_set_default_basic as adam_def
+        from .mcmc_solver import check_set_default_basic as mcmc_def
+        f = dict(fitting or {})
+        f.setdefault("solver", "askadam")
+        g = mcmc_def(f) if f["solver"].lower() == "mcmc" else adam_def(f)
+        g.setdefault("isWeighted", False)
+        g.setdefault("start", "default")
+        return g
+
+    def fit(self, data, mask=None, fitting=None, extraData=None):
+        """R1R2s/gpuJointR1R2starMapping.m:196-288.  data [x,y,z,TE,FA]."""
+        data = np.asarray(data)
+        if mask is None:
+            mask = np.ones(utils.dims3(data), dtype=bool)
+        fitting = self.check_set_default(fitting)
+        self.updateProperty(fitting)
+        fitting["modelParams"] = list(self.modelParams)
+        if not len(fitting["ub"]):
+            fitting["ub"] = self.ub[: len(self.modelParams)]
+        if not len(fitting["lb"]):
+            fitting["lb"] = self.lb[: len(self.modelParams)]
+        if isinstance(fitting["start"], str) and fitting["start"].lower() == "prior":
+            raise GacelleError(GX_EUNSUPPORTED, "start='prior' needs DESPOT1; use 'default' or pars0")
+        d3 = utils.dims3(mask)
+        pars0 = utils.initialise_x0(d3, self.modelParams, self.startPoint)
+        if data.ndim == 5:  # [x,y,z,TE,FA] -> [x,y,z,TE*FA] with TE fastest
+            data = data.reshape(data.shape[:3] + (-1,), order="F")
+        return self._solve(data, mask, None, pars0, fitting, extradata=extraData)
+
+
+class gpuNEXI(_ModelBase):
+    """Neurite exchange imaging, narrow-pulse Karger model (NEXI/gpuNEXI.m)."""
+
+    modelParams = ["fa", "Da", "De", "ra", "p2", "noise"]
+    ub = [1, 3, 3, 1, 1, 0.1]
+    lb = [np.finfo(float).eps, np.finfo(float).eps, np.finfo(float).eps, 1 / 250, np.finfo(float).eps, 0.01]
+    startPoint = [0.4, 2, 1, 0.05, 0.2, 0.005]
+    step = [0.05, 0.15, 0.15, 0.005, 0.05, 0.005]
+
+    def __init__(self, b, Delta, Nav=None, nx=14):
+        """Shells sorted by DWIutility.unique_shell_keepb0 (NEXI/gpuNEXI.m:70-104):
+        b = 0 discarded; unique Delta ascending, then unique b ascending.
+        ``nx`` is the powder-average trapezoid size (14 in the reference)."""
+        super().__init__()
+        b = np.asarray(b, dtype=np.float64).ravel()
+        D = np.asarray(Delta, dtype=np.float64).ravel()
+        bs, ds = [], []
+        for dv in np.unique(D):
+            bu = np.unique(b[D == dv])
+            bu = bu[bu > 0]
+            bs += list(bu)
+            ds += [dv] * len(bu)
+        self.b = np.array(bs, dtype=np.float32).astype(np.float64)
+        self.Delta = np.array(ds, dtype=np.float32).astype(np.float64)
+        self.Nav = np.ones(len(self.b)) if Nav is None else np.asarray(Nav, dtype=np.float64).ravel()
+        self.nx = int(nx)
+        self.lmax = 0
+
+    def _gx_model(self):
+        return _GxModelHandle(_lib.MODEL_NEXI, bval=self.b, delta=self.Delta, lmax=self.lmax, nx=self.nx)
+
+    def updateProperty(self, fitting):
+        """NEXI/gpuNEXI.m:107-133."""
+        super().updateProperty(fitting)
+        if int(fitting.get("lmax", 0)) == 0:
+            self._strip("p2")
+        self.lmax = int(fitting.get("lmax", 0))
+        return self
+
+    def FWD(self, pars, lmax=0, solver=None):
+        """NEXI/gpuNEXI.m:902-930."""
+        self.lmax = int(lmax)
+        names = ["fa", "Da", "De", "ra"] + (["p2"] if self.lmax == 2 else [])
+        return self._fwd_struct(pars, names)
+
+    @staticmethod
+    def check_set_default(fitting):
+        """NEXI/gpuNEXI.m:1101-1162."""
+        from .askadam_solver import check_set_default_basic as adam_def
+        from .mcmc_solver import check_set_default_basic as mcmc_def
+        f = dict(fitting or {})
+        f.setdefault("solver", "askadam")
+        if f["solver"].lower() == "mcmc":
+            g = mcmc_def(f)
+            g["lossFunction"] = "l2"
+        else:
+            g = adam_def(f)
+            g.setdefault("regmap", "fa")
+            if "regmap" not in f:
+                g["regmap"] = "fa"
+            if not isinstance(g["regmap"], (list, tuple)):
+                g["regmap"] = [g["regmap"]]
+            g.setdefault("regularisationType", "TV")
+            if g["regularisationType"].lower() not in ("tv", "prior"):
+                raise GacelleError(GX_EINVAL, "GACELLE:invalidRegularisationType")
+        g.setdefault("lmax", 0)
+        g.setdefault("start", "likelihood")
+        g.setdefault("dataType", "volumetric")
+        return g
+
+    def compute_optimisation_weights(self, mask, lossFunction, lmax):
+        """NEXI/gpuNEXI.m:455-477: w = Nav/(2l+1), sqrt for L1, normalised."""
+        ls = list(range(0, lmax + 1, 2))
+        w = np.concatenate([self.Nav / (2 * l + 1) for l in ls])
+        if str(lossFunction).lower() == "l1":
+            w = np.sqrt(w)
+        return w / w.max()
+
+    def fit(self, dwi, mask=None, fitting=None, pars0=None, extradata=None):
+        """NEXI/gpuNEXI.m:290-450 (volumetric data)."""
+        dwi = np.asarray(dwi)
+        if mask is None:
+            mask = np.ones(utils.dims3(dwi), dtype=bool)
+        fitting = self.check_set_default(fitting)
+        self.updateProperty(fitting)
+        fitting["modelParams"] = list(self.modelParams)
+        if not len(fitting["ub"]):
+            fitting["ub"] = self.ub[: len(self.modelParams)]
+        if not len(fitting["lb"]):
+            fitting["lb"] = self.lb[: len(self.modelParams)]
+        if fitting.get("dataType", "volumetric") != "volumetric":
+            raise GacelleError(GX_EUNSUPPORTED, "surface data are not accelerated")
+        if fitting["solver"] == "askadam" and str(fitting.get("regularisationType", "TV")).lower() == "prior" \
+                and np.atleast_1d(fitting["lambda"])[0] > 0:
+            raise GacelleError(GX_EUNSUPPORTED, "prior-distribution regularisation is not accelerated")
+        wv = self.compute_optimisation_weights(mask, fitting["lossFunction"], fitting["lmax"])
+        if pars0 is None:
+            start = fitting["start"]
+            if isinstance(start, str) and start.lower() == "likelihood":
+                raise GacelleError(GX_EUNSUPPORTED, "start='likelihood' (dictionary starting points) is "
+                                                    "not implemented by the engine; pass pars0 or start='default'")
+            pars0 = utils.initialise_x0(utils.dims3(mask), self.modelParams, self.startPoint)
+        pars0 = {p: np.clip(np.asarray(pars0[p], dtype=np.float32), fitting["lb"][k], fitting["ub"][k])
+                 for k, p in enumerate(self.modelParams)}
+        w = None
+        if not np.all(wv == 1):
+            w = np.broadcast_to(wv, utils.dims3(mask) + (wv.size,)).copy()
+        return self._solve(dwi, mask, w, pars0, fitting, extradata=extradata)

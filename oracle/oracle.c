@@ -1,0 +1,989 @@
+/*
+ * oracle.c -- FP64 CPU restatement of GACELLE's askAdam / MCMC hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (checker and CPU baseline).  Never part of the
+ * product path.  PARITY UNPINNED against MATLAB runs (no MATLAB exists here
+ * and the reference ships no golden vectors); pinned by the source formulas
+ * cited per function, finite differences, float64 autograd, the reference's
+ * stated quadrature accuracies and the Philox known-answer vectors.
+ *
+ * All reference citations are paths inside kschan0214/gacelle.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_EPS 1e-8 /* askadam.epsilon (utils/askadam.m:14), utils.epsilon */
+
+/* ------------------------------------------------------------------------ */
+/* Philox4x32-10, Salmon, Moraes, Dror & Shaw, "Parallel random numbers: as  */
+/* easy as 1, 2, 3", SC'11.                                                  */
+/* ------------------------------------------------------------------------ */
+void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Uniform on the open interval (0,1); 23 random bits so that the value is
+ * exactly representable in FP32 (the device computes the same number). */
+double orc_u01(uint32_t x) { return ((double)(x >> 9) + 0.5) * (1.0 / 8388608.0); }
+
+static uint32_t rand_below(uint32_t x, uint32_t n) { return (uint32_t)(((uint64_t)x * n) >> 32); }
+
+/* Random-stream tags (4th counter word, low byte). */
+enum { TAG_ADAM_INIT = 1, TAG_GW_INIT = 2, TAG_GW_MOVE = 3, TAG_GW_PERM = 4,
+       TAG_GW_RBPART = 5, TAG_MH_MOVE = 6 };
+
+static void philox_call(uint64_t seed, uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                        uint32_t out[4]) {
+    uint32_t ctr[4] = {a, b, c, d};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    orc_philox(ctr, key, out);
+}
+
+/* Box-Muller pair from two uniforms. */
+static void box_muller(uint32_t a, uint32_t b, double* n0, double* n1) {
+    double u1 = orc_u01(a), u2 = orc_u01(b);
+    double r = sqrt(-2.0 * log(u1));
+    double ang = 2.0 * M_PI * u2;
+    *n0 = r * cos(ang);
+    *n1 = r * sin(ang);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Models                                                                    */
+/* ------------------------------------------------------------------------ */
+int orc_nparams(const orc_model* m) {
+    switch (m->model) {
+    case ORC_MODEL_R2S: return 2;   /* M0, R2star   (R2star/gpuR2starMapping.m:24) */
+    case ORC_MODEL_R1R2S: return 3; /* M0, R1, R2star (R1R2s/gpuJointR1R2starMapping.m:25) */
+    case ORC_MODEL_NEXI: return m->lmax == 2 ? 5 : 4; /* fa, Da, De, ra[, p2] (NEXI/gpuNEXI.m:28,125-133) */
+    }
+    return 0;
+}
+
+int orc_nmeas(const orc_model* m) {
+    switch (m->model) {
+    case ORC_MODEL_R2S: return m->n_te;
+    case ORC_MODEL_R1R2S: return m->n_te * m->n_fa;
+    case ORC_MODEL_NEXI: return m->n_shell * (m->lmax / 2 + 1);
+    }
+    return 0;
+}
+
+/* S = M0 exp(-TE R2*)   (R2star/gpuR2starMapping.m:427-434) */
+static void r2s_fwd(const orc_model* m, const double* th, double* s) {
+    for (int t = 0; t < m->n_te; ++t) s[t] = th[0] * exp(-m->te[t] * th[1]);
+}
+
+static void r2s_vjp(const orc_model* m, const double* th, const double* sb, double* tb) {
+    for (int t = 0; t < m->n_te; ++t) {
+        double e = exp(-m->te[t] * th[1]);
+        tb[0] += sb[t] * e;
+        tb[1] += sb[t] * (-m->te[t] * th[0] * e);
+    }
+}
+
+/* S = M0 sin(a)(1-E1)/(1-cos(a)E1) exp(-TE R2*), E1 = exp(-TR R1), a = b1*FA,
+ * TE fastest then FA   (R1R2s/gpuJointR1R2starMapping.m:375-422,513-525) */
+static void r1r2s_fwd(const orc_model* m, const double* th, double b1, double* s) {
+    double M0 = th[0], R1 = th[1], R2 = th[2];
+    double E1 = exp(-m->tr * R1);
+    for (int f = 0; f < m->n_fa; ++f) {
+        double a = b1 * m->fa_deg[f] * (M_PI / 180.0);
+        double A = sin(a) * (1.0 - E1) / (1.0 - cos(a) * E1);
+        for (int t = 0; t < m->n_te; ++t) s[t + f * m->n_te] = M0 * A * exp(-m->te[t] * R2);
+    }
+}
+
+static void r1r2s_vjp(const orc_model* m, const double* th, double b1, const double* sb,
+                      double* tb) {
+    double M0 = th[0], R1 = th[1], R2 = th[2];
+    double E1 = exp(-m->tr * R1);
+    for (int f = 0; f < m->n_fa; ++f) {
+        double a = b1 * m->fa_deg[f] * (M_PI / 180.0);
+        double sa = sin(a), ca = cos(a);
+        double den = 1.0 - ca * E1;
+        double A = sa * (1.0 - E1) / den;
+        double dA_dE1 = sa * (ca - 1.0) / (den * den);
+        double dA_dR1 = dA_dE1 * (-m->tr * E1);
+        for (int t = 0; t < m->n_te; ++t) {
+            double g = sb[t + f * m->n_te];
+            double E2 = exp(-m->te[t] * R2);
+            tb[0] += g * A * E2;
+            tb[1] += g * M0 * E2 * dA_dR1;
+            tb[2] += g * (-m->te[t] * M0 * A * E2);
+        }
+    }
+}
+
+/* NEXI node value M(x) (NEXI/gpuNEXI.m:1090-1097) and its partials with
+ * respect to (f, d1, d2, r1, r2). */
+typedef struct { double M, df, dd1, dd2, dr1, dr2; } nexi_node;
+
+static nexi_node nexi_node_eval(double f, double d1, double d2, double r1, double r2) {
+    nexi_node n;
+    double sdiff = r1 - r2 + d1 - d2;
+    double Q = sdiff * sdiff + 4.0 * r1 * r2;
+    double l2raw = sqrt(Q) / 2.0;
+    int active = l2raw > ORC_EPS;
+    double l2 = active ? l2raw : ORC_EPS;
+    double l1 = (r1 + r2 + d1 + d2) / 2.0;
+    double lm = l1 - l2, lp = l1 + l2;
+    double N = f * d1 + (1.0 - f) * d2 - lm;
+    double Pp = N / (l2 * 2.0);
+    double ep = exp(-lp), em = exp(-lm);
+    n.M = Pp * ep + (1.0 - Pp) * em;
+    /* reverse sweep with Mbar = 1 */
+    double Ppb = ep - em;
+    double lpb = -Pp * ep;
+    double lmb = -(1.0 - Pp) * em;
+    double Nb = Ppb / (2.0 * l2);
+    double l2b = -Ppb * Pp / l2;
+    double fb = Nb * (d1 - d2);
+    double d1b = Nb * f;
+    double d2b = Nb * (1.0 - f);
+    lmb += -Nb;
+    double l1b = lpb + lmb;
+    l2b += lpb - lmb;
+    double r1b = 0.0, r2b = 0.0;
+    if (active) {
+        double Qb = l2b / (8.0 * l2raw);
+        double sb = 2.0 * sdiff * Qb;
+        r1b += 4.0 * r2 * Qb + sb;
+        r2b += 4.0 * r1 * Qb - sb;
+        d1b += sb;
+        d2b -= sb;
+    }
+    r1b += 0.5 * l1b; r2b += 0.5 * l1b; d1b += 0.5 * l1b; d2b += 0.5 * l1b;
+    n.df = fb; n.dd1 = d1b; n.dd2 = d2b; n.dr1 = r1b; n.dr2 = r2b;
+    return n;
+}
+
+/* Trapezoid weights of utils/gacelle_trapz.m:53-56 on x = linspace(0,1,nx). */
+static double trapz_w(int i, int nx) {
+    double h = 1.0 / (nx - 1);
+    return (i == 0 || i == nx - 1) ? 0.5 * h : h;
+}
+
+/* Per-shell raw (pre-min) signals: Sl0[j], and Sl2 integral T[j] when lmax=2
+ * (NEXI/gpuNEXI.m:932-996). */
+static void nexi_raw(const orc_model* m, const double* th, double* sl0, double* T2) {
+    double fa = fmax(th[0], ORC_EPS), Da = th[1], De = th[2], ra = th[3];
+    int nx = m->nx;
+    for (int j = 0; j < m->n_shell; ++j) {
+        double b = m->bval[j], D = m->delta[j];
+        double Daj = b * Da, Dej = b * De, r1 = D * ra, r2 = r1 * fa / (1.0 - fa);
+        double s0 = 0.0, s2 = 0.0;
+        for (int i = 0; i < nx; ++i) {
+            double x = (double)i / (nx - 1);
+            nexi_node n = nexi_node_eval(fa, Daj * x * x, Dej, r1, r2);
+            double w = trapz_w(i, nx);
+            s0 += w * n.M;
+            s2 += w * n.M * (3.0 * x * x - 1.0) / 2.0;
+        }
+        sl0[j] = s0;
+        if (T2) T2[j] = s2;
+    }
+}
+
+static void nexi_fwd(const orc_model* m, const double* th, double* s) {
+    int ns = m->n_shell;
+    double T2[256];
+    nexi_raw(m, th, s, m->lmax == 2 ? T2 : NULL);
+    if (m->lmax == 2)
+        for (int j = 0; j < ns; ++j) s[ns + j] = th[4] * fabs(T2[j]);
+    int nm = orc_nmeas(m);
+    for (int k = 0; k < nm; ++k) s[k] = fmin(s[k], 1.0); /* NEXI/gpuNEXI.m:928 */
+}
+
+static void nexi_vjp(const orc_model* m, const double* th, const double* sb_in, double* tb) {
+    int ns = m->n_shell, nx = m->nx;
+    double sl0[256], T2[256], sb[512];
+    nexi_raw(m, th, sl0, m->lmax == 2 ? T2 : NULL);
+    for (int j = 0; j < ns; ++j) sb[j] = sl0[j] <= 1.0 ? sb_in[j] : 0.0;
+    if (m->lmax == 2)
+        for (int j = 0; j < ns; ++j) sb[ns + j] = th[4] * fabs(T2[j]) <= 1.0 ? sb_in[ns + j] : 0.0;
+    double fa = fmax(th[0], ORC_EPS), Da = th[1], De = th[2], ra = th[3];
+    double fb = 0, Dab = 0, Deb = 0, rab = 0;
+    for (int j = 0; j < ns; ++j) {
+        double b = m->bval[j], D = m->delta[j];
+        double Dej = b * De, r1 = D * ra, r2 = r1 * fa / (1.0 - fa);
+        double sgn2 = 0.0;
+        if (m->lmax == 2) {
+            tb[4] += sb[ns + j] * fabs(T2[j]);
+            sgn2 = (T2[j] > 0) - (T2[j] < 0);
+        }
+        for (int i = 0; i < nx; ++i) {
+            double x = (double)i / (nx - 1);
+            double w = trapz_w(i, nx);
+            double Mb = sb[j] * w;
+            if (m->lmax == 2) Mb += sb[ns + j] * th[4] * sgn2 * w * (3.0 * x * x - 1.0) / 2.0;
+            if (Mb == 0.0) continue;
+            nexi_node n = nexi_node_eval(fa, b * Da * x * x, Dej, r1, r2);
+            double r2_r1 = fa / (1.0 - fa);
+            double r2_f = r1 / ((1.0 - fa) * (1.0 - fa));
+            fb += Mb * (n.df + n.dr2 * r2_f);
+            Dab += Mb * n.dd1 * b * x * x;
+            Deb += Mb * n.dd2 * b;
+            rab += Mb * (n.dr1 + n.dr2 * r2_r1) * D;
+        }
+    }
+    if (th[0] > ORC_EPS) tb[0] += fb; /* fa = max(fa, eps), NEXI/gpuNEXI.m:905 */
+    tb[1] += Dab;
+    tb[2] += Deb;
+    tb[3] += rab;
+}
+
+void orc_forward_voxel(const orc_model* m, const double* th, double b1, double* s) {
+    switch (m->model) {
+    case ORC_MODEL_R2S: r2s_fwd(m, th, s); break;
+    case ORC_MODEL_R1R2S: r1r2s_fwd(m, th, b1, s); break;
+    case ORC_MODEL_NEXI: nexi_fwd(m, th, s); break;
+    }
+}
+
+void orc_vjp_voxel(const orc_model* m, const double* th, double b1, const double* sb,
+                   double* tb) {
+    switch (m->model) {
+    case ORC_MODEL_R2S: r2s_vjp(m, th, sb, tb); break;
+    case ORC_MODEL_R1R2S: r1r2s_vjp(m, th, b1, sb, tb); break;
+    case ORC_MODEL_NEXI: nexi_vjp(m, th, sb, tb); break;
+    }
+}
+
+void orc_forward(const orc_model* m, const double* theta, const double* b1, int nvox, double* s) {
+    int np = orc_nparams(m), nm = orc_nmeas(m);
+#pragma omp parallel for schedule(static)
+    for (int v = 0; v < nvox; ++v) {
+        double th[8], sv[512];
+        for (int k = 0; k < np; ++k) th[k] = theta[(size_t)k * nvox + v];
+        orc_forward_voxel(m, th, b1 ? b1[v] : 1.0, sv);
+        for (int k = 0; k < nm; ++k) s[(size_t)k * nvox + v] = sv[k];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Bessel functions (DLMF 10.25.2 power series; 10.40.1 asymptotic series)  */
+/* ------------------------------------------------------------------------ */
+static double bessel_scaled(int nu, double x) {
+    double ax = fabs(x);
+    double v;
+    if (ax < 30.0) {
+        double t = ax * ax / 4.0, term = (nu == 0) ? 1.0 : ax / 2.0, sum = 0.0;
+        for (int k = 0; k < 500; ++k) {
+            sum += term;
+            term *= t / ((k + 1.0) * (k + 1.0 + nu));
+            if (term < 1e-18 * sum) break;
+        }
+        v = sum * exp(-ax);
+    } else {
+        double mu = 4.0 * nu * nu, sum = 1.0, prod = 1.0;
+        for (int k = 1; k < 40; ++k) {
+            double f = (2.0 * k - 1.0);
+            prod *= -(mu - f * f) / (k * 8.0 * ax);
+            sum += prod;
+            if (fabs(prod) < 1e-18) break;
+        }
+        v = sum / sqrt(2.0 * M_PI * ax);
+    }
+    if (nu == 1 && x < 0) v = -v;
+    return v;
+}
+
+double orc_i0e(double x) { return bessel_scaled(0, x); }
+double orc_i1e(double x) { return bessel_scaled(1, x); }
+
+/* I_nu(z) = 1/pi * trapz(theta, exp(z cos theta) cos(nu theta)), theta in [0,pi]
+ * (utils/gacelle_besseli.m:3-8). */
+double orc_besseli_trapz(int nu, double z, int nx) {
+    double h = M_PI / (nx - 1), s = 0.0;
+    for (int i = 0; i < nx; ++i) {
+        double th = i * h;
+        double w = (i == 0 || i == nx - 1) ? 0.5 * h : h;
+        s += w * exp(z * cos(th)) * cos(nu * th);
+    }
+    return s / M_PI;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Elementwise losses (utils/askadam.m:86-95; MATLAB l1loss/l2loss/huber/mse */
+/* with Reduction="none"), plus Gaussian and Rician negative log-likelihoods */
+/* ------------------------------------------------------------------------ */
+static double sgn(double x) { return (x > 0) - (x < 0); }
+
+double orc_loss_value(int loss, double s, double y, double w, double sigma, double mse_scale,
+                      double hd) {
+    double r = s - y;
+    switch (loss) {
+    case ORC_LOSS_L1: return w * fabs(r);
+    case ORC_LOSS_L2: return w * r * r;
+    case ORC_LOSS_HUBER: {
+        double a = fabs(r);
+        return w * (a <= hd ? 0.5 * r * r : hd * a - 0.5 * hd * hd);
+    }
+    case ORC_LOSS_MSE: return mse_scale * r * r; /* weights ignored, askadam.m:93-94 */
+    case ORC_LOSS_GAUSS: {
+        double s2 = sigma * sigma;
+        return w * (r * r / (2.0 * s2) + 0.5 * log(2.0 * M_PI * s2));
+    }
+    case ORC_LOSS_RICIAN: {
+        double s2 = sigma * sigma;
+        double x = y * s / s2, ax = fabs(x);
+        double logI0 = ax + log(orc_i0e(ax));
+        double c = y > 0 ? -log(y / s2) : 0.0;
+        return w * ((y * y + s * s) / (2.0 * s2) - logI0 + c);
+    }
+    }
+    return 0.0;
+}
+
+double orc_loss_deriv(int loss, double s, double y, double w, double sigma, double mse_scale,
+                      double hd) {
+    double r = s - y;
+    switch (loss) {
+    case ORC_LOSS_L1: return w * sgn(r);
+    case ORC_LOSS_L2: return 2.0 * w * r;
+    case ORC_LOSS_HUBER: return fabs(r) <= hd ? w * r : w * hd * sgn(r);
+    case ORC_LOSS_MSE: return 2.0 * mse_scale * r;
+    case ORC_LOSS_GAUSS: return w * r / (sigma * sigma);
+    case ORC_LOSS_RICIAN: {
+        double s2 = sigma * sigma;
+        double x = y * s / s2;
+        double ratio = orc_i1e(x) / orc_i0e(x);
+        return w * (s / s2 - (y / s2) * ratio);
+    }
+    }
+    return 0.0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Spatial TV (utils/spatial_total_variation.m:24-66): periodic forward     */
+/* differences, mask applied at the centre voxel only.                      */
+/* ------------------------------------------------------------------------ */
+static size_t lin(const int d[3], int x, int y, int z) {
+    return (size_t)x + (size_t)d[0] * ((size_t)y + (size_t)d[1] * z);
+}
+
+double orc_tv_cost(const int d[3], const unsigned char* mask, const double* img, int tv_3d,
+                   const double vs[3]) {
+    double cost = 0.0;
+    int nd = tv_3d ? 3 : 2;
+    for (int z = 0; z < d[2]; ++z)
+        for (int y = 0; y < d[1]; ++y)
+            for (int x = 0; x < d[0]; ++x) {
+                size_t p = lin(d, x, y, z);
+                if (!mask[p]) continue;
+                double c = img[p];
+                double nb[3] = {img[lin(d, (x + 1) % d[0], y, z)], img[lin(d, x, (y + 1) % d[1], z)],
+                                img[lin(d, x, y, (z + 1) % d[2])]};
+                for (int k = 0; k < nd; ++k) cost += fabs((nb[k] - c) / vs[k]);
+            }
+    return cost;
+}
+
+void orc_tv_grad(const int d[3], const unsigned char* mask, const double* img, int tv_3d,
+                 const double vs[3], double* g) {
+    int nd = tv_3d ? 3 : 2;
+    for (int z = 0; z < d[2]; ++z)
+        for (int y = 0; y < d[1]; ++y)
+            for (int x = 0; x < d[0]; ++x) {
+                size_t q = lin(d, x, y, z);
+                double c = img[q], acc = 0.0;
+                size_t fw[3] = {lin(d, (x + 1) % d[0], y, z), lin(d, x, (y + 1) % d[1], z),
+                                lin(d, x, y, (z + 1) % d[2])};
+                size_t bw[3] = {lin(d, (x + d[0] - 1) % d[0], y, z),
+                                lin(d, x, (y + d[1] - 1) % d[1], z),
+                                lin(d, x, y, (z + d[2] - 1) % d[2])};
+                for (int k = 0; k < nd; ++k) {
+                    if (mask[q]) acc -= sgn(img[fw[k]] - c) / vs[k];
+                    if (mask[bw[k]]) acc += sgn(c - img[bw[k]]) / vs[k];
+                }
+                g[q] = acc;
+            }
+}
+
+/* ------------------------------------------------------------------------ */
+/* askAdam                                                                   */
+/* ------------------------------------------------------------------------ */
+static double sigmoid(double z) { return 1.0 / (1.0 + exp(-z)); }
+
+/* unscale_parameters (utils/askadam.m:1063-1075) */
+static double unscale(const orc_adam_opts* o, int k, double z) {
+    if (o->transform == ORC_TRANSFORM_SIGMOID) return o->lb[k] + (o->ub[k] - o->lb[k]) * sigmoid(z);
+    return z * (o->ub[k] - o->lb[k]) + o->lb[k];
+}
+
+static double dunscale(const orc_adam_opts* o, int k, double z) {
+    if (o->transform == ORC_TRANSFORM_SIGMOID) {
+        double s = sigmoid(z);
+        return (o->ub[k] - o->lb[k]) * s * (1.0 - s);
+    }
+    return o->ub[k] - o->lb[k];
+}
+
+typedef struct {
+    const orc_model* m;
+    const orc_volume* vol;
+    const orc_adam_opts* o;
+    int np, nm, nv;
+    double norm;           /* 1 / (nm * Nv) */
+    unsigned char* mask;   /* full-grid mask for TV */
+    double* grid;          /* full-grid image scratch */
+    double* grid_g;
+    size_t ngrid;
+} adam_ctx;
+
+/* askadam.model_gradient (utils/askadam.m:23-117) at parameters z (linear
+ * mode: already clamped).  Returns total loss; gz [np][nv] gradient w.r.t. z. */
+static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, double* fid_out,
+                     double* reg_out, double* gtheta_out) {
+    const orc_adam_opts* o = c->o;
+    const orc_volume* vol = c->vol;
+    int np = c->np, nm = c->nm, nv = c->nv;
+    double fid = 0.0;
+    double* theta = (double*)malloc(sizeof(double) * (size_t)np * nv);
+    double* gth = (double*)calloc((size_t)np * nv, sizeof(double));
+    for (size_t i = 0; i < (size_t)np * nv; ++i) theta[i] = unscale(o, (int)(i / nv), z[i]);
+#pragma omp parallel for reduction(+ : fid) schedule(static) num_threads(o->nthreads > 0 ? o->nthreads : 1)
+    for (int v = 0; v < nv; ++v) {
+        double th[8], s[512], sb[512], tb[8] = {0};
+        for (int k = 0; k < np; ++k) th[k] = theta[(size_t)k * nv + v];
+        double b1 = vol->b1 ? vol->b1[v] : 1.0;
+        double sig = vol->sigma ? vol->sigma[v] : o->sigma;
+        orc_forward_voxel(c->m, th, b1, s);
+        double lf = 0.0;
+        for (int k = 0; k < nm; ++k) {
+            int bad = !isfinite(s[k]);
+            double sk = bad ? 0.0 : s[k]; /* utils.set_nan_inf_zero, askadam.m:80 */
+            double y = vol->data[(size_t)k * nv + v];
+            double w = vol->weights ? vol->weights[(size_t)k * nv + v] : 1.0;
+            double rv = orc_loss_value(o->loss, sk, y, w, sig, o->mse_scale, o->huber_delta);
+            if (res) res[(size_t)k * nv + v] = rv;
+            lf += rv;
+            sb[k] = bad ? 0.0 : orc_loss_deriv(o->loss, sk, y, w, sig, o->mse_scale, o->huber_delta) * c->norm;
+        }
+        fid += lf;
+        orc_vjp_voxel(c->m, th, b1, sb, tb);
+        for (int k = 0; k < np; ++k) gth[(size_t)k * nv + v] = tb[k];
+    }
+    fid *= c->norm;
+    double reg = 0.0;
+    if (o->n_reg > 0 && o->lambda[0] > 0) { /* spatial_total_variation.m:29 */
+        double nmask = (double)nv;
+        for (int r = 0; r < o->n_reg; ++r) {
+            int k = o->reg_param[r];
+            memset(c->grid, 0, sizeof(double) * c->ngrid);
+            for (int v = 0; v < nv; ++v) c->grid[vol->grid_index[v]] = theta[(size_t)k * nv + v];
+            double cost = orc_tv_cost(vol->dims, c->mask, c->grid, o->tv_3d, o->voxel_size);
+            reg += cost / nmask * o->lambda[r];
+            orc_tv_grad(vol->dims, c->mask, c->grid, o->tv_3d, o->voxel_size, c->grid_g);
+            for (int v = 0; v < nv; ++v)
+                gth[(size_t)k * nv + v] += o->lambda[r] / nmask * c->grid_g[vol->grid_index[v]];
+        }
+    }
+    for (size_t i = 0; i < (size_t)np * nv; ++i) {
+        int k = (int)(i / nv);
+        gz[i] = gth[i] * dunscale(o, k, z[i]);
+    }
+    if (gtheta_out) memcpy(gtheta_out, gth, sizeof(double) * (size_t)np * nv);
+    free(theta);
+    free(gth);
+    if (fid_out) *fid_out = fid;
+    if (reg_out) *reg_out = reg;
+    return fid + reg;
+}
+
+static int setup_ctx(adam_ctx* c, const orc_model* m, const orc_volume* vol,
+                     const orc_adam_opts* o) {
+    c->m = m; c->vol = vol; c->o = o;
+    c->np = orc_nparams(m); c->nm = orc_nmeas(m); c->nv = vol->nvox;
+    double nn = vol->norm_nvox > 0 ? vol->norm_nvox : (double)vol->nvox;
+    c->norm = 1.0 / ((double)c->nm * nn);
+    c->mask = NULL; c->grid = NULL; c->grid_g = NULL; c->ngrid = 0;
+    if (o->n_reg > 0 && o->lambda[0] > 0) {
+        if (!vol->grid_index) return -1;
+        c->ngrid = (size_t)vol->dims[0] * vol->dims[1] * vol->dims[2];
+        c->mask = (unsigned char*)calloc(c->ngrid, 1);
+        c->grid = (double*)calloc(c->ngrid, sizeof(double));
+        c->grid_g = (double*)calloc(c->ngrid, sizeof(double));
+        for (int v = 0; v < vol->nvox; ++v) c->mask[vol->grid_index[v]] = 1;
+    }
+    return 0;
+}
+
+static void free_ctx(adam_ctx* c) { free(c->mask); free(c->grid); free(c->grid_g); }
+
+double orc_model_gradient(const orc_model* m, const orc_volume* vol, const orc_adam_opts* o,
+                          const double* theta, double* gtheta, double* residual, double* fid,
+                          double* reg) {
+    adam_ctx c;
+    if (setup_ctx(&c, m, vol, o)) return NAN;
+    /* evaluate with an identity-like transform by passing z such that unscale(z) = theta:
+     * use the linear map directly. */
+    orc_adam_opts lin = *o;
+    lin.transform = ORC_TRANSFORM_LINEAR;
+    c.o = &lin;
+    size_t n = (size_t)c.np * c.nv;
+    double* z = (double*)malloc(sizeof(double) * n);
+    double* gz = (double*)malloc(sizeof(double) * n);
+    for (size_t i = 0; i < n; ++i) {
+        int k = (int)(i / c.nv);
+        z[i] = (theta[i] - o->lb[k]) / (o->ub[k] - o->lb[k]);
+    }
+    double L = eval_z(&c, z, gz, residual, fid, reg, gtheta);
+    free(z); free(gz); free_ctx(&c);
+    return L;
+}
+
+static double clamp01(double z) { return z < 0 ? 0 : (z > 1 ? 1 : z); }
+
+int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* o,
+                orc_adam_result* r) {
+    adam_ctx c;
+    if (setup_ctx(&c, m, vol, o)) return -1;
+    int np = c.np, nm = c.nm, nv = c.nv;
+    size_t n = (size_t)np * nv;
+    double* z = (double*)malloc(sizeof(double) * n);
+    double* zc = (double*)calloc(n, sizeof(double));
+    double* zmin = (double*)malloc(sizeof(double) * n);
+    double* zprev = (double*)malloc(sizeof(double) * n);
+    double* g = (double*)malloc(sizeof(double) * n);
+    double* m1 = (double*)calloc(n, sizeof(double));
+    double* m2 = (double*)calloc(n, sizeof(double));
+    double* res = (double*)malloc(sizeof(double) * (size_t)nm * nv);
+    double* resmin = (double*)malloc(sizeof(double) * (size_t)nm * nv);
+    int lin_mode = o->transform == ORC_TRANSFORM_LINEAR;
+
+    /* initialise_parameter (utils/askadam.m:368-412) */
+    for (int k = 0; k < np; ++k)
+        for (int v = 0; v < nv; ++v) {
+            uint32_t u[4];
+            philox_call(o->seed, (uint32_t)v, (uint32_t)k, 0u, TAG_ADAM_INIT, u);
+            double nrm, dummy;
+            box_muller(u[0], u[1], &nrm, &dummy);
+            double uni = orc_u01(u[2]);
+            double zz;
+            if (vol->theta0) {
+                double t0 = vol->theta0[(size_t)k * nv + v];
+                if (!lin_mode) {
+                    double eb = 1e-4 * (o->ub[k] - o->lb[k]);
+                    double tc = fmax(fmin(t0, o->ub[k] - eb), o->lb[k] + eb);
+                    double nn = (tc - o->lb[k]) / (o->ub[k] - o->lb[k]);
+                    zz = (1.0 - o->randomness) * log(nn / (1.0 - nn)) + o->randomness * nrm;
+                } else {
+                    zz = (1.0 - o->randomness) * (t0 - o->lb[k]) / (o->ub[k] - o->lb[k]) +
+                         o->randomness * uni;
+                }
+            } else {
+                zz = lin_mode ? uni : o->randomness * nrm;
+            }
+            if (lin_mode) zz = clamp01(zz); /* set_boundary01, askadam.m:185 */
+            z[(size_t)k * nv + v] = o->state_f32 ? (double)(float)zz : zz;
+        }
+
+#define EVAL(resbuf, fidp, regp)                                                           \
+    ({                                                                                     \
+        for (size_t i_ = 0; i_ < n; ++i_) zc[i_] = lin_mode ? clamp01(z[i_]) : z[i_];      \
+        double L_ = eval_z(&c, zc, g, resbuf, fidp, regp, NULL);                           \
+        if (lin_mode)                                                                      \
+            for (size_t i_ = 0; i_ < n; ++i_)                                              \
+                if (z[i_] < 0.0 || z[i_] > 1.0) g[i_] = 0.0;                               \
+        L_;                                                                                \
+    })
+
+    double fid, reg;
+    double loss = EVAL(res, &fid, &reg);
+    if (r->loss_history) r->loss_history[0] = loss;
+    double minLoss = loss, minFid = fid, minReg = reg;
+    memcpy(zmin, z, sizeof(double) * n);
+    memcpy(resmin, res, sizeof(double) * (size_t)nm * nv);
+    int minIter = 0, epoch = 0, stop = ORC_STOP_NONE;
+    double ema = loss;
+    int W = o->conv_window > 0 ? o->conv_window : 1;
+    double* buf = (double*)malloc(sizeof(double) * W);
+    for (int i = 0; i < W; ++i) buf[i] = 1.0;
+    double ewic = 0, ewis = 0, ewig = 0;
+    memcpy(zprev, z, sizeof(double) * n);
+
+    for (int e = 1; e <= o->iteration; ++e) {
+        epoch = e;
+        loss = EVAL(res, &fid, &reg);
+        if (r->loss_history) r->loss_history[e] = loss;
+        if (minLoss > loss) { /* update_min_loss, askadam.m:433-446 */
+            minLoss = loss; minFid = fid; minReg = reg;
+            memcpy(zmin, z, sizeof(double) * n);
+            memcpy(resmin, res, sizeof(double) * (size_t)nm * nv);
+            minIter = e;
+        }
+        /* update_convergence_signals, askadam.m:512-632 (robustConvergence off) */
+        double conv;
+        if (o->conv_model == ORC_CONV_EMA) {
+            double en = o->ema_decay * ema + (1.0 - o->ema_decay) * loss;
+            conv = fabs(en - ema) / (fabs(ema) + 1e-8);
+            ema = en;
+        } else {
+            for (int i = 0; i < W - 1; ++i) buf[i] = buf[i + 1];
+            buf[W - 1] = loss;
+            double xm = (W + 1) / 2.0, ym = 0, sxy = 0, sxx = 0;
+            for (int i = 0; i < W; ++i) ym += buf[i];
+            ym /= W;
+            for (int i = 0; i < W; ++i) {
+                sxy += (i + 1 - xm) * (buf[i] - ym);
+                sxx += (i + 1 - xm) * (i + 1 - xm);
+            }
+            conv = sxx > 0 ? -(sxy / sxx) : 0.0;
+        }
+        if (conv > o->conv_value || e <= o->conv_window) ewic = 0;
+        else if ((minLoss - loss) > o->conv_value) ewic = 0;
+        else ewic += 1;
+        if (o->step_tol > 0) {
+            double num = 0, den = 0;
+            for (size_t i = 0; i < n; ++i) {
+                double dd = z[i] - zprev[i];
+                num += dd * dd;
+                den += z[i] * z[i];
+            }
+            double sn = sqrt(num) / (1.0 + sqrt(den));
+            memcpy(zprev, z, sizeof(double) * n);
+            ewis = sn < o->step_tol ? ewis + 1 : 0;
+        }
+        if (o->grad_tol > 0) {
+            double gn = 0;
+            for (size_t i = 0; i < n; ++i) gn += g[i] * g[i];
+            gn = sqrt(gn);
+            ewig = gn < o->grad_tol ? ewig + 1 : 0;
+        }
+        /* check_stopping, askadam.m:634-671 */
+        if (ewic > o->patience_conv) { stop = ORC_STOP_CONVERGENCE; break; }
+        if (loss < o->tol) { stop = ORC_STOP_TOL; break; }
+        if (o->step_tol > 0 && ewis > o->patience_step) { stop = ORC_STOP_STEP; break; }
+        if (o->grad_tol > 0 && ewig > o->patience_grad) { stop = ORC_STOP_GRAD; break; }
+        /* update_parameters, askadam.m:673-691 */
+        double lr = o->lr / (1.0 + o->decay * (e - 1));
+        if (e < o->iteration) {
+            double bc1 = 1.0 - pow(o->beta1, e), bc2 = 1.0 - pow(o->beta2, e);
+            for (size_t i = 0; i < n; ++i) {
+                double gi = g[i];
+                if (o->optimiser == ORC_OPT_ADAM) {
+                    m1[i] = o->beta1 * m1[i] + (1.0 - o->beta1) * gi;
+                    m2[i] = o->beta2 * m2[i] + (1.0 - o->beta2) * gi * gi;
+                    z[i] -= lr * (m1[i] / bc1) / (sqrt(m2[i] / bc2) + o->eps);
+                } else if (o->optimiser == ORC_OPT_SGDM) {
+                    m1[i] = o->momentum * m1[i] - lr * gi;
+                    z[i] += m1[i];
+                } else {
+                    m2[i] = o->rms_decay * m2[i] + (1.0 - o->rms_decay) * gi * gi;
+                    z[i] -= lr * gi / (sqrt(m2[i]) + o->rms_eps);
+                }
+                if (o->state_f32) {
+                    z[i] = (float)z[i];
+                    m1[i] = (float)m1[i];
+                    m2[i] = (float)m2[i];
+                }
+            }
+        }
+    }
+    /* finalisation (askadam.m:312-362) */
+    for (size_t i = 0; i < n; ++i) {
+        int k = (int)(i / nv);
+        double zf = lin_mode ? clamp01(z[i]) : z[i];
+        double zm = lin_mode ? clamp01(zmin[i]) : zmin[i];
+        r->final_theta[i] = unscale(o, k, zf);
+        if (r->min_theta) r->min_theta[i] = unscale(o, k, zm);
+    }
+    if (r->final_residual) memcpy(r->final_residual, res, sizeof(double) * (size_t)nm * nv);
+    if (r->min_residual) memcpy(r->min_residual, resmin, sizeof(double) * (size_t)nm * nv);
+    r->final_loss = loss; r->final_fid = fid; r->final_reg = reg;
+    r->min_loss = minLoss; r->min_fid = minFid; r->min_reg = minReg;
+    r->final_niter = epoch; r->min_niter = minIter; r->stop_reason = stop;
+#undef EVAL
+    free(z); free(zc); free(zmin); free(zprev); free(g); free(m1); free(m2);
+    free(res); free(resmin); free(buf);
+    free_ctx(&c);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* MCMC (utils/mcmc.m)                                                       */
+/* ------------------------------------------------------------------------ */
+int orc_mcmc_nsamples(int iteration, double burnin, int thinning) {
+    int nb = burnin < 1 ? (int)floor(iteration * burnin) : (int)burnin; /* mcmc.m:788-794 */
+    if (nb + 1 > iteration) return 0;
+    return (iteration - nb - 1) / thinning + 1; /* numel(Nburnin+1:thinning:iteration) */
+}
+
+static int nburnin(const orc_mcmc_opts* o) {
+    return o->burnin < 1 ? (int)floor(o->iteration * o->burnin) : (int)o->burnin;
+}
+
+/* find_partner (mcmc.m:797-803): uniform random derangement, one per step,
+ * shared by all voxels.  Fisher-Yates with rejection of fixed points. */
+void orc_gw_partner(uint64_t seed, int step, int rep, int W, int* p) {
+    for (uint32_t attempt = 0; attempt < 4096; ++attempt) {
+        for (int i = 0; i < W; ++i) p[i] = i;
+        uint32_t u[4];
+        for (int i = W - 1, d = 0; i >= 1; --i, ++d) {
+            if ((d & 3) == 0)
+                philox_call(seed, (uint32_t)step, attempt, (uint32_t)(d >> 2),
+                            TAG_GW_PERM | ((uint32_t)rep << 16), u);
+            int j = (int)rand_below(u[d & 3], (uint32_t)(i + 1));
+            int t = p[i]; p[i] = p[j]; p[j] = t;
+        }
+        int fixed = 0;
+        for (int i = 0; i < W; ++i) fixed |= (p[i] == i);
+        if (!fixed) return;
+    }
+    for (int i = 0; i < W; ++i) p[i] = (i + 1) % W; /* unreachable in practice */
+}
+
+/* Red-black anchor draw (mcmc.m:328-329): for half-step s, the partner of
+ * the a-th active walker is frozen[randi(numel(frozen))], shared by voxels. */
+static void rb_partner(uint64_t seed, int step, int rep, int half, int na, int nf, int* out) {
+    uint32_t u[4];
+    for (int a = 0; a < na; ++a) {
+        if ((a & 3) == 0)
+            philox_call(seed, (uint32_t)step, (uint32_t)half, (uint32_t)(a >> 2),
+                        TAG_GW_RBPART | ((uint32_t)rep << 16), u);
+        out[a] = (int)rand_below(u[a & 3], (uint32_t)nf);
+    }
+}
+
+typedef struct {
+    const orc_model* m;
+    const orc_volume* vol;
+    int nm, np, nvar;
+} mc_ctx;
+
+/* logP_Gaussian(sum w (FWD - y)^2, noise, Nm)  (utils/logP_Gaussian.m:18-20) */
+static double logp(const mc_ctx* c, int v, const double* x) {
+    double s[512];
+    double b1 = c->vol->b1 ? c->vol->b1[v] : 1.0;
+    orc_forward_voxel(c->m, x, b1, s);
+    double sos = 0.0;
+    int nv = c->vol->nvox;
+    for (int k = 0; k < c->nm; ++k) {
+        double w = c->vol->weights ? c->vol->weights[(size_t)k * nv + v] : 1.0;
+        double r = s[k] - c->vol->data[(size_t)k * nv + v];
+        sos += w * r * r;
+    }
+    double noise = x[c->nvar - 1];
+    return -sos / (2.0 * noise * noise) - c->nm / 2.0 * log(2.0 * M_PI * noise * noise);
+}
+
+int orc_mcmc(const orc_model* m, const orc_volume* vol, const double* x0,
+             const orc_mcmc_opts* o, orc_mcmc_result* r) {
+    mc_ctx c = {m, vol, orc_nmeas(m), orc_nparams(m), orc_nparams(m) + 1};
+    int nvar = c.nvar, nv = vol->nvox;
+    int W = o->algorithm == 1 ? o->nwalker : 1;
+    int nb = nburnin(o);
+    int ns = orc_mcmc_nsamples(o->iteration, o->burnin, o->thinning);
+    r->ns = ns;
+    int rep = o->repetition;
+    double nsample = (double)W * ns * rep;
+    long long acc_total = 0, prop_total = 0;
+    int* perm = NULL;
+    int* rbp = NULL;
+    int h = W / 2;
+    if (o->algorithm == 1 && o->ensemble_update == ORC_GW_SIMULTANEOUS) {
+        perm = (int*)malloc(sizeof(int) * (size_t)rep * o->iteration * W);
+        for (int rr = 0; rr < rep; ++rr)
+            for (int k = 1; k <= o->iteration; ++k)
+                orc_gw_partner(o->seed, k, rr, W, perm + ((size_t)rr * o->iteration + (k - 1)) * W);
+    }
+    if (o->algorithm == 1 && o->ensemble_update == ORC_GW_REDBLACK) {
+        rbp = (int*)malloc(sizeof(int) * (size_t)rep * o->iteration * W);
+        for (int rr = 0; rr < rep; ++rr)
+            for (int k = 1; k <= o->iteration; ++k) {
+                int* base = rbp + ((size_t)rr * o->iteration + (k - 1)) * W;
+                rb_partner(o->seed, k, rr, 0, h, W - h, base);
+                rb_partner(o->seed, k, rr, 1, W - h, h, base + h);
+            }
+    }
+
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : acc_total, prop_total) num_threads(o->nthreads > 0 ? o->nthreads : 1)
+    for (int v = 0; v < nv; ++v) {
+        double xi[64 * 8], lpi[64], x[64 * 8], xo[64 * 8], lp[64];
+        double sum[8] = {0}, sumsq[8] = {0}, shift[8];
+        /* starting points (mcmc.m:125-129, 267-275) */
+        for (int w = 0; w < W; ++w) {
+            double nrm[8];
+            if (o->algorithm == 1) {
+                for (int j = 0; j * 4 < nvar; ++j) {
+                    uint32_t u[4];
+                    philox_call(o->seed, (uint32_t)v, (uint32_t)w, (uint32_t)j, TAG_GW_INIT, u);
+                    double a, b, cc, d;
+                    box_muller(u[0], u[1], &a, &b);
+                    box_muller(u[2], u[3], &cc, &d);
+                    double q[4] = {a, b, cc, d};
+                    for (int t = 0; t < 4 && 4 * j + t < nvar; ++t) nrm[4 * j + t] = q[t];
+                }
+            }
+            for (int p = 0; p < nvar; ++p) {
+                double val = x0[(size_t)p * nv + v];
+                if (o->algorithm == 1) val += (o->ub[p] - o->lb[p]) * o->start_range * nrm[p];
+                val = fmin(fmax(val, o->lb[p]), o->ub[p]);
+                xi[w * nvar + p] = val;
+            }
+            lpi[w] = logp(&c, v, xi + w * nvar);
+        }
+        /* running sums are taken about the clamped start value */
+        for (int p = 0; p < nvar; ++p) shift[p] = fmin(fmax(x0[(size_t)p * nv + v], o->lb[p]), o->ub[p]);
+        long long acc = 0, prop = 0;
+        for (int rr = 0; rr < rep; ++rr) {
+            memcpy(x, xi, sizeof(double) * W * nvar);
+            memcpy(lp, lpi, sizeof(double) * W);
+            int counter = 0;
+            for (int k = 1; k <= o->iteration; ++k) {
+                if (o->algorithm == 0) {
+                    /* metropolis_hastings, mcmc.m:144-167 */
+                    double nrm[8], xp[8];
+                    for (int j = 0; j * 4 < nvar; ++j) {
+                        uint32_t u[4];
+                        philox_call(o->seed, (uint32_t)v, (uint32_t)k, (uint32_t)j,
+                                    TAG_MH_MOVE | ((uint32_t)rr << 16), u);
+                        double a, b, cc, d;
+                        box_muller(u[0], u[1], &a, &b);
+                        box_muller(u[2], u[3], &cc, &d);
+                        double q[4] = {a, b, cc, d};
+                        for (int t = 0; t < 4 && 4 * j + t < nvar; ++t) nrm[4 * j + t] = q[t];
+                    }
+                    uint32_t ua[4];
+                    philox_call(o->seed, (uint32_t)v, (uint32_t)k, 8u, TAG_MH_MOVE | ((uint32_t)rr << 16), ua);
+                    int oob = 0;
+                    for (int p = 0; p < nvar; ++p) {
+                        xp[p] = x[p] + o->x_step[p] * nrm[p];
+                        oob |= (xp[p] < o->lb[p]) || (xp[p] > o->ub[p]);
+                        xp[p] = fmin(fmax(xp[p], o->lb[p]), o->ub[p]);
+                    }
+                    double lpp = logp(&c, v, xp);
+                    ++prop;
+                    if (!oob && (lpp - lp[0]) > log(orc_u01(ua[0]))) {
+                        memcpy(x, xp, sizeof(double) * nvar);
+                        lp[0] = lpp;
+                        ++acc;
+                    }
+                } else if (o->ensemble_update == ORC_GW_SIMULTANEOUS) {
+                    /* goodman_weare simultaneous, mcmc.m:290-318 */
+                    const int* pt = perm + ((size_t)rr * o->iteration + (k - 1)) * W;
+                    memcpy(xo, x, sizeof(double) * W * nvar);
+                    for (int w = 0; w < W; ++w) {
+                        uint32_t u[4];
+                        philox_call(o->seed, (uint32_t)v, (uint32_t)w, (uint32_t)k,
+                                    TAG_GW_MOVE | ((uint32_t)rr << 16), u);
+                        double a = o->step_size;
+                        double t = (a - 1.0) * orc_u01(u[0]) + 1.0;
+                        double zz = t * t / a;
+                        double xp[8];
+                        int oob = 0;
+                        for (int p = 0; p < nvar; ++p) {
+                            double xq = xo[pt[w] * nvar + p];
+                            xp[p] = xq + (xo[w * nvar + p] - xq) * zz;
+                            oob |= (xp[p] < o->lb[p]) || (xp[p] > o->ub[p]);
+                            xp[p] = fmin(fmax(xp[p], o->lb[p]), o->ub[p]);
+                        }
+                        double lpp = logp(&c, v, xp);
+                        ++prop;
+                        double lr = (nvar - 1) * log(zz) + (lpp - lp[w]);
+                        if (!oob && lr > log(orc_u01(u[1]))) {
+                            memcpy(x + w * nvar, xp, sizeof(double) * nvar);
+                            lp[w] = lpp;
+                            ++acc;
+                        }
+                    }
+                } else {
+                    /* goodman_weare red-black, mcmc.m:321-357 */
+                    const int* pb = rbp + ((size_t)rr * o->iteration + (k - 1)) * W;
+                    for (int s = 0; s < 2; ++s) {
+                        int a0 = s == 0 ? 0 : h, na = s == 0 ? h : W - h;
+                        int f0 = s == 0 ? h : 0;
+                        for (int ai = 0; ai < na; ++ai) {
+                            int w = a0 + ai;
+                            int q = f0 + pb[(s == 0 ? 0 : h) + ai];
+                            uint32_t u[4];
+                            philox_call(o->seed, (uint32_t)v, (uint32_t)w, (uint32_t)k,
+                                        TAG_GW_MOVE | ((uint32_t)rr << 16) | (1u << 8), u);
+                            double a = o->step_size;
+                            double t = (a - 1.0) * orc_u01(u[0]) + 1.0;
+                            double zz = t * t / a;
+                            double xp[8];
+                            int oob = 0;
+                            for (int p = 0; p < nvar; ++p) {
+                                double xq = x[q * nvar + p];
+                                xp[p] = xq + (x[w * nvar + p] - xq) * zz;
+                                oob |= (xp[p] < o->lb[p]) || (xp[p] > o->ub[p]);
+                                xp[p] = fmin(fmax(xp[p], o->lb[p]), o->ub[p]);
+                            }
+                            double lpp = logp(&c, v, xp);
+                            ++prop;
+                            double lr = (nvar - 1) * log(zz) + (lpp - lp[w]);
+                            if (!oob && lr > log(orc_u01(u[1]))) {
+                                memcpy(xo + w * nvar, xp, sizeof(double) * nvar);
+                                lp[w] = lpp;
+                                ++acc;
+                            } else {
+                                memcpy(xo + w * nvar, x + w * nvar, sizeof(double) * nvar);
+                            }
+                        }
+                        /* the active half is written back only after the whole half-step */
+                        for (int ai = 0; ai < na; ++ai)
+                            memcpy(x + (a0 + ai) * nvar, xo + (a0 + ai) * nvar, sizeof(double) * nvar);
+                    }
+                }
+                /* burn-in / thinning (mcmc.m:172-175, 363-366) */
+                if (k > nb && (k - nb + 1) % o->thinning == 0 && counter < ns) {
+                    for (int w = 0; w < W; ++w)
+                        for (int p = 0; p < nvar; ++p) {
+                            double val = x[w * nvar + p];
+                            double d = val - shift[p];
+                            sum[p] += d;
+                            sumsq[p] += d * d;
+                            if (r->posterior) {
+                                size_t idx = (size_t)v + (size_t)nv * (w + (size_t)W * (counter + (size_t)ns * rr));
+                                r->posterior[(size_t)p * nv * W * ns * rep + idx] = (float)val;
+                            }
+                        }
+                    ++counter;
+                }
+            }
+            /* unfilled sample slots stay zero in the reference's preallocated array */
+            int missing = ns - counter;
+            for (int p = 0; p < nvar; ++p) {
+                double d = 0.0 - shift[p];
+                sum[p] += (double)missing * W * d;
+                sumsq[p] += (double)missing * W * d * d;
+            }
+        }
+        for (int p = 0; p < nvar; ++p) {
+            double mean_d = sum[p] / nsample;
+            double var = nsample > 1 ? (sumsq[p] - sum[p] * mean_d) / (nsample - 1.0) : 0.0;
+            if (r->mean) r->mean[(size_t)p * nv + v] = shift[p] + mean_d;
+            if (r->std) r->std[(size_t)p * nv + v] = sqrt(fmax(var, 0.0));
+        }
+        acc_total += acc;
+        prop_total += prop;
+    }
+    r->n_accepted = acc_total;
+    r->n_proposals = prop_total;
+    free(perm);
+    free(rbp);
+    return 0;
+}

@@ -1,0 +1,150 @@
+"""MCMC parity on the GPU (C-ABI vs FP64 oracle).
+
+Both sides draw every random number from the same Philox4x32-10 streams
+(keyed by voxel, walker, step and repetition), so the FP32 device chains and
+the FP64 oracle chains follow the same path until an acceptance test falls
+within rounding of its threshold.  Checks:
+- sample paths agree for most kept samples (random-stream layout parity);
+- posterior mean and std agree within Monte-Carlo standard error.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from gacelle_b200 import _lib
+
+from helpers import models
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="ensemble", iteration=1000, thinning=10, burnin=0.1,
+                 repetition=1, nwalker=16, step_size=2.0, start_range=0.001, update="simultaneous",
+                 x_step=None, seed=7, posterior=True, weights=None):
+    nvar, nv = x0.shape
+    y = np.ascontiguousarray(y, np.float32)
+    x0 = np.ascontiguousarray(x0, np.float32)
+    lb = np.ascontiguousarray(lb, np.float64)
+    ub = np.ascontiguousarray(ub, np.float64)
+    xs = np.ascontiguousarray(x_step if x_step is not None else np.zeros(nvar), np.float64)
+    o = _lib.GxMcmcOpts(1 if algorithm == "ensemble" else 0, iteration, thinning, burnin, repetition,
+                        nwalker, step_size, start_range, 1 if update == "redblack" else 0,
+                        xs.ctypes.data_as(_lib._dp), lb.ctypes.data_as(_lib._dp), ub.ctypes.data_as(_lib._dp),
+                        seed, 0)
+    ns = oracle.lib().orc_mcmc_nsamples(iteration, burnin, thinning)
+    W = nwalker if algorithm == "ensemble" else 1
+    vol = _lib.GxVolume()
+    vol.dims[0], vol.dims[1], vol.dims[2] = nv, 1, 1
+    vol.nvox = nv
+    vol.data = y.ctypes.data_as(_lib._fp)
+    vol.theta0 = x0.ctypes.data_as(_lib._fp)
+    if weights is not None:
+        w = np.ascontiguousarray(weights, np.float32)
+        vol.weights = w.ctypes.data_as(_lib._fp)
+    mean = np.zeros((nvar, nv), np.float32)
+    std = np.zeros((nvar, nv), np.float32)
+    post = np.zeros((nvar, repetition, ns, W, nv), np.float32) if posterior else None
+    r = _lib.GxMcmcResult()
+    r.mean = mean.ctypes.data_as(_lib._fp)
+    r.std = std.ctypes.data_as(_lib._fp)
+    if post is not None:
+        r.posterior = post.ctypes.data_as(_lib._fp)
+    _lib.check(_lib.lib().gx_mcmc(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, C.byref(vol), 1, C.byref(o), C.byref(r)))
+    return {"mean": mean, "std": std, "posterior": post, "n_accepted": r.n_accepted,
+            "n_proposals": r.n_proposals, "ns": r.ns}
+
+
+def _r2s_problem(nv, seed, sigma=0.02):
+    rng = np.random.default_rng(seed)
+    gxm, om = models("r2s")
+    th = np.vstack([rng.uniform(0.5, 1.5, nv), rng.uniform(10, 60, nv)])
+    s = oracle.forward(om, th)
+    y = (s + sigma * rng.standard_normal(s.shape)).astype(np.float32)
+    x0 = np.vstack([th, np.full(nv, sigma)]).astype(np.float32)
+    lb = [0.0, 0.1, sigma]
+    ub = [2.0, 200.0, sigma]
+    return gxm, om, y, x0, lb, ub
+
+
+def _mcse(post, k):
+    """Batch-means Monte-Carlo standard error of the posterior mean per voxel:
+    the ensemble mean per kept step forms the chain, split into sqrt(L) batches."""
+    x = post[k].astype(np.float64).mean(axis=2)          # [rep, ns, nv]
+    x = x.reshape(-1, x.shape[-1])
+    L = x.shape[0]
+    B = max(int(np.sqrt(L)), 2)
+    b = L // B
+    bm = x[:B * b].reshape(B, b, -1).mean(axis=1)
+    return bm.std(axis=0, ddof=1) / np.sqrt(B)
+
+
+def _moments_agree(eng, orc, nparam, zmed=1.5, frac=0.95):
+    for k in range(nparam):
+        se = np.sqrt(_mcse(eng["posterior"], k) ** 2 + _mcse(orc["posterior"], k) ** 2) + 1e-12
+        z = np.abs(eng["mean"][k] - orc["mean"][k]) / se
+        assert np.median(z) < zmed and np.mean(z < 3.5) >= frac, (k, float(np.median(z)), float(np.mean(z < 3.5)))
+        rel = np.abs(eng["std"][k] / np.maximum(orc["std"][k], 1e-12) - 1)
+        assert np.median(rel) < 0.15, (k, float(np.median(rel)))
+
+
+@pytest.mark.parametrize("algorithm,update", [("ensemble", "simultaneous"), ("ensemble", "redblack"),
+                                              ("mh", "simultaneous")])
+def test_random_streams_match_oracle(ctx, algorithm, update):
+    """Same Philox streams: over the first steps the device and oracle chains
+    take the same moves (walker starts, stretch factors, partners, accepts)."""
+    gxm, om, y, x0, lb, ub = _r2s_problem(128, 10)
+    kw = dict(iteration=12, thinning=1, burnin=0.0, nwalker=16, seed=4, algorithm=algorithm)
+    xs = [0.01, 1.0, 0.0]
+    eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, update=update, x_step=xs, **kw)
+    orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
+                      ensemble_update=update, x_step=np.array(xs), want_posterior=True, **kw)
+    assert eng["ns"] == orc["ns"] == 12
+    pe, po = eng["posterior"][:2], orc["posterior"][:2]
+    same = np.abs(pe - po) <= 1e-4 * np.abs(po) + 1e-7
+    assert same.mean() > 0.97, same.mean()
+    assert abs(eng["n_accepted"] - orc["n_accepted"]) <= 0.01 * orc["n_proposals"]
+
+
+@pytest.mark.parametrize("update", ["simultaneous", "redblack"])
+def test_gw_matches_oracle(ctx, update):
+    gxm, om, y, x0, lb, ub = _r2s_problem(64, 11)
+    kw = dict(iteration=1500, thinning=5, burnin=0.3, nwalker=16, seed=99)
+    eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, update=update, **kw)
+    orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
+                      algorithm="ensemble", ensemble_update=update, want_posterior=True, **kw)
+    assert eng["ns"] == orc["ns"]
+    assert eng["n_proposals"] == orc["n_proposals"]
+    _moments_agree(eng, orc, 2)
+    acc_e = eng["n_accepted"] / eng["n_proposals"]
+    acc_o = orc["n_accepted"] / orc["n_proposals"]
+    assert abs(acc_e - acc_o) < 0.02
+
+
+def test_mh_matches_oracle(ctx):
+    gxm, om, y, x0, lb, ub = _r2s_problem(256, 12)
+    xs = [0.01, 1.0, 0.0]
+    kw = dict(iteration=4000, thinning=4, burnin=0.25, seed=5)
+    eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="mh", x_step=xs, **kw)
+    orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub, algorithm="mh",
+                      x_step=np.array(xs), want_posterior=True, **kw)
+    _moments_agree(eng, orc, 2)
+
+
+def test_gw_nexi_moments(ctx):
+    rng = np.random.default_rng(13)
+    gxm, om = models("nexi")
+    nv = 32
+    th = np.vstack([rng.uniform(0.3, 0.7, nv), rng.uniform(1.5, 2.5, nv), rng.uniform(0.7, 1.2, nv),
+                    rng.uniform(0.02, 0.1, nv)])
+    s = oracle.forward(om, th)
+    y = (s + 0.02 * rng.standard_normal(s.shape)).astype(np.float32)
+    x0 = np.vstack([th, np.full(nv, 0.02)]).astype(np.float32)
+    lb = [2.2e-16, 2.2e-16, 2.2e-16, 1 / 250, 0.02]
+    ub = [1.0, 3.0, 3.0, 1.0, 0.02]
+    kw = dict(iteration=800, thinning=4, burnin=0.25, nwalker=32, seed=3)
+    eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, **kw)
+    orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub, want_posterior=True,
+                      **kw)
+    _moments_agree(eng, orc, 4)
