@@ -40,6 +40,9 @@ def parse_args():
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--no-extra", action="store_true", help="skip the plain-path and MCMC side measurements")
     p.add_argument("--cpu-iters", type=int, default=40, help="iterations of the bounded CPU sample")
+    p.add_argument("--iters", type=int, default=NITER, help="askAdam iterations per fit (profiling runs)")
+    p.add_argument("--grid", default="128x128x64", help="phantom grid (profiling runs)")
+    p.add_argument("--mcmc-steps", type=int, default=200, help="GW steps of the MCMC side measurement")
     return p.parse_args()
 
 
@@ -58,15 +61,16 @@ def dist_setup(args):
     return world, rank, local
 
 
-def workload(seed=1002):
+def workload(seed=1002, grid="128x128x64", iters=NITER):
     from gacelle_b200 import phantoms, utils
-    mask = phantoms.ellipsoid_mask((128, 128, 64), 1.05)
+    dims = tuple(int(x) for x in grid.split("x"))
+    mask = phantoms.ellipsoid_mask(dims, 1.05)
     data, _ = phantoms.r2s_phantom(mask, seed)
     idx = utils.mask_index(mask)
     y = utils.reshape_ND2GD(data, idx)
     n = y.shape[1]
     th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, n))
-    fitting = {"iteration": NITER, "initialLearnRate": 0.01, "decayRate": 0.0, "lossFunction": "mse",
+    fitting = {"iteration": iters, "initialLearnRate": 0.01, "decayRate": 0.0, "lossFunction": "mse",
                "tol": 0.0, "convergenceValue": 1e-6, "patienceConvergence": float("inf"),
                "convergenceStepTol": 0.0, "convergenceGradTol": 0.0, "lambda": [1e-3], "regmap": ["R2star"],
                "TVmode": "3D", "voxelSize": [2, 2, 2], "parameterTransform": "sigmoid"}
@@ -217,7 +221,7 @@ def engine_arm(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    W = workload(seed=1002 + rank)
+    W = workload(seed=1002 + rank, grid=args.grid, iters=args.iters)
     ctx = gacelle_b200.Context(local)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
@@ -232,7 +236,7 @@ def engine_arm(args, world, rank, local):
     d_idx = torch.from_numpy(W["idx"]).to(dev)
     d_th0 = torch.from_numpy(W["th0"]).to(dev)
     d_out = [torch.empty((2, n), dtype=torch.float32, device=dev) for _ in range(2)]
-    hist = np.zeros(NITER + 1)
+    hist = np.zeros(args.iters + 1)
 
     def make_vol(y, idx, th0):
         v = _lib.GxVolume()
@@ -273,7 +277,7 @@ def engine_arm(args, world, rank, local):
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(args.warmup):
         step_device()
     torch.cuda.synchronize()
     barrier(world)
@@ -301,10 +305,10 @@ def engine_arm(args, world, rank, local):
     ms_total = sum(s.elapsed_time(e) for s, e in times)
     ms_total = max_over_ranks(ms_total, world)
     ms_step = ms_total / args.steps
-    value = world * n * args.steps / (ms_total / 1000.0)
+    value = world * n * args.steps / (ms_total / 1000.0) * (args.iters / NITER)
 
     # end to end through the C-ABI with pinned host buffers
-    for _ in range(2):
+    for _ in range(min(args.warmup, 2)):
         step_host()
     torch.cuda.synchronize()
     barrier(world)
@@ -321,7 +325,7 @@ def engine_arm(args, world, rank, local):
         t = ctx.timing()
         h2d, d2h = t["h2d_bytes"], t["d2h_bytes"]
     e2e_ms = max_over_ranks(e2e_ms, world)
-    e2e_value = world * n * args.steps / (e2e_ms / 1000.0)
+    e2e_value = world * n * args.steps / (e2e_ms / 1000.0) * (args.iters / NITER)
 
     # parity spot check of the measured fit against the oracle on a voxel subset is done in tests;
     # here only sanity: parameters finite and inside bounds
@@ -352,14 +356,17 @@ def engine_arm(args, world, rank, local):
                                 "sample": f"{n}-voxel volume, {args.cpu_iters} of {NITER} iterations "
                                           f"({dt:.1f} s on {cores} threads), extrapolated"}
         if not args.no_extra:
-            line["extra"] = extras(ctx, W, opts, model, stream)
+            line["extra"] = extras(ctx, W, opts, model, stream, args)
         print(json.dumps(line), flush=True)
 
 
-def extras(ctx, W, opts, model, stream):
-    """Plain (op-by-op) path on the same volume and GW MCMC throughput."""
-    import torch
-    from gacelle_b200 import _lib, askadam_solver as gxa
+def extras(ctx, W, opts, model, stream, args):
+    """Side measurements: the plain (op-by-op) path on the same volume, and
+    Goodman-Weare MCMC on the NEXI model (200k voxels x 64 walkers, 24 shells,
+    14-node powder average, sigma fixed at 0.02) over a bounded number of steps."""
+    from gacelle_b200 import askadam_solver as gxa
+    from gacelle_b200 import mcmc_solver, phantoms
+    from gacelle_b200.models import gpuNEXI
     out = {}
     f = gxa.check_set_default_basic(dict(W["fitting"], iteration=200))
     n = W["nvox"]
@@ -370,6 +377,30 @@ def extras(ctx, W, opts, model, stream):
     plain_ms_iter = t["main_kernel_ms"] / 200.0
     out["plain_voxel_fits_per_s"] = n / (plain_ms_iter * NITER / 1000.0)
     out["plain_ms_per_iteration"] = plain_ms_iter
+    # MCMC
+    nv, steps = 200_000, args.mcmc_steps
+    y, gt = phantoms.nexi_volume(nv, 1005, sigma=0.02, rician=False, nx=14)
+    b, d = phantoms.nexi_shells()
+    m = gpuNEXI(b, d, nx=14)
+    m.updateProperty({"solver": "mcmc", "lmax": 0})
+    x0 = np.vstack([gt["fa"], gt["Da"], gt["De"], gt["ra"], np.full(nv, 0.02)]).astype(np.float32)
+    fit = mcmc_solver.check_set_default_basic({"algorithm": "ensemble", "iteration": steps, "burnin": 0.2,
+                                               "thinning": 10, "Nwalker": 64, "StepSize": 2,
+                                               "modelParams": m.modelParams,
+                                               "lb": list(m.lb[:4]) + [0.02], "ub": list(m.ub[:4]) + [0.02],
+                                               "returnPosterior": False})
+    mc = mcmc_solver.mcmc(ctx)
+    mask = np.ones((1, nv), bool)
+    mc.optimisation(y, mask, None, {p: x0[k] for k, p in enumerate(m.modelParams)}, fit, m)
+    t = mc.last_timing
+    st = mc.last_stats
+    sec = t["main_kernel_ms"] / 1000.0
+    out["mcmc_workload"] = (f"GW NEXI, {nv} voxels x 64 walkers, 24 shells, Nx 14, {steps} steps "
+                            f"(of the 5000-step run), simultaneous update")
+    out["mcmc_proposals_per_s"] = st["n_proposals"] / sec
+    out["mcmc_accepted_samples_per_s"] = st["n_accepted"] / sec
+    out["mcmc_acceptance"] = st["n_accepted"] / st["n_proposals"]
+    out["mcmc_ms_per_step"] = t["main_kernel_ms"] / steps
     return out
 
 

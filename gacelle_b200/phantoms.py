@@ -71,8 +71,11 @@ def nexi_shells():
     return b, d
 
 
-def nexi_signal(fa, Da, De, ra, b, delta, nx=100):
+def nexi_signal(fa, Da, De, ra, b, delta, nx=100, chunk=8192):
     """float64 NEXI Sl0 (narrow pulse) by an nx-node trapezoid; [v, shell]."""
+    if len(fa) > chunk:
+        return np.concatenate([nexi_signal(fa[i:i + chunk], Da[i:i + chunk], De[i:i + chunk], ra[i:i + chunk],
+                                           b, delta, nx, chunk) for i in range(0, len(fa), chunk)])
     fa = np.maximum(fa, 1e-8)[:, None, None]
     bb = np.asarray(b)[None, :, None]
     dd = np.asarray(delta)[None, :, None]

@@ -5,7 +5,8 @@ Both sides draw every random number from the same Philox4x32-10 streams
 the FP64 oracle chains follow the same path until an acceptance test falls
 within rounding of its threshold.  Checks:
 - sample paths agree for most kept samples (random-stream layout parity);
-- posterior mean and std agree within Monte-Carlo standard error.
+- posterior mean and std differ from the oracle's by no more than two oracle
+  runs with different seeds differ from each other (Monte-Carlo error).
 """
 import ctypes as C
 
@@ -68,25 +69,18 @@ def _r2s_problem(nv, seed, sigma=0.02):
     return gxm, om, y, x0, lb, ub
 
 
-def _mcse(post, k):
-    """Batch-means Monte-Carlo standard error of the posterior mean per voxel:
-    the ensemble mean per kept step forms the chain, split into sqrt(L) batches."""
-    x = post[k].astype(np.float64).mean(axis=2)          # [rep, ns, nv]
-    x = x.reshape(-1, x.shape[-1])
-    L = x.shape[0]
-    B = max(int(np.sqrt(L)), 2)
-    b = L // B
-    bm = x[:B * b].reshape(B, b, -1).mean(axis=1)
-    return bm.std(axis=0, ddof=1) / np.sqrt(B)
-
-
-def _moments_agree(eng, orc, nparam, zmed=1.5, frac=0.95):
+def _moments_agree(eng, orc, orc_b, nparam):
+    """Engine-vs-oracle differences of the posterior mean and std, per voxel,
+    must not exceed the Monte-Carlo spread between two oracle runs that differ
+    only in seed (the engine shares the first oracle's random streams, so its
+    differences come from FP32 rounding and are normally far smaller)."""
     for k in range(nparam):
-        se = np.sqrt(_mcse(eng["posterior"], k) ** 2 + _mcse(orc["posterior"], k) ** 2) + 1e-12
-        z = np.abs(eng["mean"][k] - orc["mean"][k]) / se
-        assert np.median(z) < zmed and np.mean(z < 3.5) >= frac, (k, float(np.median(z)), float(np.mean(z < 3.5)))
-        rel = np.abs(eng["std"][k] / np.maximum(orc["std"][k], 1e-12) - 1)
-        assert np.median(rel) < 0.15, (k, float(np.median(rel)))
+        d_mean = np.abs(eng["mean"][k] - orc["mean"][k])
+        r_mean = np.abs(orc_b["mean"][k] - orc["mean"][k])
+        assert np.median(d_mean) <= 1.2 * np.median(r_mean) + 1e-12, (k, np.median(d_mean), np.median(r_mean))
+        d_std = np.abs(eng["std"][k] - orc["std"][k])
+        r_std = np.abs(orc_b["std"][k] - orc["std"][k])
+        assert np.median(d_std) <= 1.2 * np.median(r_std) + 1e-12, (k, np.median(d_std), np.median(r_std))
 
 
 @pytest.mark.parametrize("algorithm,update", [("ensemble", "simultaneous"), ("ensemble", "redblack"),
@@ -114,9 +108,11 @@ def test_gw_matches_oracle(ctx, update):
     eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, update=update, **kw)
     orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
                       algorithm="ensemble", ensemble_update=update, want_posterior=True, **kw)
+    orc_b = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
+                        algorithm="ensemble", ensemble_update=update, **dict(kw, seed=kw["seed"] + 1))
     assert eng["ns"] == orc["ns"]
     assert eng["n_proposals"] == orc["n_proposals"]
-    _moments_agree(eng, orc, 2)
+    _moments_agree(eng, orc, orc_b, 2)
     acc_e = eng["n_accepted"] / eng["n_proposals"]
     acc_o = orc["n_accepted"] / orc["n_proposals"]
     assert abs(acc_e - acc_o) < 0.02
@@ -129,7 +125,9 @@ def test_mh_matches_oracle(ctx):
     eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="mh", x_step=xs, **kw)
     orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub, algorithm="mh",
                       x_step=np.array(xs), want_posterior=True, **kw)
-    _moments_agree(eng, orc, 2)
+    orc_b = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub, algorithm="mh",
+                        x_step=np.array(xs), **dict(kw, seed=kw["seed"] + 1))
+    _moments_agree(eng, orc, orc_b, 2)
 
 
 def test_gw_nexi_moments(ctx):
@@ -147,4 +145,6 @@ def test_gw_nexi_moments(ctx):
     eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, **kw)
     orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub, want_posterior=True,
                       **kw)
-    _moments_agree(eng, orc, 4)
+    orc_b = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
+                        **dict(kw, seed=kw["seed"] + 1))
+    _moments_agree(eng, orc, orc_b, 4)
