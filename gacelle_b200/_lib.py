@@ -121,6 +121,8 @@ SIGNATURES = {
                              C.c_int32, C.POINTER(GxAskadamOpts), C.POINTER(GxAskadamResult)]),
     "gx_mcmc": (C.c_int, [C.c_void_p, C.POINTER(GxModel), C.c_int32, C.POINTER(GxVolume),
                           C.c_int32, C.POINTER(GxMcmcOpts), C.POINTER(GxMcmcResult)]),
+    "gx_askadam_noalloc": (C.c_int, [C.POINTER(GxModel), C.c_void_p, C.c_void_p, C.c_int32,
+                                     C.POINTER(GxAskadamOpts), C.c_void_p, C.c_void_p, _dp]),
 }
 
 _lib = None

@@ -1188,3 +1188,20 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     c->timing.d2h_bytes = d2h;
     return GX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Helpers for other translation units of the library (no new behaviour).
+// ---------------------------------------------------------------------------
+namespace gx {
+gx_status internal_fail(gx_status s, const char* msg) { return fail(s, "%s", msg); }
+
+gx_status internal_model(const gx_model* m, const double* lb, const double* ub, DevProtocol* P,
+                         int* np, int* nm, int* id) {
+    gx_status st = model_sizes(m, np, nm, id);
+    if (st != GX_OK) return st;
+    *P = make_protocol(m, *id, *np, *nm, lb, ub, *np);
+    return GX_OK;
+}
+
+bool internal_can_stop(const gx_askadam_opts* o) { return can_stop(o); }
+}  // namespace gx

@@ -134,3 +134,13 @@ cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, 
 extern long long g_kernel_launches;  // launches of this library's kernels (process-wide)
 
 }  // namespace gx
+
+// Helpers defined in capi.cu for the other translation units.
+#include "../../include/gacelle_b200.h"
+namespace gx {
+gx_status internal_fail(gx_status s, const char* msg);
+gx_status internal_model(const gx_model* m, const double* lb, const double* ub, DevProtocol* P,
+                         int* np, int* nm, int* id);
+bool internal_can_stop(const gx_askadam_opts* o);
+
+}  // namespace gx

@@ -233,6 +233,24 @@ gx_status gx_askadam(gx_context* ctx, const gx_model* model, int32_t mem, const 
 gx_status gx_mcmc(gx_context* ctx, const gx_model* model, int32_t mem, const gx_volume* vols,
                   int32_t nvol, const gx_mcmc_opts* opts, gx_mcmc_result* results);
 
+/* No counterpart in the reference.  The fused askAdam fit of one volume
+ * (final parameters only, every iteration run, no TV) for callers that cannot
+ * allocate device memory while they run: applications whose framework owns
+ * all device memory through its own allocator, or pipelines that reserve
+ * their memory up front and must not allocate or hit out-of-memory later.
+ * data [nmeas][nvox], theta0 [nparam][nvox] and theta_out [nparam][nvox] are
+ * device pointers of the current device; the work is queued on cuda_stream
+ * (NULL: the default stream) and finished at return; final_loss (host,
+ * nullable) receives the last epoch's loss.  Working memory is a fixed 32 MiB
+ * device array inside the library (held by every GPU that loads it until the
+ * process exits); problems that do not fit are rejected with GX_EINVAL and the
+ * maximum voxel count in gx_last_error().  The first call on a device looks up
+ * that array's device address.  Calls share the array, so calls whose GPU
+ * work overlaps race; stopping criteria must be disabled (GX_EUNSUPPORTED). */
+gx_status gx_askadam_noalloc(const gx_model* model, const float* data, const float* theta0,
+                             int32_t nvox, const gx_askadam_opts* opts, void* cuda_stream,
+                             float* theta_out, double* final_loss);
+
 #ifdef __cplusplus
 }
 #endif
