@@ -53,19 +53,13 @@ __device__ __forceinline__ void block_accumulate(const float (&q)[NQ], double* d
     }
 }
 
+__device__ __forceinline__ OptConst opt_const(const AdamParams& a) {
+    return OptConst{a.optimiser, a.beta1, a.beta2, a.eps, a.momentum, a.rms_decay, a.rms_eps};
+}
+
 __device__ __forceinline__ void opt_update(const AdamParams& a, float2 sc, float& z, float& m1,
                                            float& m2, float g) {
-    if (a.optimiser == kAdam) {  // adamupdate: bias-corrected moments
-        m1 = a.beta1 * m1 + (1.0f - a.beta1) * g;
-        m2 = a.beta2 * m2 + (1.0f - a.beta2) * g * g;
-        z -= sc.x * m1 / (sqrtf(m2 * sc.y) + a.eps);
-    } else if (a.optimiser == kSGDM) {  // sgdmupdate
-        m1 = a.momentum * m1 - sc.x * g;
-        z += m1;
-    } else {  // rmspropupdate
-        m2 = a.rms_decay * m2 + (1.0f - a.rms_decay) * g * g;
-        z -= sc.x * g / (sqrtf(m2) + a.rms_eps);
-    }
+    opt_step(opt_const(a), sc, z, m1, m2, g);
 }
 
 __device__ __forceinline__ float voxel_sigma(const AdamParams& a, int v) {
@@ -130,6 +124,8 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
     float* s_w = s_y + nm * B;
     float* s_sa = a.weights ? s_w + nm * B : s_w;
     float* s_ca = s_sa + a.P.n_fa * B;
+    __shared__ DevProtocol s_P;
+    stage_protocol(a.P, &s_P);
     for (int m = 0; m < nm; ++m) s_y[m * B + tid] = a.data[(size_t)m * a.nvtot + v];
     if (a.weights)
         for (int m = 0; m < nm; ++m) s_w[m * B + tid] = a.weights[(size_t)m * a.nvtot + v];
@@ -138,6 +134,7 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
         for (int f = 0; f < a.P.n_fa; ++f) sincosf(b1 * a.P.fa_rad[f], &s_sa[f * B + tid], &s_ca[f * B + tid]);
     VoxAux va{b1, s_sa + tid, s_ca + tid, B};
     LossAux aux = make_loss_aux(voxel_sigma(a, v));
+    __syncthreads();
 
     float z[NP], m1[NP], m2[NP], zp[NP];
 #pragma unroll
@@ -165,7 +162,7 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
         acc.aux = aux; acc.mse_scale = a.mse_scale; acc.hd = a.huber_delta;
         acc.res = (a.res_out && e == e_end && valid) ? a.res_out + v : nullptr;
         acc.rs = a.nvtot;
-        model_eval<MODEL>(a.P, th, va, acc);
+        model_eval<MODEL>(s_P, th, va, acc);
         float gz[NP];
 #pragma unroll
         for (int k = 0; k < NP; ++k) gz[k] = acc.g[k] * normf * dth[k];
@@ -233,6 +230,9 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
     constexpr int NP = ModelNP<MODEL>::value;
     constexpr int NQ = STATS ? kHistW : 2;
     __shared__ double s_red[2 * 32 * NQ];
+    __shared__ DevProtocol s_P;
+    stage_protocol(a.P, &s_P);
+    __syncthreads();
     const int B = blockDim.x, tid = threadIdx.x;
     const int v = blockIdx.x * B + tid;
     const int vol = a.blk_vol[blockIdx.x];
@@ -265,7 +265,7 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
     acc.mse_scale = a.mse_scale; acc.hd = a.huber_delta;
     acc.res = (want_res && a.res_out && valid) ? a.res_out + v : nullptr;
     acc.rs = a.nvtot;
-    model_eval<MODEL>(a.P, th, va, acc);
+    model_eval<MODEL>(s_P, th, va, acc);
     float gth[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) gth[k] = acc.g[k] * V.norm;
@@ -282,6 +282,7 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
         int bw[3] = {x > 0 ? p - sx : p + (dx - 1) * sx, y > 0 ? p - sy : p + (dy - 1) * sy,
                      zc > 0 ? p - sz : p + (dz - 1) * sz};
         const unsigned char* mk = a.maskgrid + V.grid_off;
+        bool mb[3] = {mk[bw[0]] != 0, mk[bw[1]] != 0, mk[bw[2]] != 0};
         for (int r = 0; r < a.n_reg; ++r) {
             const int k = a.reg_param[r];
             const float* G = a.grid_cur + (size_t)r * a.grid_total + V.grid_off;
@@ -289,16 +290,17 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
 #pragma unroll
             for (int kk = 0; kk < NP; ++kk)
                 if (kk == k) c = th[kk];
-            float cost = 0.0f, gr = 0.0f;
+            float f[3], b[3];
             for (int d = 0; d < nd; ++d) {
-                float f = G[fw[d]], bk = G[bw[d]];
-                cost += fabsf((f - c) * a.inv_vs[d]);
-                gr += (-sgnf(f - c) + (mk[bw[d]] ? sgnf(c - bk) : 0.0f)) * a.inv_vs[d];
+                f[d] = G[fw[d]];
+                b[d] = G[bw[d]];
             }
+            float cost, gr;
+            tv_terms(c, f, b, mb, a.inv_vs, nd, cost, gr);
             reg += V.tv_scale[r] * cost;
 #pragma unroll
             for (int kk = 0; kk < NP; ++kk)
-                if (kk == k) gth[kk] += V.tv_scale[r] * gr;
+                if (kk == k) gth[kk] = __fmaf_rn(V.tv_scale[r], gr, gth[kk]);
         }
     }
     float gz[NP];
@@ -529,17 +531,20 @@ __global__ void plain_tv_kernel(AdamParams a, PlainBufs b, const float* grid) {
         int bw[3] = {x > 0 ? p - 1 : p + (dx - 1), y > 0 ? p - sy : p + (dy - 1) * sy,
                      zc > 0 ? p - sz : p + (dz - 1) * sz};
         const unsigned char* mk = a.maskgrid + V.grid_off;
+        bool mb[3] = {mk[bw[0]] != 0, mk[bw[1]] != 0, mk[bw[2]] != 0};
         for (int r = 0; r < a.n_reg; ++r) {
             const float* G = grid + (size_t)r * a.grid_total + V.grid_off;
             float c = G[p];
-            float cost = 0.0f, gr = 0.0f;
+            float fv[3], bv[3];
             for (int d = 0; d < nd; ++d) {
-                float f = G[fw[d]], bk = G[bw[d]];
-                cost += fabsf((f - c) * a.inv_vs[d]);
-                gr += (-sgnf(f - c) + (mk[bw[d]] ? sgnf(c - bk) : 0.0f)) * a.inv_vs[d];
+                fv[d] = G[fw[d]];
+                bv[d] = G[bw[d]];
             }
+            float cost, gr;
+            tv_terms(c, fv, bv, mb, a.inv_vs, nd, cost, gr);
             reg += V.tv_scale[r] * cost;
-            b.gth[(size_t)a.reg_param[r] * a.nvtot + v] += V.tv_scale[r] * gr;
+            float* gk = b.gth + (size_t)a.reg_param[r] * a.nvtot + v;
+            *gk = __fmaf_rn(V.tv_scale[r], gr, *gk);
         }
     }
     float q[1] = {reg};

@@ -1,0 +1,405 @@
+// askadam_persistent.cu -- askAdam with spatial TV as one persistent,
+// cooperative launch over a range of epochs (R2* model).
+//
+// Each CTA owns a contiguous slice of the voxel work-list for the whole
+// launch: the slice's measurements are staged once in shared memory, each
+// thread keeps the parameters and Adam moments of VPT voxels in registers,
+// and only the regularised parameter map travels between epochs (the
+// double-buffered full-grid TV map, read through L2 with ld.global.cg since
+// other CTAs wrote it in the same launch).  Epochs are separated by a grid
+// barrier whose wait is bounded: if it expires the kernel raises an error flag
+// that the host reports as GX_ETIMEOUT, and every CTA returns.
+//
+// The per-voxel arithmetic (forward model, loss, adjoint, TV subgradient,
+// sigmoid chain rule, optimiser) is the same code as tv_step_kernel, so the
+// two paths produce the same parameters.  Reference: utils/askadam.m:23-117,
+// 673-691; utils/spatial_total_variation.m:24-66.
+#include "gx_internal.h"
+
+namespace gx {
+
+namespace {
+
+__device__ __forceinline__ float sgnp(float x) { return (float)((x > 0.0f) - (x < 0.0f)); }
+
+__device__ __forceinline__ float warp_sum_p(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Loss with the kind chosen at run time (uniform across the launch).
+struct RtLoss {
+    int kind;
+    __device__ __forceinline__ float operator()(float s, float y, float w, const LossAux& a, float ms, float hd,
+                                                float& d) const {
+        switch (kind) {
+        case kL1: return loss_elem<kL1>(s, y, w, a, ms, hd, d);
+        case kL2: return loss_elem<kL2>(s, y, w, a, ms, hd, d);
+        case kHuber: return loss_elem<kHuber>(s, y, w, a, ms, hd, d);
+        case kMSE: return loss_elem<kMSE>(s, y, w, a, ms, hd, d);
+        case kGauss: return loss_elem<kGauss>(s, y, w, a, ms, hd, d);
+        default: return loss_elem<kRician>(s, y, w, a, ms, hd, d);
+        }
+    }
+};
+
+// LossAcc equivalent whose loss kind is either fixed (LOSS >= 0) or run-time.
+template <int LOSS, int NP>
+struct PLossAcc {
+    float total;
+    float g[NP];
+    const float* y;
+    int ys;
+    const float* w;
+    int ws;
+    LossAux aux;
+    float mse_scale, hd;
+    float* res;
+    int rs;
+    RtLoss rt;
+    __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
+        bool bad = !isfinite(S);
+        float s = bad ? 0.0f : S;
+        float ww = w ? w[m * ws] : 1.0f;
+        float d;
+        float l;
+        if constexpr (LOSS >= 0) l = loss_elem<LOSS>(s, y[m * ys], ww, aux, mse_scale, hd, d);
+        else l = rt(s, y[m * ys], ww, aux, mse_scale, hd, d);
+        total += l;
+        if (res) res[m * rs] = l;
+        if (!bad) {
+#pragma unroll
+            for (int k = 0; k < NP; ++k) g[k] += d * dS[k];
+        }
+    }
+};
+
+// Grid-wide barrier for a cooperative launch, with a bounded wait.
+// Returns false (on every thread of the CTA) once any CTA has timed out.
+__device__ __forceinline__ bool grid_barrier(PersistBarrier* gb, unsigned int nblocks, unsigned int& gen) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int g = gen;
+        __threadfence();
+        unsigned int arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == nblocks - 1) {
+            gb->count = 0u;
+            __threadfence();
+            atomicExch(&gb->gen, g + 1u);
+        } else {
+            const long long t0 = clock64();
+            while (atomicAdd(&gb->gen, 0u) == g) {
+                if (*(volatile int*)&gb->error) break;
+                if (clock64() - t0 > kBarrierSpinCycles) {
+                    atomicExch(&gb->error, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = *(volatile int*)&gb->error == 0;
+        gen = g + 1u;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+}  // namespace
+
+template <int LOSS, bool STATS>
+__global__ void __launch_bounds__(kPersistMaxThreads, 1)
+tv_persistent_kernel(AdamParams a, PersistArgs p) {
+    constexpr int NP = 2;  // R2*: M0, R2star
+    constexpr int NS = STATS ? 4 : 3;  // z, m1, m2 [, z of the previous epoch]
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* s_red = reinterpret_cast<double*>(smem_raw);                     // [2][32][kHistW]
+    float* s_st = reinterpret_cast<float*>(s_red + 2 * 32 * kHistW);         // [NS][NP][slice]
+    int* s_p = reinterpret_cast<int*>(s_st + (size_t)NS * NP * p.slice);     // [slice] grid index
+    unsigned short* s_fl = reinterpret_cast<unsigned short*>(s_p + p.slice); // [slice] boundary/mask flags
+    float* s_y = reinterpret_cast<float*>(s_fl + ((p.slice + 1) & ~1));       // [nm][slice] if staged
+    const int BT = blockDim.x, tid = threadIdx.x;
+    const int base = blockIdx.x * p.slice;
+    const int n = min(base + p.slice, a.nvtot) - base;  // voxels of this slice
+    const int S = p.slice;
+    const DevVol& Vg = a.vols[a.blk_vol[base / p.pad_block]];  // a slice lies in one volume
+    struct {
+        int off, nvox;
+        float norm;
+        double normd;
+        long long grid_off;
+    } V{Vg.off, Vg.nvox, Vg.norm, Vg.normd, Vg.grid_off};
+    const float tvs0 = Vg.tv_scale[0], tvs1 = Vg.tv_scale[1];
+    const int dx = Vg.dims[0], dy = Vg.dims[1], dz = Vg.dims[2];
+    const int sy = dx, sz = dx * dy;
+    const int wx = dx - 1, wy = (dy - 1) * dx, wz = (dz - 1) * dx * dy;  // wrap offsets
+    const unsigned char* mk = a.maskgrid + V.grid_off;
+    // stage the slice's state, TV neighbourhood (and measurements, if they fit) once
+    for (int i = tid; i < n; i += BT) {
+        const int v = base + i;
+        int pp = 0;
+        unsigned short fl = 0;
+        if ((v - V.off) < V.nvox && a.n_reg > 0) {
+            pp = a.gidx[v];
+            const int x = pp % dx, yz = pp / dx, y = yz % dy, zc = yz / dy;
+            fl = (unsigned short)((x == dx - 1) | ((y == dy - 1) << 1) | ((zc == dz - 1) << 2) |
+                                  ((x == 0) << 3) | ((y == 0) << 4) | ((zc == 0) << 5));
+            const int bw0 = x > 0 ? pp - 1 : pp + wx;
+            const int bw1 = y > 0 ? pp - sy : pp + wy;
+            const int bw2 = zc > 0 ? pp - sz : pp + wz;
+            fl |= (unsigned short)((mk[bw0] ? 64 : 0) | (mk[bw1] ? 128 : 0) | (mk[bw2] ? 256 : 0));
+        }
+        s_p[i] = pp;
+        s_fl[i] = fl;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            size_t gi = (size_t)k * a.nvtot + base + i;
+            s_st[(0 * NP + k) * S + i] = a.z[gi];
+            s_st[(1 * NP + k) * S + i] = a.m1[gi];
+            s_st[(2 * NP + k) * S + i] = a.m2[gi];
+            if constexpr (STATS) s_st[(3 * NP + k) * S + i] = a.zprev ? a.zprev[gi] : 0.0f;
+        }
+        if (p.data_in_smem)
+            for (int m = 0; m < a.nm; ++m) s_y[m * S + i] = a.data[(size_t)m * a.nvtot + base + i];
+    }
+    __shared__ DevProtocol s_P;
+    stage_protocol(a.P, &s_P);
+    unsigned int gen = 0;
+    if (tid == 0) gen = atomicAdd(&p.barrier->gen, 0u);
+    __syncthreads();
+    const bool tv3 = a.tv_3d != 0;
+    const OptConst oc{a.optimiser, a.beta1, a.beta2, a.eps, a.momentum, a.rms_decay, a.rms_eps};
+    const float ivx = a.inv_vs[0], ivy = a.inv_vs[1], ivz = a.inv_vs[2];
+
+    for (int e = p.e_begin; e <= p.e_end; ++e) {
+        const float* gcur = (e >= 1 && ((e - 1) & 1)) ? p.grid1 : p.grid0;  // epoch 0 reads the start map
+        float* gnext = e & 1 ? p.grid1 : p.grid0;
+        float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f;
+        const bool upd = e <= p.update_last;
+        const float2 sc = upd ? a.sched[e] : float2{0.f, 0.f};
+        for (int i = tid; i < n; i += BT) {
+            const int v = base + i;
+            const bool ok = (v - V.off) < V.nvox;
+            float z[NP], th[NP], dth[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                z[k] = s_st[(0 * NP + k) * S + i];
+                th[k] = unscale(a.transform, a.P.lb[k], a.P.ub[k], z[k], dth[k]);
+            }
+            PLossAcc<LOSS, NP> acc;
+            acc.total = 0.0f;
+#pragma unroll
+            for (int k = 0; k < NP; ++k) acc.g[k] = 0.0f;
+            if (p.data_in_smem) {
+                acc.y = s_y + i;
+                acc.ys = S;
+            } else {
+                acc.y = a.data + v;
+                acc.ys = a.nvtot;
+            }
+            acc.w = a.weights ? a.weights + v : nullptr;
+            acc.ws = a.nvtot;
+            acc.aux = make_loss_aux(a.sigma ? a.sigma[v] : a.sigma_default);
+            acc.mse_scale = a.mse_scale;
+            acc.hd = a.huber_delta;
+            acc.res = (p.want_res && a.res_out && e == p.e_end && ok) ? a.res_out + v : nullptr;
+            acc.rs = a.nvtot;
+            acc.rt.kind = p.loss;
+            VoxAux va{1.0f, nullptr, nullptr, 1};
+            model_eval<kR2S>(s_P, th, va, acc);
+            float gth[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) gth[k] = acc.g[k] * V.norm;
+            float reg = 0.0f;
+            const int pidx = s_p[i];
+            if (ok && a.n_reg > 0) {
+                const unsigned int fl = s_fl[i];
+                const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
+                const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
+                const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
+                const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
+                const float iv[3] = {ivx, ivy, ivz};
+                for (int r = 0; r < a.n_reg && r < 2; ++r) {  // R2*: at most two maps
+                    const int k = a.reg_param[r];
+                    const float* G = gcur + (size_t)r * a.grid_total + V.grid_off;
+                    const float c = k == 0 ? th[0] : th[1];
+                    float f[3], b[3];
+                    f[0] = __ldcg(G + fw0); b[0] = __ldcg(G + bw0);
+                    f[1] = __ldcg(G + fw1); b[1] = __ldcg(G + bw1);
+                    if (tv3) { f[2] = __ldcg(G + fw2); b[2] = __ldcg(G + bw2); }
+                    else { f[2] = 0.0f; b[2] = 0.0f; }
+                    float cost, gr;
+                    tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
+                    const float tvs = r == 0 ? tvs0 : tvs1;
+                    reg += tvs * cost;
+                    if (k == 0) gth[0] = __fmaf_rn(tvs, gr, gth[0]);
+                    else gth[1] = __fmaf_rn(tvs, gr, gth[1]);
+                }
+            }
+            float gz[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) gz[k] = gth[k] * dth[k];
+            if (ok) {
+                q0 += acc.total;
+                q1 += reg;
+                if constexpr (STATS) {
+#pragma unroll
+                    for (int k = 0; k < NP; ++k) {
+                        float zpk = s_st[(3 * NP + k) * S + i];
+                        q2 += gz[k] * gz[k];
+                        q3 += z[k] * z[k];
+                        q4 += (z[k] - zpk) * (z[k] - zpk);
+                    }
+                }
+            }
+            if (upd && ok) {
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    float zz = z[k];
+                    float mm1 = s_st[(1 * NP + k) * S + i], mm2 = s_st[(2 * NP + k) * S + i];
+                    if constexpr (STATS) s_st[(3 * NP + k) * S + i] = zz;
+                    opt_step(oc, sc, zz, mm1, mm2, gz[k]);
+                    z[k] = zz;
+                    s_st[(0 * NP + k) * S + i] = zz;
+                    s_st[(1 * NP + k) * S + i] = mm1;
+                    s_st[(2 * NP + k) * S + i] = mm2;
+                    if (a.ckpt_every > 0 && (e % a.ckpt_every) == 0) {
+                        float* cp = a.ckpt + (size_t)(e / a.ckpt_every) * 3 * NP * a.nvtot;
+                        cp[(size_t)k * a.nvtot + v] = zz;
+                        cp[(size_t)(NP + k) * a.nvtot + v] = mm1;
+                        cp[(size_t)(2 * NP + k) * a.nvtot + v] = mm2;
+                    }
+                }
+                for (int r = 0; r < a.n_reg && r < 2; ++r) {
+                    const int k = a.reg_param[r];
+                    float dd;
+                    gnext[(size_t)r * a.grid_total + V.grid_off + pidx] =
+                        unscale(a.transform, a.P.lb[k], a.P.ub[k], k == 0 ? z[0] : z[1], dd);
+                }
+            }
+        }
+        if (p.record && a.hist) {
+            const int lane = tid & 31, warp = tid >> 5, nw = (BT + 31) >> 5;
+            double* buf = s_red + (e & 1) * 32 * kHistW;
+            float q[kHistW] = {q0, q1, q2, q3, q4};
+#pragma unroll
+            for (int k = 0; k < kHistW; ++k) {
+                float sum = warp_sum_p(q[k]);
+                if (lane == 0) buf[warp * kHistW + k] = (double)sum;
+            }
+            __syncthreads();
+            if (tid < kHistW) {
+                double t = 0.0;
+                for (int w = 0; w < nw; ++w) t += buf[w * kHistW + tid];
+                if (tid == 0) t *= V.normd;
+                const int vol = a.blk_vol[base / p.pad_block];
+                if (t != 0.0) atomicAdd(a.hist + ((size_t)vol * (a.niter + 1) + e) * kHistW + tid, t);
+            }
+        }
+        if (e < p.e_end)
+            if (!grid_barrier(p.barrier, gridDim.x, gen)) return;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += BT) {
+        const int v = base + i;
+        if ((v - V.off) >= V.nvox) continue;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            size_t gi = (size_t)k * a.nvtot + v;
+            a.z[gi] = s_st[(0 * NP + k) * S + i];
+            a.m1[gi] = s_st[(1 * NP + k) * S + i];
+            a.m2[gi] = s_st[(2 * NP + k) * S + i];
+            if constexpr (STATS)
+                if (a.zprev) a.zprev[gi] = s_st[(3 * NP + k) * S + i];
+        }
+    }
+}
+
+namespace {
+
+template <int LOSS>
+cudaError_t launch_persist_t(const AdamParams& a, PersistArgs p, int bt, int nblocks, size_t smem,
+                             cudaStream_t s) {
+    auto k = p.stats ? tv_persistent_kernel<LOSS, true> : tv_persistent_kernel<LOSS, false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {const_cast<void*>(static_cast<const void*>(&a)), static_cast<void*>(&p)};
+    e = cudaLaunchCooperativeKernel((const void*)k, dim3(nblocks), dim3(bt), args, smem, s);
+    ++g_kernel_launches;
+    return e;
+}
+
+template <int LOSS>
+int occupancy_t(int bt, size_t smem) {
+    int nb = 0, nb2 = 0;
+    if (cudaFuncSetAttribute(tv_persistent_kernel<LOSS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(tv_persistent_kernel<LOSS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, tv_persistent_kernel<LOSS, false>, bt, smem) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, tv_persistent_kernel<LOSS, true>, bt, smem) != cudaSuccess)
+        return 0;
+    return nb < nb2 ? nb : nb2;
+}
+
+}  // namespace
+
+// Plan a persistent launch: one CTA per SM, slice = ceil(nvtot / #SM) voxels
+// (rounded to a padding block so that a slice never straddles two volumes),
+// the slice's Adam state in shared memory (and its measurements too when they
+// fit), kPersistMaxThreads threads.  Returns false when the problem does not
+// fit, in which case the caller uses the per-epoch kernel.
+bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, const int* vol_npad, int nvol,
+                     PersistPlan* plan) {
+    if (model != kR2S) return false;
+    int dev = 0, nsm = 0, smem_optin = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
+    int slice = (a.nvtot + nsm - 1) / nsm;
+    slice = (slice + pad_block - 1) / pad_block * pad_block;
+    {
+        long long acc = 0;
+        for (int i = 0; i < nvol; ++i) {  // every volume starts on a slice boundary
+            if (acc % slice) return false;
+            acc += vol_npad[i];
+        }
+    }
+    const bool stats_any = true;  // size for the larger (statistics) variant
+    const int NS = stats_any ? 4 : 3;
+    size_t red = sizeof(double) * 2 * 32 * kHistW;
+    size_t state = sizeof(float) * (size_t)NS * 2 * slice + sizeof(int) * slice +
+                   sizeof(unsigned short) * ((slice + 1) & ~1);
+    size_t data = sizeof(float) * (size_t)a.nm * slice;
+    const size_t budget = (size_t)smem_optin - 2048;  // static shared memory (staged protocol) and slack
+    if (red + state > budget) return false;
+    int in_smem = red + state + data <= budget ? 1 : 0;
+    size_t smem = red + state + (in_smem ? data : 0);
+    // threads: as many as fit, spread so that the last pass over the slice is full
+    int passes = (slice + kPersistMaxThreads - 1) / kPersistMaxThreads;
+    int bt = ((slice + passes - 1) / passes + 31) / 32 * 32;
+    int nb = loss == kMSE ? occupancy_t<kMSE>(bt, smem) : occupancy_t<-1>(bt, smem);
+    if (nb < 1) return false;
+    plan->slice = slice;
+    plan->vpt = 0;
+    plan->threads = bt;
+    plan->ctas = (a.nvtot + slice - 1) / slice;
+    if (plan->ctas > nb * nsm) return false;
+    plan->smem = smem;
+    plan->data_in_smem = in_smem;
+    return true;
+}
+
+cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s) {
+    p.slice = plan.slice;
+    p.data_in_smem = plan.data_in_smem;
+    if (p.loss == kMSE) return launch_persist_t<kMSE>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    return launch_persist_t<-1>(a, p, plan.threads, plan.ctas, plan.smem, s);
+}
+
+}  // namespace gx

@@ -57,7 +57,7 @@ enum Slot {
     S_CKPT, S_RESF, S_RESM, S_THF, S_THM, S_RLF, S_RLM, S_BLK, S_VOLS, S_GIDX, S_MASK, S_GRID0,
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
-    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_NSLOTS
+    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_NSLOTS
 };
 
 struct gx_context {
@@ -391,6 +391,9 @@ struct AdamJob {
     DevVol* local_vols = nullptr;   // per-volume copies with off = 0 (volume views)
     float* grid[2] = {nullptr, nullptr};  // TV grids, alternating by epoch parity
     float *zr = nullptr, *m1r = nullptr, *m2r = nullptr;  // replay / plain min-loss state
+    bool use_persist = false;             // TV main pass as one cooperative launch
+    PersistPlan plan{};
+    PersistBarrier* barrier = nullptr;
 };
 
 static double sched_pow(double b, int e) { return std::pow(b, (double)e); }
@@ -625,7 +628,7 @@ static gx_status make_view(AdamJob& J, int i, const AdamParams& base, View* out)
 // Run epochs [e0, e1] on the (sub)list described by `a` (TV: one launch per
 // epoch, alternating the two grids by epoch parity).
 static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e1, int update_last,
-                            bool record, float* res_out) {
+                            bool record, float* res_out, bool persistent_ok = false) {
     gx_context* c = J.c;
     a.res_out = res_out;
     if (!record) a.hist = nullptr;
@@ -633,9 +636,27 @@ static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e
         CK(launch_fused(a, J.id, J.o->loss, J.stats && record, e0, e1, update_last, record, J.B, nblocks, c->stream));
         return GX_OK;
     }
+    if (persistent_ok && J.use_persist) {
+        PersistArgs p;
+        memset(&p, 0, sizeof(p));
+        p.e_begin = e0;
+        p.e_end = e1;
+        p.update_last = update_last;
+        p.record = record ? 1 : 0;
+        p.want_res = res_out != nullptr;
+        p.stats = (J.stats && record) ? 1 : 0;
+        p.loss = J.o->loss;
+        p.grid0 = J.grid[0];
+        p.grid1 = J.grid[1];
+        p.barrier = J.barrier;
+        p.pad_block = J.B;
+        CK(cudaMemsetAsync(J.barrier, 0, sizeof(PersistBarrier), c->stream));
+        CK(launch_tv_persistent(a, J.plan, p, c->stream));
+        return GX_OK;
+    }
     float* g[2] = {J.grid[0], J.grid[1]};
     for (int e = e0; e <= e1; ++e) {
-        a.grid_cur = g[(e - 1) & 1];
+        a.grid_cur = g[e >= 1 ? (e - 1) & 1 : 0];  // epoch 0 evaluates the start, like epoch 1
         a.grid_next = g[e & 1];
         CK(launch_tv_step(a, J.id, J.o->loss, J.stats && record, e, e <= update_last, record,
                           e == e1 && res_out != nullptr, J.B, nblocks, c->stream));
@@ -660,7 +681,7 @@ static gx_status replay_volume(AdamJob& J, int i, int target, float* th_out, flo
     V.a.ckpt = nullptr;
     CK(launch_copy_state(V.a, src, nullptr, nullptr, nullptr, false, J.B, V.nblocks, c->stream));
     int e0 = slot * J.ckpt_every + 1;
-    if (J.tv) CK(launch_tv_scatter(V.a, J.grid[(e0 - 1) & 1], J.B, V.nblocks, c->stream));
+    if (J.tv) CK(launch_tv_scatter(V.a, J.grid[(e0 - 1) & 1], J.B, V.nblocks, c->stream));  // e0 >= 1
     size_t o = J.hv[i].off;
     TRY(run_epochs(J, V.a, V.nblocks, e0, target + 1, target, false, res_out ? res_out + o : nullptr));
     CK(launch_finalize(V.a, V.a.z, th_out + o, nullptr, nullptr, J.B, V.nblocks, c->stream));
@@ -699,7 +720,15 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     const bool stop_possible = can_stop(o);
     const int chunk = stop_possible ? (o->chunk > 0 ? o->chunk : 200) : (N > 0 ? N : 1);
     TRY(alloc_outputs(J, out));
-    if (J.tv) CK(launch_tv_scatter(J.a, J.grid[0], J.B, J.nblocks, c->stream));
+    if (J.tv) {
+        CK(launch_tv_scatter(J.a, J.grid[0], J.B, J.nblocks, c->stream));
+        const char* env = getenv("GACELLE_B200_TV_KERNEL");
+        bool want = !(env && strcmp(env, "step") == 0);
+        std::vector<int> npad(J.nvol);
+        for (int i = 0; i < J.nvol; ++i) npad[i] = J.hv[i].npad;
+        J.use_persist = want && plan_persistent(J.a, J.id, o->loss, J.B, npad.data(), J.nvol, &J.plan);
+        if (J.use_persist) TRY(wsT(c, S_BAR, 1, &J.barrier));
+    }
 
     out.tr.assign(J.nvol, Tracker());
     out.final_epoch.assign(J.nvol, N);
@@ -708,14 +737,15 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     int n_main = 0;
     CK(cudaEventRecord(c->ev[2], c->stream));
     if (N == 0) {
-        TRY(run_epochs(J, J.a, J.nblocks, 0, 0, -1, true, out.resf));
+        TRY(run_epochs(J, J.a, J.nblocks, 0, 0, -1, true, out.resf, true));
         ++n_main;
     } else {
         bool all_stopped = false;
         for (int eb = 1; eb <= N && !all_stopped; eb += chunk) {
             int ee = std::min(eb + chunk - 1, N);
-            TRY(run_epochs(J, J.a, J.nblocks, eb, ee, std::min(ee, N - 1), true, ee == N ? out.resf : nullptr));
-            n_main += J.tv ? (ee - eb + 1) : 1;
+            TRY(run_epochs(J, J.a, J.nblocks, eb, ee, std::min(ee, N - 1), true, ee == N ? out.resf : nullptr,
+                           true));
+            n_main += (J.tv && !J.use_persist) ? (ee - eb + 1) : 1;
             if (cancelled(c)) return fail(GX_ECANCELLED, "cancelled");
             if (!stop_possible) continue;
             CK(cudaStreamSynchronize(c->stream));
@@ -760,6 +790,11 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
     c->timing.main_kernel_ms = ms;
     c->timing.main_launches = n_main;
+    if (J.use_persist) {
+        PersistBarrier hb;
+        CK(cudaMemcpy(&hb, J.barrier, sizeof(hb), cudaMemcpyDeviceToHost));
+        if (hb.error) return fail(GX_ETIMEOUT, "askAdam TV kernel: a grid barrier wait expired");
+    }
     for (int i = 0; i < J.nvol && N > 0; ++i) {  // the initial evaluation equals epoch 1's
         size_t base = (size_t)i * (N + 1) * kHistW;
         for (int q = 0; q < kHistW; ++q) J.hist[base + q] = J.hist[base + kHistW + q];

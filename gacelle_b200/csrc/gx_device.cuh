@@ -174,6 +174,10 @@ GX_HD float loss_elem(float s, float y, float w, const LossAux& a, float mse_sca
 // Accumulates loss and d(loss)/d(theta) over the measurements of one voxel.
 // set_nan_inf_zero (utils/askadam.m:80): a non-finite prediction becomes 0
 // and carries no gradient.
+// Models whose signal can be non-finite inside the parameter bounds (NEXI:
+// fa -> 1 makes the exchange rate r2 = r1 fa/(1-fa) overflow).
+template <int NP> struct MayBeNonFinite { static constexpr bool value = NP >= 4; };
+
 template <int LOSS, int NP>
 struct LossAcc {
     float total;
@@ -188,7 +192,7 @@ struct LossAcc {
     int rs;
 
     __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
-        bool bad = !isfinite(S);
+        bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
         float s = bad ? 0.0f : S;
         float ww = w ? w[m * ws] : 1.0f;
         float d;
@@ -401,16 +405,73 @@ struct SosSink {
     }
 };
 
-// unscale_parameters (utils/askadam.m:1063-1075) and its derivative.
+// Copies the protocol into shared memory so that the per-measurement loops
+// read it with shared-memory broadcasts instead of indexed parameter loads.
+__device__ __forceinline__ void stage_protocol(const DevProtocol& P, DevProtocol* s_P) {
+    const int* src = reinterpret_cast<const int*>(&P);
+    int* dst = reinterpret_cast<int*>(s_P);
+    for (int i = threadIdx.x; i < (int)(sizeof(DevProtocol) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+}
+
+// unscale_parameters (utils/askadam.m:1063-1075) and its derivative; the
+// logistic uses the fast reciprocal (2 ulp).
 __device__ __forceinline__ float unscale(int transform, float lb, float ub, float z, float& dth) {
     if (transform == 0) {
-        float s = 1.0f / (1.0f + __expf(-z));
+        float s = __fdividef(1.0f, 1.0f + __expf(-z));
         dth = (ub - lb) * s * (1.0f - s);
         return lb + (ub - lb) * s;
     }
     float zc = fminf(fmaxf(z, 0.0f), 1.0f);  // set_boundary01 before evaluation
     dth = (z >= 0.0f && z <= 1.0f) ? (ub - lb) : 0.0f;
     return zc * (ub - lb) + lb;
+}
+
+// Anisotropic TV at one masked voxel (utils/spatial_total_variation.m:45-66):
+// c = theta at the voxel, f[d] / b[d] = theta at the forward / backward
+// neighbour along axis d (periodic), mb[d] = backward neighbour inside the
+// mask, iv[d] = 1/voxel size.  cost = sum_d |f_d - c| iv_d;
+// d cost_total / d c = sum_d (-sgn(f_d - c) + mb_d sgn(c - b_d)) iv_d.
+// One function for every kernel so that all paths round identically.
+__device__ __forceinline__ void tv_terms(float c, const float* f, const float* b, const bool* mb,
+                                         const float* iv, int nd, float& cost, float& grad) {
+    float cs = 0.0f, gr = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (d < nd) {
+            const float df = f[d] - c;
+            cs = __fadd_rn(cs, fabsf(__fmul_rn(df, iv[d])));
+            const float t = -(float)((df > 0.0f) - (df < 0.0f)) +
+                            (mb[d] ? (float)((c - b[d] > 0.0f) - (c - b[d] < 0.0f)) : 0.0f);
+            gr = __fadd_rn(gr, __fmul_rn(t, iv[d]));
+        }
+    }
+    cost = cs;
+    grad = gr;
+}
+
+// Optimiser step of one parameter (adamupdate / sgdmupdate / rmspropupdate,
+// called from utils/askadam.m:673-691).  sc = per-epoch schedule:
+// Adam (lr_e/(1-b1^e), 1/(1-b2^e)); others (lr_e, 0).  The square root is
+// x*rsqrt(x) (exact zero kept) and the division the fast 2-ulp one.
+struct OptConst {
+    int optimiser;
+    float beta1, beta2, eps, momentum, rms_decay, rms_eps;
+};
+
+__device__ __forceinline__ float fast_sqrt0(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
+__device__ __forceinline__ void opt_step(const OptConst& o, float2 sc, float& z, float& m1, float& m2, float g) {
+    if (o.optimiser == kAdam) {
+        m1 = o.beta1 * m1 + (1.0f - o.beta1) * g;
+        m2 = o.beta2 * m2 + (1.0f - o.beta2) * g * g;
+        z -= __fdividef(sc.x * m1, fast_sqrt0(m2 * sc.y) + o.eps);
+    } else if (o.optimiser == kSGDM) {
+        m1 = o.momentum * m1 - sc.x * g;
+        z += m1;
+    } else {
+        m2 = o.rms_decay * m2 + (1.0f - o.rms_decay) * g * g;
+        z -= __fdividef(sc.x * g, fast_sqrt0(m2) + o.rms_eps);
+    }
 }
 
 #endif  // __CUDACC__

@@ -133,6 +133,37 @@ cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, 
 
 extern long long g_kernel_launches;  // launches of this library's kernels (process-wide)
 
+// Persistent cooperative TV kernel (askadam_persistent.cu).
+constexpr int kPersistMaxThreads = 1024;
+constexpr long long kBarrierSpinCycles = 4000000000LL;  // about 2 s at B200 clocks
+
+struct PersistBarrier {
+    unsigned int count;
+    unsigned int gen;
+    int error;
+    int pad;
+};
+
+struct PersistArgs {
+    int e_begin, e_end, update_last;
+    int record, want_res, stats, loss;
+    float* grid0;            // TV map of even epochs' input (parity 0)
+    float* grid1;
+    PersistBarrier* barrier; // zeroed before the launch
+    int slice;               // voxels per CTA
+    int data_in_smem;
+    int pad_block;           // block size of the work-list padding (blk_vol granularity)
+};
+
+struct PersistPlan {
+    int slice, vpt, threads, ctas, data_in_smem;
+    size_t smem;
+};
+
+bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, const int* vol_npad, int nvol,
+                     PersistPlan* plan);
+cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s);
+
 }  // namespace gx
 
 // Helpers defined in capi.cu for the other translation units.

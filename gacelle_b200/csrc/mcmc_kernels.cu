@@ -58,11 +58,11 @@ __global__ void gw_partner_kernel(McmcParams p, int* partner) {
 }
 
 template <int MODEL>
-__device__ __forceinline__ double log_prob(const McmcParams& p, const float* x, const float* y,
-                                           const float* w, const VoxAux& va) {
+__device__ __forceinline__ double log_prob(const McmcParams& p, const DevProtocol& P, const float* x,
+                                           const float* y, const float* w, const VoxAux& va) {
     constexpr int NP = ModelNP<MODEL>::value;
     SosSink<NP> sink{y, 1, w, 1, 0.0};
-    model_eval<MODEL>(p.P, x, va, sink);
+    model_eval<MODEL>(P, x, va, sink);
     double noise = (double)x[p.nvar - 1];
     double n2 = noise * noise;
     return -sink.sos / (2.0 * n2) - 0.5 * p.nm * log(6.283185307179586 * n2);
@@ -81,8 +81,9 @@ __device__ __forceinline__ int kept_index(const McmcParams& p, int k) {
 template <int MODEL>
 __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float* xstate,
                           double* lpstate, double* sum, double* sumsq) {
-    constexpr int NP = ModelNP<MODEL>::value;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ DevProtocol s_P;
+    stage_protocol(p.P, &s_P);
     const int W = p.nwalker, nvar = p.nvar, nm = p.nm;
     const int h = W / 2;
     const int tpv = p.update == 0 ? W : (W - h);
@@ -144,7 +145,7 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
     for (int o = 0; o < nown; ++o) {
         int w = wown[o];
         if (!live || w < 0 || w >= W) continue;
-        lp[o] = init ? log_prob<MODEL>(p, x[o], yv, wv, va) : lpstate[(size_t)v * W + w];
+        lp[o] = init ? log_prob<MODEL>(p, s_P, x[o], yv, wv, va) : lpstate[(size_t)v * W + w];
     }
     if (!init && live)
         for (int q = 0; q < nvar; ++q) {
@@ -173,7 +174,7 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
                     oob |= (xp < p.lb[j]) || (xp > p.ub[j]);
                     xn[j] = fminf(fmaxf(xp, p.lb[j]), p.ub[j]);
                 }
-                lpp = log_prob<MODEL>(p, xn, yv, wv, va);
+                lpp = log_prob<MODEL>(p, s_P, xn, yv, wv, va);
                 double lr = (double)(nvar - 1) * (double)logf(zz) + (lpp - lp[0]);
                 acc = !oob && lr > (double)logf(u01(u.y));
             }
@@ -206,7 +207,7 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
                         oob |= (xp < p.lb[j]) || (xp > p.ub[j]);
                         xn[j] = fminf(fmaxf(xp, p.lb[j]), p.ub[j]);
                     }
-                    double lpp = log_prob<MODEL>(p, xn, yv, wv, va);
+                    double lpp = log_prob<MODEL>(p, s_P, xn, yv, wv, va);
                     double lr = (double)(nvar - 1) * (double)logf(zz) + (lpp - lp[o]);
                     if (!oob && lr > (double)logf(u01(u.y))) {
                         for (int j = 0; j < nvar; ++j) {
@@ -257,6 +258,9 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
 template <int MODEL>
 __global__ void mh_kernel(McmcParams p, int rr, int k0, int k1, int init, float* xstate,
                           double* lpstate, double* sum, double* sumsq) {
+    __shared__ DevProtocol s_P;
+    stage_protocol(p.P, &s_P);
+    __syncthreads();
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     bool live = v < p.nvox;
     const int nvar = p.nvar, nm = p.nm;
@@ -280,7 +284,7 @@ __global__ void mh_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
         if (init) {
             for (int q = 0; q < nvar; ++q)
                 x[q] = fminf(fmaxf(p.x0[(size_t)q * p.nvox + v], p.lb[q]), p.ub[q]);
-            lp = log_prob<MODEL>(p, x, yv, wv, va);
+            lp = log_prob<MODEL>(p, s_P, x, yv, wv, va);
         } else {
             for (int q = 0; q < nvar; ++q) x[q] = xstate[(size_t)q * p.nvox + v];
             lp = lpstate[v];
@@ -303,7 +307,7 @@ __global__ void mh_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
                 oob |= (t < p.lb[q]) || (t > p.ub[q]);
                 xp[q] = fminf(fmaxf(t, p.lb[q]), p.ub[q]);
             }
-            double lpp = log_prob<MODEL>(p, xp, yv, wv, va);
+            double lpp = log_prob<MODEL>(p, s_P, xp, yv, wv, va);
             if (!oob && (lpp - lp) > (double)logf(u01(ua.x))) {
                 for (int q = 0; q < nvar; ++q) x[q] = xp[q];
                 lp = lpp;

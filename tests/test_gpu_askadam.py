@@ -204,7 +204,8 @@ def test_askadam_tv_dominated_within_fp32_band(ctx):
         assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 2 * band + 1e-4, (k, band)
         # fused and plain order their FP32 sums differently: same band
         assert rel_rmse(eng["final_theta"][k], pl["final_theta"][k]) <= 2 * band + 1e-4, k
-    assert abs(eng["final_loss"] - orc["final_loss"]) <= 1e-4 * orc["final_loss"]
+    lband = abs(o32["final_loss"] - orc["final_loss"])
+    assert abs(eng["final_loss"] - orc["final_loss"]) <= 5 * lband + 2e-5 * orc["final_loss"]
 
 
 def test_askadam_stop_on_tol_exact(ctx):
@@ -246,3 +247,38 @@ def test_askadam_stop_criteria_within_fp32_band(ctx, criterion):
     band = max(5, 2 * abs(orc["final_niter"] - o32["final_niter"]))
     assert _lib.STOP_REASONS[eng["stop_reason"]] == criterion
     assert abs(eng["final_niteration"] - orc["final_niter"]) <= band
+
+
+@pytest.mark.parametrize("case", ["plain_run", "tol_stop", "stats"])
+def test_tv_persistent_kernel_matches_per_epoch_kernel(ctx, case, monkeypatch):
+    """The one-launch persistent TV kernel and the one-launch-per-epoch kernel
+    run the same per-voxel arithmetic (shared model, loss, TV and optimiser
+    code): the same parameters, losses and stopping epochs (checkpoints
+    written by one are replayed by the other).  A well-conditioned TV weight
+    keeps compiler-level rounding differences from being amplified."""
+    y, th0, kw = _tv_problem((40, 40, 24), 7)
+    over = {"lambda": [1e-5], "regmap": ["R2star"], "TVmode": "3D"}
+    if case == "tol_stop":
+        f = fitting(iteration=400, initialLearnRate=0.01, chunk=64, **over)
+        base = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
+        h = base["loss_history"]
+        f = dict(f, tol=0.5 * (h[150] + h[151]))
+    elif case == "stats":
+        f = fitting(iteration=300, initialLearnRate=0.01, convergenceStepTol=1e-9, convergenceGradTol=1e-12,
+                    chunk=64, **over)
+    else:
+        f = fitting(iteration=300, initialLearnRate=0.01, **over)
+    monkeypatch.setenv("GACELLE_B200_TV_KERNEL", "step")
+    a = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
+    monkeypatch.setenv("GACELLE_B200_TV_KERNEL", "persistent")
+    b = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
+    assert b["timing"]["main_launches"] < a["timing"]["main_launches"]
+    for k in range(2):
+        assert rel_rmse(b["final_theta"][k], a["final_theta"][k]) <= 1e-5, k
+        assert rel_rmse(b["min_theta"][k], a["min_theta"][k]) <= 1e-5, k
+    assert a["final_niteration"] == b["final_niteration"]
+    assert a["min_niteration"] == b["min_niteration"]
+    np.testing.assert_allclose(a["loss_history"][:a["final_niteration"] + 1],
+                               b["loss_history"][:b["final_niteration"] + 1], rtol=1e-6)
+    if case == "tol_stop":
+        assert a["final_niteration"] == 151

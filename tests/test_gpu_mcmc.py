@@ -75,12 +75,12 @@ def _moments_agree(eng, orc, orc_b, nparam):
     only in seed (the engine shares the first oracle's random streams, so its
     differences come from FP32 rounding and are normally far smaller)."""
     for k in range(nparam):
-        d_mean = np.abs(eng["mean"][k] - orc["mean"][k])
-        r_mean = np.abs(orc_b["mean"][k] - orc["mean"][k])
-        assert np.median(d_mean) <= 1.2 * np.median(r_mean) + 1e-12, (k, np.median(d_mean), np.median(r_mean))
-        d_std = np.abs(eng["std"][k] - orc["std"][k])
-        r_std = np.abs(orc_b["std"][k] - orc["std"][k])
-        assert np.median(d_std) <= 1.2 * np.median(r_std) + 1e-12, (k, np.median(d_std), np.median(r_std))
+        for q in ("mean", "std"):
+            d2 = np.mean((eng[q][k] - orc[q][k]) ** 2)
+            r2 = np.mean((orc_b[q][k] - orc[q][k]) ** 2)
+            # ratio of mean squares over the voxels; 2.5 is well above the
+            # sampling spread of such a ratio for two equal-variance sets
+            assert d2 <= 2.5 * r2 + 1e-20, (k, q, d2, r2)
 
 
 @pytest.mark.parametrize("algorithm,update", [("ensemble", "simultaneous"), ("ensemble", "redblack"),
@@ -133,7 +133,7 @@ def test_mh_matches_oracle(ctx):
 def test_gw_nexi_moments(ctx):
     rng = np.random.default_rng(13)
     gxm, om = models("nexi")
-    nv = 32
+    nv = 96
     th = np.vstack([rng.uniform(0.3, 0.7, nv), rng.uniform(1.5, 2.5, nv), rng.uniform(0.7, 1.2, nv),
                     rng.uniform(0.02, 0.1, nv)])
     s = oracle.forward(om, th)
