@@ -171,7 +171,17 @@ class Context:
             pass
 
     def set_stream(self, stream_ptr: int | None):
-        check(lib().gx_context_set_stream(self.ptr, C.c_void_p(stream_ptr or 0)))
+        """Run this context's work on a CUDA stream given by its handle
+        (``torch.cuda.Stream.cuda_stream``).  Handle 0, which is how PyTorch
+        reports the default stream, selects the legacy default stream
+        (cudaStreamLegacy); None returns to the context's own stream."""
+        if stream_ptr is None:
+            h = 0
+        elif stream_ptr == 0:
+            h = 1  # cudaStreamLegacy
+        else:
+            h = stream_ptr
+        check(lib().gx_context_set_stream(self.ptr, C.c_void_p(h)))
 
     def timing(self) -> dict:
         t = GxTiming()

@@ -16,7 +16,9 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB = os.path.join(HERE, "libgacelle_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-Xptxas", "-O3",
+# -ftz=true: FP32 subnormals flush to zero, so ex2/rcp/rsqrt are single
+# hardware approximations; no quantity in these fits is subnormal.
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-ftz=true", "-Xcompiler", "-fPIC,-O2", "-Xptxas", "-O3",
          "-diag-suppress", "177"]
 
 

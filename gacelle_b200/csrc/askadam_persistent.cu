@@ -2,25 +2,32 @@
 // cooperative launch over a range of epochs (R2* model).
 //
 // Each CTA owns a contiguous slice of the voxel work-list for the whole
-// launch: the slice's measurements are staged once in shared memory, each
-// thread keeps the parameters and Adam moments of VPT voxels in registers,
-// and only the regularised parameter map travels between epochs (the
-// double-buffered full-grid TV map, read through L2 with ld.global.cg since
-// other CTAs wrote it in the same launch).  Epochs are separated by a grid
-// barrier whose wait is bounded: if it expires the kernel raises an error flag
-// that the host reports as GX_ETIMEOUT, and every CTA returns.
+// launch: the slice's Adam state lives in shared memory (and its measurements
+// too when they fit; otherwise they are read from L2, all of a voxel's echoes
+// in flight together), and only the regularised parameter map travels between
+// CTAs (the double-buffered full-grid TV map, read through L2 with
+// ld.global.cg since other CTAs wrote it in the same launch).
+//
+// An epoch runs in two passes over the slice.  The fidelity pass (forward
+// model, loss, adjoint) needs only the CTA's own voxels; the TV/update pass
+// (TV subgradient from the neighbours' map values of the previous epoch,
+// sigmoid chain rule, optimiser, new map value) needs every CTA's previous
+// map.  So the grid barrier is split: a CTA arrives after its map writes and
+// waits only before its next TV/update pass, and the wait overlaps the
+// fidelity pass.  The wait is bounded: if it expires the kernel raises an
+// error flag that the host reports as GX_ETIMEOUT, and every CTA returns.
 //
 // The per-voxel arithmetic (forward model, loss, adjoint, TV subgradient,
 // sigmoid chain rule, optimiser) is the same code as tv_step_kernel, so the
 // two paths produce the same parameters.  Reference: utils/askadam.m:23-117,
 // 673-691; utils/spatial_total_variation.m:24-66.
+#include <algorithm>
+
 #include "gx_internal.h"
 
 namespace gx {
 
 namespace {
-
-__device__ __forceinline__ float sgnp(float x) { return (float)((x > 0.0f) - (x < 0.0f)); }
 
 __device__ __forceinline__ float warp_sum_p(float v) {
 #pragma unroll
@@ -59,7 +66,7 @@ struct PLossAcc {
     int rs;
     RtLoss rt;
     __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
-        bool bad = !isfinite(S);
+        bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
         float s = bad ? 0.0f : S;
         float ww = w ? w[m * ws] : 1.0f;
         float d;
@@ -75,29 +82,42 @@ struct PLossAcc {
     }
 };
 
-// Grid-wide barrier for a cooperative launch, with a bounded wait.
-// Returns false (on every thread of the CTA) once any CTA has timed out.
-__device__ __forceinline__ bool grid_barrier(PersistBarrier* gb, unsigned int nblocks, unsigned int& gen) {
-    __shared__ int s_ok;
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Split grid barrier for a cooperative launch.  grid_arrive: every thread's
+// prior global writes are released to the other CTAs (the last CTA to arrive
+// opens generation gen+1).  grid_wait: returns once generation gen+1 is open,
+// with the other CTAs' writes visible, or false (on every thread of the CTA)
+// once any CTA's wait has expired.  gen is meaningful in thread 0 only.
+__device__ __forceinline__ void grid_arrive(PersistBarrier* gb, unsigned int nblocks, unsigned int gen) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned int g = gen;
         __threadfence();
         unsigned int arrived = atomicAdd(&gb->count, 1u);
         if (arrived == nblocks - 1) {
-            gb->count = 0u;
+            atomicExch(&gb->count, 0u);
             __threadfence();
-            atomicExch(&gb->gen, g + 1u);
-        } else {
-            const long long t0 = clock64();
-            while (atomicAdd(&gb->gen, 0u) == g) {
-                if (*(volatile int*)&gb->error) break;
-                if (clock64() - t0 > kBarrierSpinCycles) {
-                    atomicExch(&gb->error, 1);
-                    break;
-                }
-                __nanosleep(32);
+            atomicExch(&gb->gen, gen + 1u);
+        }
+    }
+}
+
+__device__ __forceinline__ bool grid_wait(PersistBarrier* gb, unsigned int& gen) {
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        const unsigned int g = gen;
+        const long long t0 = clock64();
+        while (ld_acquire_gpu(&gb->gen) == g) {
+            if (*(volatile int*)&gb->error) break;
+            if (clock64() - t0 > kBarrierSpinCycles) {
+                atomicExch(&gb->error, 1);
+                break;
             }
+            __nanosleep(20);
         }
         __threadfence();
         s_ok = *(volatile int*)&gb->error == 0;
@@ -109,15 +129,25 @@ __device__ __forceinline__ bool grid_barrier(PersistBarrier* gb, unsigned int nb
 
 }  // namespace
 
-template <int LOSS, bool STATS>
-__global__ void __launch_bounds__(kPersistMaxThreads, 1)
+// MAXM > 0: the standard configuration (MSE, sigmoid transform, Adam, one
+// regularised map) with the measurements prefetched into registers
+// (nm <= MAXM), those options folded in at compile time and the residuals of
+// the final evaluation written by a pass after the epoch loop; MAXM == 0: any
+// loss, transform, optimiser and regulariser count, measurements read one at
+// a time.
+// Threads per CTA at most: the 32-echo variant needs more than 64 registers.
+constexpr int persist_max_threads(int maxm) { return maxm > 16 ? 768 : kPersistMaxThreads; }
+
+template <int LOSS, bool STATS, int MAXM>
+__global__ void __launch_bounds__(persist_max_threads(MAXM), 1)
 tv_persistent_kernel(AdamParams a, PersistArgs p) {
     constexpr int NP = 2;  // R2*: M0, R2star
     constexpr int NS = STATS ? 4 : 3;  // z, m1, m2 [, z of the previous epoch]
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* s_red = reinterpret_cast<double*>(smem_raw);                     // [2][32][kHistW]
     float* s_st = reinterpret_cast<float*>(s_red + 2 * 32 * kHistW);         // [NS][NP][slice]
-    int* s_p = reinterpret_cast<int*>(s_st + (size_t)NS * NP * p.slice);     // [slice] grid index
+    float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NP][slice] fidelity gradient
+    int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NP * p.slice);          // [slice] grid index
     unsigned short* s_fl = reinterpret_cast<unsigned short*>(s_p + p.slice); // [slice] boundary/mask flags
     float* s_y = reinterpret_cast<float*>(s_fl + ((p.slice + 1) & ~1));       // [nm][slice] if staged
     const int BT = blockDim.x, tid = threadIdx.x;
@@ -169,8 +199,12 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     unsigned int gen = 0;
     if (tid == 0) gen = atomicAdd(&p.barrier->gen, 0u);
     __syncthreads();
+    constexpr bool STD = MAXM > 0;
     const bool tv3 = a.tv_3d != 0;
-    const OptConst oc{a.optimiser, a.beta1, a.beta2, a.eps, a.momentum, a.rms_decay, a.rms_eps};
+    const int nm = a.nm;
+    const int transform = STD ? 0 : a.transform;
+    const int nreg = STD ? 1 : min(a.n_reg, 2);  // R2*: at most two maps
+    const OptConst oc{STD ? kAdam : a.optimiser, a.beta1, a.beta2, a.eps, a.momentum, a.rms_decay, a.rms_eps};
     const float ivx = a.inv_vs[0], ivy = a.inv_vs[1], ivz = a.inv_vs[2];
 
     for (int e = p.e_begin; e <= p.e_end; ++e) {
@@ -179,49 +213,81 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f;
         const bool upd = e <= p.update_last;
         const float2 sc = upd ? a.sched[e] : float2{0.f, 0.f};
+        // pass 1: data fidelity of the slice (own voxels only)
         for (int i = tid; i < n; i += BT) {
             const int v = base + i;
             const bool ok = (v - V.off) < V.nvox;
-            float z[NP], th[NP], dth[NP];
+            float th[NP], dth[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k)
+                th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], s_st[(0 * NP + k) * S + i], dth[k]);
+            const float* yb = p.data_in_smem ? s_y + i : a.data + v;
+            const int ys = p.data_in_smem ? S : a.nvtot;
+            float tot, g0, g1;
+            if constexpr (MAXM > 0) {
+                PrefLossAcc<LOSS, NP, MAXM> acc;
+                acc.load(yb, ys, nm);
+                acc.total = 0.0f;
+                acc.g[0] = acc.g[1] = 0.0f;
+                acc.w = a.weights ? a.weights + v : nullptr;
+                acc.ws = a.nvtot;
+                acc.aux = make_loss_aux(a.sigma ? a.sigma[v] : a.sigma_default);
+                acc.mse_scale = a.mse_scale;
+                acc.hd = a.huber_delta;
+                acc.res = nullptr;  // residuals: pass after the epoch loop
+                acc.rs = a.nvtot;
+                model_r2s_unrolled<MAXM>(s_P, nm, th, acc);
+                tot = acc.total;
+                g0 = acc.g[0];
+                g1 = acc.g[1];
+            } else {
+                PLossAcc<LOSS, NP> acc;
+                acc.total = 0.0f;
+                acc.g[0] = acc.g[1] = 0.0f;
+                acc.y = yb;
+                acc.ys = ys;
+                acc.w = a.weights ? a.weights + v : nullptr;
+                acc.ws = a.nvtot;
+                acc.aux = make_loss_aux(a.sigma ? a.sigma[v] : a.sigma_default);
+                acc.mse_scale = a.mse_scale;
+                acc.hd = a.huber_delta;
+                acc.res = (p.want_res && a.res_out && e == p.e_end && ok) ? a.res_out + v : nullptr;
+                acc.rs = a.nvtot;
+                acc.rt.kind = p.loss;
+                VoxAux va{1.0f, nullptr, nullptr, 1};
+                model_eval<kR2S>(s_P, th, va, acc);
+                tot = acc.total;
+                g0 = acc.g[0];
+                g1 = acc.g[1];
+            }
+            s_gf[0 * S + i] = g0 * V.norm;
+            s_gf[1 * S + i] = g1 * V.norm;
+            if (ok) q0 += tot;
+        }
+        // every CTA's map of the previous epoch (written before its arrival)
+        if (e > p.e_begin)
+            if (!grid_wait(p.barrier, gen)) return;
+        // pass 2: TV subgradient, chain rule, optimiser, new map values
+        for (int i = tid; i < n; i += BT) {
+            const int v = base + i;
+            const bool ok = (v - V.off) < V.nvox;
+            float z[NP], th[NP], dth[NP], gth[NP];
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
                 z[k] = s_st[(0 * NP + k) * S + i];
-                th[k] = unscale(a.transform, a.P.lb[k], a.P.ub[k], z[k], dth[k]);
+                th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], z[k], dth[k]);
+                gth[k] = s_gf[k * S + i];
             }
-            PLossAcc<LOSS, NP> acc;
-            acc.total = 0.0f;
-#pragma unroll
-            for (int k = 0; k < NP; ++k) acc.g[k] = 0.0f;
-            if (p.data_in_smem) {
-                acc.y = s_y + i;
-                acc.ys = S;
-            } else {
-                acc.y = a.data + v;
-                acc.ys = a.nvtot;
-            }
-            acc.w = a.weights ? a.weights + v : nullptr;
-            acc.ws = a.nvtot;
-            acc.aux = make_loss_aux(a.sigma ? a.sigma[v] : a.sigma_default);
-            acc.mse_scale = a.mse_scale;
-            acc.hd = a.huber_delta;
-            acc.res = (p.want_res && a.res_out && e == p.e_end && ok) ? a.res_out + v : nullptr;
-            acc.rs = a.nvtot;
-            acc.rt.kind = p.loss;
-            VoxAux va{1.0f, nullptr, nullptr, 1};
-            model_eval<kR2S>(s_P, th, va, acc);
-            float gth[NP];
-#pragma unroll
-            for (int k = 0; k < NP; ++k) gth[k] = acc.g[k] * V.norm;
             float reg = 0.0f;
             const int pidx = s_p[i];
-            if (ok && a.n_reg > 0) {
+            if (ok && nreg > 0) {
                 const unsigned int fl = s_fl[i];
                 const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
                 const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
                 const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
                 const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
                 const float iv[3] = {ivx, ivy, ivz};
-                for (int r = 0; r < a.n_reg && r < 2; ++r) {  // R2*: at most two maps
+                for (int r = 0; r < nreg; ++r) {
                     const int k = a.reg_param[r];
                     const float* G = gcur + (size_t)r * a.grid_total + V.grid_off;
                     const float c = k == 0 ? th[0] : th[1];
@@ -242,7 +308,6 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
 #pragma unroll
             for (int k = 0; k < NP; ++k) gz[k] = gth[k] * dth[k];
             if (ok) {
-                q0 += acc.total;
                 q1 += reg;
                 if constexpr (STATS) {
 #pragma unroll
@@ -272,14 +337,15 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                         cp[(size_t)(2 * NP + k) * a.nvtot + v] = mm2;
                     }
                 }
-                for (int r = 0; r < a.n_reg && r < 2; ++r) {
+                for (int r = 0; r < nreg; ++r) {
                     const int k = a.reg_param[r];
                     float dd;
                     gnext[(size_t)r * a.grid_total + V.grid_off + pidx] =
-                        unscale(a.transform, a.P.lb[k], a.P.ub[k], k == 0 ? z[0] : z[1], dd);
+                        unscale(transform, a.P.lb[k], a.P.ub[k], k == 0 ? z[0] : z[1], dd);
                 }
             }
         }
+        if (e < p.e_end) grid_arrive(p.barrier, gridDim.x, gen);
         if (p.record && a.hist) {
             const int lane = tid & 31, warp = tid >> 5, nw = (BT + 31) >> 5;
             double* buf = s_red + (e & 1) * 32 * kHistW;
@@ -298,8 +364,35 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 if (t != 0.0) atomicAdd(a.hist + ((size_t)vol * (a.niter + 1) + e) * kHistW + tid, t);
             }
         }
-        if (e < p.e_end)
-            if (!grid_barrier(p.barrier, gridDim.x, gen)) return;
+    }
+    if constexpr (STD) {
+        // residuals of the final evaluation; the launch ends with an epoch
+        // without update (host-checked), so the state is the evaluated one
+        if (p.want_res && a.res_out) {
+            for (int i = tid; i < n; i += BT) {
+                const int v = base + i;
+                if ((v - V.off) >= V.nvox) continue;
+                float th[NP], dth[NP];
+#pragma unroll
+                for (int k = 0; k < NP; ++k)
+                    th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], s_st[(0 * NP + k) * S + i], dth[k]);
+                PLossAcc<LOSS, NP> acc;
+                acc.total = 0.0f;
+                acc.g[0] = acc.g[1] = 0.0f;
+                acc.y = p.data_in_smem ? s_y + i : a.data + v;
+                acc.ys = p.data_in_smem ? S : a.nvtot;
+                acc.w = a.weights ? a.weights + v : nullptr;
+                acc.ws = a.nvtot;
+                acc.aux = make_loss_aux(a.sigma ? a.sigma[v] : a.sigma_default);
+                acc.mse_scale = a.mse_scale;
+                acc.hd = a.huber_delta;
+                acc.res = a.res_out + v;
+                acc.rs = a.nvtot;
+                acc.rt.kind = p.loss;
+                VoxAux va{1.0f, nullptr, nullptr, 1};
+                model_eval<kR2S>(s_P, th, va, acc);
+            }
+        }
     }
     __syncthreads();
     for (int i = tid; i < n; i += BT) {
@@ -319,10 +412,19 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
 
 namespace {
 
-template <int LOSS>
+// Variants: MSE with up to 16 or 32 echoes (measurements prefetched into
+// registers), and any loss / echo count with the loss chosen at run time.
+int persist_variant(const AdamParams& a, int loss, bool res_after_loop) {
+    const bool std_cfg = loss == kMSE && a.transform == 0 && a.optimiser == kAdam && a.n_reg == 1 && res_after_loop;
+    if (std_cfg && a.nm <= 16) return 16;
+    if (std_cfg && a.nm <= 32) return 32;
+    return 0;
+}
+
+template <int LOSS, int MAXM>
 cudaError_t launch_persist_t(const AdamParams& a, PersistArgs p, int bt, int nblocks, size_t smem,
                              cudaStream_t s) {
-    auto k = p.stats ? tv_persistent_kernel<LOSS, true> : tv_persistent_kernel<LOSS, false>;
+    auto k = p.stats ? tv_persistent_kernel<LOSS, true, MAXM> : tv_persistent_kernel<LOSS, false, MAXM>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {const_cast<void*>(static_cast<const void*>(&a)), static_cast<void*>(&p)};
@@ -331,19 +433,23 @@ cudaError_t launch_persist_t(const AdamParams& a, PersistArgs p, int bt, int nbl
     return e;
 }
 
-template <int LOSS>
+template <int LOSS, int MAXM>
 int occupancy_t(int bt, size_t smem) {
     int nb = 0, nb2 = 0;
-    if (cudaFuncSetAttribute(tv_persistent_kernel<LOSS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(tv_persistent_kernel<LOSS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
+    auto k0 = tv_persistent_kernel<LOSS, false, MAXM>;
+    auto k1 = tv_persistent_kernel<LOSS, true, MAXM>;
+    if (cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, tv_persistent_kernel<LOSS, false>, bt, smem) != cudaSuccess)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, tv_persistent_kernel<LOSS, true>, bt, smem) != cudaSuccess)
-        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k0, bt, smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k1, bt, smem) != cudaSuccess) return 0;
     return nb < nb2 ? nb : nb2;
+}
+
+int occupancy_v(int variant, int bt, size_t smem) {
+    if (variant == 16) return occupancy_t<kMSE, 16>(bt, smem);
+    if (variant == 32) return occupancy_t<kMSE, 32>(bt, smem);
+    return occupancy_t<-1, 0>(bt, smem);
 }
 
 }  // namespace
@@ -373,17 +479,20 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     const bool stats_any = true;  // size for the larger (statistics) variant
     const int NS = stats_any ? 4 : 3;
     size_t red = sizeof(double) * 2 * 32 * kHistW;
-    size_t state = sizeof(float) * (size_t)NS * 2 * slice + sizeof(int) * slice +
-                   sizeof(unsigned short) * ((slice + 1) & ~1);
+    size_t state = sizeof(float) * (size_t)(NS + 1) * 2 * slice + sizeof(int) * slice +
+                   sizeof(unsigned short) * ((slice + 1) & ~1);  // + fidelity gradient [2][slice]
     size_t data = sizeof(float) * (size_t)a.nm * slice;
     const size_t budget = (size_t)smem_optin - 2048;  // static shared memory (staged protocol) and slack
     if (red + state > budget) return false;
     int in_smem = red + state + data <= budget ? 1 : 0;
     size_t smem = red + state + (in_smem ? data : 0);
     // threads: as many as fit, spread so that the last pass over the slice is full
-    int passes = (slice + kPersistMaxThreads - 1) / kPersistMaxThreads;
+    const int variant = persist_variant(a, loss, true);
+    const int maxt = persist_max_threads(variant);
+    int passes = (slice + maxt - 1) / maxt;
     int bt = ((slice + passes - 1) / passes + 31) / 32 * 32;
-    int nb = loss == kMSE ? occupancy_t<kMSE>(bt, smem) : occupancy_t<-1>(bt, smem);
+    int nb = occupancy_v(variant, bt, smem);
+    if (variant != 0) nb = std::min(nb, occupancy_v(0, bt, smem));
     if (nb < 1) return false;
     plan->slice = slice;
     plan->vpt = 0;
@@ -398,8 +507,12 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
 cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s) {
     p.slice = plan.slice;
     p.data_in_smem = plan.data_in_smem;
-    if (p.loss == kMSE) return launch_persist_t<kMSE>(a, p, plan.threads, plan.ctas, plan.smem, s);
-    return launch_persist_t<-1>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    // the register-prefetch variants write residuals after their epoch loop,
+    // which needs a launch whose last epoch is not followed by an update
+    const int variant = persist_variant(a, p.loss, !p.want_res || p.e_end > p.update_last);
+    if (variant == 16) return launch_persist_t<kMSE, 16>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    if (variant == 32) return launch_persist_t<kMSE, 32>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    return launch_persist_t<-1, 0>(a, p, plan.threads, plan.ctas, plan.smem, s);
 }
 
 }  // namespace gx

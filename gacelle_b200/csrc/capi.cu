@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -96,6 +97,40 @@ static gx_status wsT(gx_context* c, Slot s, size_t n, T** out) {
     *out = (T*)p;
     return GX_OK;
 }
+
+// Opt-in phase trace (environment variable GACELLE_B200_TRACE=1): the host
+// wall time of each phase of a call, with the stream drained at every phase
+// boundary so that the device work of the phase is included; printed to
+// stderr when the call returns.  Off, it costs one branch per phase.
+struct PhaseTrace {
+    bool on = false;
+    cudaStream_t s = nullptr;
+    const char* call = "";
+    std::chrono::steady_clock::time_point t0, last;
+    std::string line;
+    PhaseTrace(const char* name, cudaStream_t st) : s(st), call(name) {
+        const char* e = getenv("GACELLE_B200_TRACE");
+        on = e && e[0] && e[0] != '0';
+        if (on) {
+            cudaStreamSynchronize(s);
+            t0 = last = std::chrono::steady_clock::now();
+        }
+    }
+    void mark(const char* phase) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        auto now = std::chrono::steady_clock::now();
+        char b[96];
+        snprintf(b, sizeof(b), " %s %.3f", phase, std::chrono::duration<double, std::milli>(now - last).count());
+        line += b;
+        last = now;
+    }
+    ~PhaseTrace() {
+        if (!on) return;
+        double tot = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        fprintf(stderr, "[gacelle_b200] %s ms:%s | total %.3f\n", call, line.c_str(), tot);
+    }
+};
 
 struct CallScope {
     gx_context* c;
@@ -390,6 +425,7 @@ struct AdamJob {
     long long h2d = 0, d2h = 0;
     DevVol* local_vols = nullptr;   // per-volume copies with off = 0 (volume views)
     float* grid[2] = {nullptr, nullptr};  // TV grids, alternating by epoch parity
+    PhaseTrace* trace = nullptr;
     float *zr = nullptr, *m1r = nullptr, *m2r = nullptr;  // replay / plain min-loss state
     bool use_persist = false;             // TV main pass as one cooperative launch
     PersistPlan plan{};
@@ -501,6 +537,7 @@ static gx_status adam_setup(AdamJob& J) {
         if (anyth0 && v.theta0) TRY(upload_rows(c, th0, nv, d.off, v.theta0, J.np, v.nvox, J.mem, &J.h2d));
     }
     a.data = data; a.weights = w; a.b1 = b1; a.sigma = sig;
+    if (J.trace) J.trace->mark("upload");
     TRY(wsT(c, S_Z, (size_t)J.np * nv, &a.z));
     TRY(wsT(c, S_M1, (size_t)J.np * nv, &a.m1));
     TRY(wsT(c, S_M2, (size_t)J.np * nv, &a.m2));
@@ -549,6 +586,7 @@ static gx_status adam_setup(AdamJob& J) {
     J.nslots = N / K + 1;
     TRY(wsT(c, S_CKPT, (size_t)J.nslots * 3 * J.np * nv, &a.ckpt));
     a.ckpt_every = K;
+    if (J.trace) J.trace->mark("tables");
     // TV grids and masks
     if (J.tv) {
         int* gidx;
@@ -587,6 +625,7 @@ static gx_status adam_setup(AdamJob& J) {
         J.grid[0] = g0;
         J.grid[1] = g1;
     }
+    if (J.trace) J.trace->mark("tv_grid");
     // initial state + checkpoint slot 0
     CK(launch_init_state(a, anyth0 ? th0 : nullptr, o->randomness, o->seed, J.B, c->stream));
     if (anyth0) {
@@ -595,6 +634,7 @@ static gx_status adam_setup(AdamJob& J) {
             if (!J.vols[i].theta0) return fail(GX_EUNSUPPORTED, "mixing volumes with and without theta0");
     }
     CK(launch_copy_state(a, a.ckpt, a.z, a.m1, a.m2, true, J.B, J.nblocks, c->stream));
+    if (J.trace) J.trace->mark("init");
     return GX_OK;
 }
 
@@ -735,6 +775,7 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     J.hist.assign((size_t)J.nvol * (N + 1) * kHistW, 0.0);
     std::vector<bool> started(J.nvol, false);
     int n_main = 0;
+    if (J.trace) J.trace->mark("plan");
     CK(cudaEventRecord(c->ev[2], c->stream));
     if (N == 0) {
         TRY(run_epochs(J, J.a, J.nblocks, 0, 0, -1, true, out.resf, true));
@@ -802,6 +843,7 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     for (int i = 0; i < J.nvol; ++i)
         if (out.tr[i].stopped) out.final_epoch[i] = out.tr[i].stop_epoch;
 
+    if (J.trace) J.trace->mark("main");
     // final state: the live z holds z_{N-1}; volumes that stopped at e* are replayed to z_{e*-1}
     CK(launch_finalize(J.a, J.a.z, out.thf, nullptr, nullptr, J.B, J.nblocks, c->stream));
     for (int i = 0; i < J.nvol; ++i)
@@ -823,6 +865,7 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
             TRY(replay_volume(J, i, tmin, out.thm, out.resm));
         }
     }
+    if (J.trace) J.trace->mark("final_min");
     return GX_OK;
 }
 
@@ -996,12 +1039,15 @@ extern "C" gx_status gx_askadam(gx_context* c, const gx_model* model, int32_t me
         J.want_res_f |= results[i].final_residual || results[i].final_resloss;
         J.want_res_m |= results[i].min_residual || results[i].min_resloss;
     }
+    PhaseTrace trace("gx_askadam", c->stream);
+    J.trace = trace.on ? &trace : nullptr;
     CK(cudaEventRecord(c->ev[0], c->stream));
     TRY(adam_setup(J));
     AdamOut out;
     if (opts->path == GX_PATH_PLAIN) TRY(adam_plain(J, out));
     else TRY(adam_fused(J, out));
     gx_status st = adam_write_results(J, out, results);
+    trace.mark("write");
     CK(cudaEventRecord(c->ev[1], c->stream));
     CK(cudaEventSynchronize(c->ev[1]));
     float ms = 0.f;

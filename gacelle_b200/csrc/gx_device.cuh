@@ -212,6 +212,50 @@ template <> struct ModelNP<kR1R2S> { static constexpr int value = 3; };
 template <> struct ModelNP<kNEXI> { static constexpr int value = 4; };
 template <> struct ModelNP<kNEXI2> { static constexpr int value = 5; };
 
+// One echo of the mono-exponential model, S = M0 exp(-TE R2*), and its
+// derivatives with respect to (M0, R2*) (R2star/gpuR2starMapping.m:427-434).
+__device__ __forceinline__ void r2s_echo(float te, float M0, float R2, float& S, float (&dS)[2]) {
+    float E = __expf(-te * R2);
+    S = M0 * E;
+    dS[0] = E;
+    dS[1] = -te * S;
+}
+
+// LossAcc whose measurements are loaded into registers before the model runs
+// (load()), so that all of a voxel's loads are in flight together instead of
+// one per measurement; add() must be called with compile-time indices m
+// (an unrolled loop, model_r2s_unrolled).  Same loss arithmetic as LossAcc.
+template <int LOSS, int NP, int MAXM>
+struct PrefLossAcc {
+    float total;
+    float g[NP];
+    float yv[MAXM];
+    const float* w;   // nullptr: unit weights
+    int ws;
+    LossAux aux;
+    float mse_scale, hd;
+    float* res;       // nullptr or residual output at res[m*rs]
+    int rs;
+
+    __device__ __forceinline__ void load(const float* y, int ys, int nm) {
+#pragma unroll
+        for (int m = 0; m < MAXM; ++m) yv[m] = m < nm ? y[(size_t)m * ys] : 0.0f;  // global or shared
+    }
+    __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
+        bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
+        float s = bad ? 0.0f : S;
+        float ww = w ? w[m * ws] : 1.0f;
+        float d;
+        float l = loss_elem<LOSS>(s, yv[m], ww, aux, mse_scale, hd, d);
+        total += l;
+        if (res) res[m * rs] = l;
+        if (!bad) {
+#pragma unroll
+            for (int k = 0; k < NP; ++k) g[k] += d * dS[k];
+        }
+    }
+};
+
 // Per-voxel model inputs besides theta.
 struct VoxAux {
     float b1;                 // R1R2*: flip-angle scaling
@@ -225,11 +269,25 @@ template <class Acc>
 __device__ __forceinline__ void model_r2s(const DevProtocol& P, const float* th, Acc& acc) {
     float M0 = th[0], R2 = th[1];
     for (int m = 0; m < P.nm; ++m) {
-        float te = P.te[m];
-        float E = __expf(-te * R2);
-        float S = M0 * E;
-        float dS[2] = {E, -te * S};
+        float S, dS[2];
+        r2s_echo(P.te[m], M0, R2, S, dS);
         acc.add(m, S, dS);
+    }
+}
+
+// model_r2s with the echo loop unrolled to a compile-time bound (nm <= MAXM),
+// so that an accumulator holding the voxel's measurements in registers
+// (PrefLossAcc) is indexed by constants.  Same arithmetic per echo.
+template <int MAXM, class Acc>
+__device__ __forceinline__ void model_r2s_unrolled(const DevProtocol& P, int nm, const float* th, Acc& acc) {
+    float M0 = th[0], R2 = th[1];
+#pragma unroll
+    for (int m = 0; m < MAXM; ++m) {
+        if (m < nm) {
+            float S, dS[2];
+            r2s_echo(P.te[m], M0, R2, S, dS);
+            acc.add(m, S, dS);
+        }
     }
 }
 

@@ -210,7 +210,10 @@ size_t gx_struct_size(const char* name);
 
 gx_status gx_context_create(int32_t device, gx_context** out);
 gx_status gx_context_destroy(gx_context* ctx);
-/* Run the context's work on an external cudaStream_t (NULL: the context's own). */
+/* Run the context's work on an external cudaStream_t.  NULL selects the
+ * context's own non-blocking stream (the initial one); the CUDA default
+ * streams are selected by their handles cudaStreamLegacy (0x1) and
+ * cudaStreamPerThread (0x2). */
 gx_status gx_context_set_stream(gx_context* ctx, void* cuda_stream);
 gx_status gx_last_timing(gx_context* ctx, gx_timing* out);
 /* Host-side cancel flag polled between launches; nonzero stops the call

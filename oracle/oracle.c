@@ -462,8 +462,9 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
     double fid = 0.0;
     double* theta = (double*)malloc(sizeof(double) * (size_t)np * nv);
     double* gth = (double*)calloc((size_t)np * nv, sizeof(double));
+    double* lfv = (double*)malloc(sizeof(double) * (size_t)(nv > 0 ? nv : 1));  /* per-voxel loss */
     for (size_t i = 0; i < (size_t)np * nv; ++i) theta[i] = unscale(o, (int)(i / nv), z[i]);
-#pragma omp parallel for reduction(+ : fid) schedule(static) num_threads(o->nthreads > 0 ? o->nthreads : 1)
+#pragma omp parallel for schedule(static) num_threads(o->nthreads > 0 ? o->nthreads : 1)
     for (int v = 0; v < nv; ++v) {
         double th[8], s[512], sb[512], tb[8] = {0};
         for (int k = 0; k < np; ++k) th[k] = theta[(size_t)k * nv + v];
@@ -481,10 +482,14 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
             lf += rv;
             sb[k] = bad ? 0.0 : orc_loss_deriv(o->loss, sk, y, w, sig, o->mse_scale, o->huber_delta) * c->norm;
         }
-        fid += lf;
+        lfv[v] = lf;
         orc_vjp_voxel(c->m, th, b1, sb, tb);
         for (int k = 0; k < np; ++k) gth[(size_t)k * nv + v] = tb[k];
     }
+    /* summed in voxel order: the same state always gives the same loss,
+     * whatever the thread count */
+    for (int v = 0; v < nv; ++v) fid += lfv[v];
+    free(lfv);
     fid *= c->norm;
     double reg = 0.0;
     if (o->n_reg > 0 && o->lambda[0] > 0) { /* spatial_total_variation.m:29 */
