@@ -58,7 +58,7 @@ enum Slot {
     S_CKPT, S_RESF, S_RESM, S_THF, S_THM, S_RLF, S_RLM, S_BLK, S_VOLS, S_GIDX, S_MASK, S_GRID0,
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
-    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_NSLOTS
+    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_NSLOTS
 };
 
 struct gx_context {
@@ -1178,6 +1178,17 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     } else if (!o->x_step) {
         return fail(GX_EINVAL, "MH needs x_step (xStepSize)");
     }
+    int ng = 0;
+    if (o->is_global)
+        for (int q = 0; q < nvar; ++q) ng += o->is_global[q] != 0;
+    if (ng > 0) {
+        // goodman_weare_wglobal_constant's partition check (utils/mcmc.m:462-466)
+        if (o->algorithm != GX_MCMC_ENSEMBLE)
+            return fail(GX_EINVAL, "global parameters need the ensemble (Goodman-Weare) algorithm");
+        if (ng == nvar)
+            return fail(GX_EINVAL, "need at least one local and one global parameter (NND=0, NGlobal=%d)", ng);
+        if (o->global_warmup < 0) return fail(GX_EINVAL, "globalWarmup must be >= 0");
+    }
     int nb = o->burnin < 1 ? (int)std::floor(o->iteration * o->burnin) : (int)o->burnin;
     int ns = mcmc_nsamples(o->iteration, nb, o->thinning);
     int W = o->algorithm == GX_MCMC_ENSEMBLE ? o->nwalker : 1;
@@ -1226,11 +1237,53 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
         if (o->algorithm == GX_MCMC_ENSEMBLE) TRY(wsT(c, S_MC_PART, (size_t)o->repetition * o->iteration * W, &partner));
         p.data = data; p.weights = w; p.b1 = b1; p.x0 = x0; p.shift = shift; p.sum = sum; p.sumsq = sumsq;
         p.posterior = post; p.n_acc = nacc; p.partner = partner;
+        if (ng > 0) {
+            p.ng = ng;
+            p.nnd = nvar - ng;
+            p.global_warmup = o->global_warmup;
+            p.nsteps_g = o->iteration + o->global_warmup;
+            for (int q = 0; q < nvar; ++q) p.is_global[q] = o->is_global[q] != 0;
+            int vpb, block, nbk;
+            size_t smem;
+            gwg_launch_shape(p, o->block_size, &vpb, &block, &nbk, &smem);
+            // one allocation, carved at 256-byte boundaries
+            auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+            size_t o_gs = 0;
+            size_t o_ga = o_gs + al(sizeof(float) * nvar * W);
+            size_t o_sum = o_ga + al(sizeof(int) * W);
+            size_t o_sq = o_sum + al(sizeof(double) * nvar * W);
+            size_t o_na = o_sq + al(sizeof(double) * nvar * W);
+            size_t o_pr = o_na + al(sizeof(unsigned long long));
+            size_t o_zz = o_pr + al(sizeof(float) * nvar * W);
+            size_t o_lu = o_zz + al(sizeof(float) * W);
+            size_t o_ob = o_lu + al(sizeof(float) * W);
+            size_t o_gp = o_ob + al(sizeof(int) * W);
+            size_t o_lpg = o_gp + al(sizeof(int) * (size_t)o->repetition * p.nsteps_g * W);
+            size_t o_part = o_lpg + al(sizeof(double) * (size_t)nv * W);
+            size_t total = o_part + al(sizeof(double) * (size_t)W * nbk);
+            unsigned char* gb;
+            TRY(wsT(c, S_MC_GLOB, total, &gb));
+            p.gstate = reinterpret_cast<float*>(gb + o_gs);
+            p.gacc = reinterpret_cast<int*>(gb + o_ga);
+            p.gsum = reinterpret_cast<double*>(gb + o_sum);
+            p.gsumsq = reinterpret_cast<double*>(gb + o_sq);
+            p.n_gacc = reinterpret_cast<unsigned long long*>(gb + o_na);
+            p.gprop = reinterpret_cast<float*>(gb + o_pr);
+            p.gzz = reinterpret_cast<float*>(gb + o_zz);
+            p.glu = reinterpret_cast<float*>(gb + o_lu);
+            p.goob = reinterpret_cast<int*>(gb + o_ob);
+            p.gpartner = reinterpret_cast<int*>(gb + o_gp);
+            p.lpg = reinterpret_cast<double*>(gb + o_lpg);
+            p.partial = reinterpret_cast<double*>(gb + o_part);
+            CK(cudaMemsetAsync(gb, 0, o_gp, c->stream));  // state, decisions, sums, counter
+        }
         if (partner) CK(launch_mcmc_partners(p, partner, c->stream));
         CK(cudaEventRecord(c->ev[2], c->stream));
         CK(launch_mcmc(p, id, o->block_size, c->stream));
         CK(cudaEventRecord(c->ev[3], c->stream));
-        launches += (o->iteration + 249) / 250 * o->repetition;
+        launches += ng > 0 ? (o->ensemble_update == GX_GW_REDBLACK ? 4 : 2) * (o->iteration + o->global_warmup) *
+                                 o->repetition
+                           : (o->iteration + 249) / 250 * o->repetition;
         float *mean = nullptr, *stdv = nullptr;
         if (mem == GX_MEM_DEVICE) { mean = r.mean; stdv = r.std; }
         else {
@@ -1247,9 +1300,12 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
                 d2h += sizeof(float) * n;
             }
         }
-        unsigned long long acc = 0;
+        unsigned long long acc = 0, gacc = 0;
         CK(cudaMemcpyAsync(&acc, nacc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
+        if (ng > 0) CK(cudaMemcpyAsync(&gacc, p.n_gacc, sizeof(gacc), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
+        r.n_global_accepted = (int64_t)gacc;
+        r.n_global_proposals = ng > 0 ? (int64_t)W * (o->iteration + o->global_warmup) * o->repetition : 0;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
         kernel_ms += ms;

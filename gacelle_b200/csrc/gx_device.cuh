@@ -73,7 +73,12 @@ GX_HD float u01(uint32_t x) { return ((float)(x >> 9) + 0.5f) * (1.0f / 8388608.
 GX_HD uint32_t rand_below(uint32_t x, uint32_t n) { return (uint32_t)(((uint64_t)x * n) >> 32); }
 
 enum RngTag : uint32_t { kTagAdamInit = 1, kTagGwInit = 2, kTagGwMove = 3, kTagGwPerm = 4,
-                         kTagGwRbPart = 5, kTagMhMove = 6 };
+                         kTagGwRbPart = 5, kTagMhMove = 6, kTagGwGPerm = 7, kTagGwGRbPart = 8,
+                         kTagGwGMove = 9, kTagGwGInit = 10 };
+// flag bits above the tag: red-black move, global warm-up step; the
+// repetition index sits in bits 16-31
+constexpr uint32_t kTagRedBlack = 1u << 8;
+constexpr uint32_t kTagWarmup = 1u << 9;
 
 #if defined(__CUDACC__)
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& n0, float& n1) {
@@ -490,6 +495,9 @@ __device__ __forceinline__ float unscale(int transform, float lb, float ub, floa
 // mask, iv[d] = 1/voxel size.  cost = sum_d |f_d - c| iv_d;
 // d cost_total / d c = sum_d (-sgn(f_d - c) + mb_d sgn(c - b_d)) iv_d.
 // One function for every kernel so that all paths round identically.
+// sign(x) in {-1, 0, +1} (0 for +-0), as compare-and-select.
+__device__ __forceinline__ float sgn0(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+
 __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b, const bool* mb,
                                          const float* iv, int nd, float& cost, float& grad) {
     float cs = 0.0f, gr = 0.0f;
@@ -498,8 +506,7 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
         if (d < nd) {
             const float df = f[d] - c;
             cs = __fadd_rn(cs, fabsf(__fmul_rn(df, iv[d])));
-            const float t = -(float)((df > 0.0f) - (df < 0.0f)) +
-                            (mb[d] ? (float)((c - b[d] > 0.0f) - (c - b[d] < 0.0f)) : 0.0f);
+            const float t = -sgn0(df) + (mb[d] ? sgn0(c - b[d]) : 0.0f);
             gr = __fadd_rn(gr, __fmul_rn(t, iv[d]));
         }
     }

@@ -126,8 +126,27 @@ struct McmcParams {
     float* shift;          // [nvar][nvox]
     float* posterior;      // [nvar][rep][ns][W][nvox] or nullptr
     unsigned long long* n_acc;
+    // goodman_weare_wglobal_constant (ng > 0): parameters shared by all voxels
+    int is_global[kMaxParam];
+    int ng, nnd, global_warmup;
+    int nsteps_g;          // rows per repetition of gpartner: iteration + global_warmup
+    float* gstate;         // [nvar][W] current global values (global rows used)
+    int* gacc;             // [W] last global block's decision
+    double* lpg;           // [nvox][W] logP at the global proposal
+    double* partial;       // [W][nblocks] per-CTA sums of logP(proposal) - logP(current)
+    double* gsum;          // [nvar][W] kept global samples, shifted
+    double* gsumsq;
+    const int* gpartner;   // [rep][nsteps_g][W] global-block anchors
+    float* gprop;          // [nvar][W] global proposal of the current block
+    float* gzz;            // [W] its stretch factor
+    float* glu;            // [W] log of its acceptance uniform
+    int* goob;             // [W] proposal outside the bounds
+    unsigned long long* n_gacc;
 };
 cudaError_t launch_mcmc_partners(const McmcParams& p, int* partner, cudaStream_t s);
+// goodman_weare_wglobal_constant launch shape: voxels per CTA, threads, CTAs
+// (= rows of the partial-sum table) and dynamic shared memory.
+void gwg_launch_shape(const McmcParams& p, int block_hint, int* vpb, int* block, int* nblocks, size_t* smem);
 cudaError_t launch_mcmc(const McmcParams& p, int model, int block, cudaStream_t s);
 cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, cudaStream_t s);
 

@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib, utils
-from ._lib import GacelleError, GX_EINVAL, GX_EUNSUPPORTED
+from ._lib import GacelleError, GX_EINVAL
 from .askadam_solver import _model_of
 
 POSTERIOR_LIMIT_BYTES = 1 << 30  # default cap for returning out['posterior']
@@ -84,10 +84,15 @@ class mcmc:
         sizes = model.nparam_nmeas()
         if sizes[0] + 1 != len(names) or sizes[1] != nm:
             raise GacelleError(GX_EINVAL, "modelParams / data size do not match the model")
+        # a start field with one value while another has one per voxel marks a
+        # global parameter: the ensemble sampler becomes
+        # goodman_weare_wglobal_constant (mcmc.m:52-74, check_global_constant :775-785);
+        # Metropolis-Hastings broadcasts the value as the reference's struct2array does
         sizes_glob = [np.size(pars0[p]) for p in names]
-        if any(s == 1 for s in sizes_glob) and any(s > 1 for s in sizes_glob):
-            raise GacelleError(GX_EUNSUPPORTED, "global (shared) parameters "
-                                                "(goodman_weare_wglobal_constant) are not accelerated")
+        is_global = None
+        if fitting["algorithm"].lower() == "ensemble" and any(s == 1 for s in sizes_glob) \
+                and any(s > 1 for s in sizes_glob):
+            is_global = [1 if s == 1 else 0 for s in sizes_glob]
         x0 = np.stack([utils.param_to_GD(pars0[p], mask, idx, nv) for p in names]).astype(np.float32)
         w = None
         if weights is not None and np.size(weights) > 0:
@@ -105,10 +110,10 @@ class mcmc:
         post_bytes = 4 * len(names) * nv * W * ns * int(fitting["repetition"])
         need_post = any(m in metrics for m in ("median", "iqr", "mode"))
         want_post = fitting.get("returnPosterior", post_bytes <= POSTERIOR_LIMIT_BYTES) or need_post
-        res = self._run(model, y, w, x0, b1, names, fitting, want_post)
+        res = self._run(model, y, w, x0, b1, names, fitting, want_post, is_global)
         return self.res2out(res, fitting, mask, names)
 
-    def _run(self, model, y, w, x0, b1, names, fitting, want_post):
+    def _run(self, model, y, w, x0, b1, names, fitting, want_post, is_global=None):
         ctx = self.ctx or _lib.Context.default()
         nvar = len(names)
         nm, nv = y.shape
@@ -135,6 +140,11 @@ class mcmc:
         o.seed = int(fitting.get("seed", model.seed))
         o.block_size = int(fitting.get("blockSize", 0))
         keep = [y, x0]
+        if is_global is not None:
+            ig = np.ascontiguousarray(is_global, dtype=np.int32)
+            keep.append(ig)
+            o.is_global = ig.ctypes.data_as(_lib._i32p)
+            o.global_warmup = int(fitting.get("globalWarmup", 0))
         vol = _lib.GxVolume()
         vol.dims[0], vol.dims[1], vol.dims[2] = nv, 1, 1
         vol.nvox = nv
@@ -159,8 +169,10 @@ class mcmc:
         _lib.check(_lib.lib().gx_mcmc(ctx.ptr, C.byref(model._gx_model().s), _lib.MEM_HOST, C.byref(vol), 1,
                                       C.byref(o), C.byref(r)))
         self.last_timing = ctx.timing()
-        self.last_stats = {"n_accepted": r.n_accepted, "n_proposals": r.n_proposals, "ns": r.ns}
-        return {"mean": mean, "std": std, "posterior": post, "W": W, "ns": ns, "rep": rep}
+        self.last_stats = {"n_accepted": r.n_accepted, "n_proposals": r.n_proposals, "ns": r.ns,
+                           "n_global_accepted": r.n_global_accepted, "n_global_proposals": r.n_global_proposals}
+        return {"mean": mean, "std": std, "posterior": post, "W": W, "ns": ns, "rep": rep,
+                "is_global": list(is_global) if is_global is not None else [0] * nvar}
 
     @staticmethod
     def res2out(res, fitting, mask, names):
@@ -169,11 +181,15 @@ class mcmc:
         out = {}
         post = res["posterior"]
         nv = res["mean"].shape[1]
+        isg = res.get("is_global") or [0] * len(names)
         if post is not None:
-            # [Nv, Nwalker, Ns, rep] per parameter (MH: [Nv, Ns, rep])
+            # [Nv, Nwalker, Ns, rep] per parameter (MH: [Nv, Ns, rep]); a global
+            # parameter keeps a leading dimension of 1 (array2struct_wglobal)
             out["posterior"] = {}
             for k, p in enumerate(names):
                 a = np.transpose(post[k], (3, 2, 1, 0))  # [nv, W, ns, rep]
+                if isg[k]:
+                    a = a[:1]
                 out["posterior"][p] = a[:, 0] if res["W"] == 1 else a
         for m in [m.lower() for m in fitting["metric"]]:
             out[m] = {}
@@ -198,6 +214,10 @@ class mcmc:
                         v = (edges[mi] + edges[mi + 1]) / 2
                     else:
                         raise GacelleError(GX_EINVAL, f"unknown metric {m}")
+                if isg[k]:
+                    # one value for all voxels: a scalar, as reshape_ND2image passes it
+                    out[m][p] = float(np.asarray(v).ravel()[0])
+                    continue
                 out[m][p] = utils.reshape_GD2ND(np.asarray(v, dtype=np.float32), mask).reshape(shape, order="F")
         return out
 
@@ -208,6 +228,13 @@ class mcmc:
         return self._direct(y, x0, weights, f, FWDfunc, varargin)
 
     def goodman_weare(self, y, x0, weights, fitting, FWDfunc, *varargin):
+        f = dict(fitting)
+        f["algorithm"] = "ensemble"
+        return self._direct(y, x0, weights, f, FWDfunc, varargin)
+
+    def goodman_weare_wglobal_constant(self, y, x0, weights, fitting, FWDfunc, *varargin):
+        """Direct entry of the global-parameter sampler (utils/mcmc.m:385): the
+        fields of x0 with one value are the global parameters."""
         f = dict(fitting)
         f["algorithm"] = "ensemble"
         return self._direct(y, x0, weights, f, FWDfunc, varargin)

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define GX_ABI_VERSION 1
+#define GX_ABI_VERSION 2
 
 typedef enum {
     GX_OK = 0,
@@ -181,6 +181,14 @@ typedef struct {
     const double* ub;           /* [nvar] */
     uint64_t seed;
     int32_t block_size;         /* 0 = auto */
+    /* goodman_weare_wglobal_constant (utils/mcmc.m:385-626), chosen by the
+     * reference when a start field has one value for all voxels: nonzero
+     * entries mark parameters shared by all voxels of a volume (one value per
+     * walker; their start is drawn uniformly over [lb, ub]).  Needs the
+     * ensemble algorithm and at least one local and one global parameter.
+     * NULL: every parameter is per voxel. */
+    const int32_t* is_global;   /* [nvar] or NULL */
+    int32_t global_warmup;      /* global-only iterations before the joint loop */
 } gx_mcmc_opts;
 
 typedef struct {
@@ -189,6 +197,10 @@ typedef struct {
     float* posterior;           /* [nvar][rep][ns][nwalker][nvox] or NULL */
     int64_t n_accepted, n_proposals;
     int32_t ns;                 /* kept samples per walker and repetition */
+    /* global block of goodman_weare_wglobal_constant (walker moves); the
+     * statistics and posterior of a global parameter repeat its value for
+     * every voxel */
+    int64_t n_global_accepted, n_global_proposals;
 } gx_mcmc_result;
 
 /* Device-side timing of the last compute call on a context (CUDA events on

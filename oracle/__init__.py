@@ -71,7 +71,8 @@ class OrcMcmcOpts(C.Structure):
                 ("burnin", C.c_double), ("repetition", C.c_int), ("nwalker", C.c_int),
                 ("step_size", C.c_double), ("start_range", C.c_double),
                 ("ensemble_update", C.c_int), ("x_step", _dp), ("lb", _dp), ("ub", _dp),
-                ("seed", C.c_uint64), ("nthreads", C.c_int)]
+                ("seed", C.c_uint64), ("nthreads", C.c_int), ("is_global", _ip),
+                ("global_warmup", C.c_int)]
 
 
 class OrcMcmcResult(C.Structure):
@@ -359,23 +360,30 @@ def model_gradient(model: Model, vol: Volume, opts: OrcAdamOpts, theta):
 def mcmc(model: Model, vol: Volume, x0, lb, ub, algorithm="ensemble", iteration=1000,
          thinning=10, burnin=0.1, repetition=1, nwalker=16, step_size=2.0, start_range=0.001,
          ensemble_update="simultaneous", x_step=None, seed=0, want_posterior=False,
-         nthreads=None):
+         nthreads=None, is_global=None, global_warmup=0):
+    """is_global [nvar] (nonzero: one value per walker shared by all voxels)
+    selects goodman_weare_wglobal_constant (utils/mcmc.m:385-626)."""
     x0 = _f64(x0)
     nvar, nv = x0.shape
     lb = _f64(lb)
     ub = _f64(ub)
     xs = _f64(x_step if x_step is not None else np.zeros(nvar))
+    ig = None if is_global is None else np.ascontiguousarray(is_global, dtype=np.int32)
     o = OrcMcmcOpts(1 if algorithm == "ensemble" else 0, iteration, thinning, burnin, repetition,
                     nwalker, step_size, start_range,
                     1 if ensemble_update == "redblack" else 0, _d(xs), _d(lb), _d(ub), seed,
-                    nthreads or os.cpu_count() or 1)
+                    nthreads or os.cpu_count() or 1,
+                    None if ig is None else ig.ctypes.data_as(_ip), int(global_warmup))
     ns = lib().orc_mcmc_nsamples(iteration, burnin, thinning)
     W = nwalker if algorithm == "ensemble" else 1
     mean = np.zeros((nvar, nv))
     std = np.zeros((nvar, nv))
     post = np.zeros(nvar * nv * W * ns * repetition, dtype=np.float32) if want_posterior else None
     r = OrcMcmcResult(_d(mean), _d(std), None if post is None else post.ctypes.data_as(_fp), 0, 0, 0)
-    lib().orc_mcmc(C.byref(model.s), C.byref(vol.s), _d(x0), C.byref(o), C.byref(r))
+    st = lib().orc_mcmc(C.byref(model.s), C.byref(vol.s), _d(x0), C.byref(o), C.byref(r))
+    if st != 0:
+        raise ValueError("global parameters need the ensemble algorithm and at least one local "
+                         "and one global parameter")
     out = {"mean": mean, "std": std, "n_accepted": r.n_accepted, "n_proposals": r.n_proposals,
            "ns": r.ns}
     if post is not None:

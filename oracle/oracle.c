@@ -50,7 +50,12 @@ static uint32_t rand_below(uint32_t x, uint32_t n) { return (uint32_t)(((uint64_
 
 /* Random-stream tags (4th counter word, low byte). */
 enum { TAG_ADAM_INIT = 1, TAG_GW_INIT = 2, TAG_GW_MOVE = 3, TAG_GW_PERM = 4,
-       TAG_GW_RBPART = 5, TAG_MH_MOVE = 6 };
+       TAG_GW_RBPART = 5, TAG_MH_MOVE = 6, TAG_GW_GPERM = 7, TAG_GW_GRBPART = 8,
+       TAG_GW_GMOVE = 9, TAG_GW_GINIT = 10 };
+/* flag bits above the tag: red-black move (1<<8), global warm-up step (1<<9);
+ * the repetition index sits in bits 16-31 */
+#define TAG_RB (1u << 8)
+#define TAG_WARM (1u << 9)
 
 static void philox_call(uint64_t seed, uint32_t a, uint32_t b, uint32_t c, uint32_t d,
                         uint32_t out[4]) {
@@ -742,14 +747,13 @@ static int nburnin(const orc_mcmc_opts* o) {
 
 /* find_partner (mcmc.m:797-803): uniform random derangement, one per step,
  * shared by all voxels.  Fisher-Yates with rejection of fixed points. */
-void orc_gw_partner(uint64_t seed, int step, int rep, int W, int* p) {
+static void derangement(uint64_t seed, int step, uint32_t tag, int W, int* p) {
     for (uint32_t attempt = 0; attempt < 4096; ++attempt) {
         for (int i = 0; i < W; ++i) p[i] = i;
         uint32_t u[4];
         for (int i = W - 1, d = 0; i >= 1; --i, ++d) {
             if ((d & 3) == 0)
-                philox_call(seed, (uint32_t)step, attempt, (uint32_t)(d >> 2),
-                            TAG_GW_PERM | ((uint32_t)rep << 16), u);
+                philox_call(seed, (uint32_t)step, attempt, (uint32_t)(d >> 2), tag, u);
             int j = (int)rand_below(u[d & 3], (uint32_t)(i + 1));
             int t = p[i]; p[i] = p[j]; p[j] = t;
         }
@@ -760,16 +764,22 @@ void orc_gw_partner(uint64_t seed, int step, int rep, int W, int* p) {
     for (int i = 0; i < W; ++i) p[i] = (i + 1) % W; /* unreachable in practice */
 }
 
+void orc_gw_partner(uint64_t seed, int step, int rep, int W, int* p) {
+    derangement(seed, step, TAG_GW_PERM | ((uint32_t)rep << 16), W, p);
+}
+
 /* Red-black anchor draw (mcmc.m:328-329): for half-step s, the partner of
  * the a-th active walker is frozen[randi(numel(frozen))], shared by voxels. */
-static void rb_partner(uint64_t seed, int step, int rep, int half, int na, int nf, int* out) {
+static void rb_partner_tag(uint64_t seed, int step, uint32_t tag, int half, int na, int nf, int* out) {
     uint32_t u[4];
     for (int a = 0; a < na; ++a) {
-        if ((a & 3) == 0)
-            philox_call(seed, (uint32_t)step, (uint32_t)half, (uint32_t)(a >> 2),
-                        TAG_GW_RBPART | ((uint32_t)rep << 16), u);
+        if ((a & 3) == 0) philox_call(seed, (uint32_t)step, (uint32_t)half, (uint32_t)(a >> 2), tag, u);
         out[a] = (int)rand_below(u[a & 3], (uint32_t)nf);
     }
+}
+
+static void rb_partner(uint64_t seed, int step, int rep, int half, int na, int nf, int* out) {
+    rb_partner_tag(seed, step, TAG_GW_RBPART | ((uint32_t)rep << 16), half, na, nf, out);
 }
 
 typedef struct {
@@ -794,8 +804,16 @@ static double logp(const mc_ctx* c, int v, const double* x) {
     return -sos / (2.0 * noise * noise) - c->nm / 2.0 * log(2.0 * M_PI * noise * noise);
 }
 
+static int mcmc_gw_global(const orc_model* m, const orc_volume* vol, const double* x0,
+                          const orc_mcmc_opts* o, orc_mcmc_result* r);
+
 int orc_mcmc(const orc_model* m, const orc_volume* vol, const double* x0,
              const orc_mcmc_opts* o, orc_mcmc_result* r) {
+    if (o->is_global) {
+        int any = 0;
+        for (int p = 0; p < orc_nparams(m) + 1; ++p) any |= o->is_global[p] != 0;
+        if (any) return o->algorithm == 1 ? mcmc_gw_global(m, vol, x0, o, r) : -1;
+    }
     mc_ctx c = {m, vol, orc_nmeas(m), orc_nparams(m), orc_nparams(m) + 1};
     int nvar = c.nvar, nv = vol->nvox;
     int W = o->algorithm == 1 ? o->nwalker : 1;
@@ -990,5 +1008,286 @@ int orc_mcmc(const orc_model* m, const orc_volume* vol, const double* x0,
     r->n_proposals = prop_total;
     free(perm);
     free(rbp);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* goodman_weare_wglobal_constant (utils/mcmc.m:385-578) with gw_global_block */
+/* (:581-626): parameters split into local (per voxel) and global (shared by */
+/* all voxels, one value per walker).  Each iteration is a local stretch move */
+/* with the globals held (exponent z^(NND-1)), then a global stretch move with */
+/* the locals held, accepted on the log-likelihood difference summed over all */
+/* voxels in double (exponent z^(NGlobal-1)).  Locals start at x0 +          */
+/* (ub-lb)*startRange*randn (clamped), globals uniformly over their bounds;   */
+/* every repetition restarts from those walkers; globalWarmup global-only     */
+/* iterations precede the joint loop.  The voxel sum runs in voxel order.     */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    const mc_ctx* c;
+    const orc_mcmc_opts* o;
+    int nv, W, nvar, ng, nnd;
+    const int* isg;
+    double* x;     /* [nv][W][nvar] local slots used */
+    double* g;     /* [W][nvar] global slots used */
+    double* lp;    /* [nv][W] cached logP at the current state */
+    double* lpg;   /* [nv][W] logP of the global proposal */
+} gwg_state;
+
+static double gwg_logp(const gwg_state* S, int v, int w, const double* gw) {
+    double xx[8];
+    for (int p = 0; p < S->nvar; ++p)
+        xx[p] = S->isg[p] ? gw[p] : S->x[((size_t)v * S->W + w) * S->nvar + p];
+    return logp(S->c, v, xx);
+}
+
+/* One global block (gw_global_block): the walkers of `act` (na of them)
+ * propose around anchors `anc`; returns accepted count. */
+static long long gwg_global_sub(gwg_state* S, int k, uint32_t tagbits, const int* act, const int* anc, int na) {
+    const orc_mcmc_opts* o = S->o;
+    int W = S->W, nvar = S->nvar, nv = S->nv;
+    double* gp = (double*)malloc(sizeof(double) * (size_t)na * nvar);
+    int* oob = (int*)calloc((size_t)na, sizeof(int));
+    double* zz = (double*)malloc(sizeof(double) * (size_t)na);
+    double* lu = (double*)malloc(sizeof(double) * (size_t)na);
+    for (int i = 0; i < na; ++i) {
+        int w = act[i], q = anc[i];
+        uint32_t u[4];
+        philox_call(o->seed, (uint32_t)w, (uint32_t)k, 0u, TAG_GW_GMOVE | tagbits, u);
+        double a = o->step_size;
+        double t = (a - 1.0) * orc_u01(u[0]) + 1.0;
+        zz[i] = t * t / a;
+        lu[i] = log(orc_u01(u[1]));
+        for (int p = 0; p < nvar; ++p) {
+            if (!S->isg[p]) { gp[(size_t)i * nvar + p] = 0.0; continue; }
+            double gq = S->g[(size_t)q * nvar + p];
+            double val = gq + (S->g[(size_t)w * nvar + p] - gq) * zz[i];
+            oob[i] |= (val < o->lb[p]) || (val > o->ub[p]);
+            gp[(size_t)i * nvar + p] = fmin(fmax(val, o->lb[p]), o->ub[p]);
+        }
+    }
+#pragma omp parallel for schedule(static) num_threads(o->nthreads > 0 ? o->nthreads : 1)
+    for (int v = 0; v < nv; ++v)
+        for (int i = 0; i < na; ++i)
+            S->lpg[(size_t)v * W + act[i]] = gwg_logp(S, v, act[i], gp + (size_t)i * nvar);
+    long long nacc = 0;
+    for (int i = 0; i < na; ++i) {
+        int w = act[i];
+        double d = 0.0;
+        for (int v = 0; v < nv; ++v) d += S->lpg[(size_t)v * W + w] - S->lp[(size_t)v * W + w];
+        double lr = (S->ng - 1) * log(zz[i]) + d;
+        if (!oob[i] && lr > lu[i]) {
+            ++nacc;
+            for (int p = 0; p < nvar; ++p)
+                if (S->isg[p]) S->g[(size_t)w * nvar + p] = gp[(size_t)i * nvar + p];
+            for (int v = 0; v < nv; ++v) S->lp[(size_t)v * W + w] = S->lpg[(size_t)v * W + w];
+        }
+    }
+    free(gp); free(oob); free(zz); free(lu);
+    return nacc;
+}
+
+static void gwg_global_block(gwg_state* S, int k, int rr, int warm) {
+    const orc_mcmc_opts* o = S->o;
+    int W = S->W;
+    uint32_t bits = ((uint32_t)rr << 16) | (warm ? TAG_WARM : 0u);
+    int act[256], anc[256];
+    if (o->ensemble_update == ORC_GW_SIMULTANEOUS) {
+        int pt[256];
+        derangement(o->seed, k, TAG_GW_GPERM | bits, W, pt);
+        for (int w = 0; w < W; ++w) { act[w] = w; anc[w] = pt[w]; }
+        gwg_global_sub(S, k, bits, act, anc, W);
+    } else {
+        int h = W / 2;
+        for (int s = 0; s < 2; ++s) {
+            int a0 = s == 0 ? 0 : h, na = s == 0 ? h : W - h, f0 = s == 0 ? h : 0, nf = s == 0 ? W - h : h;
+            int pb[256];
+            rb_partner_tag(o->seed, k, TAG_GW_GRBPART | bits, s, na, nf, pb);
+            for (int i = 0; i < na; ++i) { act[i] = a0 + i; anc[i] = f0 + pb[i]; }
+            gwg_global_sub(S, k, bits | TAG_RB, act, anc, na);
+        }
+    }
+}
+
+static int mcmc_gw_global(const orc_model* m, const orc_volume* vol, const double* x0,
+                          const orc_mcmc_opts* o, orc_mcmc_result* r) {
+    mc_ctx c = {m, vol, orc_nmeas(m), orc_nparams(m), orc_nparams(m) + 1};
+    int nvar = c.nvar, nv = vol->nvox, W = o->nwalker, rep = o->repetition;
+    int nb = nburnin(o);
+    int ns = orc_mcmc_nsamples(o->iteration, o->burnin, o->thinning);
+    r->ns = ns;
+    int ng = 0;
+    for (int p = 0; p < nvar; ++p) ng += o->is_global[p] != 0;
+    if (ng == 0 || ng == nvar) return -2;
+    gwg_state S = {&c, o, nv, W, nvar, ng, nvar - ng, o->is_global, NULL, NULL, NULL, NULL};
+    size_t nx = (size_t)nv * W * nvar;
+    double* xi = (double*)malloc(sizeof(double) * nx);
+    double* gi = (double*)calloc((size_t)W * nvar, sizeof(double));
+    double* lpi = (double*)malloc(sizeof(double) * (size_t)nv * W);
+    S.x = (double*)malloc(sizeof(double) * nx);
+    S.g = (double*)malloc(sizeof(double) * (size_t)W * nvar);
+    S.lp = (double*)malloc(sizeof(double) * (size_t)nv * W);
+    S.lpg = (double*)malloc(sizeof(double) * (size_t)nv * W);
+    double* sum = (double*)calloc((size_t)nvar * nv, sizeof(double));
+    double* sumsq = (double*)calloc((size_t)nvar * nv, sizeof(double));
+    double* shift = (double*)malloc(sizeof(double) * (size_t)nvar * nv);
+    for (int p = 0; p < nvar; ++p)
+        for (int v = 0; v < nv; ++v)
+            shift[(size_t)p * nv + v] = fmin(fmax(x0[(size_t)p * nv + (o->is_global[p] ? 0 : v)], o->lb[p]), o->ub[p]);
+    /* walker start: locals as in goodman_weare (same stream), globals uniform */
+    for (int v = 0; v < nv; ++v)
+        for (int w = 0; w < W; ++w) {
+            double nrm[8];
+            for (int j = 0; j * 4 < nvar; ++j) {
+                uint32_t u[4];
+                philox_call(o->seed, (uint32_t)v, (uint32_t)w, (uint32_t)j, TAG_GW_INIT, u);
+                double a, b, cc, d;
+                box_muller(u[0], u[1], &a, &b);
+                box_muller(u[2], u[3], &cc, &d);
+                double q[4] = {a, b, cc, d};
+                for (int t = 0; t < 4 && 4 * j + t < nvar; ++t) nrm[4 * j + t] = q[t];
+            }
+            for (int p = 0; p < nvar; ++p) {
+                double val = 0.0;
+                if (!o->is_global[p]) {
+                    val = x0[(size_t)p * nv + v] + (o->ub[p] - o->lb[p]) * o->start_range * nrm[p];
+                    val = fmin(fmax(val, o->lb[p]), o->ub[p]);
+                }
+                xi[((size_t)v * W + w) * nvar + p] = val;
+            }
+        }
+    for (int w = 0; w < W; ++w)
+        for (int p = 0; p < nvar; ++p)
+            if (o->is_global[p]) {
+                uint32_t u[4];
+                philox_call(o->seed, (uint32_t)w, (uint32_t)(p >> 2), 0u, TAG_GW_GINIT, u);
+                gi[(size_t)w * nvar + p] = o->lb[p] + (o->ub[p] - o->lb[p]) * orc_u01(u[p & 3]);
+            }
+    memcpy(S.x, xi, sizeof(double) * nx);
+    memcpy(S.g, gi, sizeof(double) * (size_t)W * nvar);
+#pragma omp parallel for schedule(static) num_threads(o->nthreads > 0 ? o->nthreads : 1)
+    for (int v = 0; v < nv; ++v)
+        for (int w = 0; w < W; ++w) lpi[(size_t)v * W + w] = gwg_logp(&S, v, w, gi + (size_t)w * nvar);
+
+    long long acc_total = 0, prop_total = 0;
+    int h = W / 2;
+    int* pt = (int*)malloc(sizeof(int) * (size_t)W);
+    for (int rr = 0; rr < rep; ++rr) {
+        memcpy(S.x, xi, sizeof(double) * nx);
+        memcpy(S.g, gi, sizeof(double) * (size_t)W * nvar);
+        memcpy(S.lp, lpi, sizeof(double) * (size_t)nv * W);
+        for (int kw = 1; kw <= o->global_warmup; ++kw) gwg_global_block(&S, kw, rr, 1);
+        int counter = 0;
+        for (int k = 1; k <= o->iteration; ++k) {
+            /* LOCAL block, globals held (mcmc.m:515-553) */
+            if (o->ensemble_update == ORC_GW_SIMULTANEOUS) {
+                orc_gw_partner(o->seed, k, rr, W, pt);
+            }
+            long long acc = 0;
+#pragma omp parallel for schedule(static) reduction(+ : acc) num_threads(o->nthreads > 0 ? o->nthreads : 1)
+            for (int v = 0; v < nv; ++v) {
+                double* xv = S.x + (size_t)v * W * nvar;
+                double xo[256 * 8];
+                if (o->ensemble_update == ORC_GW_SIMULTANEOUS) {
+                    memcpy(xo, xv, sizeof(double) * W * nvar);
+                    for (int w = 0; w < W; ++w) {
+                        uint32_t u[4];
+                        philox_call(o->seed, (uint32_t)v, (uint32_t)w, (uint32_t)k, TAG_GW_MOVE | ((uint32_t)rr << 16), u);
+                        double a = o->step_size, t = (a - 1.0) * orc_u01(u[0]) + 1.0, zz = t * t / a;
+                        double xp[8];
+                        int oob = 0;
+                        for (int p = 0; p < nvar; ++p) {
+                            if (o->is_global[p]) { xp[p] = S.g[(size_t)w * nvar + p]; continue; }
+                            double xq = xo[pt[w] * nvar + p];
+                            double val = xq + (xo[w * nvar + p] - xq) * zz;
+                            oob |= (val < o->lb[p]) || (val > o->ub[p]);
+                            xp[p] = fmin(fmax(val, o->lb[p]), o->ub[p]);
+                        }
+                        double lpp = logp(&c, v, xp);
+                        double lr = (S.nnd - 1) * log(zz) + (lpp - S.lp[(size_t)v * W + w]);
+                        if (!oob && lr > log(orc_u01(u[1]))) {
+                            for (int p = 0; p < nvar; ++p)
+                                if (!o->is_global[p]) xv[w * nvar + p] = xp[p];
+                            S.lp[(size_t)v * W + w] = lpp;
+                            ++acc;
+                        }
+                    }
+                } else {
+                    int pb[256];
+                    for (int s = 0; s < 2; ++s) {
+                        int a0 = s == 0 ? 0 : h, na = s == 0 ? h : W - h, f0 = s == 0 ? h : 0, nf = s == 0 ? W - h : h;
+                        rb_partner(o->seed, k, rr, s, na, nf, pb);
+                        for (int i = 0; i < na; ++i) {
+                            int w = a0 + i, q = f0 + pb[i];
+                            uint32_t u[4];
+                            philox_call(o->seed, (uint32_t)v, (uint32_t)w, (uint32_t)k,
+                                        TAG_GW_MOVE | ((uint32_t)rr << 16) | TAG_RB, u);
+                            double a = o->step_size, t = (a - 1.0) * orc_u01(u[0]) + 1.0, zz = t * t / a;
+                            double xp[8];
+                            int oob = 0;
+                            for (int p = 0; p < nvar; ++p) {
+                                if (o->is_global[p]) { xp[p] = S.g[(size_t)w * nvar + p]; continue; }
+                                double xq = xv[q * nvar + p];
+                                double val = xq + (xv[w * nvar + p] - xq) * zz;
+                                oob |= (val < o->lb[p]) || (val > o->ub[p]);
+                                xp[p] = fmin(fmax(val, o->lb[p]), o->ub[p]);
+                            }
+                            double lpp = logp(&c, v, xp);
+                            double lr = (S.nnd - 1) * log(zz) + (lpp - S.lp[(size_t)v * W + w]);
+                            if (!oob && lr > log(orc_u01(u[1]))) {
+                                for (int p = 0; p < nvar; ++p) xo[w * nvar + p] = o->is_global[p] ? 0.0 : xp[p];
+                                S.lp[(size_t)v * W + w] = lpp;
+                                ++acc;
+                            } else {
+                                memcpy(xo + w * nvar, xv + w * nvar, sizeof(double) * nvar);
+                            }
+                        }
+                        for (int i = 0; i < na; ++i)
+                            memcpy(xv + (a0 + i) * nvar, xo + (a0 + i) * nvar, sizeof(double) * nvar);
+                    }
+                }
+            }
+            acc_total += acc;
+            prop_total += (long long)nv * W;
+            /* GLOBAL block, locals held (mcmc.m:555-558, 581-626) */
+            gwg_global_block(&S, k, rr, 0);
+            /* thinning / burn-in (mcmc.m:560-565) */
+            if (k > nb && (k - nb + 1) % o->thinning == 0 && counter < ns) {
+                for (int v = 0; v < nv; ++v)
+                    for (int w = 0; w < W; ++w)
+                        for (int p = 0; p < nvar; ++p) {
+                            double val = o->is_global[p] ? S.g[(size_t)w * nvar + p]
+                                                         : S.x[((size_t)v * W + w) * nvar + p];
+                            double d = val - shift[(size_t)p * nv + v];
+                            sum[(size_t)p * nv + v] += d;
+                            sumsq[(size_t)p * nv + v] += d * d;
+                            if (r->posterior) {
+                                size_t idx = (size_t)v + (size_t)nv * (w + (size_t)W * (counter + (size_t)ns * rr));
+                                r->posterior[(size_t)p * nv * W * ns * rep + idx] = (float)val;
+                            }
+                        }
+                ++counter;
+            }
+        }
+        int missing = ns - counter;
+        for (int p = 0; p < nvar; ++p)
+            for (int v = 0; v < nv; ++v) {
+                double d = 0.0 - shift[(size_t)p * nv + v];
+                sum[(size_t)p * nv + v] += (double)missing * W * d;
+                sumsq[(size_t)p * nv + v] += (double)missing * W * d * d;
+            }
+    }
+    double nsample = (double)W * ns * rep;
+    for (int p = 0; p < nvar; ++p)
+        for (int v = 0; v < nv; ++v) {
+            size_t i = (size_t)p * nv + v;
+            double md = sum[i] / nsample;
+            double var = nsample > 1 ? (sumsq[i] - sum[i] * md) / (nsample - 1.0) : 0.0;
+            if (r->mean) r->mean[i] = shift[i] + md;
+            if (r->std) r->std[i] = sqrt(fmax(var, 0.0));
+        }
+    r->n_accepted = acc_total;
+    r->n_proposals = prop_total;
+    free(xi); free(gi); free(lpi); free(S.x); free(S.g); free(S.lp); free(S.lpg);
+    free(sum); free(sumsq); free(shift); free(pt);
     return 0;
 }

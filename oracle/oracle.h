@@ -153,6 +153,9 @@ typedef struct {
     const double* ub;            /* [nvar] */
     uint64_t seed;
     int nthreads;
+    const int* is_global;        /* [nvar] or NULL: nonzero = shared by all voxels
+                                  * (goodman_weare_wglobal_constant) */
+    int global_warmup;           /* global-only iterations before the joint loop */
 } orc_mcmc_opts;
 
 typedef struct {
@@ -163,7 +166,9 @@ typedef struct {
     int ns;
 } orc_mcmc_result;
 
-/* nvar = orc_nparams + 1 (noise last).  x0 [nvar][nvox]. */
+/* nvar = orc_nparams + 1 (noise last).  x0 [nvar][nvox].  With is_global
+ * set (ensemble only), mean/std/posterior of a global parameter hold its value
+ * for every voxel; returns -2 when there is no local or no global parameter. */
 int orc_mcmc(const orc_model* m, const orc_volume* vol, const double* x0,
              const orc_mcmc_opts* o, orc_mcmc_result* r);
 int orc_mcmc_nsamples(int iteration, double burnin, int thinning);

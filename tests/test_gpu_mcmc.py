@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="ensemble", iteration=1000, thinning=10, burnin=0.1,
                  repetition=1, nwalker=16, step_size=2.0, start_range=0.001, update="simultaneous",
-                 x_step=None, seed=7, posterior=True, weights=None):
+                 x_step=None, seed=7, posterior=True, weights=None, is_global=None, global_warmup=0):
     nvar, nv = x0.shape
     y = np.ascontiguousarray(y, np.float32)
     x0 = np.ascontiguousarray(x0, np.float32)
@@ -34,6 +34,11 @@ def _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="ensemble", iteration=1000, 
                         nwalker, step_size, start_range, 1 if update == "redblack" else 0,
                         xs.ctypes.data_as(_lib._dp), lb.ctypes.data_as(_lib._dp), ub.ctypes.data_as(_lib._dp),
                         seed, 0)
+    ig = None
+    if is_global is not None:
+        ig = np.ascontiguousarray(is_global, np.int32)
+        o.is_global = ig.ctypes.data_as(_lib._i32p)
+        o.global_warmup = global_warmup
     ns = oracle.lib().orc_mcmc_nsamples(iteration, burnin, thinning)
     W = nwalker if algorithm == "ensemble" else 1
     vol = _lib.GxVolume()
@@ -54,7 +59,8 @@ def _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="ensemble", iteration=1000, 
         r.posterior = post.ctypes.data_as(_lib._fp)
     _lib.check(_lib.lib().gx_mcmc(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, C.byref(vol), 1, C.byref(o), C.byref(r)))
     return {"mean": mean, "std": std, "posterior": post, "n_accepted": r.n_accepted,
-            "n_proposals": r.n_proposals, "ns": r.ns}
+            "n_proposals": r.n_proposals, "ns": r.ns, "n_global_accepted": r.n_global_accepted,
+            "n_global_proposals": r.n_global_proposals}
 
 
 def _r2s_problem(nv, seed, sigma=0.02):
@@ -148,3 +154,78 @@ def test_gw_nexi_moments(ctx):
     orc_b = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
                         **dict(kw, seed=kw["seed"] + 1))
     _moments_agree(eng, orc, orc_b, 4)
+
+
+# ------------------------------------------- goodman_weare_wglobal_constant ----
+def _shared_r2s_problem(nv, seed, sigma=0.05):
+    """Voxels with their own M0 sharing R2* = 35 /s and the noise sigma."""
+    rng = np.random.default_rng(seed)
+    gxm, om = models("r2s")
+    m0 = rng.uniform(0.8, 1.2, nv)
+    th = np.vstack([m0, np.full(nv, 35.0)])
+    s = oracle.forward(om, th)
+    y = (s + sigma * rng.standard_normal(s.shape)).astype(np.float32)
+    x0 = np.vstack([m0, np.full(nv, 30.0), np.full(nv, sigma)]).astype(np.float32)
+    return gxm, om, y, x0, [0.0, 0.1, 0.02], [2.0, 200.0, 0.12]
+
+
+@pytest.mark.parametrize("update", ["simultaneous", "redblack"])
+def test_gw_global_random_streams_match_oracle(ctx, update):
+    """Global-parameter sampler (utils/mcmc.m:385-626): the device and the FP64
+    oracle draw the local moves, the global partners, stretch factors and
+    accept tests from the same streams, so the first steps coincide (locals
+    per voxel and walker, globals per walker), warm-up included."""
+    gxm, om, y, x0, lb, ub = _shared_r2s_problem(64, 30)
+    kw = dict(iteration=12, thinning=1, burnin=0.0, nwalker=16, seed=8, start_range=0.05)
+    eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, update=update, is_global=[0, 1, 1], global_warmup=3, **kw)
+    orc = oracle.mcmc(om, oracle.Volume(y.astype(np.float64)), x0.astype(np.float64), lb, ub,
+                      algorithm="ensemble", ensemble_update=update, want_posterior=True,
+                      is_global=[0, 1, 1], global_warmup=3, **kw)
+    pe, po = eng["posterior"], orc["posterior"]
+    same = np.abs(pe - po) <= 1e-4 * np.abs(po) + 1e-7
+    assert same.mean() > 0.97, same.mean()
+    # a global parameter has one value per walker: the same for every voxel
+    assert np.ptp(pe[1], axis=-1).max() == 0 and np.ptp(pe[2], axis=-1).max() == 0
+    assert eng["n_global_proposals"] == 16 * (12 + 3)
+    assert abs(eng["n_accepted"] - orc["n_accepted"]) <= 0.01 * orc["n_proposals"]
+
+
+@pytest.mark.parametrize("update", ["simultaneous", "redblack"])
+def test_gw_global_posterior_known_answer(ctx, update):
+    """Through the C-ABI: four voxels with their own M0 sharing R2* and sigma;
+    the posterior mean/std of the shared parameters match quadrature of the
+    exact marginal posterior (flat priors on the bounds)."""
+    import test_oracle
+    om, y = test_oracle._gw_global_problem()
+    gxm, _ = models("r2s")
+    nv = y.shape[1]
+    x0 = np.vstack([np.ones(nv), np.full(nv, 30.0), np.full(nv, 0.05)])
+    lb, ub = [0.0, 0.1, 0.02], [2.0, 200.0, 0.12]
+    eng = _engine_mcmc(ctx, gxm, y, x0, lb, ub, iteration=8000, thinning=2, burnin=0.2, nwalker=32, seed=5,
+                       update=update, start_range=0.05, is_global=[0, 1, 1], global_warmup=20, posterior=False)
+    mean, std = test_oracle._global_posterior_grid(y)
+    for k, q in ((1, 0), (2, 1)):
+        assert np.ptp(eng["mean"][k]) == 0 and np.ptp(eng["std"][k]) == 0
+        assert abs(eng["mean"][k][0] - mean[q]) < 0.1 * std[q], (k, eng["mean"][k][0], mean[q], std[q])
+        assert eng["std"][k][0] == pytest.approx(std[q], rel=0.06)
+
+
+def test_gw_global_through_mirror_returns_scalars(ctx):
+    """mcmc().optimisation with a scalar start field (the reference's cue for
+    a global parameter): the statistics of a global come back as scalars and
+    its posterior has a leading dimension of 1."""
+    from gacelle_b200 import gpuR2starMapping, mcmc_solver
+    gxm, om, y, x0, lb, ub = _shared_r2s_problem(50, 31)
+    te = np.arange(2.0, 40.6, 3.5) * 1e-3
+    model = gpuR2starMapping(te)
+    mask = np.ones((50, 1, 1), dtype=bool)
+    data = y.T.reshape(50, 1, 1, 12)
+    pars0 = {"M0": x0[0].reshape(50, 1, 1), "R2star": 30.0, "noise": 0.05}
+    fit = {"algorithm": "GW", "iteration": 400, "thinning": 2, "burnin": 0.25, "Nwalker": 16,
+           "lb": lb, "ub": ub, "modelParams": ["M0", "R2star", "noise"], "metric": ["mean", "std", "median"],
+           "startRange": 0.05, "globalWarmup": 5, "seed": 3}
+    out = mcmc_solver.mcmc(ctx).optimisation(data, mask, None, pars0, fit, model)
+    assert isinstance(out["mean"]["R2star"], float) and isinstance(out["median"]["noise"], float)
+    assert out["mean"]["M0"].shape == (50, 1, 1)
+    assert out["posterior"]["R2star"].shape[0] == 1 and out["posterior"]["M0"].shape[0] == 50
+    assert 25.0 < out["mean"]["R2star"] < 45.0

@@ -356,3 +356,65 @@ def test_gw_pinned_parameter_keeps_reference_exponent():
     mean, std = _posterior_grid(y, lb, ub, False)
     assert abs(r["mean"][0].mean() - mean[0]) < 0.2 * std[0]
     assert r["std"][0].mean() > 1.08 * std[0]
+
+
+def _gw_global_problem(nv=4, seed=21):
+    om = oracle.r2s(TE)
+    rng = np.random.default_rng(seed)
+    m0 = np.linspace(0.8, 1.2, nv)
+    y = oracle.forward(om, np.vstack([m0, np.full(nv, 35.0)])) + 0.05 * rng.standard_normal((12, nv))
+    return om, y
+
+
+def _global_posterior_grid(y):
+    """Marginal posterior of the shared (R2*, sigma) with each voxel's M0
+    integrated out on its own grid; flat priors on the bounds."""
+    g0 = np.linspace(0.5, 1.5, 201)
+    g1 = np.linspace(15, 55, 161)
+    g2 = np.linspace(0.02, 0.12, 101)
+    E = np.exp(-TE[None, :] * g1[:, None])                       # [R2, m]
+    logI = np.zeros((g1.size, g2.size))
+    for u in range(y.shape[1]):
+        s = g0[:, None, None] * E[None, :, :]                    # [M0, R2, m]
+        sos = np.sum((s - y[None, None, :, u]) ** 2, axis=-1)    # [M0, R2]
+        lL = -sos[:, :, None] / (2 * g2[None, None, :] ** 2) - 12 * np.log(g2)[None, None, :]
+        mx = lL.max(axis=0)
+        logI += mx + np.log(np.exp(lL - mx).sum(axis=0))
+    p = np.exp(logI - logI.max())
+    p /= p.sum()
+    R, S = np.meshgrid(g1, g2, indexing="ij")
+    mean = [np.sum(p * R), np.sum(p * S)]
+    std = [np.sqrt(np.sum(p * (R - mean[0]) ** 2)), np.sqrt(np.sum(p * (S - mean[1]) ** 2))]
+    return mean, std
+
+
+@pytest.mark.parametrize("update", ["simultaneous", "redblack"])
+def test_gw_global_parameters_known_answer(update):
+    """goodman_weare_wglobal_constant (utils/mcmc.m:385-626): four voxels with
+    their own M0 sharing R2* and the noise sigma (global, one value per walker,
+    flat priors, none pinned).  The posterior mean/std of the shared parameters
+    match quadrature of the exact marginal; a global parameter's statistics are
+    the same for every voxel."""
+    om, y = _gw_global_problem()
+    nv = y.shape[1]
+    lb, ub = [0.0, 0.1, 0.02], [2.0, 200.0, 0.12]
+    x0 = np.vstack([np.ones(nv), np.full(nv, 30.0), np.full(nv, 0.05)])
+    r = oracle.mcmc(om, oracle.Volume(y), x0, lb, ub, algorithm="ensemble", iteration=8000, thinning=2,
+                    burnin=0.2, nwalker=32, seed=5, ensemble_update=update, start_range=0.05,
+                    is_global=[0, 1, 1], global_warmup=20)
+    mean, std = _global_posterior_grid(y)
+    for k, q in ((1, 0), (2, 1)):
+        assert np.ptp(r["mean"][k]) == 0 and np.ptp(r["std"][k]) == 0
+        assert abs(r["mean"][k][0] - mean[q]) < 0.1 * std[q], (k, r["mean"][k][0], mean[q], std[q])
+        assert r["std"][k][0] == pytest.approx(std[q], rel=0.06)
+
+
+def test_gw_global_needs_local_and_global_parameters():
+    om, y = _gw_global_problem(nv=2)
+    x0 = np.vstack([np.ones(2), np.full(2, 30.0), np.full(2, 0.05)])
+    with pytest.raises(ValueError):
+        oracle.mcmc(om, oracle.Volume(y), x0, [0, 0.1, 0.02], [2, 200, 0.12], iteration=10, nwalker=8,
+                    is_global=[1, 1, 1])
+    with pytest.raises(ValueError):
+        oracle.mcmc(om, oracle.Volume(y), x0, [0, 0.1, 0.02], [2, 200, 0.12], algorithm="mh",
+                    x_step=[0.01, 1, 0.005], iteration=10, is_global=[0, 1, 0])
