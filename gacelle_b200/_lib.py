@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libgacelle_b200.so")
 GX_OK, GX_EINVAL, GX_ENOMEM, GX_ECUDA, GX_EUNSUPPORTED, GX_ETIMEOUT, GX_ENUMERIC, GX_ECANCELLED = range(8)
 STATUS_NAMES = {0: "ok", 1: "invalidArgument", 2: "outOfMemory", 3: "cuda", 4: "unsupported",
                 5: "timeout", 6: "numeric", 7: "cancelled"}
-MODEL_R2S, MODEL_R1R2S, MODEL_NEXI = 1, 2, 3
+MODEL_R2S, MODEL_R1R2S, MODEL_NEXI, MODEL_NEXI_RICE = 1, 2, 3, 4
 LOSS = {"l1": 0, "l2": 1, "huber": 2, "mse": 3, "gauss": 4, "rician": 5}
 OPTIMISER = {"adam": 0, "sgdm": 1, "rmsprop": 2}
 TRANSFORM = {"sigmoid": 0, "linear": 1}

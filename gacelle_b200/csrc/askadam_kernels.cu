@@ -133,6 +133,7 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
     if (MODEL == kR1R2S)
         for (int f = 0; f < a.P.n_fa; ++f) sincosf(b1 * a.P.fa_rad[f], &s_sa[f * B + tid], &s_ca[f * B + tid]);
     VoxAux va{b1, s_sa + tid, s_ca + tid, B};
+    va.sigma = voxel_sigma(a, v);
     LossAux aux = make_loss_aux(voxel_sigma(a, v));
     __syncthreads();
 
@@ -252,6 +253,7 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
     if (MODEL == kR1R2S)
         for (int f = 0; f < a.P.n_fa; ++f) sincosf(b1 * a.P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
+    va.sigma = voxel_sigma(a, v);
     float th[NP], dth[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) th[k] = unscale(a.transform, a.P.lb[k], a.P.ub[k], z[k], dth[k]);
@@ -441,6 +443,7 @@ __global__ void plain_forward_kernel(AdamParams a, PlainBufs b) {
     if (MODEL == kR1R2S)
         for (int f = 0; f < a.P.n_fa; ++f) sincosf(b1 * a.P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
+    va.sigma = voxel_sigma(a, v);
     SignalSink<NP> sink{b.signal + v, a.nvtot};
     model_eval<MODEL>(a.P, th, va, sink);
 }
@@ -495,6 +498,7 @@ __global__ void plain_adjoint_kernel(AdamParams a, PlainBufs b) {
     if (MODEL == kR1R2S)
         for (int f = 0; f < a.P.n_fa; ++f) sincosf(b1 * a.P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
+    va.sigma = voxel_sigma(a, v);
     DsigAcc<NP> acc;
     acc.ds = b.dsig + v;
     acc.s = a.nvtot;
@@ -605,6 +609,7 @@ __global__ void forward_only_kernel(DevProtocol P, const float* theta, const flo
     if (MODEL == kR1R2S)
         for (int f = 0; f < P.n_fa; ++f) sincosf(b1 * P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
+    va.sigma = b1;  // the aux map: b1 (R1R2*) or sigma (NEXI Rician mean)
     SignalSink<NP> sink{signal + v, nvox};
     model_eval<MODEL>(P, th, va, sink);
 }

@@ -240,6 +240,16 @@ static gx_status model_sizes(const gx_model* m, int* np, int* nm, int* id) {
         *nm = m->n_shell * (m->lmax / 2 + 1);
         *id = m->lmax == 2 ? kNEXI2 : kNEXI;
         return GX_OK;
+    case GX_MODEL_NEXI_RICE:
+        if (m->n_shell < 1 || m->n_shell > kMaxShell || !m->bval || !m->big_delta)
+            return fail(GX_EINVAL, "NEXI Rice: need 1..%d shells with b and Delta", kMaxShell);
+        // gpuNEXIrice.FWD returns the lmax-0 signal only (NEXI/gpuNEXIrice.m:645-650)
+        if (m->lmax != 0) return fail(GX_EUNSUPPORTED, "NEXI Rice: the reference's FWD computes lmax 0 only");
+        if (m->nx < 2 || m->nx > 4096) return fail(GX_EINVAL, "NEXI: nx must be in [2, 4096]");
+        *np = 4;
+        *nm = m->n_shell;
+        *id = kNEXI;
+        return GX_OK;
     }
     return fail(GX_EUNSUPPORTED, "unknown model kind %d (custom FWD handles are not accelerated)", m->kind);
 }
@@ -272,6 +282,14 @@ static DevProtocol make_protocol(const gx_model* m, int id, int np, int nm, cons
     for (int i = 0; i < nbound && i < kMaxParam; ++i) {
         P.lb[i] = lb ? (float)lb[i] : 0.0f;
         P.ub[i] = ub ? (float)ub[i] : 1.0f;
+    }
+    if (m->kind == GX_MODEL_NEXI_RICE) {
+        P.rice = 1;
+        for (int i = 1; i < kRiceNodes - 1; ++i) {  // t_i = i pi / 33 (mybesseli nodes)
+            double t = i * M_PI / (kRiceNodes - 1);
+            P.rice_cm1[i - 1] = (float)(cos(t) - 1.0);
+            P.rice_s2[i - 1] = (float)(sin(t) * sin(t));
+        }
     }
     return P;
 }
@@ -1113,6 +1131,8 @@ extern "C" gx_status gx_forward(gx_context* c, const gx_model* model, int32_t me
     CallScope scope(c);
     int np, nm, id;
     TRY(model_sizes(model, &np, &nm, &id));
+    if (model->kind == GX_MODEL_NEXI_RICE && !b1)
+        return fail(GX_EINVAL, "NEXI Rice: the per-voxel noise sigma (aux) is required");
     DevProtocol P = make_protocol(model, id, np, nm, nullptr, nullptr, 0);
     const float *dth = theta, *db1 = b1;
     float* dsig = signal;
@@ -1163,6 +1183,8 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     CallScope scope(c);
     int np, nm, id;
     TRY(model_sizes(model, &np, &nm, &id));
+    if (model->kind == GX_MODEL_NEXI_RICE)
+        return fail(GX_EUNSUPPORTED, "NEXI Rice: the reference samples gpuNEXIrice with askAdam only");
     int nvar = np + 1;
     if (o->algorithm != GX_MCMC_MH && o->algorithm != GX_MCMC_ENSEMBLE) return fail(GX_EINVAL, "unknown algorithm");
     if (o->iteration < 1 || o->thinning < 1 || o->repetition < 1) return fail(GX_EINVAL, "iteration, thinning and repetition must be >= 1");

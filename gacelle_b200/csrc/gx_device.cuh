@@ -24,6 +24,7 @@ constexpr int kMaxParam = 6;  // fitted parameters + noise
 constexpr int kMaxMeas = 128;
 
 enum ModelId { kR2S = 1, kR1R2S = 2, kNEXI = 3, kNEXI2 = 4 };
+constexpr int kRiceNodes = 34;  // mybesseli trapezoid nodes (NEXI/gpuNEXIrice.m:752)
 enum LossId { kL1 = 0, kL2 = 1, kHuber = 2, kMSE = 3, kGauss = 4, kRician = 5 };
 enum OptId { kAdam = 0, kSGDM = 1, kRMSProp = 2 };
 
@@ -42,6 +43,11 @@ struct DevProtocol {
     float bval[kMaxShell];
     float delta[kMaxShell];
     float lb[kMaxParam], ub[kMaxParam];
+    // NEXI Rician mean (gpuNEXIrice): interior nodes t_i = i pi / 33, i = 1..32,
+    // of the 34-node Bessel trapezoids: cos(t_i) - 1 and sin(t_i)^2
+    int rice;
+    float rice_cm1[kRiceNodes - 2];
+    float rice_s2[kRiceNodes - 2];
 };
 
 // ---------------------------------------------------------------------------
@@ -267,7 +273,47 @@ struct VoxAux {
     const float* sa;          // R1R2*: sin(b1*FA_f) at sa[f*fs]
     const float* ca;          // R1R2*: cos(b1*FA_f)
     int fs;
+    float sigma = 1.0f;       // NEXI Rician mean: noise sigma (normalised by b0)
 };
+
+// Rician mean of a noise-free signal S (myriceM1 / myL12 / mybesseli,
+// NEXI/gpuNEXIrice.m:726-755): M1 = max(sigma sqrt(pi/2) L(x), S) with
+// x = max(-S^2 / (2 sigma^2), -170) and L(x) = exp(x/2) ((1-x) I0(-x/2) -
+// x I1(-x/2)), the I_nu being 34-node trapezoids over t in [0, pi].  With
+// z = -x/2 the factor exp(x/2) is folded into the integrands,
+// exp(z (cos t - 1)), so nothing overflows in FP32.  dM1/dS differentiates
+// the discretised function, as autodiff does: dL/dx = -T0/2 - 3 T1/2 -
+// x V / 2 with T_nu the scaled trapezoids and V that of sin^2 t.
+__device__ __forceinline__ float rice_mean(const DevProtocol& P, float S, float sigma, float& dM1) {
+    const float s2i = 1.0f / (sigma * sigma);
+    const float xr = -0.5f * S * S * s2i;
+    const bool clamped = xr < -170.0f;
+    const float x = clamped ? -170.0f : xr;
+    const float z = -0.5f * x;
+    const float eend = __expf(-2.0f * z);   // t = pi: cos t - 1 = -2
+    float T0 = 0.5f * (1.0f + eend), T1 = 0.5f * (1.0f - eend), V = 0.0f;
+#pragma unroll 8
+    for (int i = 0; i < kRiceNodes - 2; ++i) {
+        const float c1 = P.rice_cm1[i];
+        const float e = __expf(z * c1);
+        T0 += e;
+        T1 = fmaf(e, c1 + 1.0f, T1);
+        V = fmaf(e, P.rice_s2[i], V);
+    }
+    const float hn = 1.0f / (float)(kRiceNodes - 1);  // trapezoid step / pi
+    T0 *= hn;
+    T1 *= hn;
+    V *= hn;
+    const float k = 1.2533141373155003f * sigma;  // sqrt(pi/2) sigma
+    const float M = k * ((1.0f - x) * T0 - x * T1);
+    if (M > S) {
+        const float dL = -0.5f * T0 - 1.5f * T1 - 0.5f * x * V;
+        dM1 = clamped ? 0.0f : k * dL * (-S * s2i);
+        return M;
+    }
+    dM1 = 1.0f;
+    return S;
+}
 
 // S = M0 exp(-TE R2*)  (R2star/gpuR2starMapping.m:427-434)
 template <class Acc>
@@ -325,14 +371,18 @@ __device__ __forceinline__ void model_r1r2s(const DevProtocol& P, const float* t
 // node are reduced to the five intermediate partials (f, d1, d2, r1, r2) and
 // chained to (fa, Da, De, ra) once per shell.
 template <bool LMAX2, class Acc, int NP>
-__device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const float* th, Acc& acc) {
+__device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const float* th, const VoxAux& va,
+                                                Acc& acc) {
     const float EPS = 1e-8f;
     float fa_in = th[0];
     float f = fmaxf(fa_in, EPS);
     float Da = th[1], De = th[2], ra = th[3];
     float gate = fa_in > EPS ? 1.0f : 0.0f;  // d max(fa,eps)/d fa
     float omf = 1.0f - f;
-    float rf = f / omf;
+    // gpuNEXIrice guards re = ra fa / max(1 - fa, eps) (NEXI/gpuNEXIrice.m:684)
+    const bool rice = P.rice != 0;
+    float omg = rice ? fmaxf(omf, EPS) : omf;
+    float rf = f / omg;
     int nx = P.nx;
     float h = P.h;
     int nsh = P.n_shell;
@@ -399,7 +449,7 @@ __device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const floa
                 Tr2 = fmaf(p2w, r2b, Tr2);
             }
         }
-        float r2_f = r1 / (omf * omf);
+        float r2_f = rice ? (omf > EPS ? r1 / (omf * omf) : r1 / EPS) : r1 / (omf * omf);
         {
             float S = S0 * h;
             float dS[NP];
@@ -408,6 +458,12 @@ __device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const floa
             dS[2] = h * Sd2 * b;
             dS[3] = h * (Sr1 + Sr2 * rf) * D;
             if (NP > 4) dS[NP - 1] = 0.0f;
+            if (rice) {  // Rician floor correction (NEXI/gpuNEXIrice.m:653)
+                float dM1;
+                S = rice_mean(P, S, va.sigma, dM1);
+#pragma unroll
+                for (int k = 0; k < NP; ++k) dS[k] *= dM1;
+            }
             if (S > 1.0f) {  // min(S,1), NEXI/gpuNEXI.m:928
                 S = 1.0f;
 #pragma unroll
@@ -441,8 +497,8 @@ __device__ __forceinline__ void model_eval(const DevProtocol& P, const float* th
                                            Acc& acc) {
     if constexpr (MODEL == kR2S) model_r2s(P, th, acc);
     else if constexpr (MODEL == kR1R2S) model_r1r2s(P, th, va, acc);
-    else if constexpr (MODEL == kNEXI) model_nexi_impl<false, Acc, 4>(P, th, acc);
-    else model_nexi_impl<true, Acc, 5>(P, th, acc);
+    else if constexpr (MODEL == kNEXI) model_nexi_impl<false, Acc, 4>(P, th, va, acc);
+    else model_nexi_impl<true, Acc, 5>(P, th, va, acc);
 }
 
 // Forward-only accumulation (no derivatives): used by gx_forward and MCMC.

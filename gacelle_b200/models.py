@@ -410,3 +410,109 @@ class gpuNEXI(_ModelBase):
         if not np.all(wv == 1):
             w = np.broadcast_to(wv, utils.dims3(mask) + (wv.size,)).copy()
         return self._solve(dwi, mask, w, pars0, fitting, extradata=extradata)
+
+
+class gpuNEXIrice(gpuNEXI):
+    """NEXI with the Rician noise floor in the forward model
+    (NEXI/gpuNEXIrice.m): the lmax-0 NEXI signal passed through the Rician
+    mean for each voxel's noise sigma (normalised by the b0 signal), fitted
+    with askAdam."""
+
+    eps = float(np.finfo(float).eps)
+    modelParams = ["fa", "Da", "De", "ra", "p2"]
+    ub = [1 - eps, 3, 3, 1, 1]
+    lb = [eps, eps, eps, 1 / 250, eps]
+    startPoint = [0.4, 2, 1, 0.05, 0.2]
+    step = [0.05, 0.15, 0.15, 0.005, 0.05]
+
+    def __init__(self, b, Delta, Nav=None, nx=14):
+        """NEXI/gpuNEXIrice.m:31-72: b and Delta are kept in the given order."""
+        _ModelBase.__init__(self)
+        self.b = np.asarray(b, dtype=np.float64).ravel()
+        self.Delta = np.asarray(Delta, dtype=np.float64).ravel()
+        self.Nav = np.ones(len(self.b)) if Nav is None else np.asarray(Nav, dtype=np.float64).ravel()
+        self.nx = int(nx)
+        self.lmax = 0
+
+    def _gx_model(self):
+        return _GxModelHandle(_lib.MODEL_NEXI_RICE, bval=self.b, delta=self.Delta, lmax=0, nx=self.nx)
+
+    def updateProperty(self, fitting):
+        """NEXI/gpuNEXIrice.m:74-84 (no noise parameter)."""
+        if int(fitting.get("lmax", 0)) == 0:
+            self._strip("p2")
+        else:
+            raise GacelleError(GX_EUNSUPPORTED, "gpuNEXIrice.FWD computes the lmax-0 signal only")
+        return self
+
+    def FWD(self, pars, extraData=None, solver=None):
+        """NEXI/gpuNEXIrice.m:635-662; extraData['sigma'] is the noise map."""
+        if extraData is None or "sigma" not in extraData:
+            raise GacelleError(GX_EINVAL, "gpuNEXIrice.FWD needs extraData['sigma']")
+        return self._fwd_struct(pars, ["fa", "Da", "De", "ra"], b1=extraData["sigma"])
+
+    @staticmethod
+    def check_set_default(fitting):
+        """NEXI/gpuNEXIrice.m:759-772."""
+        from .askadam_solver import check_set_default_basic as adam_def
+        f = dict(fitting or {})
+        g = adam_def(f)
+        g["solver"] = "askadam"
+        if "regmap" not in f:
+            g["regmap"] = "fa"
+        if not isinstance(g["regmap"], (list, tuple)):
+            g["regmap"] = [g["regmap"]]
+        g.setdefault("lmax", 0)
+        g.setdefault("start", "likelihood")
+        return g
+
+    def prepare_dwi_data(self, dwi, mask, extradata, lmax=0):
+        """NEXI/gpuNEXIrice.m:344-405 for rotationally invariant input: sigma
+        normalised by the mean b0 signal and floored at epsilon; voxels with
+        NaN/Inf, a signal above 1.01, sigma > 1 (SNR < 1) or a signal whose
+        correlation with the mean signal shape is below 0.1 leave the mask."""
+        dwi = np.asarray(dwi, dtype=np.float64)
+        mask = np.asarray(mask) > 0
+        ex = dict(extradata)
+        if dwi.shape[-1] / (lmax / 2 + 1) > len(self.b):
+            raise GacelleError(GX_EUNSUPPORTED, "full DWI input (rotational invariants) is not computed by "
+                                                "the engine; pass the Sl0 signal per shell")
+        if dwi.shape[-1] < len(self.b):
+            raise GacelleError(GX_EINVAL, "There are more b-shells in the class object than available in the "
+                                          "input data. Please check your input data.")
+        bval = np.asarray(ex.get("bval", np.ones(dwi.shape[-1])), dtype=np.float64).ravel()
+        b0 = bval == 0
+        dwi_b0 = np.mean(dwi[..., b0], axis=-1) if b0.any() else np.ones(mask.shape)
+        sigma = np.asarray(ex["sigma"], dtype=np.float64) / dwi_b0
+        sigma[~np.isfinite(sigma)] = 0.0
+        ex["sigma"] = np.maximum(sigma, self.epsilon)
+        bad = ~np.isfinite(dwi)
+        dwi = np.where(bad, 0.0, dwi)
+        valid = mask & (dwi.max(axis=-1) <= 1.01) & ~bad.any(axis=-1) & ~(ex["sigma"] > 1)
+        idx = utils.mask_index(valid)
+        d2 = utils.reshape_ND2GD(dwi, idx)
+        if d2.shape[1] > 1:
+            tmpl = np.nanmean(d2, axis=1)
+            tmpl = (tmpl - tmpl.mean()) / tmpl.std(ddof=1)
+            z = (d2 - d2.mean(axis=0)) / d2.std(axis=0, ddof=1)
+            r = (tmpl @ z) / (len(tmpl) - 1)
+            keep = np.ones(valid.shape, dtype=bool).reshape(-1, order="F")
+            keep[idx] = ~(r < 0.1)
+            valid &= keep.reshape(valid.shape, order="F")
+        return dwi, valid, ex
+
+    def fit(self, dwi, mask=None, fitting=None, extraData=None, pars0=None):
+        """NEXI/gpuNEXIrice.m:203-316 (argument order of the reference)."""
+        if extraData is None or "sigma" not in extraData:
+            raise GacelleError(GX_EINVAL, "gpuNEXIrice.fit needs extraData['sigma']")
+        fitting = self.check_set_default(fitting)
+        return gpuNEXI.fit(self, dwi, mask, fitting, pars0, extradata=extraData)
+
+    def estimate(self, dwi, mask, extraData, fitting=None, pars0=None):
+        """NEXI/gpuNEXIrice.m:104-199: data preparation, then fit (the engine
+        fits the whole volume in one call, no segmentation)."""
+        fitting = self.check_set_default(fitting)
+        dwi, mask, ex = self.prepare_dwi_data(dwi, mask, extraData, int(fitting["lmax"]))
+        out = self.fit(dwi, mask, fitting, ex, pars0)
+        out["mask"] = mask
+        return out

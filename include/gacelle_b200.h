@@ -63,7 +63,10 @@ typedef enum {
 typedef enum {
     GX_MODEL_R2S = 1,   /* gpuR2starMapping: M0, R2star */
     GX_MODEL_R1R2S = 2, /* gpuJointR1R2starMapping: M0, R1, R2star */
-    GX_MODEL_NEXI = 3   /* gpuNEXI: fa, Da, De, ra [, p2 if lmax = 2] */
+    GX_MODEL_NEXI = 3,  /* gpuNEXI: fa, Da, De, ra [, p2 if lmax = 2] */
+    GX_MODEL_NEXI_RICE = 4 /* gpuNEXIrice: fa, Da, De, ra; lmax 0; Rician mean of the NEXI
+                            * signal for the per-voxel noise sigma (gx_volume.sigma, or
+                            * gx_askadam_opts.sigma; gx_forward's aux map) */
 } gx_model_kind;
 
 typedef enum {
@@ -234,8 +237,11 @@ gx_status gx_set_cancel_flag(gx_context* ctx, volatile int32_t* flag);
 
 gx_status gx_model_sizes(const gx_model* model, int32_t* nparam, int32_t* nmeas);
 
+/* model.FWD (R2star/gpuR2starMapping.m:321-363, R1R2s/gpuJointR1R2starMapping.m:375-422,
+ * NEXI/gpuNEXI.m:902-930, NEXI/gpuNEXIrice.m:635-662).  aux [nvox]: b1 for
+ * R1R2* (NULL: 1), the noise sigma for GX_MODEL_NEXI_RICE (required). */
 gx_status gx_forward(gx_context* ctx, const gx_model* model, int32_t mem, const float* theta,
-                     const float* b1, int32_t nvox, float* signal);
+                     const float* aux, int32_t nvox, float* signal);
 
 gx_status gx_model_gradient(gx_context* ctx, const gx_model* model, int32_t mem,
                             const gx_volume* vol, const gx_askadam_opts* opts,

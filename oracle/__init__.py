@@ -19,7 +19,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 
-MODEL_R2S, MODEL_R1R2S, MODEL_NEXI = 1, 2, 3
+MODEL_R2S, MODEL_R1R2S, MODEL_NEXI, MODEL_NEXI_RICE = 1, 2, 3, 4
 LOSS = {"l1": 0, "l2": 1, "huber": 2, "mse": 3, "gauss": 4, "rician": 5}
 OPTIMISER = {"adam": 0, "sgdm": 1, "rmsprop": 2}
 TRANSFORM = {"sigmoid": 0, "linear": 1}
@@ -172,7 +172,14 @@ def nexi(bval, delta, lmax=0, nx=14):
     return Model(MODEL_NEXI, bval=bval, delta=delta, lmax=lmax, nx=nx)
 
 
+def nexi_rice(bval, delta, nx=14):
+    """gpuNEXIrice (NEXI/gpuNEXIrice.m): Rician mean of the lmax-0 NEXI signal;
+    the per-voxel noise sigma is passed where R1R2* takes b1."""
+    return Model(MODEL_NEXI_RICE, bval=bval, delta=delta, lmax=0, nx=nx)
+
+
 def forward(model: Model, theta, b1=None):
+    """b1: per-voxel model input (b1 for R1R2*, sigma for the NEXI Rician mean)."""
     theta = _f64(theta)
     nv = theta.shape[1]
     out = np.empty((model.nm, nv))

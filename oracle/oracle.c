@@ -81,6 +81,7 @@ int orc_nparams(const orc_model* m) {
     case ORC_MODEL_R2S: return 2;   /* M0, R2star   (R2star/gpuR2starMapping.m:24) */
     case ORC_MODEL_R1R2S: return 3; /* M0, R1, R2star (R1R2s/gpuJointR1R2starMapping.m:25) */
     case ORC_MODEL_NEXI: return m->lmax == 2 ? 5 : 4; /* fa, Da, De, ra[, p2] (NEXI/gpuNEXI.m:28,125-133) */
+    case ORC_MODEL_NEXI_RICE: return 4;                /* fa, Da, De, ra (NEXI/gpuNEXIrice.m:15,74-84) */
     }
     return 0;
 }
@@ -90,6 +91,7 @@ int orc_nmeas(const orc_model* m) {
     case ORC_MODEL_R2S: return m->n_te;
     case ORC_MODEL_R1R2S: return m->n_te * m->n_fa;
     case ORC_MODEL_NEXI: return m->n_shell * (m->lmax / 2 + 1);
+    case ORC_MODEL_NEXI_RICE: return m->n_shell;
     }
     return 0;
 }
@@ -258,11 +260,108 @@ static void nexi_vjp(const orc_model* m, const double* th, const double* sb_in, 
     tb[3] += rab;
 }
 
+/* gpuNEXIrice.FWD (NEXI/gpuNEXIrice.m:635-662): Sl0 with fa = max(fa, eps)
+ * and re = ra fa / max(1 - fa, eps) (:665-688), then the Rician mean
+ * myriceM1 (:726-737), then min(s, 1). */
+static void nexi_rice_raw(const orc_model* m, const double* th, double* sl0) {
+    double fa = fmax(th[0], ORC_EPS), Da = th[1], De = th[2], ra = th[3];
+    int nx = m->nx;
+    for (int j = 0; j < m->n_shell; ++j) {
+        double b = m->bval[j], D = m->delta[j];
+        double r1 = D * ra, r2 = r1 * fa / fmax(1.0 - fa, ORC_EPS);
+        double s0 = 0.0;
+        for (int i = 0; i < nx; ++i) {
+            double x = (double)i / (nx - 1);
+            s0 += trapz_w(i, nx) * nexi_node_eval(fa, b * Da * x * x, b * De, r1, r2).M;
+        }
+        sl0[j] = s0;
+    }
+}
+
+/* myL12 (NEXI/gpuNEXIrice.m:739-744) with mybesseli (:751-755):
+ * L(x) = exp(x/2) ((1 - x) I0(-x/2) - x I1(-x/2)), x clamped at -170, the
+ * I_nu as 34-node trapezoids of (1/pi) int_0^pi exp(z cos t) cos(nu t) dt.
+ * dLdx differentiates that discretised function (what autodiff sees):
+ * dL/dx = L/2 + exp(x/2) (-T0 - T1 - (1-x)/2 T1 + x/2 U1),  U1 = the
+ * trapezoid of cos^2 t exp(z cos t) / pi, T_nu = the I_nu trapezoids. */
+static double rice_L12(double xin, double* dLdx) {
+    int clamped = xin < -170.0;
+    double x = clamped ? -170.0 : xin;
+    double z = -x / 2.0;
+    double T0 = orc_besseli_trapz(0, z, 34), T1 = orc_besseli_trapz(1, z, 34);
+    double h = M_PI / 33.0, U1 = 0.0;
+    for (int i = 0; i < 34; ++i) {
+        double t = i * h, w = (i == 0 || i == 33) ? 0.5 * h : h;
+        U1 += w * cos(t) * cos(t) * exp(z * cos(t));
+    }
+    U1 /= M_PI;
+    double e = exp(x / 2.0);
+    double L = e * ((1.0 - x) * T0 - x * T1);
+    if (dLdx) *dLdx = clamped ? 0.0 : 0.5 * L + e * (-T0 - T1 - 0.5 * (1.0 - x) * T1 + 0.5 * x * U1);
+    return L;
+}
+
+/* M1 = max(sigma sqrt(pi/2) L12(-nu^2 / (2 sigma^2)), nu) and dM1/dnu. */
+static double rice_M1(double nu, double sigma, double* dM1) {
+    double dL;
+    double x = -nu * nu / (2.0 * sigma * sigma);
+    double M = sigma * sqrt(M_PI / 2.0) * rice_L12(x, &dL);
+    if (M > nu) {
+        *dM1 = sigma * sqrt(M_PI / 2.0) * dL * (-nu / (sigma * sigma));
+        return M;
+    }
+    *dM1 = 1.0;
+    return nu;
+}
+
+static void nexi_rice_fwd(const orc_model* m, const double* th, double sigma, double* s) {
+    nexi_rice_raw(m, th, s);
+    for (int j = 0; j < m->n_shell; ++j) {
+        double d;
+        s[j] = fmin(rice_M1(s[j], sigma, &d), 1.0);
+    }
+}
+
+static void nexi_rice_vjp(const orc_model* m, const double* th, double sigma, const double* sb_in,
+                          double* tb) {
+    int ns = m->n_shell, nx = m->nx;
+    double sl0[256], sb[256];
+    nexi_rice_raw(m, th, sl0);
+    for (int j = 0; j < ns; ++j) {
+        double d, M1 = rice_M1(sl0[j], sigma, &d);
+        sb[j] = M1 <= 1.0 ? sb_in[j] * d : 0.0;
+    }
+    double fa = fmax(th[0], ORC_EPS), Da = th[1], De = th[2], ra = th[3];
+    double omf = fmax(1.0 - fa, ORC_EPS);
+    /* d(fa / max(1-fa, eps)) / d fa */
+    double rfd = 1.0 - fa > ORC_EPS ? 1.0 / ((1.0 - fa) * (1.0 - fa)) : 1.0 / ORC_EPS;
+    double fb = 0, Dab = 0, Deb = 0, rab = 0;
+    for (int j = 0; j < ns; ++j) {
+        double b = m->bval[j], D = m->delta[j];
+        double r1 = D * ra, r2 = r1 * fa / omf;
+        for (int i = 0; i < nx; ++i) {
+            double x = (double)i / (nx - 1);
+            double Mb = sb[j] * trapz_w(i, nx);
+            if (Mb == 0.0) continue;
+            nexi_node n = nexi_node_eval(fa, b * Da * x * x, b * De, r1, r2);
+            fb += Mb * (n.df + n.dr2 * r1 * rfd);
+            Dab += Mb * n.dd1 * b * x * x;
+            Deb += Mb * n.dd2 * b;
+            rab += Mb * (n.dr1 + n.dr2 * fa / omf) * D;
+        }
+    }
+    if (th[0] > ORC_EPS) tb[0] += fb;
+    tb[1] += Dab;
+    tb[2] += Deb;
+    tb[3] += rab;
+}
+
 void orc_forward_voxel(const orc_model* m, const double* th, double b1, double* s) {
     switch (m->model) {
     case ORC_MODEL_R2S: r2s_fwd(m, th, s); break;
     case ORC_MODEL_R1R2S: r1r2s_fwd(m, th, b1, s); break;
     case ORC_MODEL_NEXI: nexi_fwd(m, th, s); break;
+    case ORC_MODEL_NEXI_RICE: nexi_rice_fwd(m, th, b1, s); break;
     }
 }
 
@@ -272,6 +371,7 @@ void orc_vjp_voxel(const orc_model* m, const double* th, double b1, const double
     case ORC_MODEL_R2S: r2s_vjp(m, th, sb, tb); break;
     case ORC_MODEL_R1R2S: r1r2s_vjp(m, th, b1, sb, tb); break;
     case ORC_MODEL_NEXI: nexi_vjp(m, th, sb, tb); break;
+    case ORC_MODEL_NEXI_RICE: nexi_rice_vjp(m, th, b1, sb, tb); break;
     }
 }
 
@@ -473,8 +573,8 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
     for (int v = 0; v < nv; ++v) {
         double th[8], s[512], sb[512], tb[8] = {0};
         for (int k = 0; k < np; ++k) th[k] = theta[(size_t)k * nv + v];
-        double b1 = vol->b1 ? vol->b1[v] : 1.0;
         double sig = vol->sigma ? vol->sigma[v] : o->sigma;
+        double b1 = c->m->model == ORC_MODEL_NEXI_RICE ? sig : (vol->b1 ? vol->b1[v] : 1.0);
         orc_forward_voxel(c->m, th, b1, s);
         double lf = 0.0;
         for (int k = 0; k < nm; ++k) {

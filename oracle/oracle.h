@@ -24,7 +24,8 @@
 extern "C" {
 #endif
 
-enum { ORC_MODEL_R2S = 1, ORC_MODEL_R1R2S = 2, ORC_MODEL_NEXI = 3 };
+enum { ORC_MODEL_R2S = 1, ORC_MODEL_R1R2S = 2, ORC_MODEL_NEXI = 3,
+       ORC_MODEL_NEXI_RICE = 4 /* gpuNEXIrice: Rician mean of the lmax-0 NEXI signal */ };
 enum { ORC_LOSS_L1 = 0, ORC_LOSS_L2 = 1, ORC_LOSS_HUBER = 2, ORC_LOSS_MSE = 3,
        ORC_LOSS_GAUSS = 4, ORC_LOSS_RICIAN = 5 };
 enum { ORC_OPT_ADAM = 0, ORC_OPT_SGDM = 1, ORC_OPT_RMSPROP = 2 };
@@ -54,6 +55,7 @@ int orc_nmeas(const orc_model* m);
 
 /* Single-voxel forward model, including the FWD-level post-processing of
  * the reference (NEXI min(S,1)).  theta[np] -> s[nm]. */
+/* aux: per-voxel model input, b1 (R1R2*) or the noise sigma (NEXI Rician mean). */
 void orc_forward_voxel(const orc_model* m, const double* theta, double b1, double* s);
 /* Vector-Jacobian product of orc_forward_voxel: thetabar[np] += J^T sbar. */
 void orc_vjp_voxel(const orc_model* m, const double* theta, double b1,

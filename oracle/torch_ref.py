@@ -64,6 +64,47 @@ def nexi_fwd(theta, bval, delta, lmax=0, nx=14):
     return torch.clamp(S, max=1.0)
 
 
+def _besseli_trapz(nu, z, nx=34):
+    """mybesseli (NEXI/gpuNEXIrice.m:751-755): (1/pi) trapz over t in
+    linspace(0, pi, nx) of exp(z cos t) cos(nu t)."""
+    t = torch.linspace(0, math.pi, nx, dtype=z.dtype)
+    f = torch.exp(z[..., None] * torch.cos(t)) * torch.cos(nu * t)
+    h = t[1] - t[0]
+    return (torch.sum(f, dim=-1) - 0.5 * (f[..., 0] + f[..., -1])) * h / math.pi
+
+
+def rice_mean(nu, sigma):
+    """myriceM1 / myL12 (NEXI/gpuNEXIrice.m:726-744): max(sigma sqrt(pi/2)
+    L12(-nu^2/(2 sigma^2)), nu) with x clamped at -170."""
+    x = torch.clamp(-nu ** 2 / (2 * sigma ** 2), min=-170.0)
+    L = torch.exp(x / 2) * ((1 - x) * _besseli_trapz(0, -x / 2) - x * _besseli_trapz(1, -x / 2))
+    return torch.maximum(sigma * math.sqrt(math.pi / 2) * L, nu)
+
+
+def nexi_rice_fwd(theta, bval, delta, sigma, nx=14):
+    """gpuNEXIrice.FWD (NEXI/gpuNEXIrice.m:635-688): fa = max(fa, eps),
+    re = ra fa / max(1 - fa, eps), Sl0, Rician mean, min(s, 1)."""
+    fa = torch.clamp(theta[0], min=EPS)
+    Da, De, ra = theta[1], theta[2], theta[3]
+    b = torch.as_tensor(bval, dtype=theta.dtype)[:, None, None]
+    D = torch.as_tensor(delta, dtype=theta.dtype)[:, None, None]
+    f = fa[None, :, None]
+    r1 = D * ra[None, :, None]
+    r2 = r1 * f / torch.clamp(1 - f, min=EPS)
+    d2 = b * De[None, :, None]
+    x = torch.linspace(0, 1, nx, dtype=theta.dtype)[None, None, :]
+    d1 = b * Da[None, :, None] * x ** 2
+    l1 = (r1 + r2 + d1 + d2) / 2
+    l2 = torch.clamp(torch.sqrt((r1 - r2 + d1 - d2) ** 2 + 4 * r1 * r2) / 2, min=EPS)
+    lm = l1 - l2
+    Pp = (f * d1 + (1 - f) * d2 - lm) / (l2 * 2)
+    M = Pp * torch.exp(-(l1 + l2)) + (1 - Pp) * torch.exp(-lm)
+    w = x[..., 1:] - x[..., :-1]
+    S = torch.sum((M[..., :-1] + M[..., 1:]) * (w / 2), dim=-1)      # [shell, v]
+    sig = torch.as_tensor(sigma, dtype=theta.dtype)
+    return torch.clamp(rice_mean(S, sig[None, :] if sig.ndim else sig), max=1.0)
+
+
 def loss_elem(kind, s, y, w=None, sigma=1.0, mse_scale=0.5, huber_delta=1.0):
     """utils/askadam.m:86-95 elementwise losses, plus Gaussian/Rician NLL."""
     r = s - y

@@ -37,11 +37,17 @@ def models(kind, **kw):
         nx = kw.get("nx", 14)
         return (_GxModelHandle(_lib.MODEL_NEXI, bval=b, delta=d, lmax=lmax, nx=nx),
                 oracle.nexi(b, d, lmax=lmax, nx=nx))
+    if kind == "nexi_rice":
+        b = kw.get("b", np.tile([1.0, 2.5, 4.0, 6.0, 8.0, 10.0], 4))
+        d = kw.get("delta", np.repeat([20.0, 27.0, 35.0, 49.0], 6))
+        return (_GxModelHandle(_lib.MODEL_NEXI_RICE, bval=b, delta=d, lmax=0, nx=14),
+                oracle.nexi_rice(b, d, nx=14))
     raise ValueError(kind)
 
 
 def bounds(kind):
-    return {"r2s": R2S_BOUNDS, "r1r2s": R1R2S_BOUNDS, "nexi": NEXI_BOUNDS, "nexi2": NEXI2_BOUNDS}[kind]
+    return {"r2s": R2S_BOUNDS, "r1r2s": R1R2S_BOUNDS, "nexi": NEXI_BOUNDS, "nexi2": NEXI2_BOUNDS,
+            "nexi_rice": NEXI_BOUNDS}[kind]
 
 
 def random_theta(kind, n, rng):
@@ -114,4 +120,4 @@ def run_oracle(kind, y, theta0, f, names, dims=None, gidx=None, b1=None, sigma=N
 
 
 NAMES = {"r2s": ["M0", "R2star"], "r1r2s": ["M0", "R1", "R2star"], "nexi": ["fa", "Da", "De", "ra"],
-         "nexi2": ["fa", "Da", "De", "ra", "p2"]}
+         "nexi2": ["fa", "Da", "De", "ra", "p2"], "nexi_rice": ["fa", "Da", "De", "ra"]}

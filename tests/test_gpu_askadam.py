@@ -371,3 +371,100 @@ def test_device_resident_call_on_torch_stream_matches_host_call(stream_kind):
     np.testing.assert_array_equal(out[1], ref["min_theta"])
     # per-epoch losses are FP64 sums over CTAs in arrival order: equal to rounding
     np.testing.assert_allclose(hist, ref["loss_history"], rtol=1e-12)
+
+
+# ------------------------------------------------ gpuNEXIrice (Rician mean) ----
+def _rice_problem(n, seed, sigma_range=(0.02, 0.15)):
+    rng = np.random.default_rng(seed)
+    gxm, om = models("nexi_rice")
+    th = random_theta("nexi_rice", n, rng)
+    sigma = rng.uniform(*sigma_range, n)
+    s = oracle.forward(om, th, b1=sigma)
+    # magnitude data around the Rician mean
+    y = np.abs(oracle.forward(models("nexi")[1], th) + sigma * rng.standard_normal(s.shape)
+               + 1j * sigma * rng.standard_normal(s.shape)).astype(np.float32)
+    return gxm, om, th, sigma.astype(np.float32), y
+
+
+def test_nexi_rice_forward_matches_oracle(ctx):
+    """GX_MODEL_NEXI_RICE forward (NEXI/gpuNEXIrice.m:635-662) against the FP64
+    oracle: relative 2e-5 (FP32, scaled Bessel trapezoids)."""
+    gxm, om, th, sigma, _ = _rice_problem(2000, 50)
+    th = th.astype(np.float32)
+    s_gpu = _forward_engine(ctx, gxm, th, sigma)
+    s_ref = oracle.forward(om, th.astype(np.float64), sigma.astype(np.float64))
+    assert np.max(np.abs(s_gpu - s_ref) / np.maximum(np.abs(s_ref), 1e-3)) < 2e-5
+    s_plain = oracle.forward(models("nexi")[1], th.astype(np.float64))
+    assert np.mean(s_ref > s_plain + 1e-4) > 0.05  # the Rician floor is exercised
+
+
+def test_nexi_rice_forward_needs_sigma(ctx):
+    gxm, _, th, _, _ = _rice_problem(10, 51)
+    with pytest.raises(_lib.GacelleError):
+        _forward_engine(ctx, gxm, th.astype(np.float32), None)
+
+
+@pytest.mark.parametrize("loss", ["mse", "l1"])
+def test_nexi_rice_model_gradient_matches_oracle(ctx, loss):
+    import ctypes as C
+    gxm, om, th, sigma, y = _rice_problem(400, 52)
+    rng = np.random.default_rng(53)
+    lb, ub = bounds("nexi_rice")
+    th_eval = np.clip(th * rng.uniform(0.9, 1.1, th.shape), np.array(lb)[:, None] + 1e-3,
+                      np.array(ub)[:, None] - 1e-3).astype(np.float32)
+    f = fitting(lossFunction=loss)
+    opts = gx_askadam.build_opts(f, NAMES["nexi_rice"], lb, ub)
+    n = y.shape[1]
+    vol = _lib.GxVolume()
+    vol.dims[0], vol.dims[1], vol.dims[2] = n, 1, 1
+    vol.nvox = n
+    vol.data = y.ctypes.data_as(_lib._fp)
+    vol.sigma = sigma.ctypes.data_as(_lib._fp)
+    g = np.zeros_like(th_eval)
+    L = C.c_double(); Lf = C.c_double(); Lr = C.c_double()
+    _lib.check(_lib.lib().gx_model_gradient(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, C.byref(vol), C.byref(opts),
+                                            th_eval.ctypes.data, g.ctypes.data, None,
+                                            C.byref(L), C.byref(Lf), C.byref(Lr)))
+    o = oracle.adam_opts(lb, ub, f)
+    ov = oracle.Volume(y.astype(np.float64), sigma=sigma.astype(np.float64))
+    Lo, go, _, _, _ = oracle.model_gradient(om, ov, o, th_eval.astype(np.float64))
+    assert abs(L.value - Lo) <= 1e-5 * abs(Lo) + 1e-7
+    for k in range(4):
+        scale = np.max(np.abs(go[k]))
+        assert np.max(np.abs(g[k] - go[k])) <= 1e-3 * scale + 1e-12, (k, np.max(np.abs(g[k] - go[k])), scale)
+
+
+def test_nexi_rice_askadam_matches_oracle(ctx):
+    """askAdam on gpuNEXIrice's forward model with per-voxel sigma: the fused
+    fit matches the FP64 oracle to 1e-4 per parameter map."""
+    gxm, om, th, sigma, y = _rice_problem(512, 54)
+    lb, ub = bounds("nexi_rice")
+    th0 = np.tile(((np.array(lb) + np.array(ub)) / 2)[:, None], (1, y.shape[1])).astype(np.float32)
+    f = fitting(iteration=300, initialLearnRate=0.01)
+    eng = run_engine("nexi_rice", y, th0, f, NAMES["nexi_rice"], sigma=sigma)
+    orc = run_oracle("nexi_rice", y, th0, f, NAMES["nexi_rice"], sigma=sigma)
+    for k in range(4):
+        assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 1e-4, k
+    assert abs(eng["final_loss"] - orc["final_loss"]) <= 1e-4 * abs(orc["final_loss"])
+
+
+def test_gpuNEXIrice_mirror_fit_and_estimate(ctx):
+    """The gpuNEXIrice mirror: FWD needs extraData['sigma'], fit keeps the
+    reference's argument order, estimate normalises sigma by b0 and masks
+    voxels with SNR < 1."""
+    from gacelle_b200 import gpuNEXIrice
+    gxm, om, th, sigma, y = _rice_problem(60, 55)
+    b = np.tile([1.0, 2.5, 4.0, 6.0, 8.0, 10.0], 4)
+    d = np.repeat([20.0, 27.0, 35.0, 49.0], 6)
+    m = gpuNEXIrice(b, d)
+    m.context = ctx
+    pars = {"fa": th[0], "Da": th[1], "De": th[2], "ra": th[3]}
+    s = m.FWD({k: v[None, :] for k, v in pars.items()}, {"sigma": sigma[None, :]})
+    np.testing.assert_allclose(s, oracle.forward(om, th, b1=sigma), rtol=2e-5, atol=1e-6)
+    dwi = y.T.reshape(6, 10, 1, 24, order="F")
+    mask = np.ones((6, 10, 1), dtype=bool)
+    sig = sigma.reshape(6, 10, 1, order="F").astype(np.float64)
+    sig[0, 0, 0] = 2.0  # SNR < 1: leaves the mask
+    out = m.estimate(dwi, mask, {"sigma": sig}, {"iteration": 100, "start": "default", "lossFunction": "mse"})
+    assert not out["mask"][0, 0, 0] and out["mask"].sum() >= 50
+    assert out["final"]["fa"].shape == (6, 10, 1)
