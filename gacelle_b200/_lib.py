@@ -64,7 +64,12 @@ class GxAskadamOpts(C.Structure):
                 ("step_tol", C.c_double), ("grad_tol", C.c_double), ("patience_step", C.c_double),
                 ("patience_grad", C.c_double), ("n_reg", C.c_int32), ("reg_param", C.c_int32 * 8),
                 ("lambda_", C.c_double * 8), ("tv_3d", C.c_int32), ("voxel_size", C.c_double * 3),
-                ("path", C.c_int32), ("chunk", C.c_int32), ("block_size", C.c_int32)]
+                ("path", C.c_int32), ("chunk", C.c_int32), ("block_size", C.c_int32),
+                ("robust_convergence", C.c_int32), ("outlier_weight", C.c_double),
+                ("weight_update_interval", C.c_int32), ("outlier_check_window", C.c_int32),
+                ("outlier_min_flag_duration", C.c_int32), ("outlier_voxel_thres", C.c_double),
+                ("outlier_pop_thres", C.c_double), ("outlier_init_thres", C.c_double),
+                ("outlier_init_pop_thres", C.c_double)]
 
 
 class GxAskadamResult(C.Structure):

@@ -169,6 +169,15 @@ def build_opts(fitting: dict, model_params, lb, ub, path="fused"):
     o.path = _lib.PATH[path]
     o.chunk = int(f.get("chunk", 0))
     o.block_size = int(f.get("blockSize", 0))
+    o.robust_convergence = 1 if f.get("robustConvergence") else 0
+    o.outlier_weight = float(f.get("outlierWeight", 0.1))
+    o.weight_update_interval = int(f.get("weightUpdateInterval", 5))
+    o.outlier_check_window = int(f.get("outlierCheckWindow", 5))
+    o.outlier_min_flag_duration = int(f.get("outlierMinFlagDuration", 5))
+    o.outlier_voxel_thres = float(f.get("outlierVoxelThres", 0.01))
+    o.outlier_pop_thres = float(f.get("outlierPopThres", 0.05))
+    o.outlier_init_thres = float(f.get("outlierInitThres", 0.05))
+    o.outlier_init_pop_thres = float(f.get("outlierInitPopThres", 0.20))
     return o
 
 
@@ -189,8 +198,6 @@ class askadam:
         """askadam.optimisation (utils/askadam.m:121-365)."""
         model = _model_of(userfuncCell)
         fitting = check_set_default_basic(fitting)
-        if fitting.get("robustConvergence"):
-            raise GacelleError(GX_EUNSUPPORTED, "robustConvergence is not implemented by the engine")
         mask = np.asarray(mask)
         d3 = utils.dims3(mask)
         idx = utils.mask_index(mask)

@@ -462,16 +462,141 @@ __global__ void plain_loss_kernel(AdamParams a, PlainBufs b) {
             float S = b.signal[i];
             bool bad = !isfinite(S);
             float s = bad ? 0.0f : S;
-            float w = a.weights ? a.weights[i] : 1.0f;
+            float w = (a.weights ? a.weights[i] : 1.0f) * (b.r.vmod ? b.r.vmod[v] : 1.0f);
             float d;
             float l = loss_elem<LOSS>(s, a.data[i], w, aux, a.mse_scale, a.huber_delta, d);
             b.res[i] = l;
             b.dsig[i] = bad ? 0.0f : d * V.norm;
             tot += l;
         }
+        if (b.r.vloss) b.r.vloss[v] = tot / (float)a.nm;  // mean(reshape(residuals, Nmeas, Nvol), 1)
     }
     float q[1] = {valid ? tot : 0.0f};
     block_accumulate<1>(q, b.acc, V.normd, s_red, 0);
+}
+
+// ---------------------------------------------------------------------------
+// robustConvergence (utils/askadam.m:448-510, 530-581) on the op-by-op path.
+// The medians enter only through "median > threshold", which needs no sort:
+// with c = #{x <= t} among n values, an odd n gives median > t iff
+// c < (n+1)/2; an even n (median = mean of the two middle values) gives true
+// for c < n/2, false for c > n/2 and, for c = n/2, compares the mean of
+// max{x <= t} and min{x > t} with t.  A NaN anywhere makes the median NaN.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned int ord_bits(float x) {
+    unsigned int u = __float_as_uint(x);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord_float(unsigned int u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ bool median_above(int n, int n_le, unsigned int max_le, unsigned int min_gt, int n_nan, float t) {
+    if (n_nan > 0 || n == 0) return false;
+    if (n & 1) return n_le < (n + 1) / 2;
+    int k = n / 2;
+    if (n_le < k) return true;
+    if (n_le > k) return false;
+    return 0.5f * (ord_float(max_le) + ord_float(min_gt)) > t;
+}
+
+__global__ void robust_reset_kernel(AdamParams a, PlainBufs b) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.nvtot) return;
+    b.r.vmod[v] = 1.0f;
+    b.r.flagcnt[v] = 0;
+    b.r.mainmask[v] = 1;
+    b.r.convmask[v] = 1;
+}
+
+// perVoxelLossInit and history = repmat(perVoxelLossInit, window, 1)
+__global__ void robust_seed_kernel(AdamParams a, PlainBufs b, int window) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.nvtot) return;
+    float l = b.r.vloss[v];
+    b.r.vinit[v] = l;
+    for (int q = 0; q < window; ++q) b.r.ring[(size_t)q * a.nvtot + v] = l;
+}
+
+// History shift (the oldest row `slot` takes the current losses; `oldest` is
+// the new oldest row), both improvements, and the statistics of each
+// improvement around its population threshold.
+__global__ void robust_check_kernel(AdamParams a, PlainBufs b, int slot, int oldest, RobustOpts ro) {
+    __shared__ int s_cnt[3];
+    __shared__ unsigned int s_ext[4];
+    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) { s_ext[0] = 0u; s_ext[1] = 0xffffffffu; s_ext[2] = 0u; s_ext[3] = 0xffffffffu; }
+    __syncthreads();
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevVol& V = a.vols[a.blk_vol[blockIdx.x]];
+    if (v < a.nvtot && (v - V.off) < V.nvox) {
+        float cur = b.r.vloss[v];
+        b.r.ring[(size_t)slot * a.nvtot + v] = cur;
+        float old = b.r.ring[(size_t)oldest * a.nvtot + v];
+        float ia = (old - cur) / (old + 1e-8f);
+        float init = b.r.vinit[v];
+        float ib = (init - cur) / (init + 1e-8f);
+        b.r.imp_a[v] = ia;
+        b.r.imp_b[v] = ib;
+        if (isnan(ia) || isnan(ib)) atomicAdd(&s_cnt[2], 1);
+        if (ia <= ro.pop_thres) { atomicAdd(&s_cnt[0], 1); atomicMax(&s_ext[0], ord_bits(ia)); }
+        else if (!isnan(ia)) atomicMin(&s_ext[1], ord_bits(ia));
+        if (ib <= ro.init_pop_thres) { atomicAdd(&s_cnt[1], 1); atomicMax(&s_ext[2], ord_bits(ib)); }
+        else if (!isnan(ib)) atomicMin(&s_ext[3], ord_bits(ib));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        RobustStat* st = b.r.stat;
+        if (s_cnt[0]) atomicAdd(&st->n_le_a, s_cnt[0]);
+        if (s_cnt[1]) atomicAdd(&st->n_le_b, s_cnt[1]);
+        if (s_cnt[2]) atomicAdd(&st->n_nan, s_cnt[2]);
+        atomicMax(&st->max_le_a, s_ext[0]);
+        atomicMin(&st->min_gt_a, s_ext[1]);
+        atomicMax(&st->max_le_b, s_ext[2]);
+        atomicMin(&st->min_gt_b, s_ext[3]);
+    }
+}
+
+// Outlier flags, main mask and weight modulator (askadam.m:483-508).
+__global__ void robust_flag_kernel(AdamParams a, PlainBufs b, RobustOpts ro, int nvox) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevVol& V = a.vols[a.blk_vol[blockIdx.x]];
+    if (v >= a.nvtot || (v - V.off) >= V.nvox) return;
+    const RobustStat st = *b.r.stat;
+    const bool med_a = median_above(nvox, st.n_le_a, st.max_le_a, st.min_gt_a, st.n_nan, ro.pop_thres);
+    const bool med_b = median_above(nvox, st.n_le_b, st.max_le_b, st.min_gt_b, st.n_nan, ro.init_pop_thres);
+    const bool fail_a = b.r.imp_a[v] < ro.voxel_thres && med_a;
+    const bool fail_b = b.r.imp_b[v] < ro.init_thres && med_b;
+    int c = b.r.flagcnt[v];
+    c = (fail_a && fail_b) ? c + 1 : (c > 0 ? c - 1 : 0);
+    b.r.flagcnt[v] = c;
+    b.r.mainmask[v] = c == 0;
+    b.r.vmod[v] = c == 0 ? 1.0f : ro.outlier_weight;
+}
+
+__global__ void robust_differs_kernel(AdamParams a, PlainBufs b) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevVol& V = a.vols[a.blk_vol[blockIdx.x]];
+    bool d = v < a.nvtot && (v - V.off) < V.nvox && b.r.mainmask[v] != b.r.convmask[v];
+    if (__syncthreads_or(d) && threadIdx.x == 0) atomicOr(&b.r.stat->differs, 1);
+}
+
+// mainMask_conv = mainMask when it changed (askadam.m:559-562)
+__global__ void robust_refresh_kernel(AdamParams a, PlainBufs b) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.nvtot || !b.r.stat->differs) return;
+    b.r.convmask[v] = b.r.mainmask[v];
+    if (v == 0) b.acc[7] = 1.0;
+}
+
+// mean(perVoxelLoss(mainMask_conv)) as sum and count into acc[5], acc[6]
+__global__ void robust_conv_kernel(AdamParams a, PlainBufs b) {
+    __shared__ double s_red[2 * 32 * 2];
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevVol& V = a.vols[a.blk_vol[blockIdx.x]];
+    bool in = v < a.nvtot && (v - V.off) < V.nvox && b.r.convmask[v];
+    float q[2] = {in ? b.r.vloss[v] : 0.0f, in ? 1.0f : 0.0f};
+    block_accumulate<2>(q, b.acc + 5, 1.0, s_red, 0);
 }
 
 template <int NP>
@@ -817,6 +942,46 @@ cudaError_t launch_forward_only(const DevProtocol& P, int model, const float* th
     case kNEXI: forward_only_kernel<kNEXI><<<nb, block, 0, s>>>(P, theta, b1, nvox, signal); break;
     default: forward_only_kernel<kNEXI2><<<nb, block, 0, s>>>(P, theta, b1, nvox, signal); break;
     }
+    ++g_kernel_launches;
+    return cudaGetLastError();
+}
+
+
+cudaError_t launch_robust_reset(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s) {
+    robust_reset_kernel<<<nblocks, block, 0, s>>>(a, b);
+    ++g_kernel_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_robust_seed(const AdamParams& a, const PlainBufs& b, int window, int block, int nblocks,
+                               cudaStream_t s) {
+    robust_seed_kernel<<<nblocks, block, 0, s>>>(a, b, window);
+    ++g_kernel_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_robust_check(const AdamParams& a, const PlainBufs& b, int slot, int oldest,
+                                const RobustOpts& ro, int nvox, int block, int nblocks, cudaStream_t s) {
+    RobustStat init{0, 0, 0, 0u, 0xffffffffu, 0u, 0xffffffffu, 0};
+    cudaError_t e = cudaMemcpyAsync(b.r.stat, &init, sizeof(init), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    robust_check_kernel<<<nblocks, block, 0, s>>>(a, b, slot, oldest, ro);
+    robust_flag_kernel<<<nblocks, block, 0, s>>>(a, b, ro, nvox);
+    g_kernel_launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_robust_window(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(&b.r.stat->differs, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    robust_differs_kernel<<<nblocks, block, 0, s>>>(a, b);
+    robust_refresh_kernel<<<nblocks, block, 0, s>>>(a, b);
+    g_kernel_launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_robust_conv(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s) {
+    robust_conv_kernel<<<nblocks, block, 0, s>>>(a, b);
     ++g_kernel_launches;
     return cudaGetLastError();
 }

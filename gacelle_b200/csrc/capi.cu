@@ -58,7 +58,7 @@ enum Slot {
     S_CKPT, S_RESF, S_RESM, S_THF, S_THM, S_RLF, S_RLM, S_BLK, S_VOLS, S_GIDX, S_MASK, S_GRID0,
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
-    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_NSLOTS
+    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_NSLOTS
 };
 
 struct gx_context {
@@ -308,6 +308,7 @@ struct Tracker {
     double ewic = 0, ewis = 0, ewig = 0;
     bool stopped = false;
     int stop_epoch = 0, reason = GX_STOP_NONE;
+    int reprime = 0;  // robustConvergence: epochs until the convergence window is clean again
 
     void init(const gx_askadam_opts* opts, double fid0, double reg0) {
         o = opts;
@@ -315,19 +316,26 @@ struct Tracker {
         ema = minLoss;
         buf.assign(o->convergence_window > 0 ? o->convergence_window : 1, 1.0);
     }
-    // Returns true if the loop stops at epoch e (before the update).
-    bool epoch(int e, double fid, double reg, double g2, double z2, double d2) {
+    // Returns true if the loop stops at epoch e (before the update).  With
+    // robustConvergence, lconv is the mean loss of the convergence voxel set
+    // and refreshed tells that the set was renewed at this epoch
+    // (utils/askadam.m:530-581).
+    bool epoch(int e, double fid, double reg, double g2, double z2, double d2, double lconv = 0.0,
+               bool refreshed = false) {
         double L = fid + reg;
         if (minLoss > L) { minLoss = L; minFid = fid; minReg = reg; minIter = e; }
+        const bool robust = o->robust_convergence != 0;
+        if (robust && refreshed) reprime = o->convergence_window;
+        const double Lc = robust ? lconv : L;
         double conv;
         if (o->convergence_model == GX_CONV_EMA) {
-            double en = o->ema_decay * ema + (1.0 - o->ema_decay) * L;
+            double en = o->ema_decay * ema + (1.0 - o->ema_decay) * Lc;
             conv = std::fabs(en - ema) / (std::fabs(ema) + 1e-8);
             ema = en;
         } else {
             int W = (int)buf.size();
             for (int i = 0; i < W - 1; ++i) buf[i] = buf[i + 1];
-            buf[W - 1] = L;
+            buf[W - 1] = Lc;
             double xm = (W + 1) / 2.0, ym = 0, sxy = 0, sxx = 0;
             for (int i = 0; i < W; ++i) ym += buf[i];
             ym /= W;
@@ -337,8 +345,9 @@ struct Tracker {
             }
             conv = sxx > 0 ? -(sxy / sxx) : 0.0;
         }
-        if (conv > o->convergence_value || e <= o->convergence_window) ewic = 0;
-        else if ((minLoss - L) > o->convergence_value) ewic = 0;
+        if (reprime > 0) { reprime -= 1; ewic = 0; }
+        else if (conv > o->convergence_value || e <= o->convergence_window) ewic = 0;
+        else if (!robust && (minLoss - L) > o->convergence_value) ewic = 0;
         else ewic += 1;
         if (o->step_tol > 0) {
             double sn = std::sqrt(d2) / (1.0 + std::sqrt(z2));
@@ -376,6 +385,10 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
     if (o->n_reg < 0 || o->n_reg > kMaxReg) return fail(GX_EINVAL, "n_reg must be in [0, %d]", kMaxReg);
     for (int r = 0; r < o->n_reg; ++r)
         if (o->reg_param[r] < 0 || o->reg_param[r] >= np) return fail(GX_EINVAL, "regmap index %d out of range", o->reg_param[r]);
+    if (o->robust_convergence && (o->weight_update_interval < 1 || o->outlier_check_window < 1 ||
+                                  o->convergence_window < 1))
+        return fail(GX_EINVAL, "robustConvergence needs weightUpdateInterval, outlierCheckWindow and "
+                               "convergenceWindow >= 1");
     bool tv = o->n_reg > 0 && o->lambda[0] > 0;
     if (tv)
         for (int d = 0; d < (o->tv_3d ? 3 : 2); ++d)
@@ -904,6 +917,39 @@ static gx_status adam_plain(AdamJob& J, AdamOut& out) {
     TRY(wsT(c, S_P_GTH, pn, &pb.gth));
     TRY(wsT(c, S_P_GZ, pn, &pb.gz));
     TRY(wsT(c, S_P_ACC, 8, &pb.acc));
+    pb.r = RobustBufs{};
+    const bool robust = o->robust_convergence != 0;
+    const int RW = robust ? o->outlier_check_window : 0;
+    RobustOpts ro{(float)o->outlier_weight, (float)o->outlier_voxel_thres, (float)o->outlier_pop_thres,
+                  (float)o->outlier_init_thres, (float)o->outlier_init_pop_thres};
+    if (robust) {
+        const size_t nv = J.nvtot;
+        auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+        size_t of[11];
+        of[0] = 0;
+        of[1] = of[0] + al(sizeof(float) * nv);              // vmod
+        of[2] = of[1] + al(sizeof(float) * nv);              // vloss
+        of[3] = of[2] + al(sizeof(float) * nv);              // vinit
+        of[4] = of[3] + al(sizeof(float) * nv * RW);         // ring
+        of[5] = of[4] + al(sizeof(float) * nv);              // imp_a
+        of[6] = of[5] + al(sizeof(float) * nv);              // imp_b
+        of[7] = of[6] + al(sizeof(int) * nv);                // flagcnt
+        of[8] = of[7] + al(nv);                              // mainmask
+        of[9] = of[8] + al(nv);                              // convmask
+        of[10] = of[9] + al(sizeof(RobustStat));
+        unsigned char* rb;
+        TRY(wsT(c, S_ROBUST, of[10], &rb));
+        pb.r.vmod = reinterpret_cast<float*>(rb + of[0]);
+        pb.r.vloss = reinterpret_cast<float*>(rb + of[1]);
+        pb.r.vinit = reinterpret_cast<float*>(rb + of[2]);
+        pb.r.ring = reinterpret_cast<float*>(rb + of[3]);
+        pb.r.imp_a = reinterpret_cast<float*>(rb + of[4]);
+        pb.r.imp_b = reinterpret_cast<float*>(rb + of[5]);
+        pb.r.flagcnt = reinterpret_cast<int*>(rb + of[6]);
+        pb.r.mainmask = rb + of[7];
+        pb.r.convmask = rb + of[8];
+        pb.r.stat = reinterpret_cast<RobustStat*>(rb + of[9]);
+    }
     if (!J.stats) {
         // plain_zgrad only touches zprev when statistics are requested
         J.a.zprev = nullptr;
@@ -921,6 +967,12 @@ static gx_status adam_plain(AdamJob& J, AdamOut& out) {
         PlainBufs b = pb;
         b.theta += off; b.dth += off; b.signal += off; b.dsig += off; b.res += off;
         b.gth += off; b.gz += off;
+        int rhead = 0;  // oldest row of the robust loss history
+        if (robust) {
+            b.r.vmod += off; b.r.vloss += off; b.r.vinit += off; b.r.ring += off; b.r.imp_a += off;
+            b.r.imp_b += off; b.r.flagcnt += off; b.r.mainmask += off; b.r.convmask += off;
+            CK(launch_robust_reset(a, b, J.B, V.nblocks, c->stream));
+        }
         Tracker& t = out.tr[i];
         float* zmin = J.zr + off;
         float* resm = out.resm ? out.resm + off : nullptr;
@@ -936,6 +988,17 @@ static gx_status adam_plain(AdamJob& J, AdamOut& out) {
             if (J.tv) CK(launch_plain_tv(a, b, J.grid[0], J.B, V.nblocks, c->stream));
             CK(launch_plain_zgrad(a, b, J.stats, J.B, V.nblocks, c->stream));
             n_main += J.tv ? 7 : 5;
+            if (robust && e >= 1) {
+                // perVoxelLossInit is the starting point's evaluation, equal to epoch 1's
+                if (e == 1) CK(launch_robust_seed(a, b, RW, J.B, V.nblocks, c->stream));
+                if (e % o->weight_update_interval == 0) {
+                    const int slot = rhead;
+                    rhead = (rhead + 1) % RW;
+                    CK(launch_robust_check(a, b, slot, rhead, ro, J.hv[i].nvox, J.B, V.nblocks, c->stream));
+                }
+                if (e % o->convergence_window == 0) CK(launch_robust_window(a, b, J.B, V.nblocks, c->stream));
+                CK(launch_robust_conv(a, b, J.B, V.nblocks, c->stream));
+            }
             double acc[8];
             CK(cudaMemcpyAsync(acc, pb.acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
@@ -949,7 +1012,8 @@ static gx_status adam_plain(AdamJob& J, AdamOut& out) {
             }
             if (e >= 1) {
                 int before = t.minIter;
-                t.epoch(e, acc[0], acc[1], acc[2], acc[3], acc[4]);
+                if (robust) t.epoch(e, acc[0], acc[1], acc[2], acc[3], acc[4], acc[5] / acc[6], acc[7] != 0.0);
+                else t.epoch(e, acc[0], acc[1], acc[2], acc[3], acc[4]);
                 snap = snap || t.minIter != before;
             }
             if (snap) {
@@ -1062,7 +1126,9 @@ extern "C" gx_status gx_askadam(gx_context* c, const gx_model* model, int32_t me
     CK(cudaEventRecord(c->ev[0], c->stream));
     TRY(adam_setup(J));
     AdamOut out;
-    if (opts->path == GX_PATH_PLAIN) TRY(adam_plain(J, out));
+    // robustConvergence couples every epoch to per-voxel losses and a
+    // readback, as the reference's loop does: it runs on the op-by-op path
+    if (opts->path == GX_PATH_PLAIN || opts->robust_convergence) TRY(adam_plain(J, out));
     else TRY(adam_fused(J, out));
     gx_status st = adam_write_results(J, out, results);
     trace.mark("write");

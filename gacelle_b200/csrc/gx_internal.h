@@ -79,6 +79,27 @@ cudaError_t launch_copy_state(const AdamParams& a, float* dst, const float* z_, 
                               cudaStream_t s);
 
 // Plain (unfused) path: one kernel per reference operation.
+// robustConvergence state of the op-by-op path (utils/askadam.m:221-241,
+// 448-510); all arrays [nvtot] unless noted, NULL when the option is off.
+struct RobustStat {
+    int n_le_a, n_le_b, n_nan;          // counts of improvements <= the population thresholds
+    unsigned int max_le_a, min_gt_a;    // order-preserving bits of the neighbours of each threshold
+    unsigned int max_le_b, min_gt_b;
+    int differs;                        // main mask differs from the convergence mask
+};
+struct RobustBufs {
+    float* vmod = nullptr;               // weight modulator (1 or outlierWeight)
+    float* vloss = nullptr;              // per-voxel mean residual of the current evaluation
+    float* vinit = nullptr;              // ... of the starting point (perVoxelLossInit)
+    float* ring = nullptr;               // [window][nvtot] loss history of the last checks
+    float* imp_a = nullptr;              // improvement over the history window
+    float* imp_b = nullptr;              // improvement since the start
+    int* flagcnt = nullptr;              // outlierFlagCount
+    unsigned char* mainmask = nullptr;   // unflagged voxels
+    unsigned char* convmask = nullptr;   // voxel set of the convergence signal (mainMask_conv)
+    RobustStat* stat = nullptr;
+};
+
 struct PlainBufs {
     float* theta;    // [np][nvtot]
     float* dth;      // [np][nvtot] dtheta/dz
@@ -87,7 +108,8 @@ struct PlainBufs {
     float* res;      // [nm][nvtot]
     float* gth;      // [np][nvtot]
     float* gz;       // [np][nvtot]
-    double* acc;     // [8] per-iteration sums
+    double* acc;     // [8] per-iteration sums; robustConvergence uses [5..7]
+    RobustBufs r;
 };
 cudaError_t launch_plain_unscale(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
 cudaError_t launch_plain_forward(const AdamParams& a, int model, const PlainBufs& b, int block,
@@ -102,6 +124,17 @@ cudaError_t launch_plain_zgrad(const AdamParams& a, const PlainBufs& b, bool sta
                                int nblocks, cudaStream_t s);
 cudaError_t launch_plain_update(const AdamParams& a, const PlainBufs& b, int e, int block,
                                 int nblocks, cudaStream_t s);
+// robustConvergence on the op-by-op path (one volume view per call).
+struct RobustOpts {
+    float outlier_weight, voxel_thres, pop_thres, init_thres, init_pop_thres;
+};
+cudaError_t launch_robust_reset(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
+cudaError_t launch_robust_seed(const AdamParams& a, const PlainBufs& b, int window, int block, int nblocks,
+                               cudaStream_t s);
+cudaError_t launch_robust_check(const AdamParams& a, const PlainBufs& b, int slot, int oldest,
+                                const RobustOpts& ro, int nvox, int block, int nblocks, cudaStream_t s);
+cudaError_t launch_robust_window(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
+cudaError_t launch_robust_conv(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
 
 // Forward only (gx_forward).
 cudaError_t launch_forward_only(const DevProtocol& P, int model, const float* theta,

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define GX_ABI_VERSION 2
+#define GX_ABI_VERSION 3
 
 typedef enum {
     GX_OK = 0,
@@ -151,6 +151,21 @@ typedef struct {
     int32_t path;               /* gx_path */
     int32_t chunk;              /* fused path: iterations per launch if stopping may trigger; 0 = auto */
     int32_t block_size;         /* 0 = auto-tuned */
+    /* robustConvergence (update_outlier_mask, utils/askadam.m:448-510, and the
+     * main-population convergence signal of :530-581): every
+     * weight_update_interval epochs, voxels that improve less than
+     * outlier_voxel_thres over the last outlier_check_window checks and less
+     * than outlier_init_thres since the start, while the population's median
+     * improvements exceed outlier_pop_thres / outlier_init_pop_thres, are
+     * flagged and their weights scaled by outlier_weight (the mse loss ignores
+     * weights, as in the reference); convergence is judged on the mean loss of
+     * the unflagged voxels.  The engine runs it on the op-by-op path, which
+     * reads the loss back every epoch as the reference's loop does.
+     * outlier_min_flag_duration is accepted and, as in the reference, unused. */
+    int32_t robust_convergence;
+    double outlier_weight;
+    int32_t weight_update_interval, outlier_check_window, outlier_min_flag_duration;
+    double outlier_voxel_thres, outlier_pop_thres, outlier_init_thres, outlier_init_pop_thres;
 } gx_askadam_opts;
 
 /* Per-volume askAdam output (out.final / out.min of utils/askadam.m:345-362).

@@ -49,7 +49,11 @@ class OrcAdamOpts(C.Structure):
                 ("step_tol", C.c_double), ("grad_tol", C.c_double), ("patience_step", C.c_double),
                 ("patience_grad", C.c_double), ("n_reg", C.c_int), ("reg_param", C.c_int * 8),
                 ("lambda_", C.c_double * 8), ("tv_3d", C.c_int), ("voxel_size", C.c_double * 3),
-                ("nthreads", C.c_int), ("state_f32", C.c_int)]
+                ("nthreads", C.c_int), ("state_f32", C.c_int), ("robust", C.c_int),
+                ("outlier_weight", C.c_double), ("weight_update_interval", C.c_int),
+                ("outlier_check_window", C.c_int), ("outlier_voxel_thres", C.c_double),
+                ("outlier_pop_thres", C.c_double), ("outlier_init_thres", C.c_double),
+                ("outlier_init_pop_thres", C.c_double)]
 
 
 class OrcVolume(C.Structure):
@@ -63,7 +67,7 @@ class OrcAdamResult(C.Structure):
                 ("min_residual", _dp), ("loss_history", _dp), ("final_loss", C.c_double),
                 ("final_fid", C.c_double), ("final_reg", C.c_double), ("min_loss", C.c_double),
                 ("min_fid", C.c_double), ("min_reg", C.c_double), ("final_niter", C.c_int),
-                ("min_niter", C.c_int), ("stop_reason", C.c_int)]
+                ("min_niter", C.c_int), ("stop_reason", C.c_int), ("ever_flagged", C.POINTER(C.c_ubyte))]
 
 
 class OrcMcmcOpts(C.Structure):
@@ -314,6 +318,14 @@ def adam_opts(lb, ub, fitting: dict):
     o.grad_tol = f["convergenceGradTol"]
     o.patience_step = float(f["patienceStep"])
     o.patience_grad = float(f["patienceGrad"])
+    o.robust = 1 if f.get("robustConvergence") else 0
+    o.outlier_weight = f.get("outlierWeight", 0.1)
+    o.weight_update_interval = int(f.get("weightUpdateInterval", 5))
+    o.outlier_check_window = int(f.get("outlierCheckWindow", 5))
+    o.outlier_voxel_thres = f.get("outlierVoxelThres", 0.01)
+    o.outlier_pop_thres = f.get("outlierPopThres", 0.05)
+    o.outlier_init_thres = f.get("outlierInitThres", 0.05)
+    o.outlier_init_pop_thres = f.get("outlierInitPopThres", 0.20)
     reg = f.get("_reg_index", [])
     lam = f.get("_reg_lambda", [])
     o.n_reg = len(reg)
@@ -343,6 +355,8 @@ def askadam(model: Model, vol: Volume, opts: OrcAdamOpts, want_min=True, want_re
     res.final_residual = _d(fr)
     res.min_residual = _d(mr)
     res.loss_history = _d(hist)
+    flagged = np.zeros(nv, dtype=np.uint8)
+    res.ever_flagged = flagged.ctypes.data_as(C.POINTER(C.c_ubyte))
     rc = lib().orc_askadam(C.byref(model.s), C.byref(vol.s), C.byref(opts), C.byref(res))
     if rc != 0:
         raise RuntimeError(f"orc_askadam failed ({rc})")
@@ -350,7 +364,7 @@ def askadam(model: Model, vol: Volume, opts: OrcAdamOpts, want_min=True, want_re
             "loss_history": hist, "final_loss": res.final_loss, "final_fid": res.final_fid,
             "final_reg": res.final_reg, "min_loss": res.min_loss, "min_fid": res.min_fid,
             "min_reg": res.min_reg, "final_niter": res.final_niter, "min_niter": res.min_niter,
-            "stop_reason": STOP_REASONS[res.stop_reason]}
+            "stop_reason": STOP_REASONS[res.stop_reason], "ever_flagged": flagged.astype(bool)}
 
 
 def model_gradient(model: Model, vol: Volume, opts: OrcAdamOpts, theta):

@@ -555,6 +555,8 @@ typedef struct {
     double* grid;          /* full-grid image scratch */
     double* grid_g;
     size_t ngrid;
+    const double* wmod;    /* [nv] robustConvergence weight modulator, or NULL */
+    double* vloss;         /* [nv] per-voxel mean residual of the last evaluation, or NULL */
 } adam_ctx;
 
 /* askadam.model_gradient (utils/askadam.m:23-117) at parameters z (linear
@@ -581,7 +583,7 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
             int bad = !isfinite(s[k]);
             double sk = bad ? 0.0 : s[k]; /* utils.set_nan_inf_zero, askadam.m:80 */
             double y = vol->data[(size_t)k * nv + v];
-            double w = vol->weights ? vol->weights[(size_t)k * nv + v] : 1.0;
+            double w = (vol->weights ? vol->weights[(size_t)k * nv + v] : 1.0) * (c->wmod ? c->wmod[v] : 1.0);
             double rv = orc_loss_value(o->loss, sk, y, w, sig, o->mse_scale, o->huber_delta);
             if (res) res[(size_t)k * nv + v] = rv;
             lf += rv;
@@ -594,6 +596,8 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
     /* summed in voxel order: the same state always gives the same loss,
      * whatever the thread count */
     for (int v = 0; v < nv; ++v) fid += lfv[v];
+    if (c->vloss)
+        for (int v = 0; v < nv; ++v) c->vloss[v] = lfv[v] / nm;  /* mean(reshape(residuals, Nmeas, Nvol), 1) */
     free(lfv);
     fid *= c->norm;
     double reg = 0.0;
@@ -629,6 +633,7 @@ static int setup_ctx(adam_ctx* c, const orc_model* m, const orc_volume* vol,
     double nn = vol->norm_nvox > 0 ? vol->norm_nvox : (double)vol->nvox;
     c->norm = 1.0 / ((double)c->nm * nn);
     c->mask = NULL; c->grid = NULL; c->grid_g = NULL; c->ngrid = 0;
+    c->wmod = NULL; c->vloss = NULL;
     if (o->n_reg > 0 && o->lambda[0] > 0) {
         if (!vol->grid_index) return -1;
         c->ngrid = (size_t)vol->dims[0] * vol->dims[1] * vol->dims[2];
@@ -665,6 +670,24 @@ double orc_model_gradient(const orc_model* m, const orc_volume* vol, const orc_a
 }
 
 static double clamp01(double z) { return z < 0 ? 0 : (z > 1 ? 1 : z); }
+
+static int cmp_double(const void* a, const void* b) {
+    double x = *(const double*)a, y = *(const double*)b;
+    return (x > y) - (x < y);
+}
+
+/* median of n values (NaN if any is NaN; even n: mean of the two middle ones) */
+static double median_d(const double* x, int n) {
+    double* t = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) {
+        if (isnan(x[i])) { free(t); return NAN; }
+        t[i] = x[i];
+    }
+    qsort(t, (size_t)n, sizeof(double), cmp_double);
+    double med = n == 0 ? NAN : (n & 1) ? t[n / 2] : 0.5 * (t[n / 2 - 1] + t[n / 2]);
+    free(t);
+    return med;
+}
 
 int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* o,
                 orc_adam_result* r) {
@@ -720,9 +743,34 @@ int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* 
         L_;                                                                                \
     })
 
+    /* robustConvergence state (utils/askadam.m:221-241) */
+    int RW = o->outlier_check_window > 0 ? o->outlier_check_window : 1;
+    double *wmod = NULL, *vloss = NULL, *vinit = NULL, *vhist = NULL, *impA = NULL, *impB = NULL;
+    int *flagcnt = NULL;
+    unsigned char *mainmask = NULL, *convmask = NULL;
+    int reprime = 0;
+    if (o->robust) {
+        wmod = (double*)malloc(sizeof(double) * nv);
+        vloss = (double*)malloc(sizeof(double) * nv);
+        vinit = (double*)malloc(sizeof(double) * nv);
+        vhist = (double*)malloc(sizeof(double) * (size_t)RW * nv);
+        impA = (double*)malloc(sizeof(double) * nv);
+        impB = (double*)malloc(sizeof(double) * nv);
+        flagcnt = (int*)calloc(nv, sizeof(int));
+        mainmask = (unsigned char*)malloc(nv);
+        convmask = (unsigned char*)malloc(nv);
+        for (int v = 0; v < nv; ++v) { wmod[v] = 1.0; mainmask[v] = 1; convmask[v] = 1; }
+        c.wmod = wmod;
+        c.vloss = vloss;
+    }
+
     double fid, reg;
     double loss = EVAL(res, &fid, &reg);
     if (r->loss_history) r->loss_history[0] = loss;
+    if (o->robust) { /* perVoxelLossInit, history = repmat(init, outlierCheckWindow, 1) */
+        memcpy(vinit, vloss, sizeof(double) * nv);
+        for (int q = 0; q < RW; ++q) memcpy(vhist + (size_t)q * nv, vloss, sizeof(double) * nv);
+    }
     double minLoss = loss, minFid = fid, minReg = reg;
     memcpy(zmin, z, sizeof(double) * n);
     memcpy(resmin, res, sizeof(double) * (size_t)nm * nv);
@@ -744,15 +792,49 @@ int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* 
             memcpy(resmin, res, sizeof(double) * (size_t)nm * nv);
             minIter = e;
         }
-        /* update_convergence_signals, askadam.m:512-632 (robustConvergence off) */
+        double loss_conv = loss;
+        if (o->robust) {
+            /* update_outlier_mask (askadam.m:448-510): the new weights apply
+             * from the next evaluation */
+            if (o->weight_update_interval > 0 && e % o->weight_update_interval == 0) {
+                memmove(vhist, vhist + nv, sizeof(double) * (size_t)(RW - 1) * nv);
+                memcpy(vhist + (size_t)(RW - 1) * nv, vloss, sizeof(double) * nv);
+                for (int v = 0; v < nv; ++v) {
+                    impA[v] = (vhist[v] - vloss[v]) / (vhist[v] + 1e-8);
+                    impB[v] = (vinit[v] - vloss[v]) / (vinit[v] + 1e-8);
+                }
+                double medA = median_d(impA, nv), medB = median_d(impB, nv);
+                for (int v = 0; v < nv; ++v) {
+                    int failA = impA[v] < o->outlier_voxel_thres && medA > o->outlier_pop_thres;
+                    int failB = impB[v] < o->outlier_init_thres && medB > o->outlier_init_pop_thres;
+                    if (failA && failB) flagcnt[v] += 1;
+                    else flagcnt[v] = flagcnt[v] > 0 ? flagcnt[v] - 1 : 0;
+                    mainmask[v] = flagcnt[v] == 0;
+                    wmod[v] = mainmask[v] ? 1.0 : o->outlier_weight;
+                    if (!mainmask[v] && r->ever_flagged) r->ever_flagged[v] = 1;
+                }
+            }
+            /* main-population loss with the mask frozen between window
+             * boundaries (askadam.m:530-563) */
+            if (e % (o->conv_window > 0 ? o->conv_window : 1) == 0 && memcmp(mainmask, convmask, nv) != 0) {
+                memcpy(convmask, mainmask, nv);
+                reprime = o->conv_window;
+            }
+            double sl = 0.0;
+            int cnt = 0;
+            for (int v = 0; v < nv; ++v)
+                if (convmask[v]) { sl += vloss[v]; ++cnt; }
+            loss_conv = sl / cnt;
+        }
+        /* update_convergence_signals, askadam.m:512-632 */
         double conv;
         if (o->conv_model == ORC_CONV_EMA) {
-            double en = o->ema_decay * ema + (1.0 - o->ema_decay) * loss;
+            double en = o->ema_decay * ema + (1.0 - o->ema_decay) * loss_conv;
             conv = fabs(en - ema) / (fabs(ema) + 1e-8);
             ema = en;
         } else {
             for (int i = 0; i < W - 1; ++i) buf[i] = buf[i + 1];
-            buf[W - 1] = loss;
+            buf[W - 1] = loss_conv;
             double xm = (W + 1) / 2.0, ym = 0, sxy = 0, sxx = 0;
             for (int i = 0; i < W; ++i) ym += buf[i];
             ym /= W;
@@ -762,8 +844,9 @@ int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* 
             }
             conv = sxx > 0 ? -(sxy / sxx) : 0.0;
         }
-        if (conv > o->conv_value || e <= o->conv_window) ewic = 0;
-        else if ((minLoss - loss) > o->conv_value) ewic = 0;
+        if (reprime > 0) { reprime -= 1; ewic = 0; }
+        else if (conv > o->conv_value || e <= o->conv_window) ewic = 0;
+        else if (!o->robust && (minLoss - loss) > o->conv_value) ewic = 0;
         else ewic += 1;
         if (o->step_tol > 0) {
             double num = 0, den = 0;
@@ -828,6 +911,8 @@ int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* 
 #undef EVAL
     free(z); free(zc); free(zmin); free(zprev); free(g); free(m1); free(m2);
     free(res); free(resmin); free(buf);
+    free(wmod); free(vloss); free(vinit); free(vhist); free(impA); free(impB);
+    free(flagcnt); free(mainmask); free(convmask);
     free_ctx(&c);
     return 0;
 }

@@ -107,6 +107,11 @@ typedef struct {
     double voxel_size[3];
     int nthreads;
     int state_f32;               /* round z, m, v to float after every update (FP32-storage emulation) */
+    /* robustConvergence (utils/askadam.m:448-510, 530-581) */
+    int robust;
+    double outlier_weight;
+    int weight_update_interval, outlier_check_window;
+    double outlier_voxel_thres, outlier_pop_thres, outlier_init_thres, outlier_init_pop_thres;
 } orc_adam_opts;
 
 typedef struct {
@@ -130,6 +135,7 @@ typedef struct {
     double final_loss, final_fid, final_reg;
     double min_loss, min_fid, min_reg;
     int final_niter, min_niter, stop_reason;
+    unsigned char* ever_flagged; /* [nvox] or NULL: robustConvergence flagged the voxel at some check */
 } orc_adam_result;
 
 int orc_askadam(const orc_model* m, const orc_volume* vol, const orc_adam_opts* o,

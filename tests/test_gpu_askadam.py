@@ -468,3 +468,61 @@ def test_gpuNEXIrice_mirror_fit_and_estimate(ctx):
     out = m.estimate(dwi, mask, {"sigma": sig}, {"iteration": 100, "start": "default", "lossFunction": "mse"})
     assert not out["mask"][0, 0, 0] and out["mask"].sum() >= 50
     assert out["final"]["fa"].shape == (6, 10, 1)
+
+
+# ----------------------------------------------------- robustConvergence ----
+def _robust_engine_vs_oracle(f, n_out, seed):
+    import test_oracle
+    om, y, th0, out = test_oracle._robust_problem(n_out=n_out, seed=seed)
+    y32 = y.astype(np.float32)
+    th0 = th0.astype(np.float32)
+    eng = run_engine("r2s", y32, th0, f, NAMES["r2s"])
+    orc = run_oracle("r2s", y32, th0, f, NAMES["r2s"])
+    return eng, orc, out
+
+
+def test_robust_convergence_matches_oracle(ctx):
+    """robustConvergence (utils/askadam.m:448-510) through the C-ABI.  The fit
+    is voxel-separable and an unflagged voxel keeps weight 1, so switching the
+    option on changes exactly the voxels it flags: that set must equal the
+    FP64 oracle's.  An L1 fit is sign-driven (chaotic in FP32), so the maps
+    are held to the FP32-state band around the FP64 oracle."""
+    import test_oracle
+    om, y, th0, out = test_oracle._robust_problem(n_out=20, seed=60)
+    y32, th0 = y.astype(np.float32), th0.astype(np.float32)
+    f = fitting(iteration=300, lossFunction="l1")
+    fr = dict(f, robustConvergence=True)
+    plain = run_engine("r2s", y32, th0, f, NAMES["r2s"], path="plain")
+    eng = run_engine("r2s", y32, th0, fr, NAMES["r2s"])
+    orc = run_oracle("r2s", y32, th0, fr, NAMES["r2s"])
+    o32 = run_oracle("r2s", y32, th0, dict(fr, _state_f32=True), NAMES["r2s"])
+    changed = np.flatnonzero(np.any(eng["final_theta"] != plain["final_theta"], axis=0))
+    np.testing.assert_array_equal(changed, np.flatnonzero(orc["ever_flagged"]))
+    for k in range(2):
+        band = rel_rmse(o32["final"][k], orc["final"][k])
+        assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 2 * band + 1e-4, (k, band)
+    assert eng["final_niteration"] == orc["final_niter"] == 300
+
+
+def test_robust_convergence_stops_with_oracle(ctx):
+    """The main-population convergence signal stops the engine where it stops
+    the oracle (well before the plain full-population signal would)."""
+    f = fitting(iteration=3000, lossFunction="l1", robustConvergence=True, patienceConvergence=5,
+                convergenceValue=1e-6, convergenceModel="linear", initialLearnRate=0.02)
+    eng, orc, out = _robust_engine_vs_oracle(f, 60, 61)
+    assert orc["stop_reason"] == "convergence"
+    assert _lib.STOP_REASONS[eng["stop_reason"]] == "convergence"
+    assert abs(eng["final_niteration"] - orc["final_niter"]) <= 10, (eng["final_niteration"], orc["final_niter"])
+
+
+def test_robust_convergence_leaves_mse_unchanged(ctx):
+    """mse ignores weights (utils/askadam.m:93-94), so with the convergence
+    test disabled robustConvergence changes nothing in an mse fit."""
+    import test_oracle
+    om, y, th0, out = test_oracle._robust_problem(seed=62)
+    y32, th0 = y.astype(np.float32), th0.astype(np.float32)
+    f = fitting(iteration=200, lossFunction="mse")
+    a = run_engine("r2s", y32, th0, f, NAMES["r2s"], path="plain")
+    b = run_engine("r2s", y32, th0, dict(f, robustConvergence=True), NAMES["r2s"])
+    np.testing.assert_array_equal(a["final_theta"], b["final_theta"])
+    np.testing.assert_array_equal(a["loss_history"], b["loss_history"])

@@ -475,3 +475,56 @@ def test_nexi_rice_vjp_matches_autograd_and_finite_differences():
             fd = (oracle.forward(om, tp[:, None], b1=[sigma[v]])[:, 0] -
                   oracle.forward(om, tm[:, None], b1=[sigma[v]])[:, 0]) @ sbar[:, v] / (2 * h)
             assert abs(fd - tb[k]) <= 1e-5 * max(1.0, abs(tb[k])), (v, k, fd, tb[k])
+
+
+# --------------------------------------------------- robustConvergence ----
+def _robust_problem(nv=200, n_out=20, seed=60):
+    """Voxels whose data the model fits well (parameters far from the start
+    point) and outlier voxels whose data are the start point's signal plus
+    large noise: their loss cannot improve, while the population improves."""
+    rng = np.random.default_rng(seed)
+    om = oracle.r2s(TE)
+    th = np.vstack([rng.uniform(0.5, 1.5, nv), rng.uniform(10, 60, nv)])
+    y = oracle.forward(om, th) + 0.005 * rng.standard_normal((12, nv))
+    out = rng.choice(nv, n_out, replace=False)
+    th0 = np.tile([[1.0], [30.0]], (1, nv))
+    y[:, out] = oracle.forward(om, th0[:, out]) + 0.3 * rng.standard_normal((12, n_out))
+    return om, y.astype(np.float32).astype(np.float64), th0, np.sort(out)
+
+
+def test_robust_convergence_downweights_exactly_the_stagnant_voxels():
+    """update_outlier_mask (utils/askadam.m:448-510): with an L1 loss (weights
+    used), voxels flagged as outliers have their gradient scaled by
+    outlierWeight, so exactly they leave the unweighted trajectory; the fit is
+    voxel-separable, so every other voxel is unchanged.  With mse (weights
+    ignored) nothing changes."""
+    om, y, th0, out = _robust_problem()
+    lb, ub = [0.0, 0.1], [2.0, 200.0]
+    for loss, expect in (("l1", True), ("mse", False)):
+        f = _fitting(iteration=300, lossFunction=loss)
+        a = oracle.askadam(om, oracle.Volume(y, theta0=th0), oracle.adam_opts(lb, ub, f))
+        b = oracle.askadam(om, oracle.Volume(y, theta0=th0),
+                           oracle.adam_opts(lb, ub, dict(f, robustConvergence=True)))
+        changed = np.flatnonzero(np.any(a["final"] != b["final"], axis=0))
+        flagged = np.flatnonzero(b["ever_flagged"])
+        assert flagged.size >= 5 and np.all(np.isin(flagged, out)), (flagged, out)
+        if expect:
+            np.testing.assert_array_equal(changed, flagged)
+        else:
+            assert changed.size == 0
+
+
+def test_robust_convergence_judges_the_main_population():
+    """With robustConvergence the convergence signal is the mean loss of the
+    unflagged voxels (askadam.m:530-581): outliers that keep the
+    full-population loss moving no longer hold the loop back, and the main
+    population's plateau stops the robust run well before the plain run."""
+    om, y, th0, out = _robust_problem(n_out=60, seed=61)
+    lb, ub = [0.0, 0.1], [2.0, 200.0]
+    f = _fitting(iteration=3000, lossFunction="l1", patienceConvergence=5, convergenceValue=1e-6,
+                 convergenceModel="linear", initialLearnRate=0.02)
+    a = oracle.askadam(om, oracle.Volume(y, theta0=th0), oracle.adam_opts(lb, ub, f))
+    b = oracle.askadam(om, oracle.Volume(y, theta0=th0), oracle.adam_opts(lb, ub, dict(f, robustConvergence=True)))
+    assert b["ever_flagged"].any() and np.all(np.isin(np.flatnonzero(b["ever_flagged"]), out))
+    assert a["stop_reason"] == b["stop_reason"] == "convergence"
+    assert b["final_niter"] < 0.6 * a["final_niter"], (b["final_niter"], a["final_niter"])
