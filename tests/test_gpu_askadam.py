@@ -526,3 +526,19 @@ def test_robust_convergence_leaves_mse_unchanged(ctx):
     b = run_engine("r2s", y32, th0, dict(f, robustConvergence=True), NAMES["r2s"])
     np.testing.assert_array_equal(a["final_theta"], b["final_theta"])
     np.testing.assert_array_equal(a["loss_history"], b["loss_history"])
+
+
+def test_fit_distributed_single_rank_equals_model_fit(ctx):
+    """segments.fit_distributed without a process group fits the whole volume
+    on this GPU: the same maps as the model's own fit."""
+    from gacelle_b200 import gpuR2starMapping, phantoms, segments
+    mask = phantoms.ellipsoid_mask((12, 10, 8), 1.0)
+    data, _ = phantoms.r2s_phantom(mask, 71)
+    te = np.arange(2.0, 40.6, 3.5) * 1e-3
+    m = gpuR2starMapping(te)
+    m.context = ctx
+    f = {"iteration": 100, "lossFunction": "mse", "start": "default", "tol": 0.0}
+    a = m.fit(data, mask, dict(f))
+    b = segments.fit_distributed(lambda d, mk, e, p: m.fit(d, mk, dict(f)), data, mask)
+    for k in ("M0", "R2star"):
+        np.testing.assert_array_equal(a["final"][k], b["final"][k])
