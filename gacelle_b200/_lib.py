@@ -117,6 +117,8 @@ SIGNATURES = {
     "gx_context_destroy": (C.c_int, [C.c_void_p]),
     "gx_context_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "gx_last_timing": (C.c_int, [C.c_void_p, C.POINTER(GxTiming)]),
+    "gx_dictionary_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                                      C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gx_set_cancel_flag": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "gx_model_sizes": (C.c_int, [C.POINTER(GxModel), _i32p, _i32p]),
     "gx_forward": (C.c_int, [C.c_void_p, C.POINTER(GxModel), C.c_int32, C.c_void_p, C.c_void_p,

@@ -58,7 +58,8 @@ enum Slot {
     S_CKPT, S_RESF, S_RESM, S_THF, S_THM, S_RLF, S_RLM, S_BLK, S_VOLS, S_GIDX, S_MASK, S_GRID0,
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
-    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_NSLOTS
+    S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
+    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_NSLOTS
 };
 
 struct gx_context {
@@ -1408,6 +1409,61 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     c->timing.total_ms = ms;
     c->timing.main_kernel_ms = kernel_ms;
     c->timing.main_launches = launches;
+    c->timing.kernel_launches = g_kernel_launches - scope.launches0;
+    c->timing.h2d_bytes = h2d;
+    c->timing.d2h_bytes = d2h;
+    return GX_OK;
+}
+
+extern "C" gx_status gx_dictionary_match(gx_context* c, int32_t mem, const float* signals, int32_t nvox,
+                                         const float* dict, int32_t ndict, int32_t nm, const float* wt,
+                                         int32_t* best, float* best_sse) {
+    if (!c || !signals || !dict || !best) return fail(GX_EINVAL, "NULL argument");
+    if (mem != GX_MEM_HOST && mem != GX_MEM_DEVICE) return fail(GX_EINVAL, "bad mem");
+    if (nvox < 1 || ndict < 1) return fail(GX_EINVAL, "nvox and ndict must be >= 1");
+    if (nm < 1 || nm > kMaxMeas) return fail(GX_EINVAL, "nm must be in [1, %d]", kMaxMeas);
+    CallScope scope(c);
+    const float *ds = signals, *dd = dict, *dw = wt;
+    int* db = best;
+    float* dsse = best_sse;
+    long long h2d = 0, d2h = 0;
+    if (mem == GX_MEM_HOST) {
+        float *s1, *s2, *s3 = nullptr, *s5 = nullptr;
+        int* s4;
+        TRY(wsT(c, S_DICT_SIG, (size_t)nm * nvox, &s1));
+        TRY(wsT(c, S_DICT_D, (size_t)nm * ndict, &s2));
+        CK(cudaMemcpyAsync(s1, signals, sizeof(float) * nm * nvox, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(s2, dict, sizeof(float) * nm * ndict, cudaMemcpyHostToDevice, c->stream));
+        h2d += sizeof(float) * ((long long)nm * nvox + (long long)nm * ndict);
+        if (wt) {
+            TRY(wsT(c, S_DICT_W, (size_t)nm, &s3));
+            CK(cudaMemcpyAsync(s3, wt, sizeof(float) * nm, cudaMemcpyHostToDevice, c->stream));
+            h2d += sizeof(float) * nm;
+        }
+        TRY(wsT(c, S_DICT_B, (size_t)nvox, &s4));
+        if (best_sse) TRY(wsT(c, S_DICT_S, (size_t)nvox, &s5));
+        ds = s1; dd = s2; dw = s3; db = s4; dsse = s5;
+    }
+    double *ie, *cj;
+    TRY(wsT(c, S_DICT_E, (size_t)ndict, &ie));
+    TRY(wsT(c, S_DICT_C, (size_t)ndict, &cj));
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CK(launch_dictionary_match(ds, nvox, dd, ndict, nm, dw, ie, cj, db, dsse, c->stream));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    if (mem == GX_MEM_HOST) {
+        CK(cudaMemcpyAsync(best, db, sizeof(int32_t) * nvox, cudaMemcpyDeviceToHost, c->stream));
+        d2h += sizeof(int32_t) * nvox;
+        if (best_sse) {
+            CK(cudaMemcpyAsync(best_sse, dsse, sizeof(float) * nvox, cudaMemcpyDeviceToHost, c->stream));
+            d2h += sizeof(float) * nvox;
+        }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+    c->timing.total_ms = ms;
+    c->timing.main_kernel_ms = ms;
+    c->timing.main_launches = 1;
     c->timing.kernel_launches = g_kernel_launches - scope.launches0;
     c->timing.h2d_bytes = h2d;
     c->timing.d2h_bytes = d2h;

@@ -136,6 +136,12 @@ cudaError_t launch_robust_check(const AdamParams& a, const PlainBufs& b, int slo
 cudaError_t launch_robust_window(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
 cudaError_t launch_robust_conv(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
 
+// Dictionary matching (dictionary.cu): invE, Cj are [ndict] double scratch.
+size_t dict_match_smem(int nm, bool weighted);
+cudaError_t launch_dictionary_match(const float* signals, int nvox, const float* dict, int ndict, int nm,
+                                    const float* wt, double* invE, double* Cj, int* best, float* best_sse,
+                                    cudaStream_t s);
+
 // Forward only (gx_forward).
 cudaError_t launch_forward_only(const DevProtocol& P, int model, const float* theta,
                                 const float* b1, int nvox, float* signal, cudaStream_t s);

@@ -372,6 +372,87 @@ class gpuNEXI(_ModelBase):
         g.setdefault("dataType", "volumetric")
         return g
 
+    # ---------------------------------------------- likelihood starting points
+    TRAIN_INTERVALS = [[0.01, 0.99], [1.5, 3.0], [0.5, 1.5], [1.0, 100.0], [0.01, 0.99]]
+
+    def traindata(self, N_samples=10000, lmax=0, intervals=None, seed=None):
+        """traindata (NEXI/gpuNEXI.m:762-811): parameters uniform in the
+        intervals (fa, Da, De, exchange time, p2; ra = (1 - fa) / time), in
+        batches of 1000, and their NEXI signals (Sl0[, Sl2]) on the engine.
+        The reference draws from MATLAB's twister seeded with the model seed;
+        here the same seed drives NumPy's PCG64."""
+        iv = np.asarray(intervals if intervals is not None else self.TRAIN_INTERVALS, dtype=np.float64)
+        batch = 1000
+        n = int(np.ceil(N_samples / batch)) * batch
+        rng = np.random.default_rng(self.seed if seed is None else seed)
+        pars = iv[:, :1] + np.diff(iv, axis=1) * rng.random((iv.shape[0], n))
+        pars[3] = 1.0 / pars[3] * (1.0 - pars[0])
+        if lmax == 0:
+            pars = pars[:4]
+        handle = _GxModelHandle(_lib.MODEL_NEXI, bval=self.b, delta=self.Delta, lmax=lmax, nx=self.nx)
+        S = self._forward_with(handle, pars)
+        out_iv = iv.copy()
+        out_iv[3] = (1.0 - iv[0, ::-1]) / iv[3, ::-1]
+        if lmax == 2:
+            out_iv = out_iv[:4]
+        return pars, S, out_iv
+
+    def _forward_with(self, handle, theta):
+        ctx = self.context or _lib.Context.default()
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        npar, nm = handle.sizes()
+        out = np.zeros((nm, theta.shape[1]), np.float32)
+        _lib.check(_lib.lib().gx_forward(ctx.ptr, C.byref(handle.s), _lib.MEM_HOST, theta.ctypes.data, None,
+                                         theta.shape[1], out.ctypes.data))
+        return out
+
+    def likelihood(self, S0, x_train, S_train, lmax=0):
+        """likelihood (NEXI/gpuNEXI.m:813-836) on the engine
+        (gx_dictionary_match): the best dictionary parameters per voxel."""
+        # kron(Nav(:), 1./(2*(0:2:lmax)+1)) flattened column-major: Sl0 weights, then Sl2 weights
+        wt = np.concatenate([self.Nav.ravel() / (2 * l + 1) for l in range(0, lmax + 1, 2)])
+        nL = lmax // 2
+        S0 = np.ascontiguousarray(np.asarray(S0, dtype=np.float32)[: len(self.b) * (nL + 1)])
+        D = np.ascontiguousarray(S_train, dtype=np.float32)
+        nm, nv = S0.shape
+        best = np.zeros(nv, np.int32)
+        sse = np.zeros(nv, np.float32)
+        w = None if np.all(wt == 1) else np.ascontiguousarray(wt, np.float32)
+        ctx = self.context or _lib.Context.default()
+        _lib.check(_lib.lib().gx_dictionary_match(ctx.ptr, _lib.MEM_HOST, S0.ctypes.data, nv, D.ctypes.data,
+                                                  D.shape[1], nm, None if w is None else w.ctypes.data,
+                                                  best.ctypes.data, sse.ctypes.data))
+        return np.asarray(x_train)[:, np.maximum(best, 0)], sse
+
+    def estimate_prior(self, dwi, mask, Nsample=None, lmax=0):
+        """estimate_prior (NEXI/gpuNEXI.m:675-760): dictionary starting points
+        for every voxel of the mask, then the CSF correction (voxels whose
+        low-b apparent diffusivity exceeds 1.5 get fa, ra (and p2) scaled by
+        0.01)."""
+        Nsample = 10000 if Nsample is None else int(Nsample)
+        x_train, S_train, _ = self.traindata(Nsample, lmax)
+        dwi = np.asarray(dwi, dtype=np.float64)
+        dims = utils.dims3(mask)
+        flat = dwi.reshape(-1, dwi.shape[-1], order="F").T           # [nmeas, nvox_all]
+        ind = np.flatnonzero(np.asarray(mask).reshape(-1, order="F") > 0)
+        npar = x_train.shape[0]  # fa, Da, De, ra [, p2 for lmax 2]
+        pars = np.zeros((npar, flat.shape[1]))
+        if ind.size:
+            pb, _ = self.likelihood(flat[:, ind], x_train, S_train, lmax)
+            pars[:, ind] = pb[:npar]
+        b = self.b
+        idx = b <= max(b.min(), 1.1)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            y = -np.log(flat[: len(b)][idx])
+            D0 = (b[idx] @ y) / (b[idx] @ b[idx])
+        D0 = np.maximum(np.where(np.isfinite(D0), D0, 0.0), 0.0)
+        csf = D0 > 1.5
+        scale = [0.01, 1.0, 1.0, 0.01, 0.01]
+        for k in range(npar):
+            pars[k, csf] *= scale[k]
+        return {p: pars[k].reshape(dims, order="F").astype(np.float32)
+                for k, p in enumerate(["fa", "Da", "De", "ra", "p2"][:npar])}
+
     def compute_optimisation_weights(self, mask, lossFunction, lmax):
         """NEXI/gpuNEXI.m:455-477: w = Nav/(2l+1), sqrt for L1, normalised."""
         ls = list(range(0, lmax + 1, 2))
@@ -401,9 +482,12 @@ class gpuNEXI(_ModelBase):
         if pars0 is None:
             start = fitting["start"]
             if isinstance(start, str) and start.lower() == "likelihood":
-                raise GacelleError(GX_EUNSUPPORTED, "start='likelihood' (dictionary starting points) is "
-                                                    "not implemented by the engine; pass pars0 or start='default'")
-            pars0 = utils.initialise_x0(utils.dims3(mask), self.modelParams, self.startPoint)
+                # determine_x0 (NEXI/gpuNEXI.m:632-662): dictionary starting points
+                pars0 = self.estimate_prior(dwi, mask, None, int(fitting["lmax"]))
+                if "noise" in self.modelParams:
+                    pars0["noise"] = np.full(utils.dims3(mask), self.startPoint[-1], np.float32)
+            else:
+                pars0 = utils.initialise_x0(utils.dims3(mask), self.modelParams, self.startPoint)
         pars0 = {p: np.clip(np.asarray(pars0[p], dtype=np.float32), fitting["lb"][k], fitting["ub"][k])
                  for k, p in enumerate(self.modelParams)}
         w = None
@@ -501,11 +585,49 @@ class gpuNEXIrice(gpuNEXI):
             valid &= keep.reshape(valid.shape, order="F")
         return dwi, valid, ex
 
+    def estimate_prior(self, dwi, mask, Nsample=None, sigma=None):
+        """estimate_prior (NEXI/gpuNEXIrice.m:449-531): as gpuNEXI's, with the
+        dictionary signals passed through the Rician mean at the scalar sigma
+        (determine_x0 uses the median of the sigma map in the mask).  The
+        engine's forward also applies min(s, 1), which only touches entries
+        above 1, a range the data mask excludes."""
+        Nsample = 10000 if Nsample is None else int(Nsample)
+        x_train, _, _ = self.traindata(Nsample, 0)
+        handle = _GxModelHandle(_lib.MODEL_NEXI_RICE, bval=self.b, delta=self.Delta, lmax=0, nx=self.nx)
+        ctx = self.context or _lib.Context.default()
+        th = np.ascontiguousarray(x_train, dtype=np.float32)
+        sig = np.full(th.shape[1], float(sigma), np.float32)
+        S_train = np.zeros((len(self.b), th.shape[1]), np.float32)
+        _lib.check(_lib.lib().gx_forward(ctx.ptr, C.byref(handle.s), _lib.MEM_HOST, th.ctypes.data,
+                                         sig.ctypes.data, th.shape[1], S_train.ctypes.data))
+        dims = utils.dims3(mask)
+        idx = utils.mask_index(mask)
+        y = utils.reshape_ND2GD(np.asarray(dwi, dtype=np.float64), idx)
+        pb, _ = self.likelihood(y, x_train, S_train, 0)
+        b = self.b
+        sel = b <= max(b.min(), 1.1)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            D0 = (b[sel] @ -np.log(y[: len(b)][sel])) / (b[sel] @ b[sel])
+        D0 = np.maximum(np.where(np.isfinite(D0), D0, 0.0), 1e-8)
+        csf = D0 > 1.5
+        for k, sc in enumerate([0.01, 1.0, 1.0, 0.01]):
+            pb[k, csf] *= sc
+        return {p: utils.reshape_GD2ND(pb[k].astype(np.float32), mask).reshape(dims, order="F")
+                for k, p in enumerate(["fa", "Da", "De", "ra"])}
+
     def fit(self, dwi, mask=None, fitting=None, extraData=None, pars0=None):
         """NEXI/gpuNEXIrice.m:203-316 (argument order of the reference)."""
         if extraData is None or "sigma" not in extraData:
             raise GacelleError(GX_EINVAL, "gpuNEXIrice.fit needs extraData['sigma']")
         fitting = self.check_set_default(fitting)
+        if mask is None:
+            mask = np.ones(utils.dims3(np.asarray(dwi)), dtype=bool)
+        start = fitting.get("start")
+        if pars0 is None and isinstance(start, str) and start.lower() == "likelihood":
+            # determine_x0 (NEXI/gpuNEXIrice.m:410-447): the median sigma in the mask
+            sig = np.asarray(extraData["sigma"], dtype=np.float64)
+            sigma = float(np.median(np.broadcast_to(sig, utils.dims3(mask))[np.asarray(mask) > 0]))
+            pars0 = self.estimate_prior(dwi, mask, None, sigma)
         return gpuNEXI.fit(self, dwi, mask, fitting, pars0, extradata=extraData)
 
     def estimate(self, dwi, mask, extraData, fitting=None, pars0=None):

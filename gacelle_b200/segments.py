@@ -94,6 +94,8 @@ def restore_segments(parts: list[dict], segs: list[dict], shape3) -> dict:
         first = vals[0]
         if isinstance(first, dict):
             return {k: merge([v[k] for v in vals], path + (k,)) for k in first}
+        if isinstance(first, (str, bytes, bool, np.bool_)):
+            return first  # character / logical scalars: kept from the first segment
         if np.isscalar(first) or (isinstance(first, np.ndarray) and first.ndim == 0):
             return np.array([float(v) for v in vals])
         if isinstance(first, np.ndarray) and first.ndim >= 3 and all(

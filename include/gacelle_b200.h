@@ -269,6 +269,17 @@ gx_status gx_askadam(gx_context* ctx, const gx_model* model, int32_t mem, const 
 gx_status gx_mcmc(gx_context* ctx, const gx_model* model, int32_t mem, const gx_volume* vols,
                   int32_t nvol, const gx_mcmc_opts* opts, gx_mcmc_result* results);
 
+/* Dictionary starting points (gpuNEXI.likelihood, NEXI/gpuNEXI.m:813-836,
+ * called by estimate_prior :675-760 for start = 'likelihood'): for each voxel
+ * the index of the first dictionary entry j minimising
+ * sum_m wt_m (S0_m - c S_jm)^2 with c = (S0 . S_j) / (S_j . S_j).
+ * signals [nm][nvox] and dict [nm][ndict] (voxel / entry fastest), wt [nm]
+ * or NULL (ones); best [nvox] (-1 when no entry scores, e.g. all-zero
+ * entries), best_sse [nvox] or NULL.  Host or device pointers per mem. */
+gx_status gx_dictionary_match(gx_context* ctx, int32_t mem, const float* signals, int32_t nvox,
+                              const float* dict, int32_t ndict, int32_t nm, const float* wt,
+                              int32_t* best, float* best_sse);
+
 /* No counterpart in the reference.  The fused askAdam fit of one volume
  * (final parameters only, every iteration run, no TV) for callers that cannot
  * allocate device memory while they run: applications whose framework owns

@@ -126,6 +126,8 @@ def lib():
                                C.POINTER(OrcMcmcOpts), C.POINTER(OrcMcmcResult)]
         L.orc_mcmc_nsamples.argtypes = [C.c_int, C.c_double, C.c_int]
         L.orc_gw_partner.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _ip]
+        L.orc_dictionary_match.argtypes = [_dp, C.c_int, _dp, C.c_int, C.c_int, _dp, _ip, _dp]
+        L.orc_dictionary_match.restype = None
         L.orc_tv_cost.argtypes = [_ip, C.POINTER(C.c_ubyte), _dp, C.c_int, _dp]
         L.orc_tv_cost.restype = C.c_double
         L.orc_tv_grad.argtypes = [_ip, C.POINTER(C.c_ubyte), _dp, C.c_int, _dp, _dp]
@@ -236,6 +238,19 @@ def gw_partner(seed, step, rep, nwalker):
     p = np.zeros(nwalker, dtype=np.int32)
     lib().orc_gw_partner(seed, step, rep, nwalker, p.ctypes.data_as(_ip))
     return p
+
+
+def dictionary_match(signals, dictionary, wt=None):
+    """gpuNEXI.likelihood (NEXI/gpuNEXI.m:813-836) on the FP64 oracle:
+    signals [nm][nvox], dictionary [nm][ndict]; returns (best index, best sse)."""
+    s = np.ascontiguousarray(signals, dtype=np.float64)
+    d = np.ascontiguousarray(dictionary, dtype=np.float64)
+    nm, nv = s.shape
+    w = None if wt is None else np.ascontiguousarray(wt, dtype=np.float64)
+    best = np.zeros(nv, dtype=np.int32)
+    sse = np.zeros(nv)
+    lib().orc_dictionary_match(_d(s), nv, _d(d), d.shape[1], nm, _d(w), best.ctypes.data_as(_ip), _d(sse))
+    return best, sse
 
 
 def tv_cost(mask3d, img3d, tv_3d=True, voxel_size=(2.0, 2.0, 2.0)):

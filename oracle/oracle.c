@@ -1476,3 +1476,33 @@ static int mcmc_gw_global(const orc_model* m, const orc_volume* vol, const doubl
     free(sum); free(sumsq); free(shift); free(pt);
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Dictionary starting points, gpuNEXI.likelihood (NEXI/gpuNEXI.m:813-836):  */
+/* sse = sum(wt .* (S0i - (S0i'*S) ./ dot(S,S) .* S).^2) in the direct form; */
+/* [sse_new, best_index] = min(sse) keeps the first minimum; NaN never wins. */
+/* ------------------------------------------------------------------------ */
+void orc_dictionary_match(const double* signals, int nvox, const double* dict, int ndict, int nm,
+                          const double* wt, int* best, double* best_sse) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nvox; ++i) {
+        double bs = INFINITY;
+        int bj = -1;
+        for (int j = 0; j < ndict; ++j) {
+            double d = 0.0, e = 0.0;
+            for (int m = 0; m < nm; ++m) {
+                double sj = dict[(size_t)m * ndict + j];
+                d += signals[(size_t)m * nvox + i] * sj;
+                e += sj * sj;
+            }
+            double c = d / e, sse = 0.0;
+            for (int m = 0; m < nm; ++m) {
+                double r = signals[(size_t)m * nvox + i] - c * dict[(size_t)m * ndict + j];
+                sse += (wt ? wt[m] : 1.0) * r * r;
+            }
+            if (sse < bs) { bs = sse; bj = j; }
+        }
+        best[i] = bj;
+        if (best_sse) best_sse[i] = bs;
+    }
+}

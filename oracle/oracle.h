@@ -183,6 +183,12 @@ int orc_mcmc_nsamples(int iteration, double burnin, int thinning);
 /* Derangement shared by all voxels at GW step k (mcmc.m:797-803). */
 void orc_gw_partner(uint64_t seed, int step, int rep, int nwalker, int* partner);
 
+/* likelihood (NEXI/gpuNEXI.m:813-836): for each voxel i the first dictionary
+ * entry j minimising sum_m wt_m (S0_im - c S_jm)^2, c = (S0_i . S_j) / (S_j . S_j).
+ * signals [nm][nvox], dict [nm][ndict] (measurement-major), wt [nm] or NULL. */
+void orc_dictionary_match(const double* signals, int nvox, const double* dict, int ndict, int nm,
+                          const double* wt, int* best, double* best_sse);
+
 /* 3-D anisotropic TV (utils/spatial_total_variation.m:24-66) on a full grid. */
 double orc_tv_cost(const int dims[3], const unsigned char* mask, const double* img,
                    int tv_3d, const double vs[3]);
