@@ -41,6 +41,8 @@ def parse_args():
     p.add_argument("--no-extra", action="store_true", help="skip the plain-path and MCMC side measurements")
     p.add_argument("--cpu-iters", type=int, default=40, help="iterations of the bounded CPU sample")
     p.add_argument("--iters", type=int, default=NITER, help="askAdam iterations per fit (profiling runs)")
+    p.add_argument("--c3-iters", type=int, default=1000, help="iterations of the batched joint R1R2* side run")
+    p.add_argument("--c4-iters", type=int, default=100, help="iterations of the NEXI Rician side run")
     p.add_argument("--grid", default="128x128x64", help="phantom grid (profiling runs)")
     p.add_argument("--mcmc-steps", type=int, default=200, help="GW steps of the MCMC side measurement")
     return p.parse_args()
@@ -415,7 +417,112 @@ def extras(ctx, W, opts, model, stream, args):
     out["mcmc_accepted_samples_per_s"] = st["n_accepted"] / sec
     out["mcmc_acceptance"] = st["n_accepted"] / st["n_proposals"]
     out["mcmc_ms_per_step"] = t["main_kernel_ms"] / steps
+    out.update(extra_r1r2s_batch(ctx, args))
+    out.update(extra_nexi_rician(ctx, args))
     return out
+
+
+def _gx_volume(y, th0, sigma=None):
+    v = _lib_mod().GxVolume()
+    nm, n = y.shape
+    v.dims[0], v.dims[1], v.dims[2] = n, 1, 1
+    v.nvox = n
+    v.data = y.ctypes.data_as(_lib_mod()._fp)
+    v.theta0 = th0.ctypes.data_as(_lib_mod()._fp)
+    if sigma is not None:
+        v.sigma = sigma.ctypes.data_as(_lib_mod()._fp)
+    return v
+
+
+def _lib_mod():
+    from gacelle_b200 import _lib
+    return _lib
+
+
+def extra_r1r2s_batch(ctx, args):
+    """Joint R1-R2* askAdam on a batch of six volumes with uneven voxel counts
+    (50k-400k, 1.26M voxels) in one call: 24 measurements (12 TE x 2 flip
+    angles), MSE, Adam lr 0.01, start (1, 1, 30), fused path."""
+    from gacelle_b200 import askadam_solver as gxa, phantoms
+    from gacelle_b200.models import _GxModelHandle
+    _lib = _lib_mod()
+    sizes = [50_000, 110_000, 170_000, 230_000, 300_000, 400_000]
+    ys = [phantoms.r1r2s_volume(n, 1003 + i)[0] for i, n in enumerate(sizes)]
+    th0s = [np.ascontiguousarray(np.tile(np.array([[1.0], [1.0], [30.0]], np.float32), (1, n))) for n in sizes]
+    model = _GxModelHandle(_lib.MODEL_R1R2S, te=phantoms.R1R2S_TE, fa_deg=phantoms.R1R2S_FA, tr=phantoms.R1R2S_TR)
+    f = gxa.check_set_default_basic({"iteration": args.c3_iters, "initialLearnRate": 0.01, "decayRate": 0.0,
+                                     "lossFunction": "mse", "tol": 0.0, "patienceConvergence": float("inf"),
+                                     "convergenceStepTol": 0.0, "convergenceGradTol": 0.0})
+    opts = gxa.build_opts(f, ["M0", "R1", "R2star"], [0.0, 0.1, 0.1], [2.0, 10.0, 200.0], "fused")
+    vols = (_lib.GxVolume * 6)(*[_gx_volume(y, t) for y, t in zip(ys, th0s)])
+    outs = [np.zeros((3, n), np.float32) for n in sizes]
+    res = (_lib.GxAskadamResult * 6)()
+    for r, o in zip(res, outs):
+        r.final_theta = o.ctypes.data_as(_lib._fp)
+    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, vols, 6, C.byref(opts), res))
+    t = ctx.timing()
+    nv = sum(sizes)
+    sec = t["main_kernel_ms"] / 1000.0
+    return {"c3_workload": f"joint R1R2* batch of 6 volumes ({nv} voxels), 24 measurements, MSE, "
+                           f"{args.c3_iters} iterations, one call",
+            "c3_voxel_fits_per_s": nv / sec, "c3_voxel_iterations_per_s": nv * args.c3_iters / sec,
+            "c3_call_ms": t["total_ms"]}
+
+
+def extra_nexi_rician(ctx, args):
+    """NEXI lmax 0 with the Rician likelihood loss, 100-node powder average,
+    500k voxels (sigma 0.02), a bounded number of iterations; and the
+    likelihood starting points of the same voxels against a 10^4-entry
+    dictionary (gpuNEXI.likelihood)."""
+    from gacelle_b200 import askadam_solver as gxa, phantoms
+    from gacelle_b200.models import _GxModelHandle, gpuNEXI
+    _lib = _lib_mod()
+    nv, nx = 500_000, 100
+    rng = np.random.default_rng(1004)
+    fa = rng.uniform(0.1, 0.9, nv)
+    tex = rng.uniform(2.0, 50.0, nv)
+    ra = (1 - fa) / tex
+    while (ra < 1 / 250).any():
+        bad = ra < 1 / 250
+        tex[bad] = rng.uniform(2.0, 50.0, bad.sum())
+        ra = (1 - fa) / tex
+    th = np.ascontiguousarray(np.vstack([fa, rng.uniform(1, 3, nv), rng.uniform(0.5, 1.5, nv), ra]),
+                              dtype=np.float32)
+    b, d = phantoms.nexi_shells()
+    model = _GxModelHandle(_lib.MODEL_NEXI, bval=b, delta=d, lmax=0, nx=nx)
+    S = np.zeros((24, nv), np.float32)
+    _lib.check(_lib.lib().gx_forward(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, th.ctypes.data, None, nv,
+                                     S.ctypes.data))
+    sig = 0.02
+    y = np.ascontiguousarray(np.sqrt((S + sig * rng.standard_normal(S.shape)) ** 2 +
+                                     (sig * rng.standard_normal(S.shape)) ** 2), dtype=np.float32)
+    lb, ub = [2.2e-16, 2.2e-16, 2.2e-16, 1 / 250], [1.0, 3.0, 3.0, 1.0]
+    th0 = np.ascontiguousarray(np.tile(np.array([[0.4], [2.0], [1.0], [0.05]], np.float32), (1, nv)))
+    f = gxa.check_set_default_basic({"iteration": args.c4_iters, "initialLearnRate": 0.01, "decayRate": 0.0,
+                                     "lossFunction": "rician", "noiseSigma": sig, "tol": 0.0,
+                                     "patienceConvergence": float("inf"), "convergenceStepTol": 0.0,
+                                     "convergenceGradTol": 0.0})
+    opts = gxa.build_opts(f, ["fa", "Da", "De", "ra"], lb, ub, "fused")
+    out = np.zeros((4, nv), np.float32)
+    vol = _gx_volume(y, th0)
+    res = _lib.GxAskadamResult()
+    res.final_theta = out.ctypes.data_as(_lib._fp)
+    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, C.byref(vol), 1, C.byref(opts),
+                                     C.byref(res)))
+    t = ctx.timing()
+    sec = t["main_kernel_ms"] / 1000.0
+    r = {"c4_workload": f"NEXI lmax 0, Rician loss, Nx {nx}, {nv} voxels, {args.c4_iters} iterations",
+         "c4_voxel_iterations_per_s": nv * args.c4_iters / sec, "c4_ms_per_iteration": t["main_kernel_ms"] / args.c4_iters}
+    # dictionary starting points of the same voxels
+    m = gpuNEXI(b, d)
+    m.context = ctx
+    x_train, S_train, _ = m.traindata(10_000, 0)
+    m.likelihood(y, x_train, S_train, 0)
+    t = ctx.timing()
+    r["dictionary_workload"] = f"likelihood starting points, {nv} voxels x {x_train.shape[1]} entries x 24 measurements"
+    r["dictionary_ms"] = t["main_kernel_ms"]
+    r["dictionary_pairs_per_s"] = nv * x_train.shape[1] / (t["main_kernel_ms"] / 1000.0)
+    return r
 
 
 def main():

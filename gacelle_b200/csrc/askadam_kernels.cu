@@ -368,6 +368,32 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
 }
 
 // Scatter the regularised maps of the current z into a TV grid.
+// Mask grid of the TV regulariser from the work-list grid indices, with the
+// input checks: an index outside its volume's grid sets bit 1 of err, an
+// index seen twice sets bit 2; bad_vol receives the lowest offending volume.
+// The byte mask is updated through 32-bit atomics on its aligned words.
+__global__ void tv_mask_kernel(AdamParams a, unsigned char* mask, int* err, int* bad_vol) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.nvtot) return;
+    const int vol = a.blk_vol[blockIdx.x];
+    const DevVol& V = a.vols[vol];
+    if (v - V.off >= V.nvox) return;
+    const int p = a.gidx[v];
+    const long long gsz = (long long)V.dims[0] * V.dims[1] * V.dims[2];
+    if (p < 0 || p >= gsz) {
+        atomicOr(err, 1);
+        atomicMin(bad_vol, vol);
+        return;
+    }
+    const size_t q = (size_t)V.grid_off + (size_t)p;
+    unsigned int* w = reinterpret_cast<unsigned int*>(mask + (q & ~(size_t)3));
+    const unsigned int bit = 1u << (8 * (q & 3));
+    if (atomicOr(w, bit) & bit) {
+        atomicOr(err, 2);
+        atomicMin(bad_vol, vol);
+    }
+}
+
 __global__ void tv_scatter_kernel(AdamParams a, float* grid) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= a.nvtot) return;
@@ -836,6 +862,13 @@ cudaError_t launch_init_state(const AdamParams& a, const float* theta0, double r
                               uint64_t seed, int block, cudaStream_t s) {
     int nb = (a.nvtot + block - 1) / block;
     init_state_kernel<<<nb, block, 0, s>>>(a, theta0, (float)randomness, seed);
+    ++g_kernel_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tv_mask(const AdamParams& a, unsigned char* mask, int* err, int* bad_vol, int block,
+                           int nblocks, cudaStream_t s) {
+    tv_mask_kernel<<<nblocks, block, 0, s>>>(a, mask, err, bad_vol);
     ++g_kernel_launches;
     return cudaGetLastError();
 }

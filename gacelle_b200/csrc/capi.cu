@@ -59,7 +59,7 @@ enum Slot {
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
-    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_NSLOTS
+    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_NSLOTS
 };
 
 struct gx_context {
@@ -605,15 +605,22 @@ static gx_status adam_setup(AdamJob& J) {
     a.sched = dsched;
     TRY(wsT(c, S_HIST, (size_t)J.nvol * (N + 1) * kHistW, &a.hist));
     CK(cudaMemsetAsync(a.hist, 0, sizeof(double) * J.nvol * (N + 1) * kHistW, c->stream));
-    // checkpoints: slot c holds the state after c*ckpt_every updates
+    // checkpoints: slot c holds the state after c*ckpt_every updates, every
+    // 16 updates within a budget of min(4 GB, free/4); free memory is only
+    // queried when the context's buffer cannot already hold that plan (the
+    // query can stall for milliseconds on a shared device)
     size_t slot_bytes = sizeof(float) * 3 * (size_t)J.np * nv;
-    size_t budget = (size_t)4 << 30;
-    size_t freeb = 0, totalb = 0;
-    if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && freeb / 4 < budget) budget = freeb / 4;
-    long long max_slots = budget / slot_bytes;
-    if (max_slots < 2) max_slots = 2;
+    const size_t cap4 = (size_t)4 << 30;
     int K = 16;
-    while ((long long)(N / K) + 1 > max_slots) K *= 2;
+    const size_t want16 = ((size_t)(N / 16) + 1) * slot_bytes;
+    if (!(want16 <= cap4 && c->cap[S_CKPT] >= want16)) {
+        size_t budget = cap4;
+        size_t freeb = 0, totalb = 0;
+        if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && freeb / 4 < budget) budget = freeb / 4;
+        long long max_slots = budget / slot_bytes;
+        if (max_slots < 2) max_slots = 2;
+        while ((long long)(N / K) + 1 > max_slots) K *= 2;
+    }
     J.ckpt_every = K;
     J.nslots = N / K + 1;
     TRY(wsT(c, S_CKPT, (size_t)J.nslots * 3 * J.np * nv, &a.ckpt));
@@ -625,33 +632,32 @@ static gx_status adam_setup(AdamJob& J) {
         unsigned char* mk;
         float *g0, *g1;
         TRY(wsT(c, S_GIDX, nv, &gidx));
-        TRY(wsT(c, S_MASK, (size_t)J.grid_total, &mk));
+        TRY(wsT(c, S_MASK, ((size_t)J.grid_total + 3) & ~(size_t)3, &mk));  // word-aligned for the mask kernel
         TRY(wsT(c, S_GRID0, (size_t)a.n_reg * J.grid_total, &g0));
         TRY(wsT(c, S_GRID1, (size_t)a.n_reg * J.grid_total, &g1));
         CK(cudaMemsetAsync(gidx, 0, sizeof(int) * nv, c->stream));
         CK(cudaMemsetAsync(g0, 0, sizeof(float) * a.n_reg * J.grid_total, c->stream));
         CK(cudaMemsetAsync(g1, 0, sizeof(float) * a.n_reg * J.grid_total, c->stream));
-        std::vector<unsigned char> hm((size_t)J.grid_total, 0);
+        CK(cudaMemsetAsync(mk, 0, ((size_t)J.grid_total + 3) & ~(size_t)3, c->stream));
+        const cudaMemcpyKind kind = copy_kind_host(J.mem) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
         for (int i = 0; i < J.nvol; ++i) {
             const gx_volume& v = J.vols[i];
-            const DevVol& d = J.hv[i];
-            std::vector<int32_t> gi((size_t)v.nvox);
-            if (J.mem == GX_MEM_HOST) memcpy(gi.data(), v.grid_index, sizeof(int32_t) * v.nvox);
-            else CK(cudaMemcpy(gi.data(), v.grid_index, sizeof(int32_t) * v.nvox, cudaMemcpyDeviceToHost));
-            long long gsz = (long long)v.dims[0] * v.dims[1] * v.dims[2];
-            for (int q = 0; q < v.nvox; ++q) {
-                if (gi[q] < 0 || gi[q] >= gsz) return fail(GX_EINVAL, "volume %d: grid_index[%d] out of range", i, q);
-                if (hm[d.grid_off + gi[q]]) return fail(GX_EINVAL, "volume %d: duplicate grid_index %d", i, gi[q]);
-                hm[d.grid_off + gi[q]] = 1;
-            }
-            CK(cudaMemcpyAsync(gidx + d.off, gi.data(), sizeof(int32_t) * v.nvox, cudaMemcpyHostToDevice, c->stream));
-            CK(cudaStreamSynchronize(c->stream));
+            CK(cudaMemcpyAsync(gidx + J.hv[i].off, v.grid_index, sizeof(int32_t) * v.nvox, kind, c->stream));
             if (J.mem == GX_MEM_HOST) J.h2d += sizeof(int32_t) * v.nvox;
         }
-        CK(cudaMemcpyAsync(mk, hm.data(), hm.size(), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
         a.gidx = gidx;
         a.maskgrid = mk;
+        // mask grid and index checks on the device
+        int* flags;
+        TRY(wsT(c, S_FLAGS, 2, &flags));
+        const int init[2] = {0, 0x7fffffff};
+        CK(cudaMemcpyAsync(flags, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+        CK(launch_tv_mask(a, mk, flags, flags + 1, J.B, J.nblocks, c->stream));
+        int hf[2];
+        CK(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (hf[0] & 1) return fail(GX_EINVAL, "volume %d: grid_index out of range", hf[1]);
+        if (hf[0] & 2) return fail(GX_EINVAL, "volume %d: duplicate grid_index", hf[1]);
         a.grid_cur = g0;
         a.grid_next = g1;
         J.grid[0] = g0;

@@ -69,6 +69,8 @@ cudaError_t launch_fused(const AdamParams& a, int model, int loss, bool stats, i
 cudaError_t launch_tv_step(const AdamParams& a, int model, int loss, bool stats, int e,
                            bool update, bool record, bool want_res, int block, int nblocks,
                            cudaStream_t s);
+cudaError_t launch_tv_mask(const AdamParams& a, unsigned char* mask, int* err, int* bad_vol, int block,
+                           int nblocks, cudaStream_t s);
 cudaError_t launch_tv_scatter(const AdamParams& a, float* grid, int block, int nblocks,
                               cudaStream_t s);
 cudaError_t launch_finalize(const AdamParams& a, const float* zsrc, float* theta_out,

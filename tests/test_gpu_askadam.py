@@ -542,3 +542,22 @@ def test_fit_distributed_single_rank_equals_model_fit(ctx):
     b = segments.fit_distributed(lambda d, mk, e, p: m.fit(d, mk, dict(f)), data, mask)
     for k in ("M0", "R2star"):
         np.testing.assert_array_equal(a["final"][k], b["final"][k])
+
+
+@pytest.mark.parametrize("bad", ["duplicate", "out_of_range"])
+def test_tv_grid_index_checked_on_device(ctx, bad):
+    """The TV mask grid is built on the device from the grid indices; a
+    repeated or out-of-range index is reported as GX_EINVAL naming the volume,
+    and the context stays usable."""
+    y, th0, kw = _tv_problem()
+    gidx = kw["gidx"].copy()
+    if bad == "duplicate":
+        gidx[5] = gidx[4]
+    else:
+        gidx[7] = int(np.prod(kw["dims"]))
+    f = fitting(iteration=20, **{"lambda": [1e-3], "regmap": ["R2star"], "TVmode": "3D"})
+    with pytest.raises(_lib.GacelleError) as ei:
+        run_engine("r2s", y, th0, f, NAMES["r2s"], dims=kw["dims"], gidx=gidx)
+    assert "grid_index" in str(ei.value) and "volume 0" in str(ei.value)
+    ok = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
+    assert np.all(np.isfinite(ok["final_theta"]))
