@@ -146,8 +146,15 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* s_red = reinterpret_cast<double*>(smem_raw);                     // [2][32][kHistW]
     float* s_st = reinterpret_cast<float*>(s_red + 2 * 32 * kHistW);         // [NS][NP][slice]
-    float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NP][slice] fidelity gradient
-    int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NP * p.slice);          // [slice] grid index
+    // CACHE: the standard configuration without statistics keeps, from the
+    // fidelity pass, the unregularised parameter's z-gradient and the
+    // regularised one's fidelity gradient, dtheta/dz and theta (in the space
+    // the previous-epoch z takes when statistics are on), so the TV/update
+    // pass does not evaluate the transform again; same operations, same order.
+    constexpr bool CACHE = MAXM > 0 && !STATS;
+    constexpr int NAUX = CACHE ? 4 : NP;
+    float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NAUX][slice] fidelity pass results
+    int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NAUX * p.slice);        // [slice] grid index
     unsigned short* s_fl = reinterpret_cast<unsigned short*>(s_p + p.slice); // [slice] boundary/mask flags
     float* s_y = reinterpret_cast<float*>(s_fl + ((p.slice + 1) & ~1));       // [nm][slice] if staged
     const int BT = blockDim.x, tid = threadIdx.x;
@@ -260,8 +267,17 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 g0 = acc.g[0];
                 g1 = acc.g[1];
             }
-            s_gf[0 * S + i] = g0 * V.norm;
-            s_gf[1 * S + i] = g1 * V.norm;
+            if constexpr (CACHE) {
+                const int kr = a.reg_param[0];
+                const float gr = (kr == 0 ? g0 : g1) * V.norm, gn = (kr == 0 ? g1 : g0) * V.norm;
+                s_gf[0 * S + i] = gn * (kr == 0 ? dth[1] : dth[0]);
+                s_gf[1 * S + i] = gr;
+                s_gf[2 * S + i] = kr == 0 ? dth[0] : dth[1];
+                s_gf[3 * S + i] = kr == 0 ? th[0] : th[1];
+            } else {
+                s_gf[0 * S + i] = g0 * V.norm;
+                s_gf[1 * S + i] = g1 * V.norm;
+            }
             if (ok) q0 += tot;
         }
         // every CTA's map of the previous epoch (written before its arrival)
@@ -272,14 +288,43 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const int v = base + i;
             const bool ok = (v - V.off) < V.nvox;
             float z[NP], th[NP], dth[NP], gth[NP];
+            float gz[NP];
+            float reg = 0.0f;
+            const int pidx = s_p[i];
+            if constexpr (CACHE) {
+#pragma unroll
+                for (int k = 0; k < NP; ++k) z[k] = s_st[(0 * NP + k) * S + i];
+                const int kr = a.reg_param[0];
+                float gr_fid = s_gf[1 * S + i];
+                const float gn = s_gf[0 * S + i], dthr = s_gf[2 * S + i], c = s_gf[3 * S + i];
+                if (ok) {
+                    const unsigned int fl = s_fl[i];
+                    const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
+                    const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
+                    const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
+                    const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
+                    const float iv[3] = {ivx, ivy, ivz};
+                    const float* G = gcur + V.grid_off;
+                    float f[3], b[3];
+                    f[0] = __ldcg(G + fw0); b[0] = __ldcg(G + bw0);
+                    f[1] = __ldcg(G + fw1); b[1] = __ldcg(G + bw1);
+                    if (tv3) { f[2] = __ldcg(G + fw2); b[2] = __ldcg(G + bw2); }
+                    else { f[2] = 0.0f; b[2] = 0.0f; }
+                    float cost, gr;
+                    tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
+                    reg += tvs0 * cost;
+                    gr_fid = __fmaf_rn(tvs0, gr, gr_fid);
+                }
+                const float gzr = gr_fid * dthr;
+                gz[0] = kr == 0 ? gzr : gn;
+                gz[1] = kr == 0 ? gn : gzr;
+            } else {
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
                 z[k] = s_st[(0 * NP + k) * S + i];
                 th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], z[k], dth[k]);
                 gth[k] = s_gf[k * S + i];
             }
-            float reg = 0.0f;
-            const int pidx = s_p[i];
             if (ok && nreg > 0) {
                 const unsigned int fl = s_fl[i];
                 const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
@@ -304,9 +349,9 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     else gth[1] = __fmaf_rn(tvs, gr, gth[1]);
                 }
             }
-            float gz[NP];
 #pragma unroll
             for (int k = 0; k < NP; ++k) gz[k] = gth[k] * dth[k];
+            }
             if (ok) {
                 q1 += reg;
                 if constexpr (STATS) {
@@ -412,10 +457,13 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
 
 namespace {
 
-// Variants: MSE with up to 16 or 32 echoes (measurements prefetched into
-// registers), and any loss / echo count with the loss chosen at run time.
+// Variants: MSE with up to 8, 12, 16 or 32 echoes (measurements prefetched
+// into registers; the smallest bound that holds the protocol), and any loss /
+// echo count with the loss chosen at run time.
 int persist_variant(const AdamParams& a, int loss, bool res_after_loop) {
     const bool std_cfg = loss == kMSE && a.transform == 0 && a.optimiser == kAdam && a.n_reg == 1 && res_after_loop;
+    if (std_cfg && a.nm <= 8) return 8;
+    if (std_cfg && a.nm <= 12) return 12;
     if (std_cfg && a.nm <= 16) return 16;
     if (std_cfg && a.nm <= 32) return 32;
     return 0;
@@ -447,6 +495,8 @@ int occupancy_t(int bt, size_t smem) {
 }
 
 int occupancy_v(int variant, int bt, size_t smem) {
+    if (variant == 8) return occupancy_t<kMSE, 8>(bt, smem);
+    if (variant == 12) return occupancy_t<kMSE, 12>(bt, smem);
     if (variant == 16) return occupancy_t<kMSE, 16>(bt, smem);
     if (variant == 32) return occupancy_t<kMSE, 32>(bt, smem);
     return occupancy_t<-1, 0>(bt, smem);
@@ -510,6 +560,8 @@ cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, P
     // the register-prefetch variants write residuals after their epoch loop,
     // which needs a launch whose last epoch is not followed by an update
     const int variant = persist_variant(a, p.loss, !p.want_res || p.e_end > p.update_last);
+    if (variant == 8) return launch_persist_t<kMSE, 8>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    if (variant == 12) return launch_persist_t<kMSE, 12>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 16) return launch_persist_t<kMSE, 16>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 32) return launch_persist_t<kMSE, 32>(a, p, plan.threads, plan.ctas, plan.smem, s);
     return launch_persist_t<-1, 0>(a, p, plan.threads, plan.ctas, plan.smem, s);
