@@ -348,7 +348,7 @@ def engine_arm(args, world, rank, local):
     achieved = alg_bytes / (avg_launch_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind,
-                "kernel": ("tv_persistent_kernel<MSE,16> (every epoch of the fit in one cooperative launch: "
+                "kernel": ("tv_persistent_kernel<MSE,12> (every epoch of the fit in one cooperative launch: "
                            "forward, loss, adjoint, TV, Adam)") if persistent else
                           "tv_step_kernel<R2S,MSE> (one epoch: forward, loss, adjoint, TV, Adam)",
                 "epochs_per_launch": epochs_per_launch,

@@ -164,6 +164,7 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
         acc.res = (a.res_out && e == e_end && valid) ? a.res_out + v : nullptr;
         acc.rs = a.nvtot;
         model_eval<MODEL>(s_P, th, va, acc);
+        acc.finish();
         float gz[NP];
 #pragma unroll
         for (int k = 0; k < NP; ++k) gz[k] = acc.g[k] * normf * dth[k];
@@ -268,6 +269,7 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
     acc.res = (want_res && a.res_out && valid) ? a.res_out + v : nullptr;
     acc.rs = a.nvtot;
     model_eval<MODEL>(s_P, th, va, acc);
+    acc.finish();
     float gth[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) gth[k] = acc.g[k] * V.norm;

@@ -68,6 +68,10 @@ struct PLossAcc {
     __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
         bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
         float s = bad ? 0.0f : S;
+        if (LOSS == kMSE || (LOSS < 0 && rt.kind == kMSE)) {
+            mse_add(s - y[m * ys], dS, bad, total, g, res, m * rs, mse_scale);
+            return;
+        }
         float ww = w ? w[m * ws] : 1.0f;
         float d;
         float l;
@@ -79,6 +83,9 @@ struct PLossAcc {
 #pragma unroll
             for (int k = 0; k < NP; ++k) g[k] += d * dS[k];
         }
+    }
+    __device__ __forceinline__ void finish() {
+        if (LOSS == kMSE || (LOSS < 0 && rt.kind == kMSE)) mse_finish(total, g, mse_scale);
     }
 };
 
@@ -244,6 +251,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 acc.res = nullptr;  // residuals: pass after the epoch loop
                 acc.rs = a.nvtot;
                 model_r2s_unrolled<MAXM>(s_P, nm, th, acc);
+                acc.finish();
                 tot = acc.total;
                 g0 = acc.g[0];
                 g1 = acc.g[1];
@@ -263,6 +271,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 acc.rt.kind = p.loss;
                 VoxAux va{1.0f, nullptr, nullptr, 1};
                 model_eval<kR2S>(s_P, th, va, acc);
+                acc.finish();
                 tot = acc.total;
                 g0 = acc.g[0];
                 g1 = acc.g[1];
@@ -395,13 +404,14 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const int lane = tid & 31, warp = tid >> 5, nw = (BT + 31) >> 5;
             double* buf = s_red + (e & 1) * 32 * kHistW;
             float q[kHistW] = {q0, q1, q2, q3, q4};
+            constexpr int NQ = STATS ? kHistW : 2;  // without statistics columns 2-4 stay zero
 #pragma unroll
-            for (int k = 0; k < kHistW; ++k) {
+            for (int k = 0; k < NQ; ++k) {
                 float sum = warp_sum_p(q[k]);
                 if (lane == 0) buf[warp * kHistW + k] = (double)sum;
             }
             __syncthreads();
-            if (tid < kHistW) {
+            if (tid < NQ) {
                 double t = 0.0;
                 for (int w = 0; w < nw; ++w) t += buf[w * kHistW + tid];
                 if (tid == 0) t *= V.normd;

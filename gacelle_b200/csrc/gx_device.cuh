@@ -189,6 +189,29 @@ GX_HD float loss_elem(float s, float y, float w, const LossAux& a, float mse_sca
 // fa -> 1 makes the exchange rate r2 = r1 fa/(1-fa) overflow).
 template <int NP> struct MayBeNonFinite { static constexpr bool value = NP >= 4; };
 
+// MSE accumulation: per measurement one FMA for sum r^2 and one per parameter
+// for sum r dS/dtheta; mse_finish applies mse_scale (loss) and 2 mse_scale
+// (gradient) once per voxel.  The residual output keeps its per-measurement
+// value mse_scale r^2.  An accumulator's finish() must follow the model.
+template <int NP>
+__device__ __forceinline__ void mse_add(float r, const float (&dS)[NP], bool bad, float& total, float (&g)[NP],
+                                        float* res, int ri, float mse_scale) {
+    total = __fmaf_rn(r, r, total);
+    if (res) res[ri] = mse_scale * r * r;
+    if (!bad) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) g[k] = __fmaf_rn(r, dS[k], g[k]);
+    }
+}
+
+template <int NP>
+__device__ __forceinline__ void mse_finish(float& total, float (&g)[NP], float mse_scale) {
+    total *= mse_scale;
+    const float s2 = 2.0f * mse_scale;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) g[k] *= s2;
+}
+
 template <int LOSS, int NP>
 struct LossAcc {
     float total;
@@ -205,6 +228,10 @@ struct LossAcc {
     __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
         bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
         float s = bad ? 0.0f : S;
+        if constexpr (LOSS == kMSE) {
+            mse_add(s - y[m * ys], dS, bad, total, g, res, m * rs, mse_scale);
+            return;
+        }
         float ww = w ? w[m * ws] : 1.0f;
         float d;
         float l = loss_elem<LOSS>(s, y[m * ys], ww, aux, mse_scale, hd, d);
@@ -214,6 +241,9 @@ struct LossAcc {
 #pragma unroll
             for (int k = 0; k < NP; ++k) g[k] += d * dS[k];
         }
+    }
+    __device__ __forceinline__ void finish() {
+        if constexpr (LOSS == kMSE) mse_finish(total, g, mse_scale);
     }
 };
 
@@ -255,6 +285,10 @@ struct PrefLossAcc {
     __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
         bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
         float s = bad ? 0.0f : S;
+        if constexpr (LOSS == kMSE) {
+            mse_add(s - yv[m], dS, bad, total, g, res, m * rs, mse_scale);
+            return;
+        }
         float ww = w ? w[m * ws] : 1.0f;
         float d;
         float l = loss_elem<LOSS>(s, yv[m], ww, aux, mse_scale, hd, d);
@@ -264,6 +298,9 @@ struct PrefLossAcc {
 #pragma unroll
             for (int k = 0; k < NP; ++k) g[k] += d * dS[k];
         }
+    }
+    __device__ __forceinline__ void finish() {
+        if constexpr (LOSS == kMSE) mse_finish(total, g, mse_scale);
     }
 };
 
