@@ -12,9 +12,13 @@
 // model, loss, adjoint) needs only the CTA's own voxels; the TV/update pass
 // (TV subgradient from the neighbours' map values of the previous epoch,
 // sigmoid chain rule, optimiser, new map value) needs every CTA's previous
-// map.  So the grid barrier is split: a CTA arrives after its map writes and
-// waits only before its next TV/update pass, and the wait overlaps the
-// fidelity pass.  The wait is bounded: if it expires the kernel raises an
+// map.  The voxels are processed by worker warps that never wait for one
+// another: a worker warp arrives on a shared-memory mbarrier (with its
+// partial loss-history sums) after its map writes, runs its next fidelity
+// pass, and waits only before its next TV/update pass.  The CTA's last warp
+// is a barrier warp: it collects the worker arrivals, adds the epoch's loss
+// history, runs the grid barrier and opens the next TV/update pass (a second
+// mbarrier).  Every wait is bounded: if one expires the kernel raises an
 // error flag that the host reports as GX_ETIMEOUT, and every CTA returns.
 //
 // The per-voxel arithmetic (forward model, loss, adjoint, TV subgradient,
@@ -95,43 +99,72 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
     return v;
 }
 
-// Split grid barrier for a cooperative launch.  grid_arrive: every thread's
-// prior global writes are released to the other CTAs (the last CTA to arrive
-// opens generation gen+1).  grid_wait: returns once generation gen+1 is open,
-// with the other CTAs' writes visible, or false (on every thread of the CTA)
-// once any CTA's wait has expired.  gen is meaningful in thread 0 only.
-__device__ __forceinline__ void grid_arrive(PersistBarrier* gb, unsigned int nblocks, unsigned int gen) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
+// Grid barrier of a cooperative launch, run by one thread per CTA (the last
+// lane of the CTA's barrier warp): after the CTA's writes are acquired at CTA
+// scope, it releases them to the other CTAs (the last CTA to arrive opens
+// generation gen+1) and waits until generation gen+1 is open.  The wait is
+// bounded; false once any CTA's wait has expired.
+__device__ __forceinline__ bool grid_sync_one(PersistBarrier* gb, unsigned int nblocks, unsigned int& gen) {
+    __threadfence();
+    const unsigned int g = gen;
+    unsigned int arrived = atomicAdd(&gb->count, 1u);
+    if (arrived == nblocks - 1) {
+        atomicExch(&gb->count, 0u);
         __threadfence();
-        unsigned int arrived = atomicAdd(&gb->count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&gb->count, 0u);
-            __threadfence();
-            atomicExch(&gb->gen, gen + 1u);
-        }
+        atomicExch(&gb->gen, g + 1u);
     }
+    const long long t0 = clock64();
+    while (ld_acquire_gpu(&gb->gen) == g) {
+        if (*(volatile int*)&gb->error) return false;
+        if (clock64() - t0 > kBarrierSpinCycles) {
+            atomicExch(&gb->error, 1);
+            return false;
+        }
+        __nanosleep(20);
+    }
+    gen = g + 1u;
+    return *(volatile int*)&gb->error == 0;
 }
 
-__device__ __forceinline__ bool grid_wait(PersistBarrier* gb, unsigned int& gen) {
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) {
-        const unsigned int g = gen;
-        const long long t0 = clock64();
-        while (ld_acquire_gpu(&gb->gen) == g) {
-            if (*(volatile int*)&gb->error) break;
-            if (clock64() - t0 > kBarrierSpinCycles) {
-                atomicExch(&gb->error, 1);
-                break;
-            }
-            __nanosleep(20);
+// Shared-memory mbarriers between the worker warps and the barrier warp:
+// arrive has release and try_wait acquire semantics at CTA scope, and a
+// thread waiting in try_wait is suspended, taking no issue slots from the
+// warps that still work.
+__device__ __forceinline__ unsigned int smem_u32(const void* p) {
+    return (unsigned int)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned int count) {
+    asm volatile("mbarrier.init.shared.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned int parity) {
+    unsigned int done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Wait for the completion of the barrier's phase with the given parity
+// (the barrier is never more than one phase ahead of the waiter).  Bounded:
+// false, with the grid's error flag raised, once the wait has expired.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned int parity, PersistBarrier* gb) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > kBarrierSpinCycles) {
+            atomicExch(&gb->error, 1);
+            return false;
         }
-        __threadfence();
-        s_ok = *(volatile int*)&gb->error == 0;
-        gen = g + 1u;
     }
-    __syncthreads();
-    return s_ok != 0;
+    return true;
 }
 
 }  // namespace
@@ -210,8 +243,16 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     }
     __shared__ DevProtocol s_P;
     stage_protocol(a.P, &s_P);
-    unsigned int gen = 0;
-    if (tid == 0) gen = atomicAdd(&p.barrier->gen, 0u);
+    // bar_arrive: one arrival per worker warp and epoch; bar_open: one per
+    // epoch boundary (the grid barrier has passed, or s_err is set)
+    __shared__ unsigned long long bar_arrive, bar_open;
+    __shared__ int s_err;
+    const int NWT = BT - 32;  // worker threads; the last warp is the barrier warp
+    if (tid == 0) {
+        mbar_init(&bar_arrive, (unsigned int)(NWT >> 5));
+        mbar_init(&bar_open, 1u);
+        s_err = 0;
+    }
     __syncthreads();
     constexpr bool STD = MAXM > 0;
     const bool tv3 = a.tv_3d != 0;
@@ -221,6 +262,42 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     const OptConst oc{STD ? kAdam : a.optimiser, a.beta1, a.beta2, a.eps, a.momentum, a.rms_decay, a.rms_eps};
     const float ivx = a.inv_vs[0], ivy = a.inv_vs[1], ivz = a.inv_vs[2];
 
+    if (tid >= NWT) {
+        // barrier warp: history of each epoch, grid barrier between epochs
+        const int lane = tid & 31, nw = NWT >> 5;
+        constexpr int NQ = STATS ? kHistW : 2;  // without statistics columns 2-4 stay zero
+        unsigned int gen = 0;
+        if (lane == 31) gen = atomicAdd(&p.barrier->gen, 0u);
+        const int vol = a.blk_vol[base / p.pad_block];
+        for (int e = p.e_begin; e <= p.e_end; ++e) {
+            const unsigned int ph = (unsigned int)(e - p.e_begin) & 1u;
+            if (!mbar_wait(&bar_arrive, ph, p.barrier)) {
+                if (lane == 31) {
+                    *(volatile int*)&s_err = 1;
+                    mbar_arrive(&bar_open);
+                }
+                return;
+            }
+            if (p.record && a.hist && lane < NQ) {
+                const double* buf = s_red + (e & 1) * 32 * kHistW;
+                double t = 0.0;
+                for (int w = 0; w < nw; ++w) t += buf[w * kHistW + lane];
+                if (lane == 0) t *= V.normd;
+                if (t != 0.0) atomicAdd(a.hist + ((size_t)vol * (a.niter + 1) + e) * kHistW + lane, t);
+            }
+            __syncwarp();  // the history buffer of epoch e is read before epoch e+1 opens
+            if (e < p.e_end) {
+                int ok = 1;
+                if (lane == 31) {
+                    ok = grid_sync_one(p.barrier, gridDim.x, gen);
+                    if (!ok) *(volatile int*)&s_err = 1;
+                    mbar_arrive(&bar_open);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 31);
+                if (!ok) return;
+            }
+        }
+    } else
     for (int e = p.e_begin; e <= p.e_end; ++e) {
         const float* gcur = (e >= 1 && ((e - 1) & 1)) ? p.grid1 : p.grid0;  // epoch 0 reads the start map
         float* gnext = e & 1 ? p.grid1 : p.grid0;
@@ -228,7 +305,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const bool upd = e <= p.update_last;
         const float2 sc = upd ? a.sched[e] : float2{0.f, 0.f};
         // pass 1: data fidelity of the slice (own voxels only)
-        for (int i = tid; i < n; i += BT) {
+        for (int i = tid; i < n; i += NWT) {
             const int v = base + i;
             const bool ok = (v - V.off) < V.nvox;
             float th[NP], dth[NP];
@@ -291,9 +368,11 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         }
         // every CTA's map of the previous epoch (written before its arrival)
         if (e > p.e_begin)
-            if (!grid_wait(p.barrier, gen)) return;
+            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier) ||
+                *(volatile int*)&s_err)
+                return;
         // pass 2: TV subgradient, chain rule, optimiser, new map values
-        for (int i = tid; i < n; i += BT) {
+        for (int i = tid; i < n; i += NWT) {
             const int v = base + i;
             const bool ok = (v - V.off) < V.nvox;
             float z[NP], th[NP], dth[NP], gth[NP];
@@ -399,27 +478,22 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 }
             }
         }
-        if (e < p.e_end) grid_arrive(p.barrier, gridDim.x, gen);
+        // arrival: this warp's map writes and partial history sums
+        const int lane = tid & 31, warp = tid >> 5;
         if (p.record && a.hist) {
-            const int lane = tid & 31, warp = tid >> 5, nw = (BT + 31) >> 5;
             double* buf = s_red + (e & 1) * 32 * kHistW;
             float q[kHistW] = {q0, q1, q2, q3, q4};
-            constexpr int NQ = STATS ? kHistW : 2;  // without statistics columns 2-4 stay zero
+            constexpr int NQ = STATS ? kHistW : 2;
 #pragma unroll
             for (int k = 0; k < NQ; ++k) {
                 float sum = warp_sum_p(q[k]);
                 if (lane == 0) buf[warp * kHistW + k] = (double)sum;
             }
-            __syncthreads();
-            if (tid < NQ) {
-                double t = 0.0;
-                for (int w = 0; w < nw; ++w) t += buf[w * kHistW + tid];
-                if (tid == 0) t *= V.normd;
-                const int vol = a.blk_vol[base / p.pad_block];
-                if (t != 0.0) atomicAdd(a.hist + ((size_t)vol * (a.niter + 1) + e) * kHistW + tid, t);
-            }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bar_arrive);
     }
+    __syncthreads();
     if constexpr (STD) {
         // residuals of the final evaluation; the launch ends with an epoch
         // without update (host-checked), so the state is the evaluated one
@@ -515,10 +589,11 @@ int occupancy_v(int variant, int bt, size_t smem) {
 }  // namespace
 
 // Plan a persistent launch: one CTA per SM, slice = ceil(nvtot / #SM) voxels
-// (rounded to a padding block so that a slice never straddles two volumes),
-// the slice's Adam state in shared memory (and its measurements too when they
-// fit), kPersistMaxThreads threads.  Returns false when the problem does not
-// fit, in which case the caller uses the per-epoch kernel.
+// (rounded to whole warps, or with several volumes to a padding block so that
+// a slice never straddles two volumes), the slice's Adam state in shared
+// memory (and its measurements too when they fit), up to kPersistMaxThreads
+// threads (worker warps and a barrier warp).  Returns false when the problem
+// does not fit, in which case the caller uses the per-epoch kernel.
 bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, const int* vol_npad, int nvol,
                      PersistPlan* plan) {
     if (model != kR2S) return false;
@@ -527,8 +602,11 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
+    // one volume: slices of whole warps; several: of padding blocks, so that
+    // every volume starts on a slice boundary
+    const int gran = nvol == 1 ? 32 : pad_block;
     int slice = (a.nvtot + nsm - 1) / nsm;
-    slice = (slice + pad_block - 1) / pad_block * pad_block;
+    slice = (slice + gran - 1) / gran * gran;
     {
         long long acc = 0;
         for (int i = 0; i < nvol; ++i) {  // every volume starts on a slice boundary
@@ -546,11 +624,12 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     if (red + state > budget) return false;
     int in_smem = red + state + data <= budget ? 1 : 0;
     size_t smem = red + state + (in_smem ? data : 0);
-    // threads: as many as fit, spread so that the last pass over the slice is full
+    // worker threads: as many as fit beside the barrier warp, spread so that
+    // the last pass over the slice is full
     const int variant = persist_variant(a, loss, true);
-    const int maxt = persist_max_threads(variant);
-    int passes = (slice + maxt - 1) / maxt;
-    int bt = ((slice + passes - 1) / passes + 31) / 32 * 32;
+    const int maxw = persist_max_threads(variant) - 32;
+    int passes = (slice + maxw - 1) / maxw;
+    int bt = ((slice + passes - 1) / passes + 31) / 32 * 32 + 32;
     int nb = occupancy_v(variant, bt, smem);
     if (variant != 0) nb = std::min(nb, occupancy_v(0, bt, smem));
     if (nb < 1) return false;
