@@ -167,6 +167,36 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned int 
     return true;
 }
 
+// The six face neighbours' values in a TV map G (grid index pidx, staging
+// flags fl: bits 0-2 on the last x/y/z plane, 3-5 on the first, where the
+// neighbour wraps around periodically).  Interior voxels, almost all of a
+// masked volume, take the plain offsets.
+struct Neighbours {
+    int sy, sz, wx, wy, wz;
+    bool tv3;
+    __device__ __forceinline__ void load(const float* G, int pidx, unsigned int fl, float (&f)[3],
+                                         float (&b)[3]) const {
+        if (!(fl & (tv3 ? 63u : 27u))) {
+            const float* g = G + pidx;
+            f[0] = __ldcg(g + 1); b[0] = __ldcg(g - 1);
+            f[1] = __ldcg(g + sy); b[1] = __ldcg(g - sy);
+            if (tv3) { f[2] = __ldcg(g + sz); b[2] = __ldcg(g - sz); }
+            else { f[2] = 0.0f; b[2] = 0.0f; }
+            return;
+        }
+        const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
+        const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
+        f[0] = __ldcg(G + fw0); b[0] = __ldcg(G + bw0);
+        f[1] = __ldcg(G + fw1); b[1] = __ldcg(G + bw1);
+        if (tv3) {
+            const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
+            f[2] = __ldcg(G + fw2); b[2] = __ldcg(G + bw2);
+        } else {
+            f[2] = 0.0f; b[2] = 0.0f;
+        }
+    }
+};
+
 }  // namespace
 
 // MAXM > 0: the standard configuration (MSE, sigmoid transform, Adam, one
@@ -212,6 +242,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     const int dx = Vg.dims[0], dy = Vg.dims[1], dz = Vg.dims[2];
     const int sy = dx, sz = dx * dy;
     const int wx = dx - 1, wy = (dy - 1) * dx, wz = (dz - 1) * dx * dy;  // wrap offsets
+    const Neighbours nb{sy, sz, wx, wy, wz, a.tv_3d != 0};
     const unsigned char* mk = a.maskgrid + V.grid_off;
     // stage the slice's state, TV neighbourhood (and measurements, if they fit) once
     for (int i = tid; i < n; i += BT) {
@@ -317,7 +348,8 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             float tot, g0, g1;
             if constexpr (MAXM > 0) {
                 PrefLossAcc<LOSS, NP, MAXM> acc;
-                acc.load(yb, ys, nm);
+                if (p.data_quads) acc.load_quads(p.data_quads + v, (size_t)a.nvtot);
+                else acc.load(yb, ys, nm);
                 acc.total = 0.0f;
                 acc.g[0] = acc.g[1] = 0.0f;
                 acc.w = a.weights ? a.weights + v : nullptr;
@@ -327,7 +359,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 acc.hd = a.huber_delta;
                 acc.res = nullptr;  // residuals: pass after the epoch loop
                 acc.rs = a.nvtot;
-                model_r2s_unrolled<MAXM>(s_P, nm, th, acc);
+                model_r2s_unrolled<MAXM>(a.P, nm, th, acc);  // echo constants as constant-bank operands
                 acc.finish();
                 tot = acc.total;
                 g0 = acc.g[0];
@@ -387,17 +419,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 const float gn = s_gf[0 * S + i], dthr = s_gf[2 * S + i], c = s_gf[3 * S + i];
                 if (ok) {
                     const unsigned int fl = s_fl[i];
-                    const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
-                    const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
-                    const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
                     const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
                     const float iv[3] = {ivx, ivy, ivz};
-                    const float* G = gcur + V.grid_off;
                     float f[3], b[3];
-                    f[0] = __ldcg(G + fw0); b[0] = __ldcg(G + bw0);
-                    f[1] = __ldcg(G + fw1); b[1] = __ldcg(G + bw1);
-                    if (tv3) { f[2] = __ldcg(G + fw2); b[2] = __ldcg(G + bw2); }
-                    else { f[2] = 0.0f; b[2] = 0.0f; }
+                    nb.load(gcur + V.grid_off, pidx, fl, f, b);
                     float cost, gr;
                     tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
                     reg += tvs0 * cost;
@@ -415,20 +440,13 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             }
             if (ok && nreg > 0) {
                 const unsigned int fl = s_fl[i];
-                const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
-                const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
-                const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
                 const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
                 const float iv[3] = {ivx, ivy, ivz};
                 for (int r = 0; r < nreg; ++r) {
                     const int k = a.reg_param[r];
-                    const float* G = gcur + (size_t)r * a.grid_total + V.grid_off;
                     const float c = k == 0 ? th[0] : th[1];
                     float f[3], b[3];
-                    f[0] = __ldcg(G + fw0); b[0] = __ldcg(G + bw0);
-                    f[1] = __ldcg(G + fw1); b[1] = __ldcg(G + bw1);
-                    if (tv3) { f[2] = __ldcg(G + fw2); b[2] = __ldcg(G + bw2); }
-                    else { f[2] = 0.0f; b[2] = 0.0f; }
+                    nb.load(gcur + (size_t)r * a.grid_total + V.grid_off, pidx, fl, f, b);
                     float cost, gr;
                     tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
                     const float tvs = r == 0 ? tvs0 : tvs1;
@@ -640,6 +658,7 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     if (plan->ctas > nb * nsm) return false;
     plan->smem = smem;
     plan->data_in_smem = in_smem;
+    plan->quad_width = (!in_smem && variant > 0) ? variant : 0;
     return true;
 }
 
@@ -649,11 +668,37 @@ cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, P
     // the register-prefetch variants write residuals after their epoch loop,
     // which needs a launch whose last epoch is not followed by an update
     const int variant = persist_variant(a, p.loss, !p.want_res || p.e_end > p.update_last);
+    if (variant != plan.quad_width) p.data_quads = nullptr;  // quads for another width: read [nm][nvtot]
     if (variant == 8) return launch_persist_t<kMSE, 8>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 12) return launch_persist_t<kMSE, 12>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 16) return launch_persist_t<kMSE, 16>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 32) return launch_persist_t<kMSE, 32>(a, p, plan.threads, plan.ctas, plan.smem, s);
     return launch_persist_t<-1, 0>(a, p, plan.threads, plan.ctas, plan.smem, s);
+}
+
+namespace {
+
+__global__ void echo_quads_kernel(const float* data, int nm, int nvtot, int width, float4* out) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvtot) return;
+    for (int j = 0; j < width / 4; ++j) {
+        float t[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int m = 4 * j + c;
+            t[c] = m < nm ? data[(size_t)m * nvtot + v] : 0.0f;
+        }
+        out[(size_t)j * nvtot + v] = make_float4(t[0], t[1], t[2], t[3]);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, float4* out, cudaStream_t s) {
+    if (width % 4 != 0 || nm > width) return cudaErrorInvalidValue;
+    echo_quads_kernel<<<(nvtot + 255) / 256, 256, 0, s>>>(data, nm, nvtot, width, out);
+    ++g_kernel_launches;
+    return cudaGetLastError();
 }
 
 }  // namespace gx

@@ -59,7 +59,7 @@ enum Slot {
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
-    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_NSLOTS
+    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_NSLOTS
 };
 
 struct gx_context {
@@ -276,7 +276,11 @@ static DevProtocol make_protocol(const gx_model* m, int id, int np, int nm, cons
     P.nx = m->nx;
     P.tr = (float)m->tr;
     P.h = m->nx > 1 ? (float)(1.0 / (m->nx - 1)) : 0.0f;
-    if (m->te) for (int i = 0; i < m->n_te && i < kMaxTE; ++i) P.te[i] = (float)m->te[i];
+    if (m->te)
+        for (int i = 0; i < m->n_te && i < kMaxTE; ++i) {
+            P.te[i] = (float)m->te[i];
+            P.te_l2e[i] = (float)(m->te[i] * M_LOG2E);
+        }
     if (m->fa_deg) for (int i = 0; i < m->n_fa && i < kMaxFA; ++i) P.fa_rad[i] = (float)(m->fa_deg[i] * M_PI / 180.0);
     if (m->bval) for (int i = 0; i < m->n_shell && i < kMaxShell; ++i) P.bval[i] = (float)m->bval[i];
     if (m->big_delta) for (int i = 0; i < m->n_shell && i < kMaxShell; ++i) P.delta[i] = (float)m->big_delta[i];
@@ -462,6 +466,7 @@ struct AdamJob {
     bool use_persist = false;             // TV main pass as one cooperative launch
     PersistPlan plan{};
     PersistBarrier* barrier = nullptr;
+    float4* data_quads = nullptr;         // echo quads of the measurements for the persistent kernel
 };
 
 static double sched_pow(double b, int e) { return std::pow(b, (double)e); }
@@ -728,6 +733,7 @@ static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e
         p.grid1 = J.grid[1];
         p.barrier = J.barrier;
         p.pad_block = J.B;
+        p.data_quads = J.data_quads;
         CK(cudaMemsetAsync(J.barrier, 0, sizeof(PersistBarrier), c->stream));
         CK(launch_tv_persistent(a, J.plan, p, c->stream));
         return GX_OK;
@@ -806,6 +812,10 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
         for (int i = 0; i < J.nvol; ++i) npad[i] = J.hv[i].npad;
         J.use_persist = want && plan_persistent(J.a, J.id, o->loss, J.B, npad.data(), J.nvol, &J.plan);
         if (J.use_persist) TRY(wsT(c, S_BAR, 1, &J.barrier));
+        if (J.use_persist && J.plan.quad_width > 0) {
+            TRY(wsT(c, S_DATA_QUADS, (size_t)J.nvtot * (J.plan.quad_width / 4), &J.data_quads));
+            CK(launch_echo_quads(J.a.data, J.nm, J.nvtot, J.plan.quad_width, J.data_quads, c->stream));
+        }
     }
 
     out.tr.assign(J.nvol, Tracker());

@@ -39,6 +39,7 @@ struct DevProtocol {
     float tr;    // [s]
     float h;     // NEXI node spacing 1/(nx-1)
     float te[kMaxTE];
+    float te_l2e[kMaxTE];   // te * log2(e): exp(-te R2*) = 2^(-te_l2e R2*)
     float fa_rad[kMaxFA];
     float bval[kMaxShell];
     float delta[kMaxShell];
@@ -214,6 +215,7 @@ __device__ __forceinline__ void mse_finish(float& total, float (&g)[NP], float m
 
 template <int LOSS, int NP>
 struct LossAcc {
+    static constexpr bool kMse = LOSS == kMSE;
     float total;
     float g[NP];
     const float* y;   // measurement m at y[m*ys]
@@ -245,6 +247,7 @@ struct LossAcc {
     __device__ __forceinline__ void finish() {
         if constexpr (LOSS == kMSE) mse_finish(total, g, mse_scale);
     }
+    __device__ __forceinline__ float meas(int m) const { return y[m * ys]; }
 };
 
 template <int MODEL> struct ModelNP;
@@ -268,6 +271,7 @@ __device__ __forceinline__ void r2s_echo(float te, float M0, float R2, float& S,
 // (an unrolled loop, model_r2s_unrolled).  Same loss arithmetic as LossAcc.
 template <int LOSS, int NP, int MAXM>
 struct PrefLossAcc {
+    static constexpr bool kMse = LOSS == kMSE;
     float total;
     float g[NP];
     float yv[MAXM];
@@ -281,6 +285,20 @@ struct PrefLossAcc {
     __device__ __forceinline__ void load(const float* y, int ys, int nm) {
 #pragma unroll
         for (int m = 0; m < MAXM; ++m) yv[m] = m < nm ? y[(size_t)m * ys] : 0.0f;  // global or shared
+    }
+    // measurements in echo quads: quad j of the voxel (measurements 4j..4j+3,
+    // zero-padded) at q[j*qs], so that a warp reads 512 contiguous bytes
+    // per quad
+    __device__ __forceinline__ void load_quads(const float4* q, size_t qs) {
+        static_assert(MAXM % 4 == 0, "whole quads");
+#pragma unroll
+        for (int j = 0; j < MAXM / 4; ++j) {
+            const float4 t = __ldcg(q + j * qs);
+            yv[4 * j] = t.x;
+            yv[4 * j + 1] = t.y;
+            yv[4 * j + 2] = t.z;
+            yv[4 * j + 3] = t.w;
+        }
     }
     __device__ __forceinline__ void add(int m, float S, const float (&dS)[NP]) {
         bool bad = MayBeNonFinite<NP>::value ? !isfinite(S) : false;
@@ -302,7 +320,12 @@ struct PrefLossAcc {
     __device__ __forceinline__ void finish() {
         if constexpr (LOSS == kMSE) mse_finish(total, g, mse_scale);
     }
+    __device__ __forceinline__ float meas(int m) const { return yv[m]; }
 };
+
+// Accumulators that take the fused R2*/MSE echo path (kMse true).
+template <class A, class = void> struct AccMse { static constexpr bool value = false; };
+template <class A> struct AccMse<A, decltype(void(A::kMse))> { static constexpr bool value = A::kMse; };
 
 // Per-voxel model inputs besides theta.
 struct VoxAux {
@@ -352,14 +375,53 @@ __device__ __forceinline__ float rice_mean(const DevProtocol& P, float S, float 
     return S;
 }
 
+// 2^x by the PTX base-2 exponential (ex2.approx, subnormals flushed).
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// One echo of R2*/MSE, fused: E = exp(-te R2*) = 2^(-(te log2 e) R2*),
+// r = M0 E - y, and with q = r E the sums sum r^2, sum q (dS/dM0 = E) and
+// sum te q (dS/dR2* = -te M0 E, the factor -M0 applied once per voxel).
+// Explicit roundings, so that every kernel evaluates it identically.
+struct R2sMseSums {
+    float sse = 0.0f, g0 = 0.0f, g1 = 0.0f;
+    __device__ __forceinline__ float echo(float te, float te_l2e, float M0, float R2, float y) {
+        const float E = ex2_ftz(__fmul_rn(-te_l2e, R2));
+        const float r = __fmaf_rn(M0, E, -y);
+        sse = __fmaf_rn(r, r, sse);
+        const float q = __fmul_rn(r, E);
+        g0 = __fadd_rn(g0, q);
+        g1 = __fmaf_rn(te, q, g1);
+        return r;
+    }
+    template <class Acc>
+    __device__ __forceinline__ void store(float M0, Acc& acc) const {
+        acc.total = __fadd_rn(acc.total, sse);
+        acc.g[0] = __fadd_rn(acc.g[0], g0);
+        acc.g[1] = __fmaf_rn(-M0, g1, acc.g[1]);
+    }
+};
+
 // S = M0 exp(-TE R2*)  (R2star/gpuR2starMapping.m:427-434)
 template <class Acc>
 __device__ __forceinline__ void model_r2s(const DevProtocol& P, const float* th, Acc& acc) {
     float M0 = th[0], R2 = th[1];
-    for (int m = 0; m < P.nm; ++m) {
-        float S, dS[2];
-        r2s_echo(P.te[m], M0, R2, S, dS);
-        acc.add(m, S, dS);
+    if constexpr (AccMse<Acc>::value) {
+        R2sMseSums u;
+        for (int m = 0; m < P.nm; ++m) {
+            const float r = u.echo(P.te[m], P.te_l2e[m], M0, R2, acc.meas(m));
+            if (acc.res) acc.res[m * acc.rs] = acc.mse_scale * r * r;
+        }
+        u.store(M0, acc);
+    } else {
+        for (int m = 0; m < P.nm; ++m) {
+            float S, dS[2];
+            r2s_echo(P.te[m], M0, R2, S, dS);
+            acc.add(m, S, dS);
+        }
     }
 }
 
@@ -369,12 +431,23 @@ __device__ __forceinline__ void model_r2s(const DevProtocol& P, const float* th,
 template <int MAXM, class Acc>
 __device__ __forceinline__ void model_r2s_unrolled(const DevProtocol& P, int nm, const float* th, Acc& acc) {
     float M0 = th[0], R2 = th[1];
+    if constexpr (AccMse<Acc>::value) {
+        R2sMseSums u;
 #pragma unroll
-    for (int m = 0; m < MAXM; ++m) {
-        if (m < nm) {
-            float S, dS[2];
-            r2s_echo(P.te[m], M0, R2, S, dS);
-            acc.add(m, S, dS);
+        for (int m = 0; m < MAXM; ++m)
+            if (m < nm) {
+                const float r = u.echo(P.te[m], P.te_l2e[m], M0, R2, acc.meas(m));
+                if (acc.res) acc.res[m * acc.rs] = acc.mse_scale * r * r;
+            }
+        u.store(M0, acc);
+    } else {
+#pragma unroll
+        for (int m = 0; m < MAXM; ++m) {
+            if (m < nm) {
+                float S, dS[2];
+                r2s_echo(P.te[m], M0, R2, S, dS);
+                acc.add(m, S, dS);
+            }
         }
     }
 }

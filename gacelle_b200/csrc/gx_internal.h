@@ -213,16 +213,20 @@ struct PersistArgs {
     int slice;               // voxels per CTA
     int data_in_smem;
     int pad_block;           // block size of the work-list padding (blk_vol granularity)
+    const float4* data_quads; // [quad_width/4][nvtot] echo quads of the measurements, or nullptr
 };
 
 struct PersistPlan {
     int slice, vpt, threads, ctas, data_in_smem;
+    int quad_width;          // > 0: the launch reads echo quads, this many measurements wide
     size_t smem;
 };
 
 bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, const int* vol_npad, int nvol,
                      PersistPlan* plan);
 cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s);
+// out[j][v] = (data[4j][v], .., data[4j+3][v]), 0 for nm <= m < width (width % 4 == 0)
+cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, float4* out, cudaStream_t s);
 
 }  // namespace gx
 
