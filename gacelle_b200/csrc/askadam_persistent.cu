@@ -339,17 +339,20 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         for (int i = tid; i < n; i += NWT) {
             const int v = base + i;
             const bool ok = (v - V.off) < V.nvox;
+            const float* yb = p.data_in_smem ? s_y + i : a.data + v;
+            const int ys = p.data_in_smem ? S : a.nvtot;
+            PrefLossAcc<LOSS, NP, (MAXM > 0 ? MAXM : 4)> pacc;
+            if constexpr (MAXM > 0) {  // the measurement loads first: in flight during the transform
+                if (p.data_quads) pacc.load_quads(p.data_quads + v, (size_t)a.nvtot);
+                else pacc.load(yb, ys, nm);
+            }
             float th[NP], dth[NP];
 #pragma unroll
             for (int k = 0; k < NP; ++k)
                 th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], s_st[(0 * NP + k) * S + i], dth[k]);
-            const float* yb = p.data_in_smem ? s_y + i : a.data + v;
-            const int ys = p.data_in_smem ? S : a.nvtot;
             float tot, g0, g1;
             if constexpr (MAXM > 0) {
-                PrefLossAcc<LOSS, NP, MAXM> acc;
-                if (p.data_quads) acc.load_quads(p.data_quads + v, (size_t)a.nvtot);
-                else acc.load(yb, ys, nm);
+                auto& acc = pacc;
                 acc.total = 0.0f;
                 acc.g[0] = acc.g[1] = 0.0f;
                 acc.w = a.weights ? a.weights + v : nullptr;
@@ -643,7 +646,8 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     int in_smem = red + state + data <= budget ? 1 : 0;
     size_t smem = red + state + (in_smem ? data : 0);
     // worker threads: as many as fit beside the barrier warp, spread so that
-    // the last pass over the slice is full
+    // the last pass over the slice is full (every worker warp reaches the
+    // grid barrier after the same number of voxels)
     const int variant = persist_variant(a, loss, true);
     const int maxw = persist_max_threads(variant) - 32;
     int passes = (slice + maxw - 1) / maxw;
