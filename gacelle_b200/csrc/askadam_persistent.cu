@@ -205,11 +205,15 @@ struct Neighbours {
 // the final evaluation written by a pass after the epoch loop; MAXM == 0: any
 // loss, transform, optimiser and regulariser count, measurements read one at
 // a time.
-// Threads per CTA at most: the 32-echo variant needs more than 64 registers.
-constexpr int persist_max_threads(int maxm) { return maxm > 16 ? 768 : kPersistMaxThreads; }
+// Threads per CTA at most: the 32-echo variant and the pair variants (two
+// voxels' measurements per thread) need more than 64 registers.
+__host__ __device__ constexpr bool persist_pairs(int maxm, bool stats) { return maxm > 0 && maxm <= 16 && !stats; }
+__host__ __device__ constexpr int persist_max_threads(int maxm, bool stats) {
+    return (maxm > 16 || persist_pairs(maxm, stats)) ? 768 : kPersistMaxThreads;
+}
 
 template <int LOSS, bool STATS, int MAXM>
-__global__ void __launch_bounds__(persist_max_threads(MAXM), 1)
+__global__ void __launch_bounds__(persist_max_threads(MAXM, STATS), 1)
 tv_persistent_kernel(AdamParams a, PersistArgs p) {
     constexpr int NP = 2;  // R2*: M0, R2star
     constexpr int NS = STATS ? 4 : 3;  // z, m1, m2 [, z of the previous epoch]
@@ -221,7 +225,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     // regularised one's fidelity gradient, dtheta/dz and theta (in the space
     // the previous-epoch z takes when statistics are on), so the TV/update
     // pass does not evaluate the transform again; same operations, same order.
-    constexpr bool CACHE = MAXM > 0 && !STATS;
+    // PAIR (up to 16 measurements, without statistics): two voxels per
+    // thread, pair instructions, with the fidelity-pass cache (CACHE)
+    constexpr bool PAIR = persist_pairs(MAXM, STATS);
+    constexpr bool CACHE = PAIR;
     constexpr int NAUX = CACHE ? 4 : NP;
     float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NAUX][slice] fidelity pass results
     int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NAUX * p.slice);        // [slice] grid index
@@ -335,6 +342,134 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f, q4 = 0.f;
         const bool upd = e <= p.update_last;
         const float2 sc = upd ? a.sched[e] : float2{0.f, 0.f};
+        if constexpr (PAIR) {
+        // two voxels (i, i+1) per thread and pass; the parameter, gradient and
+        // optimiser arithmetic in pair instructions, lane l on voxel i+l
+        const int kr = a.reg_param[0];  // the regularised parameter
+        const float lbr = a.P.lb[kr], ubr = a.P.ub[kr];
+        const size_t half = (size_t)(a.nvtot >> 1);
+        // measurements of the pair at slice position i: echo m of both voxels
+        // pass 1: data fidelity of the slice (own voxels only)
+        for (int i = 2 * tid; i < n; i += 2 * NWT) {
+            const int v = base + i;
+            const bool ok0 = (v - V.off) < V.nvox, ok1 = (v + 1 - V.off) < V.nvox;
+            float2 y[MAXM];  // measurement m of both voxels
+            if (p.data_quads) {
+                const float4* q = p.data_quads + (v >> 1);
+#pragma unroll
+                for (int j = 0; j < MAXM / 2; ++j) {
+                    const float4 t = __ldcg(q + j * half);
+                    y[2 * j] = make_float2(t.x, t.y);
+                    y[2 * j + 1] = make_float2(t.z, t.w);
+                }
+            } else {
+                const float* yb = p.data_in_smem ? s_y + i : a.data + v;
+                const size_t ys = p.data_in_smem ? (size_t)S : (size_t)a.nvtot;
+#pragma unroll
+                for (int m = 0; m < MAXM; ++m)
+                    y[m] = m < nm ? *reinterpret_cast<const float2*>(yb + m * ys) : make_float2(0.f, 0.f);
+            }
+            float2 th[NP], dth[NP];
+#pragma unroll
+            for (int k = 0; k < NP; ++k)
+                th[k] = unscale_sig2(a.P.lb[k], a.P.ub[k], *reinterpret_cast<const float2*>(s_st + k * S + i),
+                                     dth[k]);
+            // R2sMseSums on both lanes with the residual negated, y - M0 E:
+            // every partial sum is the exact negative of the scalar one
+            float2 sse = make_float2(0.f, 0.f), g0n = sse, g1n = sse;
+            const float2 nM0 = make_float2(-th[0].x, -th[0].y), R2 = th[1];
+#pragma unroll
+            for (int m = 0; m < MAXM; ++m)
+                if (m < nm) {
+                    const float2 x = mul2(bcast2(-a.P.te_l2e[m]), R2);
+                    const float2 E = make_float2(ex2_ftz(x.x), ex2_ftz(x.y));
+                    const float2 rn = fma2(nM0, E, y[m]);
+                    sse = fma2(rn, rn, sse);
+                    const float2 qn = mul2(rn, E);
+                    g0n = add2(g0n, qn);
+                    g1n = fma2(bcast2(a.P.te[m]), qn, g1n);
+                }
+            const float2 zero = make_float2(0.f, 0.f);
+            const float s2 = mul1(2.0f, a.mse_scale);
+            const float2 tot = mul2(add2(zero, sse), bcast2(a.mse_scale));
+            float2 g[NP];
+            g[0] = mul2(sub2(zero, g0n), bcast2(s2));
+            g[1] = mul2(fma2(th[0], g1n, zero), bcast2(s2));
+            const float2 nrm = bcast2(V.norm);
+            const float2 gr = mul2(kr == 0 ? g[0] : g[1], nrm), gn = mul2(kr == 0 ? g[1] : g[0], nrm);
+            *reinterpret_cast<float2*>(s_gf + 0 * S + i) = mul2(gn, kr == 0 ? dth[1] : dth[0]);
+            *reinterpret_cast<float2*>(s_gf + 1 * S + i) = gr;
+            *reinterpret_cast<float2*>(s_gf + 2 * S + i) = kr == 0 ? dth[0] : dth[1];
+            *reinterpret_cast<float2*>(s_gf + 3 * S + i) = kr == 0 ? th[0] : th[1];
+            if (ok0) q0 += tot.x;
+            if (ok1) q0 += tot.y;
+        }
+        // every CTA's map of the previous epoch (written before its arrival)
+        if (e > p.e_begin)
+            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier) ||
+                *(volatile int*)&s_err)
+                return;
+        const bool ckpt = upd && a.ckpt_every > 0 && (e % a.ckpt_every) == 0;
+        float* cp = ckpt ? a.ckpt + (size_t)(e / a.ckpt_every) * 3 * NP * a.nvtot : nullptr;
+        const float* G = gcur + V.grid_off;
+        float* Gn = gnext + V.grid_off;
+        const float iv[3] = {ivx, ivy, ivz};
+        // pass 2: TV subgradient, chain rule, optimiser, new map values
+        for (int i = 2 * tid; i < n; i += 2 * NWT) {
+            const int v = base + i;
+            const bool ok0 = (v - V.off) < V.nvox, ok1 = (v + 1 - V.off) < V.nvox;
+            const float2 gn = *reinterpret_cast<const float2*>(s_gf + 0 * S + i);
+            float2 grf = *reinterpret_cast<const float2*>(s_gf + 1 * S + i);
+            const float2 dthr = *reinterpret_cast<const float2*>(s_gf + 2 * S + i);
+            const float2 c = *reinterpret_cast<const float2*>(s_gf + 3 * S + i);
+            const int2 pidx = *reinterpret_cast<const int2*>(s_p + i);
+            const unsigned int fl2 = *reinterpret_cast<const unsigned int*>(s_fl + i);
+            if (ok0) {
+                const unsigned int fl = fl2 & 0xffffu;
+                const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
+                float f[3], b[3], cost, gt;
+                nb.load(G, pidx.x, fl, f, b);
+                tv_terms(c.x, f, b, mb, iv, tv3 ? 3 : 2, cost, gt);
+                q1 = __fmaf_rn(tvs0, cost, q1);
+                grf.x = __fmaf_rn(tvs0, gt, grf.x);
+            }
+            if (ok1) {
+                const unsigned int fl = fl2 >> 16;
+                const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
+                float f[3], b[3], cost, gt;
+                nb.load(G, pidx.y, fl, f, b);
+                tv_terms(c.y, f, b, mb, iv, tv3 ? 3 : 2, cost, gt);
+                q1 = __fmaf_rn(tvs0, cost, q1);
+                grf.y = __fmaf_rn(tvs0, gt, grf.y);
+            }
+            if (upd) {
+                const float2 gzr = mul2(grf, dthr);
+                const float2 gz[NP] = {kr == 0 ? gzr : gn, kr == 0 ? gn : gzr};
+                float2 zr = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    float2* pz = reinterpret_cast<float2*>(s_st + (0 * NP + k) * S + i);
+                    float2* p1 = reinterpret_cast<float2*>(s_st + (1 * NP + k) * S + i);
+                    float2* p2 = reinterpret_cast<float2*>(s_st + (2 * NP + k) * S + i);
+                    float2 zz = *pz, mm1 = *p1, mm2 = *p2;
+                    adam_step2(oc, sc, zz, mm1, mm2, gz[k]);
+                    *pz = zz;
+                    *p1 = mm1;
+                    *p2 = mm2;
+                    if (k == kr) zr = zz;
+                    if (ckpt) {  // padding lanes included: never read back
+                        *reinterpret_cast<float2*>(cp + (size_t)k * a.nvtot + v) = zz;
+                        *reinterpret_cast<float2*>(cp + (size_t)(NP + k) * a.nvtot + v) = mm1;
+                        *reinterpret_cast<float2*>(cp + (size_t)(2 * NP + k) * a.nvtot + v) = mm2;
+                    }
+                }
+                float2 dd;
+                const float2 thr = unscale_sig2(lbr, ubr, zr, dd);
+                if (ok0) Gn[pidx.x] = thr.x;
+                if (ok1) Gn[pidx.y] = thr.y;
+            }
+        }
+        } else {
         // pass 1: data fidelity of the slice (own voxels only)
         for (int i = tid; i < n; i += NWT) {
             const int v = base + i;
@@ -388,17 +523,8 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 g0 = acc.g[0];
                 g1 = acc.g[1];
             }
-            if constexpr (CACHE) {
-                const int kr = a.reg_param[0];
-                const float gr = (kr == 0 ? g0 : g1) * V.norm, gn = (kr == 0 ? g1 : g0) * V.norm;
-                s_gf[0 * S + i] = gn * (kr == 0 ? dth[1] : dth[0]);
-                s_gf[1 * S + i] = gr;
-                s_gf[2 * S + i] = kr == 0 ? dth[0] : dth[1];
-                s_gf[3 * S + i] = kr == 0 ? th[0] : th[1];
-            } else {
-                s_gf[0 * S + i] = g0 * V.norm;
-                s_gf[1 * S + i] = g1 * V.norm;
-            }
+            s_gf[0 * S + i] = g0 * V.norm;
+            s_gf[1 * S + i] = g1 * V.norm;
             if (ok) q0 += tot;
         }
         // every CTA's map of the previous epoch (written before its arrival)
@@ -414,27 +540,6 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             float gz[NP];
             float reg = 0.0f;
             const int pidx = s_p[i];
-            if constexpr (CACHE) {
-#pragma unroll
-                for (int k = 0; k < NP; ++k) z[k] = s_st[(0 * NP + k) * S + i];
-                const int kr = a.reg_param[0];
-                float gr_fid = s_gf[1 * S + i];
-                const float gn = s_gf[0 * S + i], dthr = s_gf[2 * S + i], c = s_gf[3 * S + i];
-                if (ok) {
-                    const unsigned int fl = s_fl[i];
-                    const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
-                    const float iv[3] = {ivx, ivy, ivz};
-                    float f[3], b[3];
-                    nb.load(gcur + V.grid_off, pidx, fl, f, b);
-                    float cost, gr;
-                    tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
-                    reg += tvs0 * cost;
-                    gr_fid = __fmaf_rn(tvs0, gr, gr_fid);
-                }
-                const float gzr = gr_fid * dthr;
-                gz[0] = kr == 0 ? gzr : gn;
-                gz[1] = kr == 0 ? gn : gzr;
-            } else {
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
                 z[k] = s_st[(0 * NP + k) * S + i];
@@ -460,7 +565,6 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             }
 #pragma unroll
             for (int k = 0; k < NP; ++k) gz[k] = gth[k] * dth[k];
-            }
             if (ok) {
                 q1 += reg;
                 if constexpr (STATS) {
@@ -498,6 +602,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                         unscale(transform, a.P.lb[k], a.P.ub[k], k == 0 ? z[0] : z[1], dd);
                 }
             }
+        }
         }
         // arrival: this warp's map writes and partial history sums
         const int lane = tid & 31, warp = tid >> 5;
@@ -615,8 +720,8 @@ int occupancy_v(int variant, int bt, size_t smem) {
 // memory (and its measurements too when they fit), up to kPersistMaxThreads
 // threads (worker warps and a barrier warp).  Returns false when the problem
 // does not fit, in which case the caller uses the per-epoch kernel.
-bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, const int* vol_npad, int nvol,
-                     PersistPlan* plan) {
+bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int pad_block, const int* vol_npad,
+                     int nvol, PersistPlan* plan) {
     if (model != kR2S) return false;
     int dev = 0, nsm = 0, smem_optin = 0, coop = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
@@ -649,9 +754,12 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     // the last pass over the slice is full (every worker warp reaches the
     // grid barrier after the same number of voxels)
     const int variant = persist_variant(a, loss, true);
-    const int maxw = persist_max_threads(variant) - 32;
-    int passes = (slice + maxw - 1) / maxw;
-    int bt = ((slice + passes - 1) / passes + 31) / 32 * 32 + 32;
+    const bool pairs = persist_pairs(variant, stats);  // the kernel takes two voxels per thread
+    const int units = pairs ? slice / 2 : slice;
+    // every variant that may run with this thread count must allow it
+    const int maxw = std::min(persist_max_threads(variant, stats), persist_max_threads(variant, !stats)) - 32;
+    int passes = (units + maxw - 1) / maxw;
+    int bt = ((units + passes - 1) / passes + 31) / 32 * 32 + 32;
     int nb = occupancy_v(variant, bt, smem);
     if (variant != 0) nb = std::min(nb, occupancy_v(0, bt, smem));
     if (nb < 1) return false;
@@ -663,6 +771,7 @@ bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, co
     plan->smem = smem;
     plan->data_in_smem = in_smem;
     plan->quad_width = (!in_smem && variant > 0) ? variant : 0;
+    plan->quad_pairs = pairs ? 1 : 0;
     return true;
 }
 
@@ -672,7 +781,8 @@ cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, P
     // the register-prefetch variants write residuals after their epoch loop,
     // which needs a launch whose last epoch is not followed by an update
     const int variant = persist_variant(a, p.loss, !p.want_res || p.e_end > p.update_last);
-    if (variant != plan.quad_width) p.data_quads = nullptr;  // quads for another width: read [nm][nvtot]
+    const int pairs = persist_pairs(variant, p.stats != 0) ? 1 : 0;
+    if (variant != plan.quad_width || pairs != plan.quad_pairs) p.data_quads = nullptr;  // read [nm][nvtot]
     if (variant == 8) return launch_persist_t<kMSE, 8>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 12) return launch_persist_t<kMSE, 12>(a, p, plan.threads, plan.ctas, plan.smem, s);
     if (variant == 16) return launch_persist_t<kMSE, 16>(a, p, plan.threads, plan.ctas, plan.smem, s);
@@ -696,11 +806,28 @@ __global__ void echo_quads_kernel(const float* data, int nm, int nvtot, int widt
     }
 }
 
+// Pair quads: out[j][u] = (y_2j(2u), y_2j(2u+1), y_2j+1(2u), y_2j+1(2u+1)).
+__global__ void pair_quads_kernel(const float* data, int nm, int nvtot, int width, float4* out) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int npair = nvtot >> 1;
+    if (u >= npair) return;
+    for (int j = 0; j < width / 2; ++j) {
+        const int m0 = 2 * j, m1 = 2 * j + 1;
+        const float2 a = m0 < nm ? *reinterpret_cast<const float2*>(data + (size_t)m0 * nvtot + 2 * u)
+                                 : make_float2(0.f, 0.f);
+        const float2 b = m1 < nm ? *reinterpret_cast<const float2*>(data + (size_t)m1 * nvtot + 2 * u)
+                                 : make_float2(0.f, 0.f);
+        out[(size_t)j * npair + u] = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
 }  // namespace
 
-cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, float4* out, cudaStream_t s) {
-    if (width % 4 != 0 || nm > width) return cudaErrorInvalidValue;
-    echo_quads_kernel<<<(nvtot + 255) / 256, 256, 0, s>>>(data, nm, nvtot, width, out);
+cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, bool pairs, float4* out,
+                              cudaStream_t s) {
+    if (width % 4 != 0 || nm > width || (nvtot & 1)) return cudaErrorInvalidValue;
+    if (pairs) pair_quads_kernel<<<(nvtot / 2 + 255) / 256, 256, 0, s>>>(data, nm, nvtot, width, out);
+    else echo_quads_kernel<<<(nvtot + 255) / 256, 256, 0, s>>>(data, nm, nvtot, width, out);
     ++g_kernel_launches;
     return cudaGetLastError();
 }

@@ -810,11 +810,12 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
         bool want = !(env && strcmp(env, "step") == 0);
         std::vector<int> npad(J.nvol);
         for (int i = 0; i < J.nvol; ++i) npad[i] = J.hv[i].npad;
-        J.use_persist = want && plan_persistent(J.a, J.id, o->loss, J.B, npad.data(), J.nvol, &J.plan);
+        J.use_persist = want && plan_persistent(J.a, J.id, o->loss, J.stats, J.B, npad.data(), J.nvol, &J.plan);
         if (J.use_persist) TRY(wsT(c, S_BAR, 1, &J.barrier));
         if (J.use_persist && J.plan.quad_width > 0) {
             TRY(wsT(c, S_DATA_QUADS, (size_t)J.nvtot * (J.plan.quad_width / 4), &J.data_quads));
-            CK(launch_echo_quads(J.a.data, J.nm, J.nvtot, J.plan.quad_width, J.data_quads, c->stream));
+            CK(launch_echo_quads(J.a.data, J.nm, J.nvtot, J.plan.quad_width, J.plan.quad_pairs != 0, J.data_quads,
+                                 c->stream));
         }
     }
 

@@ -183,6 +183,80 @@ GX_HD float loss_elem(float s, float y, float w, const LossAux& a, float mse_sca
 
 #if defined(__CUDACC__)
 
+// ---------------------------------------------------------------------------
+// FP32 operations with explicit rounding (to nearest, subnormals flushed), on
+// scalars and on packed pairs (PTX f32x2: one instruction for two lanes of a
+// 64-bit register pair).  The optimiser, the parameter transform and the
+// R2*/MSE sums are written with these in every kernel, so that a kernel that
+// updates two voxels per thread with pair instructions produces bit for bit
+// what the one-voxel-per-thread kernels produce.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float add1(float a, float b) {
+    float d;
+    asm("add.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float sub1(float a, float b) {
+    float d;
+    asm("sub.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float mul1(float a, float b) {
+    float d;
+    asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float fma1(float a, float b, float c) {
+    float d;
+    asm("fma.rn.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+// 2^x and 1/x by the PTX approximations (ex2.approx, rcp.approx), subnormals
+// flushed; exp(x) = 2^(x log2 e) and a / b = a * (1/b) are built on them.
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ unsigned long long pk2(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(d);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(d);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    unsigned long long d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+    return upk2(d);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    unsigned long long d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+    return upk2(d);
+}
+__device__ __forceinline__ float2 bcast2(float a) { return make_float2(a, a); }
+
 // Accumulates loss and d(loss)/d(theta) over the measurements of one voxel.
 // set_nan_inf_zero (utils/askadam.m:80): a non-finite prediction becomes 0
 // and carries no gradient.
@@ -207,10 +281,10 @@ __device__ __forceinline__ void mse_add(float r, const float (&dS)[NP], bool bad
 
 template <int NP>
 __device__ __forceinline__ void mse_finish(float& total, float (&g)[NP], float mse_scale) {
-    total *= mse_scale;
-    const float s2 = 2.0f * mse_scale;
+    total = mul1(total, mse_scale);
+    const float s2 = mul1(2.0f, mse_scale);
 #pragma unroll
-    for (int k = 0; k < NP; ++k) g[k] *= s2;
+    for (int k = 0; k < NP; ++k) g[k] = mul1(g[k], s2);
 }
 
 template <int LOSS, int NP>
@@ -258,8 +332,8 @@ template <> struct ModelNP<kNEXI2> { static constexpr int value = 5; };
 
 // One echo of the mono-exponential model, S = M0 exp(-TE R2*), and its
 // derivatives with respect to (M0, R2*) (R2star/gpuR2starMapping.m:427-434).
-__device__ __forceinline__ void r2s_echo(float te, float M0, float R2, float& S, float (&dS)[2]) {
-    float E = __expf(-te * R2);
+__device__ __forceinline__ void r2s_echo(float te, float te_l2e, float M0, float R2, float& S, float (&dS)[2]) {
+    const float E = ex2_ftz(mul1(-te_l2e, R2));  // exp(-te R2*), as in the fused R2*/MSE sums
     S = M0 * E;
     dS[0] = E;
     dS[1] = -te * S;
@@ -375,13 +449,6 @@ __device__ __forceinline__ float rice_mean(const DevProtocol& P, float S, float 
     return S;
 }
 
-// 2^x by the PTX base-2 exponential (ex2.approx, subnormals flushed).
-__device__ __forceinline__ float ex2_ftz(float x) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
 // One echo of R2*/MSE, fused: E = exp(-te R2*) = 2^(-(te log2 e) R2*),
 // r = M0 E - y, and with q = r E the sums sum r^2, sum q (dS/dM0 = E) and
 // sum te q (dS/dR2* = -te M0 E, the factor -M0 applied once per voxel).
@@ -389,19 +456,19 @@ __device__ __forceinline__ float ex2_ftz(float x) {
 struct R2sMseSums {
     float sse = 0.0f, g0 = 0.0f, g1 = 0.0f;
     __device__ __forceinline__ float echo(float te, float te_l2e, float M0, float R2, float y) {
-        const float E = ex2_ftz(__fmul_rn(-te_l2e, R2));
-        const float r = __fmaf_rn(M0, E, -y);
-        sse = __fmaf_rn(r, r, sse);
-        const float q = __fmul_rn(r, E);
-        g0 = __fadd_rn(g0, q);
-        g1 = __fmaf_rn(te, q, g1);
+        const float E = ex2_ftz(mul1(-te_l2e, R2));
+        const float r = fma1(M0, E, -y);
+        sse = fma1(r, r, sse);
+        const float q = mul1(r, E);
+        g0 = add1(g0, q);
+        g1 = fma1(te, q, g1);
         return r;
     }
     template <class Acc>
     __device__ __forceinline__ void store(float M0, Acc& acc) const {
-        acc.total = __fadd_rn(acc.total, sse);
-        acc.g[0] = __fadd_rn(acc.g[0], g0);
-        acc.g[1] = __fmaf_rn(-M0, g1, acc.g[1]);
+        acc.total = add1(acc.total, sse);
+        acc.g[0] = add1(acc.g[0], g0);
+        acc.g[1] = fma1(-M0, g1, acc.g[1]);
     }
 };
 
@@ -419,7 +486,7 @@ __device__ __forceinline__ void model_r2s(const DevProtocol& P, const float* th,
     } else {
         for (int m = 0; m < P.nm; ++m) {
             float S, dS[2];
-            r2s_echo(P.te[m], M0, R2, S, dS);
+            r2s_echo(P.te[m], P.te_l2e[m], M0, R2, S, dS);
             acc.add(m, S, dS);
         }
     }
@@ -445,7 +512,7 @@ __device__ __forceinline__ void model_r2s_unrolled(const DevProtocol& P, int nm,
         for (int m = 0; m < MAXM; ++m) {
             if (m < nm) {
                 float S, dS[2];
-                r2s_echo(P.te[m], M0, R2, S, dS);
+                r2s_echo(P.te[m], P.te_l2e[m], M0, R2, S, dS);
                 acc.add(m, S, dS);
             }
         }
@@ -642,13 +709,15 @@ __device__ __forceinline__ void stage_protocol(const DevProtocol& P, DevProtocol
     for (int i = threadIdx.x; i < (int)(sizeof(DevProtocol) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
 }
 
-// unscale_parameters (utils/askadam.m:1063-1075) and its derivative; the
-// logistic uses the fast reciprocal (2 ulp).
+// unscale_parameters (utils/askadam.m:1063-1075) and its derivative: the
+// logistic s = 1 / (1 + exp(-z)) with exp(-z) = 2^(-z log2 e) and the fast
+// reciprocal; theta = lb + (ub-lb) s, dtheta/dz = (ub-lb) s (1-s).
 __device__ __forceinline__ float unscale(int transform, float lb, float ub, float z, float& dth) {
     if (transform == 0) {
-        float s = __fdividef(1.0f, 1.0f + __expf(-z));
-        dth = (ub - lb) * s * (1.0f - s);
-        return lb + (ub - lb) * s;
+        const float s = rcp_ftz(add1(1.0f, ex2_ftz(mul1(z, -kLog2e))));
+        const float d = sub1(ub, lb);
+        dth = mul1(mul1(d, s), sub1(1.0f, s));
+        return fma1(d, s, lb);
     }
     float zc = fminf(fmaxf(z, 0.0f), 1.0f);  // set_boundary01 before evaluation
     dth = (z >= 0.0f && z <= 1.0f) ? (ub - lb) : 0.0f;
@@ -683,19 +752,21 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
 // Optimiser step of one parameter (adamupdate / sgdmupdate / rmspropupdate,
 // called from utils/askadam.m:673-691).  sc = per-epoch schedule:
 // Adam (lr_e/(1-b1^e), 1/(1-b2^e)); others (lr_e, 0).  The square root is
-// x*rsqrt(x) (exact zero kept) and the division the fast 2-ulp one.
+// x*rsqrt(x) (exact zero kept) and the Adam quotient a * rcp(b).
 struct OptConst {
     int optimiser;
     float beta1, beta2, eps, momentum, rms_decay, rms_eps;
 };
 
-__device__ __forceinline__ float fast_sqrt0(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+__device__ __forceinline__ float fast_sqrt0(float x) { return x > 0.0f ? mul1(x, rsqrtf(x)) : 0.0f; }
 
+// Adam: m1 = b1 m1 + (1-b1) g, m2 = b2 m2 + ((1-b2) g) g,
+// z -= (lr_e m1) / (sqrt(m2 / (1-b2^e)) + eps).
 __device__ __forceinline__ void opt_step(const OptConst& o, float2 sc, float& z, float& m1, float& m2, float g) {
     if (o.optimiser == kAdam) {
-        m1 = o.beta1 * m1 + (1.0f - o.beta1) * g;
-        m2 = o.beta2 * m2 + (1.0f - o.beta2) * g * g;
-        z -= __fdividef(sc.x * m1, fast_sqrt0(m2 * sc.y) + o.eps);
+        m1 = fma1(o.beta1, m1, mul1(sub1(1.0f, o.beta1), g));
+        m2 = fma1(o.beta2, m2, mul1(mul1(sub1(1.0f, o.beta2), g), g));
+        z = sub1(z, mul1(mul1(sc.x, m1), rcp_ftz(add1(fast_sqrt0(mul1(m2, sc.y)), o.eps))));
     } else if (o.optimiser == kSGDM) {
         m1 = o.momentum * m1 - sc.x * g;
         z += m1;
@@ -703,6 +774,27 @@ __device__ __forceinline__ void opt_step(const OptConst& o, float2 sc, float& z,
         m2 = o.rms_decay * m2 + (1.0f - o.rms_decay) * g * g;
         z -= __fdividef(sc.x * g, fast_sqrt0(m2) + o.rms_eps);
     }
+}
+
+// The same transform and Adam step on a pair of voxels (pair instructions;
+// bit for bit the scalar ones on each lane).
+__device__ __forceinline__ float2 unscale_sig2(float lb, float ub, float2 z, float2& dth) {
+    const float2 e = mul2(z, bcast2(-kLog2e));
+    const float2 den = add2(bcast2(1.0f), make_float2(ex2_ftz(e.x), ex2_ftz(e.y)));
+    const float2 s = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
+    const float2 d = bcast2(sub1(ub, lb));
+    dth = mul2(mul2(d, s), sub2(bcast2(1.0f), s));
+    return fma2(d, s, bcast2(lb));
+}
+
+__device__ __forceinline__ void adam_step2(const OptConst& o, float2 sc, float2& z, float2& m1, float2& m2,
+                                           float2 g) {
+    m1 = fma2(bcast2(o.beta1), m1, mul2(bcast2(sub1(1.0f, o.beta1)), g));
+    m2 = fma2(bcast2(o.beta2), m2, mul2(mul2(bcast2(sub1(1.0f, o.beta2)), g), g));
+    const float2 v = mul2(m2, bcast2(sc.y));
+    const float2 den = add2(make_float2(fast_sqrt0(v.x), fast_sqrt0(v.y)), bcast2(o.eps));
+    const float2 num = mul2(bcast2(sc.x), m1);
+    z = sub2(z, mul2(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y))));
 }
 
 #endif  // __CUDACC__

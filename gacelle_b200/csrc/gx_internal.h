@@ -219,14 +219,18 @@ struct PersistArgs {
 struct PersistPlan {
     int slice, vpt, threads, ctas, data_in_smem;
     int quad_width;          // > 0: the launch reads echo quads, this many measurements wide
+    int quad_pairs;          // the quads are pair quads (two voxels per thread)
     size_t smem;
 };
 
-bool plan_persistent(const AdamParams& a, int model, int loss, int pad_block, const int* vol_npad, int nvol,
-                     PersistPlan* plan);
+bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int pad_block, const int* vol_npad,
+                     int nvol, PersistPlan* plan);
 cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s);
-// out[j][v] = (data[4j][v], .., data[4j+3][v]), 0 for nm <= m < width (width % 4 == 0)
-cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, float4* out, cudaStream_t s);
+// Echo quads out[j][v] = (data[4j][v], .., data[4j+3][v]), or with pairs
+// out[j][u] = (data[2j][2u], data[2j][2u+1], data[2j+1][2u], data[2j+1][2u+1]);
+// 0 for nm <= m < width (width % 4 == 0, nvtot even)
+cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, bool pairs, float4* out,
+                              cudaStream_t s);
 
 }  // namespace gx
 
