@@ -343,37 +343,42 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const bool upd = e <= p.update_last;
         const float2 sc = upd ? a.sched[e] : float2{0.f, 0.f};
         if constexpr (PAIR) {
-        // two voxels (i, i+1) per thread and pass; the parameter, gradient and
-        // optimiser arithmetic in pair instructions, lane l on voxel i+l
+        // two voxels per thread and pass: pair q takes voxels i0 = 64 (q / 32)
+        // + q % 32 and i1 = i0 + 32 of the slice (a warp covers 64
+        // consecutive voxels, and each of its per-voxel accesses 32
+        // consecutive ones); the parameter, gradient and optimiser arithmetic
+        // in pair instructions, lane .x on voxel i0 and .y on voxel i1
         const int kr = a.reg_param[0];  // the regularised parameter
         const float lbr = a.P.lb[kr], ubr = a.P.ub[kr];
         const size_t half = (size_t)(a.nvtot >> 1);
-        // measurements of the pair at slice position i: echo m of both voxels
+        const int npair = n >> 1;  // n is a multiple of 64 in pair mode
+        auto ld2 = [](const float* b, int i0) { return make_float2(b[i0], b[i0 + 32]); };
+        auto st2 = [](float* b, int i0, float2 x) {
+            b[i0] = x.x;
+            b[i0 + 32] = x.y;
+        };
         // pass 1: data fidelity of the slice (own voxels only)
-        for (int i = 2 * tid; i < n; i += 2 * NWT) {
-            const int v = base + i;
-            const bool ok0 = (v - V.off) < V.nvox, ok1 = (v + 1 - V.off) < V.nvox;
+        for (int q = tid; q < npair; q += NWT) {
+            const int i0 = ((q >> 5) << 6) + (q & 31), v0 = base + i0;
+            const bool ok0 = (v0 - V.off) < V.nvox, ok1 = (v0 + 32 - V.off) < V.nvox;
             float2 y[MAXM];  // measurement m of both voxels
             if (p.data_quads) {
-                const float4* q = p.data_quads + (v >> 1);
+                const float4* pq = p.data_quads + (base >> 1) + q;
 #pragma unroll
                 for (int j = 0; j < MAXM / 2; ++j) {
-                    const float4 t = __ldcg(q + j * half);
+                    const float4 t = __ldcg(pq + j * half);
                     y[2 * j] = make_float2(t.x, t.y);
                     y[2 * j + 1] = make_float2(t.z, t.w);
                 }
             } else {
-                const float* yb = p.data_in_smem ? s_y + i : a.data + v;
+                const float* yb = p.data_in_smem ? s_y + i0 : a.data + v0;
                 const size_t ys = p.data_in_smem ? (size_t)S : (size_t)a.nvtot;
 #pragma unroll
-                for (int m = 0; m < MAXM; ++m)
-                    y[m] = m < nm ? *reinterpret_cast<const float2*>(yb + m * ys) : make_float2(0.f, 0.f);
+                for (int m = 0; m < MAXM; ++m) y[m] = m < nm ? ld2(yb + m * ys, 0) : make_float2(0.f, 0.f);
             }
             float2 th[NP], dth[NP];
 #pragma unroll
-            for (int k = 0; k < NP; ++k)
-                th[k] = unscale_sig2(a.P.lb[k], a.P.ub[k], *reinterpret_cast<const float2*>(s_st + k * S + i),
-                                     dth[k]);
+            for (int k = 0; k < NP; ++k) th[k] = unscale_sig2(a.P.lb[k], a.P.ub[k], ld2(s_st + k * S, i0), dth[k]);
             // R2sMseSums on both lanes with the residual negated, y - M0 E:
             // every partial sum is the exact negative of the scalar one
             float2 sse = make_float2(0.f, 0.f), g0n = sse, g1n = sse;
@@ -397,10 +402,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             g[1] = mul2(fma2(th[0], g1n, zero), bcast2(s2));
             const float2 nrm = bcast2(V.norm);
             const float2 gr = mul2(kr == 0 ? g[0] : g[1], nrm), gn = mul2(kr == 0 ? g[1] : g[0], nrm);
-            *reinterpret_cast<float2*>(s_gf + 0 * S + i) = mul2(gn, kr == 0 ? dth[1] : dth[0]);
-            *reinterpret_cast<float2*>(s_gf + 1 * S + i) = gr;
-            *reinterpret_cast<float2*>(s_gf + 2 * S + i) = kr == 0 ? dth[0] : dth[1];
-            *reinterpret_cast<float2*>(s_gf + 3 * S + i) = kr == 0 ? th[0] : th[1];
+            st2(s_gf + 0 * S, i0, mul2(gn, kr == 0 ? dth[1] : dth[0]));
+            st2(s_gf + 1 * S, i0, gr);
+            st2(s_gf + 2 * S, i0, kr == 0 ? dth[0] : dth[1]);
+            st2(s_gf + 3 * S, i0, kr == 0 ? th[0] : th[1]);
             if (ok0) q0 += tot.x;
             if (ok1) q0 += tot.y;
         }
@@ -415,29 +420,28 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         float* Gn = gnext + V.grid_off;
         const float iv[3] = {ivx, ivy, ivz};
         // pass 2: TV subgradient, chain rule, optimiser, new map values
-        for (int i = 2 * tid; i < n; i += 2 * NWT) {
-            const int v = base + i;
-            const bool ok0 = (v - V.off) < V.nvox, ok1 = (v + 1 - V.off) < V.nvox;
-            const float2 gn = *reinterpret_cast<const float2*>(s_gf + 0 * S + i);
-            float2 grf = *reinterpret_cast<const float2*>(s_gf + 1 * S + i);
-            const float2 dthr = *reinterpret_cast<const float2*>(s_gf + 2 * S + i);
-            const float2 c = *reinterpret_cast<const float2*>(s_gf + 3 * S + i);
-            const int2 pidx = *reinterpret_cast<const int2*>(s_p + i);
-            const unsigned int fl2 = *reinterpret_cast<const unsigned int*>(s_fl + i);
+        for (int q = tid; q < npair; q += NWT) {
+            const int i0 = ((q >> 5) << 6) + (q & 31), i1 = i0 + 32, v0 = base + i0;
+            const bool ok0 = (v0 - V.off) < V.nvox, ok1 = (v0 + 32 - V.off) < V.nvox;
+            const float2 gn = ld2(s_gf + 0 * S, i0);
+            float2 grf = ld2(s_gf + 1 * S, i0);
+            const float2 dthr = ld2(s_gf + 2 * S, i0);
+            const float2 c = ld2(s_gf + 3 * S, i0);
+            const int p0 = s_p[i0], p1 = s_p[i1];
             if (ok0) {
-                const unsigned int fl = fl2 & 0xffffu;
+                const unsigned int fl = s_fl[i0];
                 const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
                 float f[3], b[3], cost, gt;
-                nb.load(G, pidx.x, fl, f, b);
+                nb.load(G, p0, fl, f, b);
                 tv_terms(c.x, f, b, mb, iv, tv3 ? 3 : 2, cost, gt);
                 q1 = __fmaf_rn(tvs0, cost, q1);
                 grf.x = __fmaf_rn(tvs0, gt, grf.x);
             }
             if (ok1) {
-                const unsigned int fl = fl2 >> 16;
+                const unsigned int fl = s_fl[i1];
                 const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
                 float f[3], b[3], cost, gt;
-                nb.load(G, pidx.y, fl, f, b);
+                nb.load(G, p1, fl, f, b);
                 tv_terms(c.y, f, b, mb, iv, tv3 ? 3 : 2, cost, gt);
                 q1 = __fmaf_rn(tvs0, cost, q1);
                 grf.y = __fmaf_rn(tvs0, gt, grf.y);
@@ -448,25 +452,25 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 float2 zr = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int k = 0; k < NP; ++k) {
-                    float2* pz = reinterpret_cast<float2*>(s_st + (0 * NP + k) * S + i);
-                    float2* p1 = reinterpret_cast<float2*>(s_st + (1 * NP + k) * S + i);
-                    float2* p2 = reinterpret_cast<float2*>(s_st + (2 * NP + k) * S + i);
-                    float2 zz = *pz, mm1 = *p1, mm2 = *p2;
+                    float* pz = s_st + (0 * NP + k) * S;
+                    float* p1s = s_st + (1 * NP + k) * S;
+                    float* p2s = s_st + (2 * NP + k) * S;
+                    float2 zz = ld2(pz, i0), mm1 = ld2(p1s, i0), mm2 = ld2(p2s, i0);
                     adam_step2(oc, sc, zz, mm1, mm2, gz[k]);
-                    *pz = zz;
-                    *p1 = mm1;
-                    *p2 = mm2;
+                    st2(pz, i0, zz);
+                    st2(p1s, i0, mm1);
+                    st2(p2s, i0, mm2);
                     if (k == kr) zr = zz;
-                    if (ckpt) {  // padding lanes included: never read back
-                        *reinterpret_cast<float2*>(cp + (size_t)k * a.nvtot + v) = zz;
-                        *reinterpret_cast<float2*>(cp + (size_t)(NP + k) * a.nvtot + v) = mm1;
-                        *reinterpret_cast<float2*>(cp + (size_t)(2 * NP + k) * a.nvtot + v) = mm2;
+                    if (ckpt) {  // padding voxels included: never read back
+                        st2(cp + (size_t)k * a.nvtot, v0, zz);
+                        st2(cp + (size_t)(NP + k) * a.nvtot, v0, mm1);
+                        st2(cp + (size_t)(2 * NP + k) * a.nvtot, v0, mm2);
                     }
                 }
                 float2 dd;
                 const float2 thr = unscale_sig2(lbr, ubr, zr, dd);
-                if (ok0) Gn[pidx.x] = thr.x;
-                if (ok1) Gn[pidx.y] = thr.y;
+                if (ok0) Gn[p0] = thr.x;
+                if (ok1) Gn[p1] = thr.y;
             }
         }
         } else {
@@ -670,6 +674,9 @@ namespace {
 // Variants: MSE with up to 8, 12, 16 or 32 echoes (measurements prefetched
 // into registers; the smallest bound that holds the protocol), and any loss /
 // echo count with the loss chosen at run time.
+// The pair variant covers a slice in chunks of 64 voxels (pairs i, i+32).
+bool pair_layout_ok(int nvtot, int slice) { return nvtot % 64 == 0 && slice % 64 == 0; }
+
 int persist_variant(const AdamParams& a, int loss, bool res_after_loop) {
     const bool std_cfg = loss == kMSE && a.transform == 0 && a.optimiser == kAdam && a.n_reg == 1 && res_after_loop;
     if (std_cfg && a.nm <= 8) return 8;
@@ -728,9 +735,9 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
-    // one volume: slices of whole warps; several: of padding blocks, so that
-    // every volume starts on a slice boundary
-    const int gran = nvol == 1 ? 32 : pad_block;
+    // one volume: slices of 64 voxels (the pair variant's chunks); several:
+    // of padding blocks, so that every volume starts on a slice boundary
+    const int gran = nvol == 1 ? 64 : pad_block;
     int slice = (a.nvtot + nsm - 1) / nsm;
     slice = (slice + gran - 1) / gran * gran;
     {
@@ -754,7 +761,7 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
     // the last pass over the slice is full (every worker warp reaches the
     // grid barrier after the same number of voxels)
     const int variant = persist_variant(a, loss, true);
-    const bool pairs = persist_pairs(variant, stats);  // the kernel takes two voxels per thread
+    const bool pairs = persist_pairs(variant, stats) && pair_layout_ok(a.nvtot, slice);  // two voxels per thread
     const int units = pairs ? slice / 2 : slice;
     // every variant that may run with this thread count must allow it
     const int maxw = std::min(persist_max_threads(variant, stats), persist_max_threads(variant, !stats)) - 32;
@@ -781,12 +788,16 @@ cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, P
     // the register-prefetch variants write residuals after their epoch loop,
     // which needs a launch whose last epoch is not followed by an update
     const int variant = persist_variant(a, p.loss, !p.want_res || p.e_end > p.update_last);
-    const int pairs = persist_pairs(variant, p.stats != 0) ? 1 : 0;
-    if (variant != plan.quad_width || pairs != plan.quad_pairs) p.data_quads = nullptr;  // read [nm][nvtot]
-    if (variant == 8) return launch_persist_t<kMSE, 8>(a, p, plan.threads, plan.ctas, plan.smem, s);
-    if (variant == 12) return launch_persist_t<kMSE, 12>(a, p, plan.threads, plan.ctas, plan.smem, s);
-    if (variant == 16) return launch_persist_t<kMSE, 16>(a, p, plan.threads, plan.ctas, plan.smem, s);
-    if (variant == 32) return launch_persist_t<kMSE, 32>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    // the pair variant needs slices and a work-list of whole 64-voxel chunks;
+    // otherwise the run-time variant takes the launch
+    int var = variant;
+    if (persist_pairs(var, p.stats != 0) && !pair_layout_ok(a.nvtot, plan.slice)) var = 0;
+    const int pairs = persist_pairs(var, p.stats != 0) ? 1 : 0;
+    if (var != plan.quad_width || pairs != plan.quad_pairs) p.data_quads = nullptr;  // read [nm][nvtot]
+    if (var == 8) return launch_persist_t<kMSE, 8>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    if (var == 12) return launch_persist_t<kMSE, 12>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    if (var == 16) return launch_persist_t<kMSE, 16>(a, p, plan.threads, plan.ctas, plan.smem, s);
+    if (var == 32) return launch_persist_t<kMSE, 32>(a, p, plan.threads, plan.ctas, plan.smem, s);
     return launch_persist_t<-1, 0>(a, p, plan.threads, plan.ctas, plan.smem, s);
 }
 
@@ -806,18 +817,19 @@ __global__ void echo_quads_kernel(const float* data, int nm, int nvtot, int widt
     }
 }
 
-// Pair quads: out[j][u] = (y_2j(2u), y_2j(2u+1), y_2j+1(2u), y_2j+1(2u+1)).
+// Pair quads: with the voxel pairs (u0, u0 + 32), u0 = 64 (u / 32) + u % 32,
+// out[j][u] = (y_2j(u0), y_2j(u0+32), y_2j+1(u0), y_2j+1(u0+32)).
 __global__ void pair_quads_kernel(const float* data, int nm, int nvtot, int width, float4* out) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int npair = nvtot >> 1;
     if (u >= npair) return;
+    const int u0 = ((u >> 5) << 6) + (u & 31);
     for (int j = 0; j < width / 2; ++j) {
         const int m0 = 2 * j, m1 = 2 * j + 1;
-        const float2 a = m0 < nm ? *reinterpret_cast<const float2*>(data + (size_t)m0 * nvtot + 2 * u)
-                                 : make_float2(0.f, 0.f);
-        const float2 b = m1 < nm ? *reinterpret_cast<const float2*>(data + (size_t)m1 * nvtot + 2 * u)
-                                 : make_float2(0.f, 0.f);
-        out[(size_t)j * npair + u] = make_float4(a.x, a.y, b.x, b.y);
+        const float* r0 = data + (size_t)m0 * nvtot + u0;
+        const float* r1 = data + (size_t)m1 * nvtot + u0;
+        out[(size_t)j * npair + u] = make_float4(m0 < nm ? r0[0] : 0.f, m0 < nm ? r0[32] : 0.f,
+                                                 m1 < nm ? r1[0] : 0.f, m1 < nm ? r1[32] : 0.f);
     }
 }
 
@@ -825,7 +837,7 @@ __global__ void pair_quads_kernel(const float* data, int nm, int nvtot, int widt
 
 cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, bool pairs, float4* out,
                               cudaStream_t s) {
-    if (width % 4 != 0 || nm > width || (nvtot & 1)) return cudaErrorInvalidValue;
+    if (width % 4 != 0 || nm > width || (pairs ? nvtot % 64 : nvtot % 2)) return cudaErrorInvalidValue;
     if (pairs) pair_quads_kernel<<<(nvtot / 2 + 255) / 256, 256, 0, s>>>(data, nm, nvtot, width, out);
     else echo_quads_kernel<<<(nvtot + 255) / 256, 256, 0, s>>>(data, nm, nvtot, width, out);
     ++g_kernel_launches;
