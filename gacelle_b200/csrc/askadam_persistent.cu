@@ -100,21 +100,16 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
 }
 
 // Grid barrier of a cooperative launch, run by one thread per CTA (the last
-// lane of the CTA's barrier warp): after the CTA's writes are acquired at CTA
-// scope, it releases them to the other CTAs (the last CTA to arrive opens
-// generation gen+1) and waits until generation gen+1 is open.  The wait is
-// bounded; false once any CTA's wait has expired.
-__device__ __forceinline__ bool grid_sync_one(PersistBarrier* gb, unsigned int nblocks, unsigned int& gen) {
-    __threadfence();
-    const unsigned int g = gen;
-    unsigned int arrived = atomicAdd(&gb->count, 1u);
-    if (arrived == nblocks - 1) {
-        atomicExch(&gb->count, 0u);
-        __threadfence();
-        atomicExch(&gb->gen, g + 1u);
-    }
+// lane of the CTA's barrier warp) on a counter that only grows (zeroed before
+// the launch): after the CTA's writes are acquired at CTA scope, one
+// release-add publishes them to the other CTAs, and the barrier of the k-th
+// epoch boundary is open once the counter reaches (k+1) x #CTAs, so the last
+// CTA's add itself opens it.  The wait is bounded; false once any CTA's wait
+// has expired.
+__device__ __forceinline__ bool grid_sync_one(PersistBarrier* gb, unsigned int target) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gb->count) : "memory");
     const long long t0 = clock64();
-    while (ld_acquire_gpu(&gb->gen) == g) {
+    while (ld_acquire_gpu(&gb->count) < target) {
         if (*(volatile int*)&gb->error) return false;
         if (clock64() - t0 > kBarrierSpinCycles) {
             atomicExch(&gb->error, 1);
@@ -122,7 +117,6 @@ __device__ __forceinline__ bool grid_sync_one(PersistBarrier* gb, unsigned int n
         }
         __nanosleep(20);
     }
-    gen = g + 1u;
     return *(volatile int*)&gb->error == 0;
 }
 
@@ -304,8 +298,6 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         // barrier warp: history of each epoch, grid barrier between epochs
         const int lane = tid & 31, nw = NWT >> 5;
         constexpr int NQ = STATS ? kHistW : 2;  // without statistics columns 2-4 stay zero
-        unsigned int gen = 0;
-        if (lane == 31) gen = atomicAdd(&p.barrier->gen, 0u);
         const int vol = a.blk_vol[base / p.pad_block];
         for (int e = p.e_begin; e <= p.e_end; ++e) {
             const unsigned int ph = (unsigned int)(e - p.e_begin) & 1u;
@@ -327,7 +319,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             if (e < p.e_end) {
                 int ok = 1;
                 if (lane == 31) {
-                    ok = grid_sync_one(p.barrier, gridDim.x, gen);
+                    ok = grid_sync_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x);
                     if (!ok) *(volatile int*)&s_err = 1;
                     mbar_arrive(&bar_open);
                 }

@@ -198,10 +198,9 @@ constexpr int kPersistMaxThreads = 1024;
 constexpr long long kBarrierSpinCycles = 4000000000LL;  // about 2 s at B200 clocks
 
 struct PersistBarrier {
-    unsigned int count;
-    unsigned int gen;
-    int error;
-    int pad;
+    unsigned int count;  // CTA arrivals since the launch (zeroed before it)
+    int error;           // a bounded wait expired
+    int pad[2];
 };
 
 struct PersistArgs {
