@@ -106,8 +106,11 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
 // epoch boundary is open once the counter reaches (k+1) x #CTAs, so the last
 // CTA's add itself opens it.  The wait is bounded; false once any CTA's wait
 // has expired.
-__device__ __forceinline__ bool grid_sync_one(PersistBarrier* gb, unsigned int target) {
+__device__ __forceinline__ void grid_arrive_one(PersistBarrier* gb) {
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gb->count) : "memory");
+}
+
+__device__ __forceinline__ bool grid_wait_one(PersistBarrier* gb, unsigned int target) {
     const long long t0 = clock64();
     while (ld_acquire_gpu(&gb->count) < target) {
         if (*(volatile int*)&gb->error) return false;
@@ -308,6 +311,14 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 }
                 return;
             }
+            // lane 31 publishes the CTA's maps and waits for the other CTAs
+            // while lanes 0-4 add the epoch's loss history
+            int ok = 1;
+            if (e < p.e_end && lane == 31) {
+                grid_arrive_one(p.barrier);
+                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x);
+                if (!ok) *(volatile int*)&s_err = 1;
+            }
             if (p.record && a.hist && lane < NQ) {
                 const double* buf = s_red + (e & 1) * 32 * kHistW;
                 double t = 0.0;
@@ -317,12 +328,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             }
             __syncwarp();  // the history buffer of epoch e is read before epoch e+1 opens
             if (e < p.e_end) {
-                int ok = 1;
-                if (lane == 31) {
-                    ok = grid_sync_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x);
-                    if (!ok) *(volatile int*)&s_err = 1;
-                    mbar_arrive(&bar_open);
-                }
+                if (lane == 31) mbar_arrive(&bar_open);
                 ok = __shfl_sync(0xffffffffu, ok, 31);
                 if (!ok) return;
             }
