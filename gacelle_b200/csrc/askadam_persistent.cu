@@ -384,13 +384,13 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
 #pragma unroll
             for (int m = 0; m < MAXM; ++m)
                 if (m < nm) {
-                    const float2 x = mul2(bcast2(-a.P.te_l2e[m]), R2);
+                    const float2 x = mul2(a.P.nl2e_pair[m], R2);
                     const float2 E = make_float2(ex2_ftz(x.x), ex2_ftz(x.y));
                     const float2 rn = fma2(nM0, E, y[m]);
                     sse = fma2(rn, rn, sse);
                     const float2 qn = mul2(rn, E);
                     g0n = add2(g0n, qn);
-                    g1n = fma2(bcast2(a.P.te[m]), qn, g1n);
+                    g1n = fma2(a.P.te_pair[m], qn, g1n);
                 }
             const float2 zero = make_float2(0.f, 0.f);
             const float s2 = mul1(2.0f, a.mse_scale);

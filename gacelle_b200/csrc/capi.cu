@@ -280,6 +280,10 @@ static DevProtocol make_protocol(const gx_model* m, int id, int np, int nm, cons
         for (int i = 0; i < m->n_te && i < kMaxTE; ++i) {
             P.te[i] = (float)m->te[i];
             P.te_l2e[i] = (float)(m->te[i] * M_LOG2E);
+            if (i < kPairTE) {
+                P.te_pair[i] = make_float2(P.te[i], P.te[i]);
+                P.nl2e_pair[i] = make_float2(-P.te_l2e[i], -P.te_l2e[i]);
+            }
         }
     if (m->fa_deg) for (int i = 0; i < m->n_fa && i < kMaxFA; ++i) P.fa_rad[i] = (float)(m->fa_deg[i] * M_PI / 180.0);
     if (m->bval) for (int i = 0; i < m->n_shell && i < kMaxShell; ++i) P.bval[i] = (float)m->bval[i];

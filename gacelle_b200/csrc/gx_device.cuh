@@ -18,6 +18,7 @@
 namespace gx {
 
 constexpr int kMaxTE = 64;
+constexpr int kPairTE = 16;  // echoes of the pair variant of the persistent TV kernel
 constexpr int kMaxFA = 16;
 constexpr int kMaxShell = 64;
 constexpr int kMaxParam = 6;  // fitted parameters + noise
@@ -40,6 +41,10 @@ struct DevProtocol {
     float h;     // NEXI node spacing 1/(nx-1)
     float te[kMaxTE];
     float te_l2e[kMaxTE];   // te * log2(e): exp(-te R2*) = 2^(-te_l2e R2*)
+    // the first kPairTE of te and -te_l2e duplicated into (x, x) pairs: 64-bit
+    // operands of the two-voxel pair instructions
+    float2 te_pair[kPairTE];
+    float2 nl2e_pair[kPairTE];
     float fa_rad[kMaxFA];
     float bval[kMaxShell];
     float delta[kMaxShell];
