@@ -100,7 +100,10 @@ class GxMcmcResult(C.Structure):
 class GxTiming(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("main_kernel_ms", C.c_double),
                 ("main_launches", C.c_int32), ("kernel_launches", C.c_int64),
-                ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
+                ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("tv_path", C.c_int32)]
+
+
+TV_PERSISTENT, TV_PAIRS, TV_DATA_SMEM, TV_DATA_QUADS = 1, 2, 4, 8
 
 
 STRUCTS = {"gx_model": GxModel, "gx_volume": GxVolume, "gx_askadam_opts": GxAskadamOpts,

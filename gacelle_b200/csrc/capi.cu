@@ -884,6 +884,9 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
     c->timing.main_kernel_ms = ms;
     c->timing.main_launches = n_main;
+    c->timing.tv_path = !J.use_persist ? 0
+                        : GX_TV_PERSISTENT | (J.plan.quad_pairs ? GX_TV_PAIRS : 0) |
+                              (J.plan.data_in_smem ? GX_TV_DATA_SMEM : 0) | (J.data_quads ? GX_TV_DATA_QUADS : 0);
     if (J.use_persist) {
         PersistBarrier hb;
         CK(cudaMemcpy(&hb, J.barrier, sizeof(hb), cudaMemcpyDeviceToHost));

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define GX_ABI_VERSION 3
+#define GX_ABI_VERSION 4
 
 typedef enum {
     GX_OK = 0,
@@ -229,7 +229,14 @@ typedef struct {
     int32_t main_launches;      /* number of main-kernel launches timed */
     int64_t kernel_launches;    /* launches of this library's kernels in the call */
     int64_t h2d_bytes, d2h_bytes;
+    int32_t tv_path;            /* askAdam with TV: GX_TV_* flags of the main pass, else 0 */
 } gx_timing;
+
+/* gx_timing.tv_path flags */
+#define GX_TV_PERSISTENT 1      /* all epochs of a launch in one cooperative kernel */
+#define GX_TV_PAIRS 2           /* two voxels per thread (FP32x2 pair instructions) */
+#define GX_TV_DATA_SMEM 4       /* measurements staged in shared memory */
+#define GX_TV_DATA_QUADS 8      /* measurements read from L2 as echo / pair quads */
 
 const char* gx_version(void);
 int32_t gx_abi_version(void);

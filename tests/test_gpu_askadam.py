@@ -249,25 +249,42 @@ def test_askadam_stop_criteria_within_fp32_band(ctx, criterion):
     assert abs(eng["final_niteration"] - orc["final_niter"]) <= band
 
 
-@pytest.mark.parametrize("case", ["plain_run", "tol_stop", "stats", "echoes24", "l1_loss", "linear_transform"])
+_ECHOES = {"echoes24": 24, "echoes16": 16, "echoes10": 10, "echoes6": 6}
+P_, PAIRS_, SMEM_, QUADS_ = _lib.TV_PERSISTENT, _lib.TV_PAIRS, _lib.TV_DATA_SMEM, _lib.TV_DATA_QUADS
+_TV_PATH = {"plain_run": P_ | PAIRS_ | SMEM_, "tol_stop": P_ | PAIRS_ | SMEM_, "stats": P_ | SMEM_,
+            "echoes24": P_ | SMEM_, "echoes16": P_ | PAIRS_ | SMEM_, "echoes10": P_ | PAIRS_ | SMEM_,
+            "echoes6": P_ | PAIRS_ | SMEM_, "l1_loss": P_ | SMEM_, "linear_transform": P_ | SMEM_,
+            "large_l2": P_ | PAIRS_ | QUADS_}
+
+
+@pytest.mark.parametrize("case", ["plain_run", "tol_stop", "stats", "echoes24", "echoes16", "echoes10", "echoes6",
+                                  "large_l2", "l1_loss", "linear_transform"])
 def test_tv_persistent_kernel_matches_per_epoch_kernel(ctx, case, monkeypatch):
     """The one-launch persistent TV kernel and the one-launch-per-epoch kernel
     run the same per-voxel arithmetic (shared model, loss, TV and optimiser
-    code): the same parameters, losses, residuals and stopping epochs
-    (checkpoints written by one are replayed by the other).  A well-conditioned
-    TV weight keeps compiler-level rounding differences from being amplified.
-    The cases cover the kernel's variants: up to 16 echoes and 17-32 echoes
-    with the standard options (MSE, sigmoid, Adam), and the generic variant
-    (another loss or transform).  The L1 loss (sign subgradient) and the
-    linear transform (clamped at the bounds) amplify single-rounding
-    differences between the two kernels' compiled code, so for those the two
-    kernels must each stay inside the FP32 band around the FP64 oracle."""
+    code; the two-voxels-per-thread variant computes every lane bit for bit
+    as the one-voxel code): the same parameters, losses, residuals and
+    stopping epochs (checkpoints written by one are replayed by the other).  A
+    well-conditioned TV weight keeps rounding differences from being
+    amplified.  The cases cover the kernel's variants, checked through the
+    call's reported TV path: the pair variant with 6, 10, 12 and 16 echoes
+    (echo bounds 8, 12, 16, zero-padded above the protocol), the one-voxel
+    variants for 24 echoes and with statistics, the generic variant (another
+    loss or transform), and measurements staged in shared memory or, for a
+    volume whose slices do not fit (482k voxels), read from L2 as pair
+    quads.  The L1 loss (sign subgradient) and the linear transform (clamped
+    at the bounds) amplify single-rounding differences between the two
+    kernels' compiled code, so for those the two kernels must each stay
+    inside the FP32 band around the FP64 oracle."""
     model_kw = {}
-    if case == "echoes24":
+    if case in _ECHOES or case == "large_l2":
         from gacelle_b200 import phantoms, utils
-        te = np.linspace(2.0, 48.0, 24) * 1e-3
+        nte = _ECHOES.get(case, 12)
+        te = np.linspace(2.0, 2.0 + 2.0 * (nte - 1), nte) * 1e-3 if case != "large_l2" else \
+            np.arange(2.0, 40.6, 3.5) * 1e-3
         model_kw = {"te": te}
-        mask = phantoms.ellipsoid_mask((40, 40, 24), 1.0)
+        shape = (112, 112, 64) if case == "large_l2" else (40, 40, 24)
+        mask = phantoms.ellipsoid_mask(shape, 1.0)
         data, _ = phantoms.r2s_phantom(mask, 7, te=te)
         idx = utils.mask_index(mask)
         y = utils.reshape_ND2GD(data, idx)
@@ -290,12 +307,14 @@ def test_tv_persistent_kernel_matches_per_epoch_kernel(ctx, case, monkeypatch):
         f = fitting(iteration=300, initialLearnRate=0.01, convergenceStepTol=1e-9, convergenceGradTol=1e-12,
                     chunk=64, **over)
     else:
-        f = fitting(iteration=300, initialLearnRate=0.01, **over)
+        f = fitting(iteration=200 if case == "large_l2" else 300, initialLearnRate=0.01, **over)
     monkeypatch.setenv("GACELLE_B200_TV_KERNEL", "step")
     a = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
     monkeypatch.setenv("GACELLE_B200_TV_KERNEL", "persistent")
     b = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
     assert b["timing"]["main_launches"] < a["timing"]["main_launches"]
+    assert a["timing"]["tv_path"] == 0
+    assert b["timing"]["tv_path"] == _TV_PATH[case], (case, b["timing"]["tv_path"])
     if case in ("l1_loss", "linear_transform"):
         orc = run_oracle("r2s", y, th0, f, NAMES["r2s"], **kw)
         o32 = run_oracle("r2s", y, th0, dict(f, _state_f32=True), NAMES["r2s"], **kw)
