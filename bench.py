@@ -29,6 +29,12 @@ sys.path.insert(0, ROOT)
 
 NITER = 4000
 ALG_BYTES_PER_VOXEL_ITER = 100.0   # 12 echoes x 4 B data + (z, m, v) x 2 params read+write + 4 B TV map
+# compute per voxel-iteration of the standard R2* + TV step, counted from the kernel source:
+# MUFU ops = 12 ex2 (echoes) + 3 x (ex2 + rcp) (sigmoid, twice in the fidelity pass, once for the
+# map) + 2 x (rsqrt + rcp) (Adam); FP32 FLOP (FMA = 2) = 12 x 9 (echoes) + 3 x 8 (sigmoid)
+# + 8 (loss / gradient scaling) + 24 (TV, 3 axes) + 2 x 13 (Adam)
+SFU_OPS_PER_VOXEL_ITER = 22.0
+FP32_FLOP_PER_VOXEL_ITER = 190.0
 METRIC = "askAdam voxel-fits/s & MCMC samples/s, fused vs plain GPU, equal FP64 error"
 
 
@@ -356,6 +362,20 @@ def engine_arm(args, world, rank, local):
                 "avg_launch_ms": avg_launch_ms,
                 "voxel_iterations_per_s": n * epochs_per_launch / (avg_launch_ms / 1000.0),
                 "traffic": profile_traffic(kname)}
+    # the compute roofs of the same launch (the kernel keeps its state on chip, so the HBM figure
+    # is a streaming-equivalent rate): MUFU 16 ops/clk/SM, FP32 128 FMA/clk/SM at the sampled clock
+    vit = roofline["voxel_iterations_per_s"]
+    ghz = (clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0) / 1000.0
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    sfu_peak, fp32_peak = 16 * nsm * ghz * 1e9, 2 * 128 * nsm * ghz * 1e9
+    roofline["compute"] = {"sfu_ops_per_voxel_iter": SFU_OPS_PER_VOXEL_ITER,
+                           "sfu_achieved_per_s": vit * SFU_OPS_PER_VOXEL_ITER, "sfu_peak_per_s": sfu_peak,
+                           "sfu_frac": vit * SFU_OPS_PER_VOXEL_ITER / sfu_peak,
+                           "fp32_flop_per_voxel_iter": FP32_FLOP_PER_VOXEL_ITER,
+                           "fp32_achieved_tflops": vit * FP32_FLOP_PER_VOXEL_ITER / 1e12,
+                           "fp32_peak_tflops": fp32_peak / 1e12,
+                           "fp32_frac": vit * FP32_FLOP_PER_VOXEL_ITER / fp32_peak,
+                           "peak_kind": "nominal per-SM rates x SM count x sampled SM clock"}
     line = {"metric": METRIC, "value": value, "unit": "voxel-fits/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, seed 1002+rank)",
