@@ -19,6 +19,8 @@
 // Reference: utils/askadam.m (model_gradient :23-117, optimisation :121-365,
 // initialise_parameter :368-412, update_parameters :673-691,
 // unscale_parameters :1063-1075), utils/spatial_total_variation.m.
+#include <climits>
+
 #include "gx_internal.h"
 
 namespace gx {
@@ -149,6 +151,8 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
     const float normf = V.norm;
     const double normd = V.normd;
     const size_t slot = (size_t)3 * NP * a.nvtot;
+    // the next checkpoint epoch (a multiple of ckpt_every), kept as a counter
+    int next_ck = a.ckpt_every > 0 ? (e_begin + a.ckpt_every - 1) / a.ckpt_every * a.ckpt_every : INT_MAX;
 
     for (int e = e_begin; e <= e_end; ++e) {
         float th[NP], dth[NP];
@@ -196,14 +200,16 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
                 if (STATS) zp[k] = z[k];
                 opt_update(a, sc, z[k], m1[k], m2[k], gz[k]);
             }
-            if (a.ckpt_every > 0 && (e % a.ckpt_every) == 0 && valid) {
+            if (e == next_ck) {
+                next_ck += a.ckpt_every;
                 float* c = a.ckpt + (size_t)(e / a.ckpt_every) * slot;
+                if (valid)
 #pragma unroll
-                for (int k = 0; k < NP; ++k) {
-                    c[(size_t)k * a.nvtot + v] = z[k];
-                    c[(size_t)(NP + k) * a.nvtot + v] = m1[k];
-                    c[(size_t)(2 * NP + k) * a.nvtot + v] = m2[k];
-                }
+                    for (int k = 0; k < NP; ++k) {
+                        c[(size_t)k * a.nvtot + v] = z[k];
+                        c[(size_t)(NP + k) * a.nvtot + v] = m1[k];
+                        c[(size_t)(2 * NP + k) * a.nvtot + v] = m2[k];
+                    }
             }
         }
     }

@@ -483,9 +483,14 @@ __device__ __forceinline__ void model_r2s(const DevProtocol& P, const float* th,
     float M0 = th[0], R2 = th[1];
     if constexpr (AccMse<Acc>::value) {
         R2sMseSums u;
-        for (int m = 0; m < P.nm; ++m) {
-            const float r = u.echo(P.te[m], P.te_l2e[m], M0, R2, acc.meas(m));
-            if (acc.res) acc.res[m * acc.rs] = acc.mse_scale * r * r;
+        if (acc.res) {
+            for (int m = 0; m < P.nm; ++m) {
+                const float r = u.echo(P.te[m], P.te_l2e[m], M0, R2, acc.meas(m));
+                acc.res[m * acc.rs] = acc.mse_scale * r * r;
+            }
+        } else {
+#pragma unroll 4
+            for (int m = 0; m < P.nm; ++m) u.echo(P.te[m], P.te_l2e[m], M0, R2, acc.meas(m));
         }
         u.store(M0, acc);
     } else {
@@ -524,12 +529,86 @@ __device__ __forceinline__ void model_r2s_unrolled(const DevProtocol& P, int nm,
     }
 }
 
+// R1-R2*/MSE, fused (up to NFA flip angles; exactly NFA when EXACT): exp(-te
+// R2*) once per echo time, shared by the flip angles (2^x with te log2 e, as
+// for R2*), r = (A M0) E2 - y, and per flip angle f the sums sum q and sum
+// te q with q = r E2, so that dS/dM0 = A E2, dS/dR1 = M0 E2 dA/dR1 and dS/dR2*
+// = -te A M0 E2 are applied once per voxel.  Explicit roundings; echo times
+// outer, flip angles inner.  RES: the residual output is written.
+template <int NFA, bool EXACT, bool RES, class Acc>
+__device__ __forceinline__ void r1r2s_mse_sums(const DevProtocol& P, float R2, int nfa, const float (&AM0)[NFA],
+                                               float& sse, float (&Sq)[NFA], float (&Stq)[NFA], Acc& acc) {
+    const int nte = P.n_te;
+#pragma unroll 2
+    for (int t = 0; t < nte; ++t) {
+        const float te = P.te[t];
+        const float E2 = ex2_ftz(mul1(-P.te_l2e[t], R2));
+#pragma unroll
+        for (int f = 0; f < NFA; ++f)
+            if (EXACT || f < nfa) {
+                const int m = t + f * nte;
+                const float r = fma1(AM0[f], E2, -acc.meas(m));
+                sse = fma1(r, r, sse);
+                if (RES) acc.res[m * acc.rs] = acc.mse_scale * r * r;
+                const float q = mul1(r, E2);
+                Sq[f] = add1(Sq[f], q);
+                Stq[f] = fma1(te, q, Stq[f]);
+            }
+    }
+}
+
+template <int NFA, bool EXACT, class Acc>
+__device__ __forceinline__ void r1r2s_mse(const DevProtocol& P, float M0, float R1, float R2, const VoxAux& va,
+                                          Acc& acc) {
+    const float E1 = __expf(-P.tr * R1);
+    const int nfa = EXACT ? NFA : P.n_fa;
+    float A[NFA], dA[NFA], AM0[NFA], Sq[NFA], Stq[NFA];
+#pragma unroll
+    for (int f = 0; f < NFA; ++f) {
+        A[f] = dA[f] = AM0[f] = 0.0f;
+        if (EXACT || f < nfa) {
+            const float sa = va.sa[f * va.fs], ca = va.ca[f * va.fs];
+            const float inv = 1.0f / (1.0f - ca * E1);
+            A[f] = sa * (1.0f - E1) * inv;
+            dA[f] = sa * (ca - 1.0f) * inv * inv * (-P.tr * E1);
+            AM0[f] = mul1(A[f], M0);
+        }
+        Sq[f] = 0.0f;
+        Stq[f] = 0.0f;
+    }
+    float sse = 0.0f;
+    if (acc.res) r1r2s_mse_sums<NFA, EXACT, true>(P, R2, nfa, AM0, sse, Sq, Stq, acc);
+    else r1r2s_mse_sums<NFA, EXACT, false>(P, R2, nfa, AM0, sse, Sq, Stq, acc);
+    float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+#pragma unroll
+    for (int f = 0; f < NFA; ++f)
+        if (EXACT || f < nfa) {
+            g0 = fma1(A[f], Sq[f], g0);
+            g1 = fma1(dA[f], Sq[f], g1);
+            g2 = fma1(A[f], Stq[f], g2);
+        }
+    acc.total = add1(acc.total, sse);
+    acc.g[0] = add1(acc.g[0], g0);
+    acc.g[1] = fma1(M0, g1, acc.g[1]);
+    acc.g[2] = fma1(-M0, g2, acc.g[2]);
+}
+
 // S = M0 sin(a)(1-E1)/(1-cos(a)E1) exp(-TE R2*), E1 = exp(-TR R1), a = b1*FA;
 // measurement index TE fastest then FA (R1R2s/gpuJointR1R2starMapping.m:375-422,513-525)
 template <class Acc>
 __device__ __forceinline__ void model_r1r2s(const DevProtocol& P, const float* th,
                                             const VoxAux& va, Acc& acc) {
     float M0 = th[0], R1 = th[1], R2 = th[2];
+    if constexpr (AccMse<Acc>::value) {
+        if (P.n_fa == 2) {
+            r1r2s_mse<2, true>(P, M0, R1, R2, va, acc);
+            return;
+        }
+        if (P.n_fa <= 4) {
+            r1r2s_mse<4, false>(P, M0, R1, R2, va, acc);
+            return;
+        }
+    }
     float E1 = __expf(-P.tr * R1);
     for (int f = 0; f < P.n_fa; ++f) {
         float sa = va.sa[f * va.fs], ca = va.ca[f * va.fs];
