@@ -657,59 +657,76 @@ __device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const floa
         float q4 = 4.0f * r1 * r2;
         float bDa = b * Da;
         float fd2 = omf * d2;
-        float S0 = 0.f, Sf = 0.f, Sd1 = 0.f, Sd2 = 0.f, Sr1 = 0.f, Sr2 = 0.f;
-        float T0 = 0.f, Tf = 0.f, Td1 = 0.f, Td2 = 0.f, Tr1 = 0.f, Tr2 = 0.f;
-        for (int i = 0; i < nx; ++i) {
-            float x = (float)i * h;
-            float x2 = x * x;
-            float d1 = bDa * x2;
-            float s = base + d1;
-            float Q = fmaf(s, s, q4);
-            float rs = rsqrtf(Q);
-            float l2raw = 0.5f * Q * rs;
-            bool active = l2raw > EPS;
-            float l2 = active ? l2raw : EPS;
-            float inv_l2 = active ? 2.0f * rs : 1.0f / EPS;
-            float l1 = 0.5f * (c1 + d1);
-            float lm = l1 - l2, lp = l1 + l2;
-            float N = fmaf(f, d1, fd2) - lm;
-            float Pp = 0.5f * N * inv_l2;
-            float em = __expf(-lm), ep = __expf(-lp);
-            float M = Pp * ep + (1.0f - Pp) * em;
+        // nodes in pairs (i, i+1) on the two lanes of pair instructions, an
+        // odd node count padded with a node of weight 0; per lane the same
+        // operations as a node at a time, the sums kept per lane and folded
+        // at the end
+        const float2 z2 = make_float2(0.f, 0.f), half = bcast2(0.5f), one = bcast2(1.0f), two = bcast2(2.0f);
+        const float2 bDa2 = bcast2(bDa), base2 = bcast2(base), q42 = bcast2(q4), c12 = bcast2(c1);
+        const float2 f2 = bcast2(f), fd22 = bcast2(fd2), d22 = bcast2(d2), omf2 = bcast2(omf);
+        const float2 r2x4 = bcast2(4.0f * r2), r1x4 = bcast2(4.0f * r1);
+        float2 S0p = z2, Sfp = z2, Sd1p = z2, Sd2p = z2, Sr1p = z2, Sr2p = z2;
+        float2 T0p = z2, Tfp = z2, Td1p = z2, Td2p = z2, Tr1p = z2, Tr2p = z2;
+        for (int i = 0; i < nx; i += 2) {
+            const float2 x = make_float2((float)i * h, (float)(i + 1) * h);
+            const float2 x2 = mul2(x, x);
+            const float2 d1 = mul2(bDa2, x2);
+            const float2 s = add2(base2, d1);
+            const float2 Q = fma2(s, s, q42);
+            const float2 rs = make_float2(rsqrtf(Q.x), rsqrtf(Q.y));
+            const float2 l2raw = mul2(mul2(half, Q), rs);
+            const bool ax = l2raw.x > EPS, ay = l2raw.y > EPS;
+            const float2 l2 = make_float2(ax ? l2raw.x : EPS, ay ? l2raw.y : EPS);
+            const float2 rs2 = mul2(two, rs);
+            const float2 inv_l2 = make_float2(ax ? rs2.x : 1.0f / EPS, ay ? rs2.y : 1.0f / EPS);
+            const float2 l1 = mul2(half, add2(c12, d1));
+            const float2 lm = sub2(l1, l2), lp = add2(l1, l2);
+            const float2 N = sub2(fma2(f2, d1, fd22), lm);
+            const float2 Pp = mul2(mul2(half, N), inv_l2);
+            const float2 em = make_float2(__expf(-lm.x), __expf(-lm.y));
+            const float2 ep = make_float2(__expf(-lp.x), __expf(-lp.y));
+            const float2 omP = sub2(one, Pp);
+            const float2 M = fma2(Pp, ep, mul2(omP, em));
             // reverse sweep with Mbar = 1
-            float Ppb = ep - em;
-            float lpb = -Pp * ep;
-            float lmb = -(1.0f - Pp) * em;
-            float Nb = 0.5f * Ppb * inv_l2;
-            float l2b = -Ppb * Pp * inv_l2;
-            lmb -= Nb;
-            float l1b = lpb + lmb;
-            l2b += lpb - lmb;
-            float Qb = active ? 0.125f * l2b * inv_l2 : 0.0f;
-            float sb = 2.0f * s * Qb;
-            float hl1 = 0.5f * l1b;
-            float fb = Nb * (d1 - d2);
-            float d1b = Nb * f + sb + hl1;
-            float d2b = Nb * omf - sb + hl1;
-            float r1b = 4.0f * r2 * Qb + sb + hl1;
-            float r2b = 4.0f * r1 * Qb - sb + hl1;
-            float wt = (i == 0 || i == nx - 1) ? 0.5f : 1.0f;
-            S0 = fmaf(wt, M, S0);
-            Sf = fmaf(wt, fb, Sf);
-            Sd1 = fmaf(wt * x2, d1b, Sd1);
-            Sd2 = fmaf(wt, d2b, Sd2);
-            Sr1 = fmaf(wt, r1b, Sr1);
-            Sr2 = fmaf(wt, r2b, Sr2);
+            const float2 Ppb = sub2(ep, em);
+            const float2 lpb = mul2(make_float2(-Pp.x, -Pp.y), ep);
+            float2 lmb = mul2(make_float2(-omP.x, -omP.y), em);
+            const float2 Nb = mul2(mul2(half, Ppb), inv_l2);
+            float2 l2b = mul2(mul2(make_float2(-Ppb.x, -Ppb.y), Pp), inv_l2);
+            lmb = sub2(lmb, Nb);
+            const float2 l1b = add2(lpb, lmb);
+            l2b = add2(l2b, sub2(lpb, lmb));
+            const float2 Qbr = mul2(mul2(bcast2(0.125f), l2b), inv_l2);
+            const float2 Qb = make_float2(ax ? Qbr.x : 0.0f, ay ? Qbr.y : 0.0f);
+            const float2 sb = mul2(mul2(two, s), Qb);
+            const float2 hl1 = mul2(half, l1b);
+            const float2 fb = mul2(Nb, sub2(d1, d22));
+            const float2 d1b = add2(add2(mul2(Nb, f2), sb), hl1);
+            const float2 d2b = add2(sub2(mul2(Nb, omf2), sb), hl1);
+            const float2 r1b = add2(add2(mul2(r2x4, Qb), sb), hl1);
+            const float2 r2b = add2(sub2(mul2(r1x4, Qb), sb), hl1);
+            const float2 wt = make_float2((i == 0 || i == nx - 1) ? 0.5f : 1.0f,
+                                          i + 1 >= nx ? 0.0f : (i + 1 == nx - 1 ? 0.5f : 1.0f));
+            S0p = fma2(wt, M, S0p);
+            Sfp = fma2(wt, fb, Sfp);
+            Sd1p = fma2(mul2(wt, x2), d1b, Sd1p);
+            Sd2p = fma2(wt, d2b, Sd2p);
+            Sr1p = fma2(wt, r1b, Sr1p);
+            Sr2p = fma2(wt, r2b, Sr2p);
             if (LMAX2) {
-                float p2w = wt * (1.5f * x2 - 0.5f);
-                T0 = fmaf(p2w, M, T0);
-                Tf = fmaf(p2w, fb, Tf);
-                Td1 = fmaf(p2w * x2, d1b, Td1);
-                Td2 = fmaf(p2w, d2b, Td2);
-                Tr1 = fmaf(p2w, r1b, Tr1);
-                Tr2 = fmaf(p2w, r2b, Tr2);
+                const float2 p2w = mul2(wt, fma2(bcast2(1.5f), x2, bcast2(-0.5f)));
+                T0p = fma2(p2w, M, T0p);
+                Tfp = fma2(p2w, fb, Tfp);
+                Td1p = fma2(mul2(p2w, x2), d1b, Td1p);
+                Td2p = fma2(p2w, d2b, Td2p);
+                Tr1p = fma2(p2w, r1b, Tr1p);
+                Tr2p = fma2(p2w, r2b, Tr2p);
             }
         }
+        const float S0 = S0p.x + S0p.y, Sf = Sfp.x + Sfp.y, Sd1 = Sd1p.x + Sd1p.y, Sd2 = Sd2p.x + Sd2p.y;
+        const float Sr1 = Sr1p.x + Sr1p.y, Sr2 = Sr2p.x + Sr2p.y;
+        const float T0 = T0p.x + T0p.y, Tf = Tfp.x + Tfp.y, Td1 = Td1p.x + Td1p.y, Td2 = Td2p.x + Td2p.y;
+        const float Tr1 = Tr1p.x + Tr1p.y, Tr2 = Tr2p.x + Tr2p.y;
         float r2_f = rice ? (omf > EPS ? r1 / (omf * omf) : r1 / EPS) : r1 / (omf * omf);
         {
             float S = S0 * h;
