@@ -310,7 +310,7 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
             reg += V.tv_scale[r] * cost;
 #pragma unroll
             for (int kk = 0; kk < NP; ++kk)
-                if (kk == k) gth[kk] = __fmaf_rn(V.tv_scale[r], gr, gth[kk]);
+                if (kk == k) gth[kk] = fma1(V.tv_scale[r], gr, gth[kk]);
         }
     }
     float gz[NP];
@@ -707,7 +707,7 @@ __global__ void plain_tv_kernel(AdamParams a, PlainBufs b, const float* grid) {
             tv_terms(c, fv, bv, mb, a.inv_vs, nd, cost, gr);
             reg += V.tv_scale[r] * cost;
             float* gk = b.gth + (size_t)a.reg_param[r] * a.nvtot + v;
-            *gk = __fmaf_rn(V.tv_scale[r], gr, *gk);
+            *gk = fma1(V.tv_scale[r], gr, *gk);
         }
     }
     float q[1] = {reg};

@@ -426,23 +426,21 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const float2 dthr = ld2(s_gf + 2 * S, i0);
             const float2 c = ld2(s_gf + 3 * S, i0);
             const int p0 = s_p[i0], p1 = s_p[i1];
+            const unsigned int fl0 = s_fl[i0], fl1 = s_fl[i1];
+            float f0[3] = {0.f, 0.f, 0.f}, b0[3] = {0.f, 0.f, 0.f}, f1[3] = {0.f, 0.f, 0.f}, b1[3] = {0.f, 0.f, 0.f};
+            if (ok0) nb.load(G, p0, fl0, f0, b0);
+            if (ok1) nb.load(G, p1, fl1, f1, b1);
+            const bool mb0[3] = {(fl0 & 64) != 0, (fl0 & 128) != 0, (fl0 & 256) != 0};
+            const bool mb1[3] = {(fl1 & 64) != 0, (fl1 & 128) != 0, (fl1 & 256) != 0};
+            float2 cost, gt;
+            tv_terms2(c, f0, b0, f1, b1, mb0, mb1, iv, tv3 ? 3 : 2, cost, gt);
             if (ok0) {
-                const unsigned int fl = s_fl[i0];
-                const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
-                float f[3], b[3], cost, gt;
-                nb.load(G, p0, fl, f, b);
-                tv_terms(c.x, f, b, mb, iv, tv3 ? 3 : 2, cost, gt);
-                q1 = __fmaf_rn(tvs0, cost, q1);
-                grf.x = __fmaf_rn(tvs0, gt, grf.x);
+                q1 = __fmaf_rn(tvs0, cost.x, q1);
+                grf.x = fma1(tvs0, gt.x, grf.x);
             }
             if (ok1) {
-                const unsigned int fl = s_fl[i1];
-                const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
-                float f[3], b[3], cost, gt;
-                nb.load(G, p1, fl, f, b);
-                tv_terms(c.y, f, b, mb, iv, tv3 ? 3 : 2, cost, gt);
-                q1 = __fmaf_rn(tvs0, cost, q1);
-                grf.y = __fmaf_rn(tvs0, gt, grf.y);
+                q1 = __fmaf_rn(tvs0, cost.y, q1);
+                grf.y = fma1(tvs0, gt.y, grf.y);
             }
             if (upd) {
                 const float2 gzr = mul2(grf, dthr);
@@ -561,8 +559,8 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
                     const float tvs = r == 0 ? tvs0 : tvs1;
                     reg += tvs * cost;
-                    if (k == 0) gth[0] = __fmaf_rn(tvs, gr, gth[0]);
-                    else gth[1] = __fmaf_rn(tvs, gr, gth[1]);
+                    if (k == 0) gth[0] = fma1(tvs, gr, gth[0]);
+                    else gth[1] = fma1(tvs, gr, gth[1]);
                 }
             }
 #pragma unroll

@@ -840,10 +840,33 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (d < nd) {
-            const float df = f[d] - c;
-            cs = __fadd_rn(cs, fabsf(__fmul_rn(df, iv[d])));
-            const float t = -sgn0(df) + (mb[d] ? sgn0(c - b[d]) : 0.0f);
-            gr = __fadd_rn(gr, __fmul_rn(t, iv[d]));
+            const float df = sub1(f[d], c);
+            cs = add1(cs, fabsf(mul1(df, iv[d])));
+            const float t = -sgn0(df) + (mb[d] ? sgn0(sub1(c, b[d])) : 0.0f);  // small integers: exact
+            gr = add1(gr, mul1(t, iv[d]));
+        }
+    }
+    cost = cs;
+    grad = gr;
+}
+
+// tv_terms for two voxels on the lanes of pair instructions (lane results
+// bit for bit those of tv_terms); mb0 / mb1 as in tv_terms.
+__device__ __forceinline__ void tv_terms2(float2 c, const float (&f0)[3], const float (&b0)[3], const float (&f1)[3],
+                                          const float (&b1)[3], const bool (&mb0)[3], const bool (&mb1)[3],
+                                          const float* iv, int nd, float2& cost, float2& grad) {
+    float2 cs = make_float2(0.0f, 0.0f), gr = cs;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (d < nd) {
+            const float2 ivd = make_float2(iv[d], iv[d]);
+            const float2 df = sub2(make_float2(f0[d], f1[d]), c);
+            const float2 m = mul2(df, ivd);
+            cs = add2(cs, make_float2(fabsf(m.x), fabsf(m.y)));
+            const float2 cb = sub2(c, make_float2(b0[d], b1[d]));
+            const float2 t = make_float2(-sgn0(df.x) + (mb0[d] ? sgn0(cb.x) : 0.0f),
+                                         -sgn0(df.y) + (mb1[d] ? sgn0(cb.y) : 0.0f));
+            gr = add2(gr, mul2(t, ivd));
         }
     }
     cost = cs;
@@ -853,13 +876,19 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
 // Optimiser step of one parameter (adamupdate / sgdmupdate / rmspropupdate,
 // called from utils/askadam.m:673-691).  sc = per-epoch schedule:
 // Adam (lr_e/(1-b1^e), 1/(1-b2^e)); others (lr_e, 0).  The square root is
-// x*rsqrt(x) (exact zero kept) and the Adam quotient a * rcp(b).
+// the approximate one (fast_sqrt0) and the Adam quotient a * rcp(b).
 struct OptConst {
     int optimiser;
     float beta1, beta2, eps, momentum, rms_decay, rms_eps;
 };
 
-__device__ __forceinline__ float fast_sqrt0(float x) { return x > 0.0f ? mul1(x, rsqrtf(x)) : 0.0f; }
+// sqrt(x), x >= 0, by the PTX approximate square root (sqrt.approx,
+// subnormals flushed); the optimisers' second moments are never negative
+__device__ __forceinline__ float fast_sqrt0(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
 // Adam: m1 = b1 m1 + (1-b1) g, m2 = b2 m2 + ((1-b2) g) g,
 // z -= (lr_e m1) / (sqrt(m2 / (1-b2^e)) + eps).
