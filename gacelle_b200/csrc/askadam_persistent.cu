@@ -235,6 +235,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     const int base = blockIdx.x * p.slice;
     const int n = min(base + p.slice, a.nvtot) - base;  // voxels of this slice
     const int S = p.slice;
+    // shared-memory position of slice voxel i: the pair variant stores the
+    // voxel pair (64c + l, 64c + l + 32) of pair q = 32c + l at positions 2q,
+    // 2q + 1, so that a pair is one 8-byte access
+    auto sidx = [](int i) { return PAIR ? (i & ~63) | ((i & 31) << 1) | ((i >> 5) & 1) : i; };
     const DevVol& Vg = a.vols[a.blk_vol[base / p.pad_block]];  // a slice lies in one volume
     struct {
         int off, nvox;
@@ -263,18 +267,19 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const int bw2 = zc > 0 ? pp - sz : pp + wz;
             fl |= (unsigned short)((mk[bw0] ? 64 : 0) | (mk[bw1] ? 128 : 0) | (mk[bw2] ? 256 : 0));
         }
-        s_p[i] = pp;
-        s_fl[i] = fl;
+        const int j = sidx(i);
+        s_p[j] = pp;
+        s_fl[j] = fl;
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             size_t gi = (size_t)k * a.nvtot + base + i;
-            s_st[(0 * NP + k) * S + i] = a.z[gi];
-            s_st[(1 * NP + k) * S + i] = a.m1[gi];
-            s_st[(2 * NP + k) * S + i] = a.m2[gi];
-            if constexpr (STATS) s_st[(3 * NP + k) * S + i] = a.zprev ? a.zprev[gi] : 0.0f;
+            s_st[(0 * NP + k) * S + j] = a.z[gi];
+            s_st[(1 * NP + k) * S + j] = a.m1[gi];
+            s_st[(2 * NP + k) * S + j] = a.m2[gi];
+            if constexpr (STATS) s_st[(3 * NP + k) * S + j] = a.zprev ? a.zprev[gi] : 0.0f;
         }
         if (p.data_in_smem)
-            for (int m = 0; m < a.nm; ++m) s_y[m * S + i] = a.data[(size_t)m * a.nvtot + base + i];
+            for (int m = 0; m < a.nm; ++m) s_y[m * S + j] = a.data[(size_t)m * a.nvtot + base + i];
     }
     __shared__ DevProtocol s_P;
     stage_protocol(a.P, &s_P);
@@ -350,10 +355,12 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const float lbr = a.P.lb[kr], ubr = a.P.ub[kr];
         const size_t half = (size_t)(a.nvtot >> 1);
         const int npair = n >> 1;  // n is a multiple of 64 in pair mode
-        auto ld2 = [](const float* b, int i0) { return make_float2(b[i0], b[i0 + 32]); };
-        auto st2 = [](float* b, int i0, float2 x) {
-            b[i0] = x.x;
-            b[i0 + 32] = x.y;
+        // shared memory: pair q at float2 position q; global: voxels v0, v0+32
+        auto ld2 = [](const float* b, int q) { return reinterpret_cast<const float2*>(b)[q]; };
+        auto st2 = [](float* b, int q, float2 x) { reinterpret_cast<float2*>(b)[q] = x; };
+        auto st2g = [](float* b, int v0, float2 x) {
+            b[v0] = x.x;
+            b[v0 + 32] = x.y;
         };
         // pass 1: data fidelity of the slice (own voxels only)
         for (int q = tid; q < npair; q += NWT) {
@@ -369,14 +376,16 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     y[2 * j + 1] = make_float2(t.z, t.w);
                 }
             } else {
-                const float* yb = p.data_in_smem ? s_y + i0 : a.data + v0;
-                const size_t ys = p.data_in_smem ? (size_t)S : (size_t)a.nvtot;
 #pragma unroll
-                for (int m = 0; m < MAXM; ++m) y[m] = m < nm ? ld2(yb + m * ys, 0) : make_float2(0.f, 0.f);
+                for (int m = 0; m < MAXM; ++m)
+                    y[m] = m >= nm ? make_float2(0.f, 0.f)
+                           : p.data_in_smem ? ld2(s_y + (size_t)m * S, q)
+                                            : make_float2(a.data[(size_t)m * a.nvtot + v0],
+                                                          a.data[(size_t)m * a.nvtot + v0 + 32]);
             }
             float2 th[NP], dth[NP];
 #pragma unroll
-            for (int k = 0; k < NP; ++k) th[k] = unscale_sig2(a.P.lb[k], a.P.ub[k], ld2(s_st + k * S, i0), dth[k]);
+            for (int k = 0; k < NP; ++k) th[k] = unscale_sig2(a.P.lb[k], a.P.ub[k], ld2(s_st + k * S, q), dth[k]);
             // R2sMseSums on both lanes with the residual negated, y - M0 E:
             // every partial sum is the exact negative of the scalar one
             float2 sse = make_float2(0.f, 0.f), g0n = sse, g1n = sse;
@@ -400,10 +409,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             g[1] = mul2(fma2(th[0], g1n, zero), bcast2(s2));
             const float2 nrm = bcast2(V.norm);
             const float2 gr = mul2(kr == 0 ? g[0] : g[1], nrm), gn = mul2(kr == 0 ? g[1] : g[0], nrm);
-            st2(s_gf + 0 * S, i0, mul2(gn, kr == 0 ? dth[1] : dth[0]));
-            st2(s_gf + 1 * S, i0, gr);
-            st2(s_gf + 2 * S, i0, kr == 0 ? dth[0] : dth[1]);
-            st2(s_gf + 3 * S, i0, kr == 0 ? th[0] : th[1]);
+            st2(s_gf + 0 * S, q, mul2(gn, kr == 0 ? dth[1] : dth[0]));
+            st2(s_gf + 1 * S, q, gr);
+            st2(s_gf + 2 * S, q, kr == 0 ? dth[0] : dth[1]);
+            st2(s_gf + 3 * S, q, kr == 0 ? th[0] : th[1]);
             if (ok0) q0 += tot.x;
             if (ok1) q0 += tot.y;
         }
@@ -419,14 +428,16 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const float iv[3] = {ivx, ivy, ivz};
         // pass 2: TV subgradient, chain rule, optimiser, new map values
         for (int q = tid; q < npair; q += NWT) {
-            const int i0 = ((q >> 5) << 6) + (q & 31), i1 = i0 + 32, v0 = base + i0;
+            const int i0 = ((q >> 5) << 6) + (q & 31), v0 = base + i0;
             const bool ok0 = (v0 - V.off) < V.nvox, ok1 = (v0 + 32 - V.off) < V.nvox;
-            const float2 gn = ld2(s_gf + 0 * S, i0);
-            float2 grf = ld2(s_gf + 1 * S, i0);
-            const float2 dthr = ld2(s_gf + 2 * S, i0);
-            const float2 c = ld2(s_gf + 3 * S, i0);
-            const int p0 = s_p[i0], p1 = s_p[i1];
-            const unsigned int fl0 = s_fl[i0], fl1 = s_fl[i1];
+            const float2 gn = ld2(s_gf + 0 * S, q);
+            float2 grf = ld2(s_gf + 1 * S, q);
+            const float2 dthr = ld2(s_gf + 2 * S, q);
+            const float2 c = ld2(s_gf + 3 * S, q);
+            const int2 pp = reinterpret_cast<const int2*>(s_p)[q];
+            const int p0 = pp.x, p1 = pp.y;
+            const unsigned int fl01 = reinterpret_cast<const unsigned int*>(s_fl)[q];
+            const unsigned int fl0 = fl01 & 0xffffu, fl1 = fl01 >> 16;
             float f0[3] = {0.f, 0.f, 0.f}, b0[3] = {0.f, 0.f, 0.f}, f1[3] = {0.f, 0.f, 0.f}, b1[3] = {0.f, 0.f, 0.f};
             if (ok0) nb.load(G, p0, fl0, f0, b0);
             if (ok1) nb.load(G, p1, fl1, f1, b1);
@@ -451,16 +462,16 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     float* pz = s_st + (0 * NP + k) * S;
                     float* p1s = s_st + (1 * NP + k) * S;
                     float* p2s = s_st + (2 * NP + k) * S;
-                    float2 zz = ld2(pz, i0), mm1 = ld2(p1s, i0), mm2 = ld2(p2s, i0);
+                    float2 zz = ld2(pz, q), mm1 = ld2(p1s, q), mm2 = ld2(p2s, q);
                     adam_step2(oc, sc, zz, mm1, mm2, gz[k]);
-                    st2(pz, i0, zz);
-                    st2(p1s, i0, mm1);
-                    st2(p2s, i0, mm2);
+                    st2(pz, q, zz);
+                    st2(p1s, q, mm1);
+                    st2(p2s, q, mm2);
                     if (k == kr) zr = zz;
                     if (ckpt) {  // padding voxels included: never read back
-                        st2(cp + (size_t)k * a.nvtot, v0, zz);
-                        st2(cp + (size_t)(NP + k) * a.nvtot, v0, mm1);
-                        st2(cp + (size_t)(2 * NP + k) * a.nvtot, v0, mm2);
+                        st2g(cp + (size_t)k * a.nvtot, v0, zz);
+                        st2g(cp + (size_t)(NP + k) * a.nvtot, v0, mm1);
+                        st2g(cp + (size_t)(2 * NP + k) * a.nvtot, v0, mm2);
                     }
                 }
                 float2 dd;
@@ -630,11 +641,11 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 float th[NP], dth[NP];
 #pragma unroll
                 for (int k = 0; k < NP; ++k)
-                    th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], s_st[(0 * NP + k) * S + i], dth[k]);
+                    th[k] = unscale(transform, a.P.lb[k], a.P.ub[k], s_st[(0 * NP + k) * S + sidx(i)], dth[k]);
                 PLossAcc<LOSS, NP> acc;
                 acc.total = 0.0f;
                 acc.g[0] = acc.g[1] = 0.0f;
-                acc.y = p.data_in_smem ? s_y + i : a.data + v;
+                acc.y = p.data_in_smem ? s_y + sidx(i) : a.data + v;
                 acc.ys = p.data_in_smem ? S : a.nvtot;
                 acc.w = a.weights ? a.weights + v : nullptr;
                 acc.ws = a.nvtot;
@@ -656,11 +667,12 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             size_t gi = (size_t)k * a.nvtot + v;
-            a.z[gi] = s_st[(0 * NP + k) * S + i];
-            a.m1[gi] = s_st[(1 * NP + k) * S + i];
-            a.m2[gi] = s_st[(2 * NP + k) * S + i];
+            const int j = sidx(i);
+            a.z[gi] = s_st[(0 * NP + k) * S + j];
+            a.m1[gi] = s_st[(1 * NP + k) * S + j];
+            a.m2[gi] = s_st[(2 * NP + k) * S + j];
             if constexpr (STATS)
-                if (a.zprev) a.zprev[gi] = s_st[(3 * NP + k) * S + i];
+                if (a.zprev) a.zprev[gi] = s_st[(3 * NP + k) * S + j];
         }
     }
 }
