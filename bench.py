@@ -31,7 +31,7 @@ NITER = 4000
 ALG_BYTES_PER_VOXEL_ITER = 100.0   # 12 echoes x 4 B data + (z, m, v) x 2 params read+write + 4 B TV map
 # compute per voxel-iteration of the standard R2* + TV step, counted from the kernel source:
 # MUFU ops = 12 ex2 (echoes) + 3 x (ex2 + rcp) (sigmoid, twice in the fidelity pass, once for the
-# map) + 2 x (rsqrt + rcp) (Adam); FP32 FLOP (FMA = 2) = 12 x 9 (echoes) + 3 x 8 (sigmoid)
+# map) + 2 x (sqrt + rcp) (Adam); FP32 FLOP (FMA = 2) = 12 x 9 (echoes) + 3 x 8 (sigmoid)
 # + 8 (loss / gradient scaling) + 24 (TV, 3 axes) + 2 x 13 (Adam)
 SFU_OPS_PER_VOXEL_ITER = 22.0
 FP32_FLOP_PER_VOXEL_ITER = 190.0
