@@ -580,3 +580,63 @@ def test_tv_grid_index_checked_on_device(ctx, bad):
     assert "grid_index" in str(ei.value) and "volume 0" in str(ei.value)
     ok = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
     assert np.all(np.isfinite(ok["final_theta"]))
+
+
+def _fit_batch(ctx, vols, f):
+    """One gx_askadam call over several volumes (y [nm, nv], theta0, dims,
+    grid index each); per volume the final parameters, loss history, final
+    loss and stopping epoch."""
+    import ctypes as C
+    gxm, _ = models("r2s")
+    lb, ub = bounds("r2s")
+    opts = gx_askadam.build_opts(f, NAMES["r2s"], lb, ub, "fused")
+    keep, outs = [], []
+    cv = (_lib.GxVolume * len(vols))()
+    cr = (_lib.GxAskadamResult * len(vols))()
+    for i, (y, th0, dims, gidx) in enumerate(vols):
+        arrs = [np.ascontiguousarray(y, np.float32), np.ascontiguousarray(th0, np.float32),
+                np.ascontiguousarray(gidx, np.int32)]
+        keep += arrs
+        for d in range(3):
+            cv[i].dims[d] = dims[d]
+        cv[i].nvox = y.shape[1]
+        cv[i].data = arrs[0].ctypes.data_as(_lib._fp)
+        cv[i].theta0 = arrs[1].ctypes.data_as(_lib._fp)
+        cv[i].grid_index = arrs[2].ctypes.data_as(_lib._i32p)
+        o = {"final_theta": np.zeros((2, y.shape[1]), np.float32),
+             "loss_history": np.zeros(opts.iteration + 1, np.float64)}
+        cr[i].final_theta = o["final_theta"].ctypes.data_as(_lib._fp)
+        cr[i].loss_history = o["loss_history"].ctypes.data_as(_lib._dp)
+        outs.append(o)
+    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, cv, len(vols), C.byref(opts), cr))
+    for o, r in zip(outs, cr):
+        o["final_loss"], o["final_niteration"] = r.final_loss, r.final_niteration
+    return outs
+
+
+@pytest.mark.parametrize("tv", [False, True])
+def test_batch_of_volumes_equals_separate_fits(ctx, tv):
+    """Volumes fitted together in one call are independent of one another:
+    each gets the parameters, loss history and stopping epoch of a call that
+    fits it alone (the loss is normalised per volume and the TV map of each
+    volume lives on its own grid; batching only packs the work-list, and the
+    per-voxel arithmetic is shared by every kernel path)."""
+    from gacelle_b200 import phantoms, utils
+    vols = []
+    for shape, seed in (((24, 20, 12), 31), ((30, 26, 16), 32)):
+        mask = phantoms.ellipsoid_mask(shape, 1.0)
+        data, _ = phantoms.r2s_phantom(mask, seed)
+        idx = utils.mask_index(mask)
+        y = utils.reshape_ND2GD(data, idx)
+        th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, y.shape[1]))
+        vols.append((y, th0, mask.shape, idx))
+    over = {"lambda": [1e-5], "regmap": ["R2star"], "TVmode": "3D"} if tv else {}
+    f = fitting(iteration=200, initialLearnRate=0.01, **over)
+    both = _fit_batch(ctx, vols, f)
+    for v, b in zip(vols, both):
+        a = _fit_batch(ctx, [v], f)[0]
+        for k in range(2):
+            assert rel_rmse(b["final_theta"][k], a["final_theta"][k]) <= 1e-5, (tv, k)
+        assert a["final_niteration"] == b["final_niteration"]
+        np.testing.assert_allclose(b["loss_history"], a["loss_history"], rtol=1e-6)
+        assert abs(b["final_loss"] - a["final_loss"]) <= 1e-6 * abs(a["final_loss"])
