@@ -243,6 +243,56 @@ class gpuR2starMapping(_ModelBase):
         return out
 
 
+class despot1:
+    """DESPOT1 T1 / M0 from variable-flip-angle spoiled GRE
+    (MCRMWI/private/despot1.m:28-160, the 'regression' solver used by the
+    joint R1-R2* model).  Per voxel, with a = b1 FA: S / sin(a) = E1 S / tan(a)
+    + M0 (1 - E1), E1 = exp(-TR/T1); the two coefficients are the least-squares
+    solution over the flip angles, T1 = -TR / log(E1), M0 = b / (1 - E1)
+    (real parts, as the reference takes them when E1 <= 0)."""
+
+    def __init__(self, tr, fa):
+        self.tr = float(tr)
+        self.fa = np.asarray(fa, dtype=np.float64).ravel()
+
+    def fit(self, S, b1=1.0):
+        """One or many voxels: S [..., nFA] -> (m0, t1), FP64."""
+        S = np.asarray(S, dtype=np.float64)
+        if S.shape[-1] < 2:
+            raise GacelleError(GX_EINVAL, "DESPOT1: only one point to fit")
+        if S.shape[-1] != self.fa.size:
+            raise GacelleError(GX_EINVAL, "DESPOT1: size of signal is not equal to size of flip angle")
+        a = np.deg2rad(self.fa * np.asarray(b1, dtype=np.float64)[..., None])
+        y = S / np.sin(a)
+        x = S / np.tan(a)
+        # normal equations of [x 1] [E1 b]' = y, solved in closed form
+        n = S.shape[-1]
+        sx, sy = x.sum(-1), y.sum(-1)
+        sxx, sxy = (x * x).sum(-1), (x * y).sum(-1)
+        det = n * sxx - sx * sx
+        with np.errstate(divide="ignore", invalid="ignore"):
+            e1 = (n * sxy - sx * sy) / det
+            bb = (sxx * sy - sx * sxy) / det
+            t1 = -self.tr / np.log(e1.astype(np.complex128))
+            m0 = bb / (1 - np.exp(-self.tr / t1))
+        return np.real(m0), np.real(t1)
+
+    def estimate(self, img, mask=None, b1=None):
+        """img [x,y,z,nFA] -> (t1, m0, mask_fitted): voxels whose signals sum
+        to zero get 0; physically infeasible fits (T1 <= 0, M0 < 0, non-finite)
+        are zeroed and left out of mask_fitted."""
+        img = np.abs(np.asarray(img, dtype=np.float64))
+        d3 = img.shape[:3]
+        mask = np.ones(d3, dtype=bool) if mask is None else np.asarray(mask).reshape(d3) > 0
+        b1 = np.ones(d3) if b1 is None else np.asarray(b1, dtype=np.float64).reshape(d3)
+        t1 = np.zeros(d3)
+        m0 = np.zeros(d3)
+        sel = mask & (img.sum(-1) != 0)
+        m0[sel], t1[sel] = self.fit(img[sel], b1[sel])
+        ok = (t1 > 0) & np.isfinite(t1) & (m0 >= 0) & np.isfinite(m0) & mask
+        return np.where(ok, t1, 0.0), np.where(ok, m0, 0.0), ok
+
+
 class gpuJointR1R2starMapping(_ModelBase):
     """Joint R1-R2* mapping from vFA multi-echo GRE (R1R2s/gpuJointR1R2starMapping.m)."""
 
@@ -293,13 +343,71 @@ class gpuJointR1R2starMapping(_ModelBase):
             fitting["ub"] = self.ub[: len(self.modelParams)]
         if not len(fitting["lb"]):
             fitting["lb"] = self.lb[: len(self.modelParams)]
-        if isinstance(fitting["start"], str) and fitting["start"].lower() == "prior":
-            raise GacelleError(GX_EUNSUPPORTED, "start='prior' needs DESPOT1; use 'default' or pars0")
         d3 = utils.dims3(mask)
-        pars0 = utils.initialise_x0(d3, self.modelParams, self.startPoint)
+        if isinstance(fitting["start"], str) and fitting["start"].lower() == "prior":
+            pars0 = self.estimate_prior(data, mask, extraData)
+        else:  # numeric starts are ignored, as determine_x0 does (R1R2s/...:315-317)
+            pars0 = utils.initialise_x0(d3, self.modelParams, self.startPoint)
+        pars0 = {p: np.clip(v, fitting["lb"][k], fitting["ub"][k]).astype(np.float32)
+                 for k, (p, v) in enumerate(pars0.items())}
         if data.ndim == 5:  # [x,y,z,TE,FA] -> [x,y,z,TE*FA] with TE fastest
             data = data.reshape(data.shape[:3] + (-1,), order="F")
         return self._solve(data, mask, None, pars0, fitting, extradata=extraData)
+
+    def _b1(self, extraData, d3):
+        if extraData is not None and "b1" in extraData and extraData["b1"] is not None:
+            return np.asarray(extraData["b1"], dtype=np.float64).reshape(d3)
+        return np.ones(d3)
+
+    def estimate_prior(self, data, mask, extraData=None):
+        """R1R2s/gpuJointR1R2starMapping.m:327-368: R2* from the trapezoid
+        closed form on the flip-angle mean, T1 and M0 from DESPOT1 on the first
+        echo, each clamped to the bounds (non-finite values to the lower
+        bound), and R2* set to R1/2 where it falls below R1."""
+        data = np.asarray(data, dtype=np.float64)
+        d3 = utils.dims3(mask)
+        data = data.reshape(d3 + (self.te.size, self.fa.size), order="F")
+        lb, ub = self.lb, self.ub
+
+        def clamp(v, k):
+            v = np.where(np.isfinite(v), v, lb[k])
+            return np.minimum(np.maximum(v, lb[k]), ub[k])
+
+        r2 = clamp(gpuR2starMapping.R2star_trapezoidal(np.abs(data).mean(axis=4), self.te), 2)
+        t1, m0, _ = despot1(self.tr, self.fa).estimate(np.abs(data[:, :, :, 0, :]), mask, self._b1(extraData, d3))
+        with np.errstate(divide="ignore"):
+            r1 = 1.0 / t1
+        m0, r1 = clamp(m0, 0), clamp(r1, 1)
+        r2 = np.where(r1 > r2, r1 / 2, r2)
+        pars0 = utils.initialise_x0(d3, self.modelParams, self.startPoint)  # noise keeps its start point
+        pars0.update({"M0": m0.astype(np.float32), "R1": r1.astype(np.float32), "R2star": r2.astype(np.float32)})
+        return pars0
+
+    def prepare_data(self, img, mask, extraData=None):
+        """R1R2s/gpuJointR1R2starMapping.m:474-492: the data divided by the
+        98th percentile of the DESPOT1 M0 over the fitted voxels (first echo),
+        then non-finite values zeroed and left out of the mask."""
+        img = np.asarray(img, dtype=np.float64)
+        mask = np.asarray(mask) > 0
+        d3 = utils.dims3(mask)
+        img5 = img.reshape(d3 + (self.te.size, self.fa.size), order="F")
+        _, m0, ok = despot1(self.tr, self.fa).estimate(np.abs(img5[:, :, :, 0, :]), mask, self._b1(extraData, d3))
+        scale = float(np.percentile(m0[ok], 98, method="hazen"))
+        img = img / scale
+        img, bad = utils.set_nan_inf_zero(img)
+        mask = mask & ~np.any(bad.reshape(d3 + (-1,), order="F"), axis=-1)
+        return img, mask, scale
+
+    def estimate(self, data, mask, fitting=None, extraData=None):
+        """R1R2s/gpuJointR1R2starMapping.m:120-194 (one segment): scaled data,
+        fit, M0 scaled back."""
+        fitting = self.check_set_default(fitting)
+        data, mask, scale = self.prepare_data(data, mask, extraData)
+        out = self.fit(data.astype(np.float32), mask, fitting, extraData)
+        for which in ("final", "min", "mean"):
+            if which in out and "M0" in out[which]:
+                out[which]["M0"] = out[which]["M0"] * scale
+        return out
 
 
 class gpuNEXI(_ModelBase):
