@@ -16,6 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib, utils
+from . import dwi as dwi_util
 from ._lib import GacelleError, GX_EINVAL, GX_EUNSUPPORTED
 
 
@@ -424,14 +425,7 @@ class gpuNEXI(_ModelBase):
         b = 0 discarded; unique Delta ascending, then unique b ascending.
         ``nx`` is the powder-average trapezoid size (14 in the reference)."""
         super().__init__()
-        b = np.asarray(b, dtype=np.float64).ravel()
-        D = np.asarray(Delta, dtype=np.float64).ravel()
-        bs, ds = [], []
-        for dv in np.unique(D):
-            bu = np.unique(b[D == dv])
-            bu = bu[bu > 0]
-            bs += list(bu)
-            ds += [dv] * len(bu)
+        bs, _, ds, _ = dwi_util.DWIutility.unique_shell_keepb0(b, None, Delta, None, True)
         self.b = np.array(bs, dtype=np.float32).astype(np.float64)
         self.Delta = np.array(ds, dtype=np.float32).astype(np.float64)
         self.Nav = np.ones(len(self.b)) if Nav is None else np.asarray(Nav, dtype=np.float64).ravel()
@@ -569,6 +563,70 @@ class gpuNEXI(_ModelBase):
             w = np.sqrt(w)
         return w / w.max()
 
+    thres_similarity = 0.1
+    thres_impossible = 0.1
+    thres_bkg = 0.01
+
+    def prepare_dwi_data(self, data, mask, extradata, lmax=0, fitting=None):
+        """NEXI/gpuNEXI.m:480-633 (volumetric data).  A full acquisition
+        (more volumes than shells x (lmax/2+1)) becomes rotationally
+        invariant signals through
+        DWIutility.compute_rotationally_invariant_signal with the little
+        delta left empty and one TE.  The mask then loses voxels whose S_0
+        exceeds 1 + 0.1 in magnitude on any shell, whose first-shell S_0 is
+        below 0.01, whose S_0 decay correlates below 0.1 with the median
+        decay of the voxels that passed the two tests (a flat decay counts as
+        0), or that hold NaN/Inf (set to 0 in the returned data)."""
+        data = np.asarray(data, dtype=np.float64)
+        mask = np.asarray(mask) > 0
+        ex = dict(extradata or {})
+        if fitting is not None and fitting.get("dataType", "volumetric") != "volumetric":
+            raise GacelleError(GX_EUNSUPPORTED, "surface data are not accelerated")
+        nsl = lmax // 2 + 1
+        if data.shape[-1] / nsl > len(self.b):
+            for k in ("bval", "bvec", "BDELTA"):
+                if k not in ex:
+                    raise GacelleError(GX_EINVAL, f"full DWI input needs extradata['{k}']")
+            data = dwi_util.DWIutility().compute_rotationally_invariant_signal(
+                data, ex["bval"], ex["bvec"], None, ex["BDELTA"], None, lmax)[0]
+        elif data.shape[-1] < len(self.b) * nsl:
+            raise GacelleError(GX_EINVAL, f"Input has {data.shape[-1]} volumes but model expects "
+                                          f"{len(self.b) * nsl}. Check lmax or input data.")
+        ns = len(self.b)
+        sl0 = data[..., :ns]
+        with np.errstate(invalid="ignore"):
+            valid = ~np.any(np.abs(sl0) > 1 + self.thres_impossible, axis=-1)
+            valid &= ~(sl0[..., 0] < self.thres_bkg)
+        idx = utils.mask_index(valid)
+        d2 = utils.reshape_ND2GD(sl0, idx)
+        incoherent = np.zeros(valid.shape, dtype=bool)
+        if d2.shape[1] > 0:
+            with np.errstate(invalid="ignore", divide="ignore"):
+                tmpl = np.nanmedian(d2, axis=1)
+                tsd = np.nanstd(tmpl, ddof=1) if np.sum(np.isfinite(tmpl)) > 1 else 0.0
+                tmpl = (tmpl - np.nanmean(tmpl)) / tsd
+                sd = d2.std(axis=0, ddof=1) if ns > 1 else np.zeros(d2.shape[1])
+                xc = tmpl - tmpl.mean()
+                yc = d2 - d2.mean(axis=0)
+                r = (xc @ yc) / np.sqrt((xc @ xc) * np.sum(yc * yc, axis=0))
+            r = np.where(sd < np.finfo(float).eps, 0.0, r)
+            rc = np.zeros(valid.size)
+            rc[idx] = r
+            incoherent = rc.reshape(valid.shape, order="F") < self.thres_similarity
+        valid &= ~incoherent
+        data, bad = utils.set_nan_inf_zero(data)
+        valid &= mask & ~bad.any(axis=-1)
+        return data, valid, ex
+
+    def estimate(self, dwi, mask, extradata=None, fitting=None, pars0=None):
+        """NEXI/gpuNEXI.m:148-252: data preparation, then fit (the engine
+        fits the whole volume in one call, no segmentation)."""
+        fitting = self.check_set_default(fitting)
+        dwi, mask, ex = self.prepare_dwi_data(dwi, mask, extradata, int(fitting["lmax"]), fitting)
+        out = self.fit(dwi.astype(np.float32), mask, fitting, pars0, ex)
+        out["mask"] = mask
+        return out
+
     def fit(self, dwi, mask=None, fitting=None, pars0=None, extradata=None):
         """NEXI/gpuNEXI.m:290-450 (volumetric data)."""
         dwi = np.asarray(dwi)
@@ -666,18 +724,26 @@ class gpuNEXIrice(gpuNEXI):
         dwi = np.asarray(dwi, dtype=np.float64)
         mask = np.asarray(mask) > 0
         ex = dict(extradata)
-        if dwi.shape[-1] / (lmax / 2 + 1) > len(self.b):
-            raise GacelleError(GX_EUNSUPPORTED, "full DWI input (rotational invariants) is not computed by "
-                                                "the engine; pass the Sl0 signal per shell")
-        if dwi.shape[-1] < len(self.b):
-            raise GacelleError(GX_EINVAL, "There are more b-shells in the class object than available in the "
-                                          "input data. Please check your input data.")
         bval = np.asarray(ex.get("bval", np.ones(dwi.shape[-1])), dtype=np.float64).ravel()
         b0 = bval == 0
         dwi_b0 = np.mean(dwi[..., b0], axis=-1) if b0.any() else np.ones(mask.shape)
-        sigma = np.asarray(ex["sigma"], dtype=np.float64) / dwi_b0
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sigma = np.asarray(ex["sigma"], dtype=np.float64) / dwi_b0
         sigma[~np.isfinite(sigma)] = 0.0
         ex["sigma"] = np.maximum(sigma, self.epsilon)
+        if dwi.shape[-1] / (lmax / 2 + 1) > len(self.b):
+            # full acquisition: per-(little delta, big delta) invariants, each
+            # group normalised by its own b = 0 mean (DWIutility.get_Sl_all)
+            for k in ("bval", "bvec", "ldelta", "BDELTA"):
+                if k not in ex:
+                    raise GacelleError(GX_EINVAL, f"full DWI input needs extradata['{k}']")
+            ld = np.asarray(ex["ldelta"], dtype=np.float64).ravel()
+            if ld.size == 1:
+                ex["ldelta"] = np.full(bval.size, float(ld[0]))
+            dwi, _ = dwi_util.DWIutility().get_Sl_all(dwi, bval, ex["bvec"], ex["ldelta"], ex["BDELTA"], lmax)
+        elif dwi.shape[-1] < len(self.b):
+            raise GacelleError(GX_EINVAL, "There are more b-shells in the class object than available in the "
+                                          "input data. Please check your input data.")
         bad = ~np.isfinite(dwi)
         dwi = np.where(bad, 0.0, dwi)
         valid = mask & (dwi.max(axis=-1) <= 1.01) & ~bad.any(axis=-1) & ~(ex["sigma"] > 1)

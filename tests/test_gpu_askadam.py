@@ -489,6 +489,62 @@ def test_gpuNEXIrice_mirror_fit_and_estimate(ctx):
     assert out["final"]["fa"].shape == (6, 10, 1)
 
 
+@pytest.mark.parametrize("rice", [False, True])
+def test_nexi_estimate_from_full_acquisition(ctx, rice):
+    """gpuNEXI / gpuNEXIrice .estimate on a full acquisition (b = 0 volumes
+    and 18 directions per shell) gives exactly the fit of the per-shell
+    signal: the directional signal is isotropic at a float32 value, so its
+    rotational invariant rounds back to that value."""
+    from gacelle_b200 import gpuNEXI, gpuNEXIrice
+    from gacelle_b200.dwi import DWIutility
+    rng = np.random.default_rng(56)
+    dims = (5, 4, 2)
+    n = int(np.prod(dims))
+    bs = [1.0, 2.5, 4.0, 6.0]
+    Ds = [20.0, 35.0]
+    cls = gpuNEXIrice if rice else gpuNEXI
+    m = cls(np.tile(bs, 2), np.repeat(Ds, 4))
+    m.context = ctx
+    th = random_theta("nexi", n, rng)
+    sigma = np.full((1, n), 0.02)
+    pars = {k: th[i][None, :] for i, k in enumerate(["fa", "Da", "De", "ra"])}
+    sl0 = (m.FWD(pars, {"sigma": sigma}) if rice else m.FWD(pars)).astype(np.float32)   # [8, n]
+    sl0_img = sl0.T.reshape(dims + (8,), order="F").astype(np.float64)
+    vols, bval, bvec, BD = [], [], [], []
+    for j, D in enumerate(Ds):
+        vols += [np.full(dims, 2.0)] * 2
+        bval += [0.0, 0.0]
+        bvec += [[0.0, 0.0, 0.0]] * 2
+        BD += [D, D]
+        for i, b in enumerate(bs):
+            g = rng.standard_normal((18, 3))
+            g /= np.linalg.norm(g, axis=1, keepdims=True)
+            vols += [2.0 * sl0_img[..., 4 * j + i]] * 18
+            bval += [b] * 18
+            bvec += list(g)
+            BD += [D] * 18
+    dwi = np.stack(vols, axis=-1)
+    ex = {"bval": np.array(bval), "bvec": np.array(bvec).T, "BDELTA": np.array(BD), "ldelta": 8.0}
+    if rice:
+        ex["sigma"] = np.full(dims, 0.04)   # normalised by the b = 0 mean (2) to the 0.02 above
+    mask = np.ones(dims, dtype=bool)
+    f = {"iteration": 60, "start": "default", "lossFunction": "mse"}
+    full = cls(np.tile(bs, 2), np.repeat(Ds, 4))
+    full.context = ctx
+    if rice:
+        out = full.estimate(dwi, mask, ex, dict(f))
+        ref = m.fit(sl0_img.astype(np.float32), out["mask"], dict(f), {"sigma": np.full(dims, 0.02)})
+    else:
+        out = full.estimate(dwi, mask, ex, dict(f))
+        ref = m.fit(sl0_img.astype(np.float32), out["mask"], dict(f))
+    inv = DWIutility().compute_rotationally_invariant_signal(dwi, ex["bval"], ex["bvec"], None, ex["BDELTA"],
+                                                             None, 0)[0]
+    assert np.array_equal(inv.astype(np.float32), sl0_img.astype(np.float32))
+    assert out["mask"].sum() >= 0.9 * n
+    for p in ["fa", "Da", "De", "ra"]:
+        np.testing.assert_array_equal(out["final"][p], ref["final"][p])
+
+
 # ----------------------------------------------------- robustConvergence ----
 def _robust_engine_vs_oracle(f, n_out, seed):
     import test_oracle
