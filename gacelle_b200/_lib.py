@@ -22,6 +22,7 @@ OPTIMISER = {"adam": 0, "sgdm": 1, "rmsprop": 2}
 TRANSFORM = {"sigmoid": 0, "linear": 1}
 CONV_MODEL = {"ema": 0, "linear": 1}
 PATH = {"fused": 0, "plain": 1}
+REG_TV, REG_PRIOR = 0, 1
 STOP_REASONS = {0: "none", 1: "convergence", 2: "tol", 3: "step", 4: "grad"}
 MEM_HOST, MEM_DEVICE = 0, 1
 
@@ -48,7 +49,8 @@ class GxModel(C.Structure):
 
 class GxVolume(C.Structure):
     _fields_ = [("dims", C.c_int32 * 3), ("nvox", C.c_int32), ("grid_index", _i32p),
-                ("data", _fp), ("weights", _fp), ("theta0", _fp), ("b1", _fp), ("sigma", _fp)]
+                ("data", _fp), ("weights", _fp), ("theta0", _fp), ("b1", _fp), ("sigma", _fp),
+                ("prior_mu", _fp), ("prior_sd", _fp), ("prior_offset", C.c_double)]
 
 
 class GxAskadamOpts(C.Structure):
@@ -69,7 +71,7 @@ class GxAskadamOpts(C.Structure):
                 ("weight_update_interval", C.c_int32), ("outlier_check_window", C.c_int32),
                 ("outlier_min_flag_duration", C.c_int32), ("outlier_voxel_thres", C.c_double),
                 ("outlier_pop_thres", C.c_double), ("outlier_init_thres", C.c_double),
-                ("outlier_init_pop_thres", C.c_double)]
+                ("outlier_init_pop_thres", C.c_double), ("reg_type", C.c_int32)]
 
 
 class GxAskadamResult(C.Structure):

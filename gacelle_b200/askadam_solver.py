@@ -89,11 +89,23 @@ def check_set_default_basic(fitting: dict | None) -> dict:
     return g
 
 
+def _regulariser_of(userfunc):
+    """The regulariser of a two-function ``userFcn`` cell (askadam.model_gradient,
+    utils/askadam.m:58-71): only gpuNEXI.prior_distribution_normal is
+    accelerated; None for the default spatial TV."""
+    if isinstance(userfunc, (list, tuple)) and len(userfunc) > 1:
+        reg = userfunc[1]
+        if getattr(reg, "__name__", "") != "prior_distribution_normal":
+            raise GacelleError(GX_EUNSUPPORTED, "custom regularisation functions other than "
+                                                "prior_distribution_normal are not accelerated")
+        return "prior"
+    return None
+
+
 def _model_of(userfunc):
     """The built-in model object behind ``userfunc`` (object or bound FWD)."""
     if isinstance(userfunc, (list, tuple)):
-        if len(userfunc) > 1:
-            raise GacelleError(GX_EUNSUPPORTED, "custom regularisation functions are not accelerated")
+        _regulariser_of(userfunc)
         userfunc = userfunc[0]
     obj = getattr(userfunc, "__self__", userfunc)
     if not hasattr(obj, "_gx_model"):
@@ -162,6 +174,7 @@ def build_opts(fitting: dict, model_params, lb, ub, path="fused"):
                 raise GacelleError(GX_EINVAL, f"regmap {name} is not a model parameter")
             o.reg_param[i] = list(model_params).index(name)
             o.lambda_[i] = l
+    o.reg_type = _lib.REG_PRIOR if str(f.get("regularisationType", "TV")).lower() == "prior" else _lib.REG_TV
     o.tv_3d = 1 if str(f["TVmode"]).upper() == "3D" else 0
     vs = [float(x) for x in np.atleast_1d(f["voxelSize"])] + [1.0, 1.0, 1.0]
     for i in range(3):
@@ -198,6 +211,14 @@ class askadam:
         """askadam.optimisation (utils/askadam.m:121-365)."""
         model = _model_of(userfuncCell)
         fitting = check_set_default_basic(fitting)
+        prior = None
+        if _regulariser_of(userfuncCell) == "prior":
+            # userInput = {{model inputs}, {mask, lambda, regmap, mu, sigma}} (NEXI/gpuNEXI.m:411-415)
+            _, lam, regmap, mu, sd = varargin[0][1]
+            fitting = dict(fitting, regularisationType="prior", regmap=list(np.atleast_1d(regmap)))
+            fitting["lambda"] = list(np.atleast_1d(lam))
+            prior = (mu, sd)
+            varargin = ()
         mask = np.asarray(mask)
         d3 = utils.dims3(mask)
         idx = utils.mask_index(mask)
@@ -229,10 +250,34 @@ class askadam:
         sig = utils.param_to_GD(ex["sigma"], mask, idx, nv).astype(np.float32) if "sigma" in ex else None
         gidx = idx.astype(np.int32)
         opts = build_opts(fitting, model_params, lb, ub, self.path)
-        res = self._run(gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_)
+        pr = self._prior_maps(prior, fitting, mask, idx, nv) if prior is not None and opts.n_reg > 0 else None
+        res = self._run(gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_, pr)
         return self._to_out(res, model_params, mask, fitting, nm, nv)
 
-    def _run(self, gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_):
+    @staticmethod
+    def _prior_maps(prior, fitting, mask, idx, nv):
+        """mu / SD rows of the regularised parameters at the mask's voxels, and
+        the regulariser's loss from the grid points outside the mask, where the
+        reference's parameter image is 0 (NEXI/gpuNEXI.m:1296-1303)."""
+        mu, sd = prior
+        regmap = list(fitting["regmap"])
+        lam = [float(x) for x in np.atleast_1d(fitting["lambda"])]
+        mus, sds, off = [], [], 0.0
+        outside = np.asarray(mask).ravel(order="F") == 0
+        for name, l in zip(regmap, lam):
+            m = np.asarray(mu[name], dtype=np.float32)
+            s = np.asarray(sd[name], dtype=np.float32)
+            mus.append(utils.param_to_GD(m, mask, idx, nv))
+            sds.append(utils.param_to_GD(s, mask, idx, nv))
+            # a scalar broadcasts over the grid; a [1, Nvox] row has no grid
+            m, s = (np.full(outside.size, x.ravel()[0], np.float32) if x.size == 1 else x for x in (m, s))
+            if m.size == outside.size and s.size == outside.size and outside.any():
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    z = (np.float32(0) - m.ravel(order="F")[outside]) / s.ravel(order="F")[outside]
+                off += l / nv * float(np.sum(np.abs(z[np.isfinite(z)]), dtype=np.float64))
+        return np.stack(mus).astype(np.float32), np.stack(sds).astype(np.float32), off
+
+    def _run(self, gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_, prior=None):
         ctx = self.ctx or _lib.Context.default()
         nv = y.shape[1]
         keep = []
@@ -256,6 +301,10 @@ class askadam:
         vol.theta0 = fp(theta0)
         vol.b1 = fp(b1)
         vol.sigma = fp(sig)
+        if prior is not None:
+            vol.prior_mu = fp(prior[0])
+            vol.prior_sd = fp(prior[1])
+            vol.prior_offset = float(prior[2])
         out = {"final_theta": np.zeros((np_, nv), np.float32), "min_theta": np.zeros((np_, nv), np.float32),
                "final_residual": np.zeros((nm, nv), np.float32), "min_residual": np.zeros((nm, nv), np.float32),
                "final_resloss": np.zeros(nv, np.float32), "min_resloss": np.zeros(nv, np.float32),

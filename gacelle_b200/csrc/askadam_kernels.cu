@@ -68,6 +68,28 @@ __device__ __forceinline__ float voxel_sigma(const AdamParams& a, int v) {
     return a.sigma ? a.sigma[v] : a.sigma_default;
 }
 
+// Add the prior regulariser of voxel v to its physical-parameter gradient g
+// and regularisation loss reg (in regmap order, like the TV terms).
+template <int NP>
+__device__ __forceinline__ void prior_voxel(const AdamParams& a, const DevVol& V, int v, const float (&th)[NP],
+                                            float (&g)[NP], float& reg) {
+    for (int r = 0; r < a.n_reg; ++r) {
+        const int k = a.reg_param[r];
+        const size_t i = (size_t)r * a.nvtot + v;
+        float t = 0.0f;
+#pragma unroll
+        for (int kk = 0; kk < NP; ++kk)
+            if (kk == k) t = th[kk];
+        float cost, gr;
+        prior_terms(t, a.prior_mu[i], a.prior_sd[i], cost, gr);
+        reg = fma1(V.tv_scale[r], cost, reg);
+#pragma unroll
+        for (int kk = 0; kk < NP; ++kk)
+            if (kk == k) g[kk] = fma1(V.tv_scale[r], gr, g[kk]);
+    }
+    if (v == V.off) reg = add1(reg, V.prior_off);
+}
+
 // ---------------------------------------------------------------------------
 // State initialisation (initialise_parameter, utils/askadam.m:368-412).
 // ---------------------------------------------------------------------------
@@ -170,8 +192,18 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
         model_eval<MODEL>(s_P, th, va, acc);
         acc.finish();
         float gz[NP];
+        float reg = 0.0f;
+        if (a.prior_mu) {  // prior regulariser (the host records it through STATS)
+            float gth[NP];
 #pragma unroll
-        for (int k = 0; k < NP; ++k) gz[k] = acc.g[k] * normf * dth[k];
+            for (int k = 0; k < NP; ++k) gth[k] = acc.g[k] * normf;
+            if (valid) prior_voxel<NP>(a, V, v, th, gth, reg);
+#pragma unroll
+            for (int k = 0; k < NP; ++k) gz[k] = gth[k] * dth[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < NP; ++k) gz[k] = acc.g[k] * normf * dth[k];
+        }
         if (record) {
             float q[NQ];
             q[0] = valid ? acc.total : 0.0f;
@@ -183,7 +215,7 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
                     z2 += z[k] * z[k];
                     d2 += (z[k] - zp[k]) * (z[k] - zp[k]);
                 }
-                q[NQ > 1 ? 1 : 0] = 0.0f;
+                q[NQ > 1 ? 1 : 0] = reg;
                 if (NQ > 4) {
                     q[2] = valid ? g2 : 0.f;
                     q[3] = valid ? z2 : 0.f;
@@ -714,6 +746,29 @@ __global__ void plain_tv_kernel(AdamParams a, PlainBufs b, const float* grid) {
     block_accumulate<1>(q, b.acc + 1, 1.0, s_red, 0);
 }
 
+// Prior regulariser of the op-by-op path: gth += its gradient, acc[1] += its loss.
+__global__ void plain_prior_kernel(AdamParams a, PlainBufs b) {
+    __shared__ double s_red[2 * 32];
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevVol& V = a.vols[a.blk_vol[blockIdx.x]];
+    bool valid = v < a.nvtot && (v - V.off) < V.nvox;
+    float reg = 0.0f;
+    if (valid) {
+        for (int r = 0; r < a.n_reg; ++r) {
+            const int k = a.reg_param[r];
+            const size_t i = (size_t)r * a.nvtot + v;
+            float cost, gr;
+            prior_terms(b.theta[(size_t)k * a.nvtot + v], a.prior_mu[i], a.prior_sd[i], cost, gr);
+            reg = fma1(V.tv_scale[r], cost, reg);
+            float* gk = b.gth + (size_t)k * a.nvtot + v;
+            *gk = fma1(V.tv_scale[r], gr, *gk);
+        }
+        if (v == V.off) reg = add1(reg, V.prior_off);
+    }
+    float q[1] = {reg};
+    block_accumulate<1>(q, b.acc + 1, 1.0, s_red, 0);
+}
+
 template <bool STATS>
 __global__ void plain_zgrad_kernel(AdamParams a, PlainBufs b) {
     __shared__ double s_red[2 * 32 * 3];
@@ -954,6 +1009,12 @@ cudaError_t launch_plain_tv(const AdamParams& a, const PlainBufs& b, float* grid
     plain_scatter_kernel<<<nblocks, block, 0, s>>>(a, b, grid);
     plain_tv_kernel<<<nblocks, block, 0, s>>>(a, b, grid);
     g_kernel_launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_prior(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s) {
+    plain_prior_kernel<<<nblocks, block, 0, s>>>(a, b);
+    ++g_kernel_launches;
     return cudaGetLastError();
 }
 

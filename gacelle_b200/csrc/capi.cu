@@ -59,7 +59,7 @@ enum Slot {
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
-    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_NSLOTS
+    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_NSLOTS
 };
 
 struct gx_context {
@@ -398,7 +398,13 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
                                   o->convergence_window < 1))
         return fail(GX_EINVAL, "robustConvergence needs weightUpdateInterval, outlierCheckWindow and "
                                "convergenceWindow >= 1");
-    bool tv = o->n_reg > 0 && o->lambda[0] > 0;
+    if (o->reg_type != GX_REG_TV && o->reg_type != GX_REG_PRIOR)
+        return fail(GX_EINVAL, "unknown regularisation type %d", o->reg_type);
+    const bool reg = o->n_reg > 0 && o->lambda[0] > 0;
+    const bool prior = reg && o->reg_type == GX_REG_PRIOR;
+    const bool tv = reg && !prior;
+    if (prior && o->robust_convergence)
+        return fail(GX_EUNSUPPORTED, "robustConvergence with the prior regulariser");
     if (tv)
         for (int d = 0; d < (o->tv_3d ? 3 : 2); ++d)
             if (!(o->voxel_size[d] > 0)) return fail(GX_EINVAL, "voxel_size must be positive");
@@ -410,6 +416,8 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
         const gx_volume& v = vols[i];
         if (v.nvox < 1) return fail(GX_EINVAL, "volume %d: nvox must be >= 1", i);
         if (!v.data) return fail(GX_EINVAL, "volume %d: data is NULL", i);
+        if (prior && (!v.prior_mu || !v.prior_sd))
+            return fail(GX_EINVAL, "volume %d: the prior regulariser needs prior_mu and prior_sd", i);
         if (tv) {
             if (!v.grid_index) return fail(GX_EINVAL, "volume %d: TV needs grid_index", i);
             long long g = (long long)v.dims[0] * v.dims[1] * v.dims[2];
@@ -455,6 +463,7 @@ struct AdamJob {
     int np, nm, id;
     int B;
     bool tv, stats, want_min, want_res_f, want_res_m;
+    bool prior = false;                   // prior-distribution regulariser (instead of TV)
     std::vector<DevVol> hv;
     std::vector<int> hblk;
     int nvtot = 0, nblocks = 0;
@@ -481,7 +490,8 @@ static gx_status adam_setup(AdamJob& J) {
     int N = o->iteration;
     J.B = o->block_size > 0 ? o->block_size : 128;
     if (J.B % 32 || J.B < 32 || J.B > 1024) return fail(GX_EINVAL, "block_size must be a multiple of 32 in [32,1024]");
-    J.tv = o->n_reg > 0 && o->lambda[0] > 0;
+    J.prior = o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == GX_REG_PRIOR;
+    J.tv = o->n_reg > 0 && o->lambda[0] > 0 && !J.prior;
     J.stats = o->step_tol > 0 || o->grad_tol > 0;
     // work-list layout
     J.hv.resize(J.nvol);
@@ -499,6 +509,7 @@ static gx_status adam_setup(AdamJob& J) {
         for (int q = 0; q < 3; ++q) d.dims[q] = J.tv ? v.dims[q] : (q == 0 ? v.nvox : 1);
         d.grid_off = goff;
         for (int r = 0; r < o->n_reg && r < kMaxReg; ++r) d.tv_scale[r] = (float)(o->lambda[r] / (double)v.nvox);
+        d.prior_off = J.prior ? (float)v.prior_offset : 0.0f;
         if (J.tv) goff += (long long)v.dims[0] * v.dims[1] * v.dims[2];
         for (int b = 0; b < d.npad / J.B; ++b) J.hblk.push_back(i);
         off += d.npad;
@@ -522,7 +533,7 @@ static gx_status adam_setup(AdamJob& J) {
     a.mse_scale = (float)o->mse_scale;
     a.huber_delta = (float)o->huber_delta;
     a.sigma_default = (float)o->sigma;
-    a.n_reg = J.tv ? o->n_reg : 0;
+    a.n_reg = (J.tv || J.prior) ? o->n_reg : 0;
     for (int r = 0; r < a.n_reg; ++r) a.reg_param[r] = o->reg_param[r];
     a.tv_3d = o->tv_3d;
     for (int d = 0; d < 3; ++d) a.inv_vs[d] = o->voxel_size[d] > 0 ? (float)(1.0 / o->voxel_size[d]) : 0.0f;
@@ -577,12 +588,27 @@ static gx_status adam_setup(AdamJob& J) {
         }
         if (anyth0 && v.theta0) TRY(upload_rows(c, th0, nv, d.off, v.theta0, J.np, v.nvox, J.mem, &J.h2d));
     }
+    if (J.prior) {
+        // mean and SD maps of the regularised parameters; padding voxels get 0 / 0
+        float *mu, *sd;
+        TRY(wsT(c, S_PRIOR_MU, (size_t)o->n_reg * nv, &mu));
+        TRY(wsT(c, S_PRIOR_SD, (size_t)o->n_reg * nv, &sd));
+        CK(cudaMemsetAsync(mu, 0, sizeof(float) * o->n_reg * nv, c->stream));
+        CK(cudaMemsetAsync(sd, 0, sizeof(float) * o->n_reg * nv, c->stream));
+        for (int i = 0; i < J.nvol; ++i) {
+            const gx_volume& v = J.vols[i];
+            TRY(upload_rows(c, mu, nv, J.hv[i].off, v.prior_mu, o->n_reg, v.nvox, J.mem, &J.h2d));
+            TRY(upload_rows(c, sd, nv, J.hv[i].off, v.prior_sd, o->n_reg, v.nvox, J.mem, &J.h2d));
+        }
+        a.prior_mu = mu;
+        a.prior_sd = sd;
+    }
     a.data = data; a.weights = w; a.b1 = b1; a.sigma = sig;
     if (J.trace) J.trace->mark("upload");
     TRY(wsT(c, S_Z, (size_t)J.np * nv, &a.z));
     TRY(wsT(c, S_M1, (size_t)J.np * nv, &a.m1));
     TRY(wsT(c, S_M2, (size_t)J.np * nv, &a.m2));
-    if (J.stats) TRY(wsT(c, S_ZP, (size_t)J.np * nv, &a.zprev));
+    if (J.stats || J.prior) TRY(wsT(c, S_ZP, (size_t)J.np * nv, &a.zprev));
     int* blk;
     DevVol* dvols;
     TRY(wsT(c, S_BLK, J.hblk.size(), &blk));
@@ -705,6 +731,7 @@ static gx_status make_view(AdamJob& J, int i, const AdamParams& base, View* out)
     if (a.zprev) a.zprev += o;
     if (a.ckpt) a.ckpt += o;
     if (a.gidx) a.gidx += o;
+    if (a.prior_mu) { a.prior_mu += o; a.prior_sd += o; }
     a.blk_vol += d.off / J.B;
     a.vols = J.local_vols;
     out->a = a;
@@ -720,7 +747,9 @@ static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e
     a.res_out = res_out;
     if (!record) a.hist = nullptr;
     if (!J.tv) {
-        CK(launch_fused(a, J.id, J.o->loss, J.stats && record, e0, e1, update_last, record, J.B, nblocks, c->stream));
+        // the prior's loss is recorded in the statistics columns of the history
+        CK(launch_fused(a, J.id, J.o->loss, (J.stats || J.prior) && record, e0, e1, update_last, record, J.B,
+                        nblocks, c->stream));
         return GX_OK;
     }
     if (persistent_ok && J.use_persist) {
@@ -1011,8 +1040,9 @@ static gx_status adam_plain(AdamJob& J, AdamOut& out) {
             CK(launch_plain_loss(a, o->loss, b, J.B, V.nblocks, c->stream));
             CK(launch_plain_adjoint(a, J.id, b, J.B, V.nblocks, c->stream));
             if (J.tv) CK(launch_plain_tv(a, b, J.grid[0], J.B, V.nblocks, c->stream));
+            if (J.prior) CK(launch_plain_prior(a, b, J.B, V.nblocks, c->stream));
             CK(launch_plain_zgrad(a, b, J.stats, J.B, V.nblocks, c->stream));
-            n_main += J.tv ? 7 : 5;
+            n_main += J.tv ? 7 : (J.prior ? 6 : 5);
             if (robust && e >= 1) {
                 // perVoxelLossInit is the starting point's evaluation, equal to epoch 1's
                 if (e == 1) CK(launch_robust_seed(a, b, RW, J.B, V.nblocks, c->stream));
@@ -1203,6 +1233,7 @@ extern "C" gx_status gx_model_gradient(gx_context* c, const gx_model* model, int
     CK(launch_plain_loss(a, opts->loss, b, J.B, J.nblocks, c->stream));
     CK(launch_plain_adjoint(a, J.id, b, J.B, J.nblocks, c->stream));
     if (J.tv) CK(launch_plain_tv(a, b, J.grid[0], J.B, J.nblocks, c->stream));
+    if (J.prior) CK(launch_plain_prior(a, b, J.B, J.nblocks, c->stream));
     double acc[8];
     CK(cudaMemcpyAsync(acc, b.acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
     TRY(download_rows(c, gtheta, b.gth, J.nvtot, 0, J.np, vol->nvox, mem, &J.d2h));

@@ -850,6 +850,16 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
     grad = gr;
 }
 
+// Prior-distribution regulariser of one parameter (gpuNEXI.prior_distribution_normal,
+// NEXI/gpuNEXI.m:1256-1307): z = (theta - mu) / sd; a finite z adds |z| to the
+// cost and sgn(z) / sd to d cost / d theta, a non-finite one nothing.
+__device__ __forceinline__ void prior_terms(float th, float mu, float sd, float& cost, float& grad) {
+    const float z = __fdiv_rn(sub1(th, mu), sd);
+    const bool ok = isfinite(z);
+    cost = ok ? fabsf(z) : 0.0f;
+    grad = ok ? __fdiv_rn(sgn0(z), sd) : 0.0f;
+}
+
 // tv_terms for two voxels on the lanes of pair instructions (lane results
 // bit for bit those of tv_terms); mb0 / mb1 as in tv_terms.
 __device__ __forceinline__ void tv_terms2(float2 c, const float (&f0)[3], const float (&b0)[3], const float (&f1)[3],

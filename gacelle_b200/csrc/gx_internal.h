@@ -23,7 +23,8 @@ struct DevVol {
     double normd;
     int dims[3];        // TV grid
     long long grid_off; // offset of the volume's grid in the TV grid buffers
-    float tv_scale[kMaxReg];  // lambda_k / Nmask (spatial_total_variation.m:40)
+    float tv_scale[kMaxReg];  // lambda_k / Nmask (spatial_total_variation.m:40; also the prior's)
+    float prior_off;    // prior regulariser loss of the grid points outside the mask
 };
 
 // Parameters shared by the askAdam kernels (passed by value).
@@ -58,6 +59,9 @@ struct AdamParams {
     const float* grid_cur;        // [n_reg][grid total]
     float* grid_next;
     long long grid_total;
+    // prior-distribution regulariser (instead of TV): [n_reg][nvtot], or nullptr
+    const float* prior_mu;
+    const float* prior_sd;
 };
 
 // Kernel launchers (askadam_kernels.cu).  Return cudaError_t of the launch.
@@ -122,6 +126,7 @@ cudaError_t launch_plain_adjoint(const AdamParams& a, int model, const PlainBufs
                                  int nblocks, cudaStream_t s);
 cudaError_t launch_plain_tv(const AdamParams& a, const PlainBufs& b, float* grid, int block,
                             int nblocks, cudaStream_t s);
+cudaError_t launch_plain_prior(const AdamParams& a, const PlainBufs& b, int block, int nblocks, cudaStream_t s);
 cudaError_t launch_plain_zgrad(const AdamParams& a, const PlainBufs& b, bool stats, int block,
                                int nblocks, cudaStream_t s);
 cudaError_t launch_plain_update(const AdamParams& a, const PlainBufs& b, int e, int block,

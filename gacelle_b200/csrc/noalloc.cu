@@ -79,7 +79,7 @@ extern "C" gx_status gx_askadam_noalloc(const gx_model* model, const float* data
     if (o->iteration < 0) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: iteration must be >= 0");
     if (!o->lb || !o->ub) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: lb/ub are required");
     if (o->n_reg > 0 && o->lambda[0] > 0)
-        return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: TV regularisation needs gx_askadam");
+        return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: regularisation (TV or prior) needs gx_askadam");
     if (o->path != GX_PATH_FUSED) return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: fused path only");
     if (internal_can_stop(o))
         return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: runs every iteration; disable the stopping "

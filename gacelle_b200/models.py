@@ -641,9 +641,20 @@ class gpuNEXI(_ModelBase):
             fitting["lb"] = self.lb[: len(self.modelParams)]
         if fitting.get("dataType", "volumetric") != "volumetric":
             raise GacelleError(GX_EUNSUPPORTED, "surface data are not accelerated")
-        if fitting["solver"] == "askadam" and str(fitting.get("regularisationType", "TV")).lower() == "prior" \
-                and np.atleast_1d(fitting["lambda"])[0] > 0:
-            raise GacelleError(GX_EUNSUPPORTED, "prior-distribution regularisation is not accelerated")
+        prior = fitting["solver"] == "askadam" and str(fitting.get("regularisationType", "TV")).lower() == "prior" \
+            and np.atleast_1d(fitting["lambda"])[0] > 0
+        if prior:
+            # NEXI/gpuNEXI.m:382-410: mu / sigma structs with a field per regmap name
+            ex = extradata or {}
+            if not isinstance(ex.get("mu"), dict) or not isinstance(ex.get("sigma"), dict):
+                raise GacelleError(GX_EINVAL, "fitting.regularisationType is 'prior' and fitting.lambda > 0, but "
+                                              "extradata.mu/extradata.sigma were not provided to fit().")
+            miss_mu = [r for r in fitting["regmap"] if r not in ex["mu"]]
+            miss_sd = [r for r in fitting["regmap"] if r not in ex["sigma"]]
+            if miss_mu or miss_sd:
+                raise GacelleError(GX_EINVAL, "extradata.mu/extradata.sigma must have a field for every name in "
+                                              f"fitting.regmap. Missing from mu: {{{', '.join(miss_mu)}}}. "
+                                              f"Missing from sigma: {{{', '.join(miss_sd)}}}.")
         wv = self.compute_optimisation_weights(mask, fitting["lossFunction"], fitting["lmax"])
         if pars0 is None:
             start = fitting["start"]
@@ -659,7 +670,37 @@ class gpuNEXI(_ModelBase):
         w = None
         if not np.all(wv == 1):
             w = np.broadcast_to(wv, utils.dims3(mask) + (wv.size,)).copy()
+        if prior:
+            from .askadam_solver import askadam
+            ex = extradata or {}
+            userFcn = [self.FWD, self.prior_distribution_normal]
+            userInput = [[fitting["lmax"], fitting["solver"]],
+                         [mask, fitting["lambda"], fitting["regmap"], ex["mu"], ex["sigma"]]]
+            return askadam(self.context, fitting.get("path", "fused")).optimisation(
+                dwi, mask, w, pars0, fitting, userFcn, userInput)
         return self._solve(dwi, mask, w, pars0, fitting, extradata=extradata)
+
+    @staticmethod
+    def prior_distribution_normal(parameters, mask, lambda_, regmap, mu, sigma):
+        """gpuNEXI.prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307): the
+        regularisation loss sum_r lambda_r / Nmask * sum |(theta_r - mu_r) /
+        sigma_r| over the grid's finite z-scores, theta_r being the parameter
+        image (0 outside the mask).  As a userFcn entry it selects the
+        engine's prior regulariser; called directly it evaluates the loss of
+        [1, Nvox] parameter rows on the host."""
+        lam = [float(x) for x in np.atleast_1d(lambda_)]
+        if not lam or lam[0] <= 0:
+            return 0.0
+        mask = np.asarray(mask)
+        nmask = int(np.count_nonzero(mask))
+        loss = 0.0
+        for name, l in zip(np.atleast_1d(regmap), lam):
+            th = utils.reshape_GD2ND(np.asarray(parameters[name], dtype=np.float32).reshape(1, -1), mask)
+            th = th.reshape(mask.shape, order="F")
+            with np.errstate(divide="ignore", invalid="ignore"):
+                z = (th - np.asarray(mu[name], dtype=np.float32)) / np.asarray(sigma[name], dtype=np.float32)
+            loss += float(np.sum(np.abs(z[np.isfinite(z)]), dtype=np.float64)) / nmask * l
+        return loss
 
 
 class gpuNEXIrice(gpuNEXI):

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define GX_ABI_VERSION 4
+#define GX_ABI_VERSION 5
 
 typedef enum {
     GX_OK = 0,
@@ -89,6 +89,9 @@ typedef enum {
 typedef enum { GX_MCMC_MH = 0, GX_MCMC_ENSEMBLE = 1 } gx_mcmc_algorithm;
 typedef enum { GX_GW_SIMULTANEOUS = 0, GX_GW_REDBLACK = 1 } gx_gw_update;
 typedef enum { GX_MEM_HOST = 0, GX_MEM_DEVICE = 1 } gx_memory;
+/* fitting.regularisationType: the spatial TV of utils/spatial_total_variation.m,
+ * or gpuNEXI.prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307) */
+typedef enum { GX_REG_TV = 0, GX_REG_PRIOR = 1 } gx_reg_type;
 
 typedef struct gx_context gx_context;
 
@@ -117,6 +120,15 @@ typedef struct {
     const float* theta0;        /* [nparam][nvox] starting point, physical units, or NULL */
     const float* b1;            /* R1R2*: [nvox] B1 scaling of the flip angle, or NULL (= 1) */
     const float* sigma;         /* GAUSS/RICIAN loss: [nvox] noise sigma, or NULL (= opts sigma) */
+    /* GX_REG_PRIOR: mean and SD of each regmap parameter, [n_reg][nvox] in
+     * regmap order (required then, ignored otherwise).  The regulariser adds
+     * lambda_r / nvox * |(theta - mu) / sd| over the voxels whose z-score is
+     * finite, plus prior_offset: the part of the reference's loss from grid
+     * points outside the mask, where the parameter image is 0 (a constant
+     * with no gradient; 0 when the caller has no grid). */
+    const float* prior_mu;
+    const float* prior_sd;
+    double prior_offset;
 } gx_volume;
 
 /* askAdam options: the `fitting` struct after askadam.check_set_default_basic
@@ -143,7 +155,7 @@ typedef struct {
     int32_t convergence_model;  /* gx_conv_model */
     double ema_decay;
     double step_tol, grad_tol, patience_step, patience_grad;
-    int32_t n_reg;              /* regularised parameters (TV) */
+    int32_t n_reg;              /* regularised parameters (TV or prior, per reg_type) */
     int32_t reg_param[8];       /* parameter index of each regmap entry */
     double lambda[8];
     int32_t tv_3d;              /* 0 = '2D', 1 = '3D' */
@@ -166,6 +178,7 @@ typedef struct {
     double outlier_weight;
     int32_t weight_update_interval, outlier_check_window, outlier_min_flag_duration;
     double outlier_voxel_thres, outlier_pop_thres, outlier_init_thres, outlier_init_pop_thres;
+    int32_t reg_type;           /* gx_reg_type of the n_reg / reg_param / lambda entries */
 } gx_askadam_opts;
 
 /* Per-volume askAdam output (out.final / out.min of utils/askadam.m:345-362).

@@ -53,13 +53,13 @@ class OrcAdamOpts(C.Structure):
                 ("outlier_weight", C.c_double), ("weight_update_interval", C.c_int),
                 ("outlier_check_window", C.c_int), ("outlier_voxel_thres", C.c_double),
                 ("outlier_pop_thres", C.c_double), ("outlier_init_thres", C.c_double),
-                ("outlier_init_pop_thres", C.c_double)]
+                ("outlier_init_pop_thres", C.c_double), ("reg_type", C.c_int)]
 
 
 class OrcVolume(C.Structure):
     _fields_ = [("dims", C.c_int * 3), ("nvox", C.c_int), ("grid_index", _ip),
                 ("data", _dp), ("weights", _dp), ("theta0", _dp), ("b1", _dp), ("sigma", _dp),
-                ("norm_nvox", C.c_double)]
+                ("norm_nvox", C.c_double), ("prior_mu", _dp), ("prior_sd", _dp), ("prior_offset", C.c_double)]
 
 
 class OrcAdamResult(C.Structure):
@@ -277,7 +277,7 @@ class Volume:
     """One masked volume in the oracle's SoA layout: arrays are [k][nvox]."""
 
     def __init__(self, data, dims=None, grid_index=None, weights=None, theta0=None, b1=None,
-                 sigma=None, norm_nvox=0.0):
+                 sigma=None, norm_nvox=0.0, prior_mu=None, prior_sd=None, prior_offset=0.0):
         self.data = _f64(data)
         nv = self.data.shape[1]
         self.grid_index = None if grid_index is None else np.ascontiguousarray(grid_index, np.int32)
@@ -290,6 +290,11 @@ class Volume:
                            None if self.grid_index is None else self.grid_index.ctypes.data_as(_ip),
                            _d(self.data), _d(self.weights), _d(self.theta0), _d(self.b1),
                            _d(self.sigma), float(norm_nvox))
+        self.prior_mu = _f64(prior_mu)
+        self.prior_sd = _f64(prior_sd)
+        self.s.prior_mu = _d(self.prior_mu)
+        self.s.prior_sd = _d(self.prior_sd)
+        self.s.prior_offset = float(prior_offset)
 
     @property
     def nvox(self):
@@ -347,6 +352,7 @@ def adam_opts(lb, ub, fitting: dict):
     for i, (k, l) in enumerate(zip(reg, lam)):
         o.reg_param[i] = k
         o.lambda_[i] = l
+    o.reg_type = 1 if str(f.get("regularisationType", "TV")).lower() == "prior" else 0
     o.tv_3d = 1 if str(f.get("TVmode", "2D")).upper() == "3D" else 0
     vs = list(f.get("voxelSize", [2, 2, 2])) + [1.0] * 3
     for i in range(3):

@@ -601,7 +601,26 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
     free(lfv);
     fid *= c->norm;
     double reg = 0.0;
-    if (o->n_reg > 0 && o->lambda[0] > 0) { /* spatial_total_variation.m:29 */
+    if (o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == 1) {
+        /* prior_distribution_normal (NEXI/gpuNEXI.m:1296-1303): lambda / Nmask *
+         * sum |(theta - mu) / sigma| over the finite z-scores; the gradient of a
+         * finite one is lambda / Nmask * sgn(z) / sigma */
+        double nmask = (double)nv;
+        for (int r = 0; r < o->n_reg; ++r) {
+            int k = o->reg_param[r];
+            double sr = 0.0;
+            for (int v = 0; v < nv; ++v) {
+                double sd = vol->prior_sd[(size_t)r * nv + v];
+                double zs = (theta[(size_t)k * nv + v] - vol->prior_mu[(size_t)r * nv + v]) / sd;
+                if (!isfinite(zs)) continue;
+                sr += fabs(zs);
+                double sg = zs > 0 ? 1.0 : (zs < 0 ? -1.0 : 0.0);
+                gth[(size_t)k * nv + v] += o->lambda[r] / nmask * sg / sd;
+            }
+            reg += sr / nmask * o->lambda[r];
+        }
+        reg += vol->prior_offset;
+    } else if (o->n_reg > 0 && o->lambda[0] > 0) { /* spatial_total_variation.m:29 */
         double nmask = (double)nv;
         for (int r = 0; r < o->n_reg; ++r) {
             int k = o->reg_param[r];
@@ -634,7 +653,9 @@ static int setup_ctx(adam_ctx* c, const orc_model* m, const orc_volume* vol,
     c->norm = 1.0 / ((double)c->nm * nn);
     c->mask = NULL; c->grid = NULL; c->grid_g = NULL; c->ngrid = 0;
     c->wmod = NULL; c->vloss = NULL;
-    if (o->n_reg > 0 && o->lambda[0] > 0) {
+    if (o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == 1) {
+        if (!vol->prior_mu || !vol->prior_sd) return -1;
+    } else if (o->n_reg > 0 && o->lambda[0] > 0) {
         if (!vol->grid_index) return -1;
         c->ngrid = (size_t)vol->dims[0] * vol->dims[1] * vol->dims[2];
         c->mask = (unsigned char*)calloc(c->ngrid, 1);

@@ -112,6 +112,7 @@ typedef struct {
     double outlier_weight;
     int weight_update_interval, outlier_check_window;
     double outlier_voxel_thres, outlier_pop_thres, outlier_init_thres, outlier_init_pop_thres;
+    int reg_type;                /* 0: spatial TV; 1: prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307) */
 } orc_adam_opts;
 
 typedef struct {
@@ -124,6 +125,9 @@ typedef struct {
     const double* b1;            /* [nvox] or NULL */
     const double* sigma;         /* [nvox] or NULL */
     double norm_nvox;            /* voxel count used by the mean; 0 -> nvox */
+    const double* prior_mu;      /* [n_reg][nvox] prior mean (reg_type 1) */
+    const double* prior_sd;      /* [n_reg][nvox] prior SD */
+    double prior_offset;         /* prior loss of the grid points outside the mask */
 } orc_volume;
 
 typedef struct {

@@ -89,7 +89,7 @@ def reg_fields(f, names):
 
 
 def run_engine(kind, y, theta0, f, names, path="fused", dims=None, gidx=None, b1=None, sigma=None,
-               weights=None, context=None, **model_kw):
+               weights=None, context=None, prior=None, **model_kw):
     gxm, _ = models(kind, **model_kw)
     lb, ub = bounds(kind)
     opts = gx_askadam.build_opts(f, names, lb, ub, path)
@@ -98,13 +98,14 @@ def run_engine(kind, y, theta0, f, names, path="fused", dims=None, gidx=None, b1
     d3 = dims if dims is not None else (nv, 1, 1)
     g = gidx if gidx is not None else np.arange(nv, dtype=np.int32)
     solver = gx_askadam.askadam(context, path)
-    res = solver._run(gxm, y, weights, theta0, b1, sigma, g, d3, opts, nm, len(names))
+    res = solver._run(gxm, y, weights, theta0, b1, sigma, g, d3, opts, nm, len(names), prior)
     res["timing"] = solver.last_timing
     return res
 
 
 def run_oracle(kind, y, theta0, f, names, dims=None, gidx=None, b1=None, sigma=None, weights=None,
-               norm_nvox=0.0, **model_kw):
+               norm_nvox=0.0, prior=None, **model_kw):
+    """prior: (mu [n_reg][nvox], sd [n_reg][nvox], offset) of the prior regulariser."""
     _, om = models(kind, **model_kw)
     f = reg_fields(dict(f), names)
     o = _oracle_opts(kind, f)
@@ -115,7 +116,10 @@ def run_oracle(kind, y, theta0, f, names, dims=None, gidx=None, b1=None, sigma=N
                         theta0=None if theta0 is None else np.asarray(theta0, np.float64),
                         b1=None if b1 is None else np.asarray(b1, np.float64),
                         sigma=None if sigma is None else np.asarray(sigma, np.float64),
-                        norm_nvox=norm_nvox)
+                        norm_nvox=norm_nvox,
+                        prior_mu=None if prior is None else np.asarray(prior[0], np.float64),
+                        prior_sd=None if prior is None else np.asarray(prior[1], np.float64),
+                        prior_offset=0.0 if prior is None else float(prior[2]))
     return oracle.askadam(om, vol, o, want_residual=True)
 
 

@@ -291,6 +291,78 @@ def test_oracle_gradient_of_mean_normalisation():
     np.testing.assert_allclose(g2[:, :10], g1 / 2, rtol=1e-12)
 
 
+def _prior_problem(nv=50, seed=12):
+    """An R2* problem with a prior on both parameters; some SDs are 0 (an
+    infinite z-score) and one voxel sits on its mean with SD 0 (NaN): both
+    drop out of the regulariser."""
+    rng = np.random.default_rng(seed)
+    th = _theta("r2s", nv, rng)
+    y = oracle.forward(oracle.r2s(TE), th) + 0.01 * rng.standard_normal((12, nv))
+    mu = np.vstack([rng.uniform(0.8, 1.2, nv), rng.uniform(20, 40, nv)])
+    sd = np.vstack([rng.uniform(0.05, 0.2, nv), rng.uniform(2, 8, nv)])
+    sd[0, 3] = 0.0
+    sd[1, 7] = 0.0
+    th_eval = th * rng.uniform(0.9, 1.1, th.shape)
+    th_eval[1, 9] = mu[1, 9]
+    sd[1, 9] = 0.0
+    return y, th_eval, mu, sd
+
+
+def test_prior_regulariser_matches_autograd():
+    """prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307) in the oracle's
+    model_gradient against torch autograd of fidelity + lambda/N sum|z|."""
+    y, th, mu, sd = _prior_problem()
+    nv = y.shape[1]
+    lam = [2e-3, 5e-4]
+    f = _fitting(**{"lambda": lam, "regmap": ["M0", "R2star"], "regularisationType": "prior"})
+    f["_reg_index"], f["_reg_lambda"] = [0, 1], lam
+    o = oracle.adam_opts([0.0, 0.1], [2.0, 200.0], f)
+    vol = oracle.Volume(y, prior_mu=mu, prior_sd=sd, prior_offset=0.125)
+    L, g, _, fid, reg = oracle.model_gradient(oracle.r2s(TE), vol, o, th)
+    t = torch.tensor(th, requires_grad=True)
+    loss_fid = torch.mean(0.5 * (T.r2s_fwd(t, TE) - torch.tensor(y)) ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ok = torch.tensor(np.isfinite((th - mu) / sd))
+    # the dropped entries contribute no gradient (autodiff through the 0 SD
+    # itself would give 0/0 there)
+    sds = torch.tensor(np.where(sd == 0, 1.0, sd))
+    z = (t - torch.tensor(mu)) / sds
+    loss_reg = sum(lam[r] / nv * torch.sum(torch.abs(z[r][ok[r]])) for r in range(2)) + 0.125
+    (loss_fid + loss_reg).backward()
+    assert reg == pytest.approx(loss_reg.item(), rel=1e-13)
+    assert fid == pytest.approx(loss_fid.item(), rel=1e-12)
+    np.testing.assert_allclose(g, t.grad.numpy(), rtol=1e-10, atol=1e-16)
+    assert np.isfinite(g).all()
+
+
+def test_prior_host_loss_and_grid_offset():
+    """gpuNEXI.prior_distribution_normal on the host equals the oracle's
+    regulariser once the solver's offset for the grid points outside the
+    mask (parameter image 0 there) is added."""
+    from gacelle_b200 import gpuNEXI, utils
+    from gacelle_b200.askadam_solver import askadam
+    rng = np.random.default_rng(13)
+    shape = (5, 4, 3)
+    mask = rng.random(shape) > 0.4
+    idx = utils.mask_index(mask)
+    nv = idx.size
+    fa = rng.uniform(0.2, 0.8, nv)
+    mu = {"fa": rng.uniform(0.3, 0.7, shape).astype(np.float32)}
+    sd = {"fa": rng.uniform(0.05, 0.2, shape).astype(np.float32)}
+    sd["fa"][0, 0, 0] = 0.0
+    host = gpuNEXI.prior_distribution_normal({"fa": fa[None, :]}, mask, [0.01], ["fa"], mu, sd)
+    fitting = {"lambda": [0.01], "regmap": ["fa"]}
+    m_rows, s_rows, off = askadam._prior_maps((mu, sd), fitting, mask, idx, nv)
+    f = _fitting(**{"lambda": [0.01], "regmap": ["fa"], "regularisationType": "prior"})
+    f["_reg_index"], f["_reg_lambda"] = [0], [0.01]
+    om = oracle.nexi(np.array([1.0, 2.0]), np.array([20.0, 20.0]))
+    th = np.vstack([fa.astype(np.float32), np.full(nv, 2.0), np.full(nv, 1.0), np.full(nv, 0.1)])
+    vol = oracle.Volume(np.zeros((2, nv)), prior_mu=m_rows, prior_sd=s_rows, prior_offset=off)
+    _, _, _, _, reg = oracle.model_gradient(om, vol, oracle.adam_opts([0, 0, 0, 0.004], [1, 3, 3, 1], f), th)
+    assert off > 0
+    assert reg == pytest.approx(host, rel=1e-6)   # float32 z-scores on the host
+
+
 # ------------------------------------------------------------------ MCMC ----
 def test_partner_is_uniform_derangement():
     counts = np.zeros((8, 8))
