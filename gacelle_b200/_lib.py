@@ -22,7 +22,7 @@ OPTIMISER = {"adam": 0, "sgdm": 1, "rmsprop": 2}
 TRANSFORM = {"sigmoid": 0, "linear": 1}
 CONV_MODEL = {"ema": 0, "linear": 1}
 PATH = {"fused": 0, "plain": 1}
-REG_TV, REG_PRIOR = 0, 1
+REG_TV, REG_PRIOR, REG_SURFACE_TV = 0, 1, 2
 STOP_REASONS = {0: "none", 1: "convergence", 2: "tol", 3: "step", 4: "grad"}
 MEM_HOST, MEM_DEVICE = 0, 1
 
@@ -50,7 +50,8 @@ class GxModel(C.Structure):
 class GxVolume(C.Structure):
     _fields_ = [("dims", C.c_int32 * 3), ("nvox", C.c_int32), ("grid_index", _i32p),
                 ("data", _fp), ("weights", _fp), ("theta0", _fp), ("b1", _fp), ("sigma", _fp),
-                ("prior_mu", _fp), ("prior_sd", _fp), ("prior_offset", C.c_double)]
+                ("prior_mu", _fp), ("prior_sd", _fp), ("prior_offset", C.c_double),
+                ("max_neighbours", C.c_int32), ("neighbours", _i32p), ("edge_length", _fp)]
 
 
 class GxAskadamOpts(C.Structure):

@@ -94,11 +94,14 @@ def _regulariser_of(userfunc):
     utils/askadam.m:58-71): only gpuNEXI.prior_distribution_normal is
     accelerated; None for the default spatial TV."""
     if isinstance(userfunc, (list, tuple)) and len(userfunc) > 1:
-        reg = userfunc[1]
-        if getattr(reg, "__name__", "") != "prior_distribution_normal":
-            raise GacelleError(GX_EUNSUPPORTED, "custom regularisation functions other than "
-                                                "prior_distribution_normal are not accelerated")
-        return "prior"
+        name = getattr(userfunc[1], "__name__", "")
+        if name == "prior_distribution_normal":
+            return "prior"
+        if name == "surface_total_variation":
+            return "surface"
+        raise GacelleError(GX_EUNSUPPORTED, "custom regularisation functions other than "
+                                            "prior_distribution_normal and surface_total_variation are not "
+                                            "accelerated")
     return None
 
 
@@ -174,7 +177,12 @@ def build_opts(fitting: dict, model_params, lb, ub, path="fused"):
                 raise GacelleError(GX_EINVAL, f"regmap {name} is not a model parameter")
             o.reg_param[i] = list(model_params).index(name)
             o.lambda_[i] = l
-    o.reg_type = _lib.REG_PRIOR if str(f.get("regularisationType", "TV")).lower() == "prior" else _lib.REG_TV
+    if str(f.get("regularisationType", "TV")).lower() == "prior":
+        o.reg_type = _lib.REG_PRIOR
+    elif str(f.get("dataType", "volumetric")).lower() == "surface":
+        o.reg_type = _lib.REG_SURFACE_TV
+    else:
+        o.reg_type = _lib.REG_TV
     o.tv_3d = 1 if str(f["TVmode"]).upper() == "3D" else 0
     vs = [float(x) for x in np.atleast_1d(f["voxelSize"])] + [1.0, 1.0, 1.0]
     for i in range(3):
@@ -211,13 +219,21 @@ class askadam:
         """askadam.optimisation (utils/askadam.m:121-365)."""
         model = _model_of(userfuncCell)
         fitting = check_set_default_basic(fitting)
-        prior = None
-        if _regulariser_of(userfuncCell) == "prior":
+        prior = surface = None
+        reg_kind = _regulariser_of(userfuncCell)
+        if reg_kind == "prior":
             # userInput = {{model inputs}, {mask, lambda, regmap, mu, sigma}} (NEXI/gpuNEXI.m:411-415)
             _, lam, regmap, mu, sd = varargin[0][1]
             fitting = dict(fitting, regularisationType="prior", regmap=list(np.atleast_1d(regmap)))
             fitting["lambda"] = list(np.atleast_1d(lam))
             prior = (mu, sd)
+            varargin = ()
+        elif reg_kind == "surface":
+            # userInput = {{model inputs}, {mask, neighbours, lambda, regmap, edgeLength}} (NEXI/gpuNEXI.m:430-432)
+            _, nbrs, lam, regmap, elen = varargin[0][1]
+            fitting = dict(fitting, regularisationType="TV", dataType="surface", regmap=list(np.atleast_1d(regmap)))
+            fitting["lambda"] = list(np.atleast_1d(lam))
+            surface = (nbrs, elen)
             varargin = ()
         mask = np.asarray(mask)
         d3 = utils.dims3(mask)
@@ -251,7 +267,8 @@ class askadam:
         gidx = idx.astype(np.int32)
         opts = build_opts(fitting, model_params, lb, ub, self.path)
         pr = self._prior_maps(prior, fitting, mask, idx, nv) if prior is not None and opts.n_reg > 0 else None
-        res = self._run(gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_, pr)
+        sf = self._surface_tables(surface, mask, idx) if surface is not None and opts.n_reg > 0 else None
+        res = self._run(gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_, pr, sf)
         return self._to_out(res, model_params, mask, fitting, nm, nv)
 
     @staticmethod
@@ -277,7 +294,26 @@ class askadam:
                 off += l / nv * float(np.sum(np.abs(z[np.isfinite(z)]), dtype=np.float64))
         return np.stack(mus).astype(np.float32), np.stack(sds).astype(np.float32), off
 
-    def _run(self, gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_, prior=None):
+    @staticmethod
+    def _surface_tables(surface, mask, idx):
+        """Neighbour grid indices and edge lengths, [maxNeighbours][Nvox], of
+        the masked vertices from the reference's [1, Nvertex, Nhemi,
+        maxNeighbours] arrays of 1-based per-hemisphere vertex indices
+        (utils.get_surface_neighbours; NEXI/gpuNEXI.m:1224-1229 makes them
+        global with a hemisphere offset)."""
+        nbrs, elen = surface
+        nbrs = np.asarray(nbrs)
+        elen = np.asarray(elen, dtype=np.float32)
+        d3 = utils.dims3(mask)
+        nvert = d3[1]
+        maxnb = nbrs.shape[3] if nbrs.ndim == 4 else 1
+        nb = nbrs.reshape((-1, maxnb), order="F").astype(np.int64)
+        hemi = np.arange(nb.shape[0]) // (d3[0] * nvert)
+        glob = (nb - 1) + (hemi * nvert)[:, None]
+        ln = elen.reshape((-1, maxnb), order="F")
+        return (np.ascontiguousarray(glob[idx].T, dtype=np.int32), np.ascontiguousarray(ln[idx].T))
+
+    def _run(self, gxm, y, w, theta0, b1, sig, gidx, d3, opts, nm, np_, prior=None, surface=None):
         ctx = self.ctx or _lib.Context.default()
         nv = y.shape[1]
         keep = []
@@ -305,6 +341,12 @@ class askadam:
             vol.prior_mu = fp(prior[0])
             vol.prior_sd = fp(prior[1])
             vol.prior_offset = float(prior[2])
+        if surface is not None:
+            nbt = np.ascontiguousarray(surface[0], dtype=np.int32)
+            keep.append(nbt)
+            vol.max_neighbours = nbt.shape[0]
+            vol.neighbours = nbt.ctypes.data_as(_lib._i32p)
+            vol.edge_length = fp(surface[1])
         out = {"final_theta": np.zeros((np_, nv), np.float32), "min_theta": np.zeros((np_, nv), np.float32),
                "final_residual": np.zeros((nm, nv), np.float32), "min_residual": np.zeros((nm, nv), np.float32),
                "final_resloss": np.zeros(nv, np.float32), "min_resloss": np.zeros(nv, np.float32),

@@ -313,7 +313,23 @@ __global__ void tv_step_kernel(AdamParams a, int e, int update, int record, int 
     for (int k = 0; k < NP; ++k) gth[k] = acc.g[k] * V.norm;
 
     float reg = 0.0f;
-    if (valid) {
+    if (valid && a.surf_nb) {
+        const unsigned char* mk = a.maskgrid + V.grid_off;
+        for (int r = 0; r < a.n_reg; ++r) {
+            const int k = a.reg_param[r];
+            const float* G = a.grid_cur + (size_t)r * a.grid_total + V.grid_off;
+            float c = 0.0f;
+#pragma unroll
+            for (int kk = 0; kk < NP; ++kk)
+                if (kk == k) c = th[kk];
+            float cost, gr;
+            surf_tv_terms(c, G, mk, a.surf_nb + v, a.surf_len + v, a.surf_maxnb, a.nvtot, cost, gr);
+            reg += V.tv_scale[r] * cost;
+#pragma unroll
+            for (int kk = 0; kk < NP; ++kk)
+                if (kk == k) gth[kk] = fma1(V.tv_scale[r], gr, gth[kk]);
+        }
+    } else if (valid) {
         const int dx = V.dims[0], dy = V.dims[1], dz = V.dims[2];
         const int p = a.gidx[v];
         const int x = p % dx, yz = p / dx, y = yz % dy, zc = yz / dy;
@@ -424,6 +440,14 @@ __global__ void tv_mask_kernel(AdamParams a, unsigned char* mask, int* err, int*
         atomicOr(err, 1);
         atomicMin(bad_vol, vol);
         return;
+    }
+    for (int j = 0; a.surf_nb && j < a.surf_maxnb; ++j) {
+        const int nb = a.surf_nb[(size_t)j * a.nvtot + v];
+        if (nb < 0 || nb >= gsz) {
+            atomicOr(err, 4);
+            atomicMin(bad_vol, vol);
+            return;
+        }
     }
     const size_t q = (size_t)V.grid_off + (size_t)p;
     unsigned int* w = reinterpret_cast<unsigned int*>(mask + (q & ~(size_t)3));
@@ -715,7 +739,18 @@ __global__ void plain_tv_kernel(AdamParams a, PlainBufs b, const float* grid) {
     const DevVol& V = a.vols[a.blk_vol[blockIdx.x]];
     bool valid = v < a.nvtot && (v - V.off) < V.nvox;
     float reg = 0.0f;
-    if (valid) {
+    if (valid && a.surf_nb) {
+        const unsigned char* mk = a.maskgrid + V.grid_off;
+        const int p = a.gidx[v];
+        for (int r = 0; r < a.n_reg; ++r) {
+            const float* G = grid + (size_t)r * a.grid_total + V.grid_off;
+            float cost, gr;
+            surf_tv_terms(G[p], G, mk, a.surf_nb + v, a.surf_len + v, a.surf_maxnb, a.nvtot, cost, gr);
+            reg += V.tv_scale[r] * cost;
+            float* gk = b.gth + (size_t)a.reg_param[r] * a.nvtot + v;
+            *gk = fma1(V.tv_scale[r], gr, *gk);
+        }
+    } else if (valid) {
         const int dx = V.dims[0], dy = V.dims[1], dz = V.dims[2];
         const int p = a.gidx[v];
         const int x = p % dx, yz = p / dx, y = yz % dy, zc = yz / dy;

@@ -59,7 +59,7 @@ enum Slot {
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
-    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_NSLOTS
+    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_SURF_NB, S_SURF_LEN, S_NSLOTS
 };
 
 struct gx_context {
@@ -398,11 +398,12 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
                                   o->convergence_window < 1))
         return fail(GX_EINVAL, "robustConvergence needs weightUpdateInterval, outlierCheckWindow and "
                                "convergenceWindow >= 1");
-    if (o->reg_type != GX_REG_TV && o->reg_type != GX_REG_PRIOR)
+    if (o->reg_type != GX_REG_TV && o->reg_type != GX_REG_PRIOR && o->reg_type != GX_REG_SURFACE_TV)
         return fail(GX_EINVAL, "unknown regularisation type %d", o->reg_type);
     const bool reg = o->n_reg > 0 && o->lambda[0] > 0;
     const bool prior = reg && o->reg_type == GX_REG_PRIOR;
-    const bool tv = reg && !prior;
+    const bool surf = reg && o->reg_type == GX_REG_SURFACE_TV;
+    const bool tv = reg && !prior && !surf;
     if (prior && o->robust_convergence)
         return fail(GX_EUNSUPPORTED, "robustConvergence with the prior regulariser");
     if (tv)
@@ -418,7 +419,10 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
         if (!v.data) return fail(GX_EINVAL, "volume %d: data is NULL", i);
         if (prior && (!v.prior_mu || !v.prior_sd))
             return fail(GX_EINVAL, "volume %d: the prior regulariser needs prior_mu and prior_sd", i);
-        if (tv) {
+        if (surf && (!v.neighbours || !v.edge_length || v.max_neighbours < 1 || v.max_neighbours > 64))
+            return fail(GX_EINVAL, "volume %d: surface TV needs neighbours, edge_length and max_neighbours "
+                                   "in [1, 64]", i);
+        if (tv || surf) {
             if (!v.grid_index) return fail(GX_EINVAL, "volume %d: TV needs grid_index", i);
             long long g = (long long)v.dims[0] * v.dims[1] * v.dims[2];
             if (v.dims[0] < 1 || v.dims[1] < 1 || v.dims[2] < 1 || g < v.nvox || g > (1LL << 31) - 1)
@@ -464,6 +468,7 @@ struct AdamJob {
     int B;
     bool tv, stats, want_min, want_res_f, want_res_m;
     bool prior = false;                   // prior-distribution regulariser (instead of TV)
+    bool surf = false;                    // surface TV: TV grids with mesh neighbour tables
     std::vector<DevVol> hv;
     std::vector<int> hblk;
     int nvtot = 0, nblocks = 0;
@@ -484,6 +489,47 @@ struct AdamJob {
 
 static double sched_pow(double b, int e) { return std::pow(b, (double)e); }
 
+// Mesh neighbour tables of the surface TV, [maxnb][nvtot] in the work-list
+// layout; a volume with fewer slots than the widest repeats its own grid
+// index (a zero difference) with length 1 in the extra rows.
+static gx_status upload_surface(AdamJob& J, int* gidx) {
+    gx_context* c = J.c;
+    int maxnb = 0;
+    for (int i = 0; i < J.nvol; ++i) maxnb = std::max(maxnb, (int)J.vols[i].max_neighbours);
+    const size_t nv = J.nvtot;
+    int* nb;
+    float* len;
+    TRY(wsT(c, S_SURF_NB, (size_t)maxnb * nv, &nb));
+    TRY(wsT(c, S_SURF_LEN, (size_t)maxnb * nv, &len));
+    CK(cudaMemsetAsync(nb, 0, sizeof(int) * maxnb * nv, c->stream));
+    CK(cudaMemsetAsync(len, 0, sizeof(float) * maxnb * nv, c->stream));
+    const cudaMemcpyKind kind = copy_kind_host(J.mem) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int i = 0; i < J.nvol; ++i) {
+        const gx_volume& v = J.vols[i];
+        const size_t off = J.hv[i].off;
+        for (int j = 0; j < maxnb; ++j) {
+            if (j < v.max_neighbours) {
+                CK(cudaMemcpyAsync(nb + j * nv + off, v.neighbours + (size_t)j * v.nvox, sizeof(int32_t) * v.nvox,
+                                   kind, c->stream));
+                TRY(upload_rows(c, len + j * nv, nv, off, v.edge_length + (size_t)j * v.nvox, 1, v.nvox, J.mem,
+                                &J.h2d));
+                if (J.mem == GX_MEM_HOST) J.h2d += sizeof(int32_t) * v.nvox;
+            } else {
+                CK(cudaMemcpyAsync(nb + j * nv + off, gidx + off, sizeof(int) * v.nvox, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+                std::vector<float> ones((size_t)v.nvox, 1.0f);
+                CK(cudaMemcpyAsync(len + j * nv + off, ones.data(), sizeof(float) * v.nvox, cudaMemcpyHostToDevice,
+                                   c->stream));
+                CK(cudaStreamSynchronize(c->stream));
+            }
+        }
+    }
+    J.a.surf_nb = nb;
+    J.a.surf_len = len;
+    J.a.surf_maxnb = maxnb;
+    return GX_OK;
+}
+
 static gx_status adam_setup(AdamJob& J) {
     gx_context* c = J.c;
     const gx_askadam_opts* o = J.o;
@@ -491,7 +537,8 @@ static gx_status adam_setup(AdamJob& J) {
     J.B = o->block_size > 0 ? o->block_size : 128;
     if (J.B % 32 || J.B < 32 || J.B > 1024) return fail(GX_EINVAL, "block_size must be a multiple of 32 in [32,1024]");
     J.prior = o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == GX_REG_PRIOR;
-    J.tv = o->n_reg > 0 && o->lambda[0] > 0 && !J.prior;
+    J.surf = o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == GX_REG_SURFACE_TV;
+    J.tv = o->n_reg > 0 && o->lambda[0] > 0 && !J.prior;   // grid TV or surface TV
     J.stats = o->step_tol > 0 || o->grad_tol > 0;
     // work-list layout
     J.hv.resize(J.nvol);
@@ -682,6 +729,7 @@ static gx_status adam_setup(AdamJob& J) {
         }
         a.gidx = gidx;
         a.maskgrid = mk;
+        if (J.surf) TRY(upload_surface(J, gidx));
         // mask grid and index checks on the device
         int* flags;
         TRY(wsT(c, S_FLAGS, 2, &flags));
@@ -693,6 +741,7 @@ static gx_status adam_setup(AdamJob& J) {
         CK(cudaStreamSynchronize(c->stream));
         if (hf[0] & 1) return fail(GX_EINVAL, "volume %d: grid_index out of range", hf[1]);
         if (hf[0] & 2) return fail(GX_EINVAL, "volume %d: duplicate grid_index", hf[1]);
+        if (hf[0] & 4) return fail(GX_EINVAL, "volume %d: mesh neighbour index out of range", hf[1]);
         a.grid_cur = g0;
         a.grid_next = g1;
         J.grid[0] = g0;
@@ -732,6 +781,7 @@ static gx_status make_view(AdamJob& J, int i, const AdamParams& base, View* out)
     if (a.ckpt) a.ckpt += o;
     if (a.gidx) a.gidx += o;
     if (a.prior_mu) { a.prior_mu += o; a.prior_sd += o; }
+    if (a.surf_nb) { a.surf_nb += o; a.surf_len += o; }
     a.blk_vol += d.off / J.B;
     a.vols = J.local_vols;
     out->a = a;
@@ -843,7 +893,8 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
         bool want = !(env && strcmp(env, "step") == 0);
         std::vector<int> npad(J.nvol);
         for (int i = 0; i < J.nvol; ++i) npad[i] = J.hv[i].npad;
-        J.use_persist = want && plan_persistent(J.a, J.id, o->loss, J.stats, J.B, npad.data(), J.nvol, &J.plan);
+        J.use_persist = want && !J.surf &&
+                        plan_persistent(J.a, J.id, o->loss, J.stats, J.B, npad.data(), J.nvol, &J.plan);
         if (J.use_persist) TRY(wsT(c, S_BAR, 1, &J.barrier));
         if (J.use_persist && J.plan.quad_width > 0) {
             TRY(wsT(c, S_DATA_QUADS, (size_t)J.nvtot * (J.plan.quad_width / 4), &J.data_quads));

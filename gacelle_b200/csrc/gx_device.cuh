@@ -850,6 +850,29 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
     grad = gr;
 }
 
+// Surface TV of one vertex (gpuNEXI.surface_total_variation, NEXI/gpuNEXI.m:
+// 1165-1254): its cost sum_j |q_j|, q_j = (theta_v - theta_nb_j) / len_j over
+// the neighbour slots j (G: the parameter on the vertex grid, 0 off the mask;
+// a non-finite q_j is dropped), and the derivative of the whole regulariser
+// with respect to theta_v: every masked neighbour also holds the edge back to
+// v (mesh adjacency is symmetric, with the same length), hence
+// sum_j (1 + mask(nb_j)) sgn(q_j) / len_j.  A padding slot names v itself.
+__device__ __forceinline__ void surf_tv_terms(float c, const float* G, const unsigned char* mk, const int* nb,
+                                              const float* len, int maxnb, size_t stride, float& cost,
+                                              float& grad) {
+    float cs = 0.0f, gr = 0.0f;
+    for (int j = 0; j < maxnb; ++j) {
+        const int q = nb[(size_t)j * stride];
+        const float l = len[(size_t)j * stride];
+        const float t = __fdiv_rn(sub1(c, G[q]), l);
+        if (!isfinite(t)) continue;
+        cs = add1(cs, fabsf(t));
+        gr = add1(gr, __fdiv_rn(mul1(mk[q] ? 2.0f : 1.0f, sgn0(t)), l));
+    }
+    cost = cs;
+    grad = gr;
+}
+
 // Prior-distribution regulariser of one parameter (gpuNEXI.prior_distribution_normal,
 // NEXI/gpuNEXI.m:1256-1307): z = (theta - mu) / sd; a finite z adds |z| to the
 // cost and sgn(z) / sd to d cost / d theta, a non-finite one nothing.

@@ -62,6 +62,11 @@ struct AdamParams {
     // prior-distribution regulariser (instead of TV): [n_reg][nvtot], or nullptr
     const float* prior_mu;
     const float* prior_sd;
+    // surface TV (instead of the grid stencil): [surf_maxnb][nvtot] neighbour
+    // grid indices and edge lengths, or nullptr
+    const int* surf_nb;
+    const float* surf_len;
+    int surf_maxnb;
 };
 
 // Kernel launchers (askadam_kernels.cu).  Return cudaError_t of the launch.

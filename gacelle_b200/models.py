@@ -1,7 +1,8 @@
 """Host-side mirrors of GACELLE's built-in model classes whose fits run on the
 B200 engine: gpuR2starMapping (R2star/gpuR2starMapping.m),
-gpuJointR1R2starMapping (R1R2s/gpuJointR1R2starMapping.m) and gpuNEXI
-(NEXI/gpuNEXI.m).
+gpuJointR1R2starMapping (R1R2s/gpuJointR1R2starMapping.m), gpuNEXI
+(NEXI/gpuNEXI.m; volumetric and surface data, TV or prior-distribution
+regularisation) and gpuNEXIrice (NEXI/gpuNEXIrice.m).
 
 Each class keeps the reference's parameter contract (modelParams, lb, ub,
 startPoint, step, index-aligned), ``updateProperty``, ``fit`` and ``FWD``.
@@ -567,8 +568,57 @@ class gpuNEXI(_ModelBase):
     thres_impossible = 0.1
     thres_bkg = 0.01
 
+    def get_surface_geometry(self, surf_dir, depth=0.5, hemisphere=("lh", "rh")):
+        """NEXI/gpuNEXI.m:258-287: utils.get_surface_neighbours, cached on the
+        object for the last (surf_dir, depth, hemisphere); returns
+        (neighbours, edgeLength)."""
+        from . import surface
+        depth = 0.5 if depth is None else depth
+        hemisphere = [hemisphere] if isinstance(hemisphere, str) else list(hemisphere)
+        key = (str(surf_dir), float(depth), tuple(hemisphere))
+        cache = getattr(self, "_surface_cache", None)
+        if cache is not None and cache[0] == key:
+            return cache[1], cache[2]
+        nb, _, edge = surface.get_surface_neighbours(surf_dir, depth, hemisphere)
+        nb = nb.astype(np.float32)
+        edge = edge.astype(np.float32)
+        self._surface_cache = (key, nb, edge)
+        return nb, edge
+
+    def _prepare_surface(self, data, mask, ex, fitting):
+        """The surface branch of NEXI/gpuNEXI.m:482-548: [1, Nvertex, Nhemi]
+        data and mask; with TV, the mesh geometry from extradata surf_dir /
+        hemisphere / depth into extradata neighbours / dr; segmentation only
+        as none or one segment per hemisphere."""
+        if mask.shape[0] != 1 or data.shape[0] != 1:
+            raise GacelleError(GX_EINVAL, "Surface mode expects data/mask in [1, Nvertex, Nhemi] convention "
+                                          f"(singleton 1st dimension), got mask size {list(utils.dims3(mask))}.")
+        nhemi = utils.dims3(mask)[2]
+        if str(fitting.get("regularisationType", "TV")).lower() == "tv" and np.atleast_1d(fitting["lambda"])[0] > 0:
+            if not ex.get("surf_dir"):
+                raise GacelleError(GX_EINVAL, "fitting.dataType is 'surface' but extradata.surf_dir was not provided.")
+            if not ex.get("hemisphere"):
+                raise GacelleError(GX_EINVAL, "fitting.dataType is 'surface' but extradata.hemisphere was not "
+                                              "provided.")
+            hemi = [ex["hemisphere"]] if isinstance(ex["hemisphere"], str) else list(ex["hemisphere"])
+            if len(hemi) != nhemi:
+                raise GacelleError(GX_EINVAL, f"extradata.hemisphere has {len(hemi)} entries but mask dim3 (Nhemi) "
+                                              f"= {nhemi}; these must match.")
+            depth = ex.get("depth") if ex.get("depth") is not None else 0.5
+            nb, edge = self.get_surface_geometry(ex["surf_dir"], depth, hemi)
+            if nb.shape[2] != nhemi:
+                raise GacelleError(GX_EINVAL, f"Computed surface neighbour geometry has {nb.shape[2]} hemisphere(s) "
+                                              f"but mask has {nhemi}.")
+            ex["neighbours"], ex["dr"] = nb, edge
+        nseg = fitting.get("NSegmentUser") or 1
+        if nseg not in (1, nhemi):
+            raise GacelleError(GX_EINVAL, "Surface segmentation is exact-only and limited to fitting.NSegmentUser "
+                                          f"= 1 (no split) or {nhemi} (exact per-hemisphere split); got {nseg}.")
+        return ex
+
     def prepare_dwi_data(self, data, mask, extradata, lmax=0, fitting=None):
-        """NEXI/gpuNEXI.m:480-633 (volumetric data).  A full acquisition
+        """NEXI/gpuNEXI.m:480-633.  Surface data ([1, Nvertex, Nhemi]) get
+        their mesh geometry for TV and no mask rules.  A full acquisition
         (more volumes than shells x (lmax/2+1)) becomes rotationally
         invariant signals through
         DWIutility.compute_rotationally_invariant_signal with the little
@@ -580,8 +630,9 @@ class gpuNEXI(_ModelBase):
         data = np.asarray(data, dtype=np.float64)
         mask = np.asarray(mask) > 0
         ex = dict(extradata or {})
-        if fitting is not None and fitting.get("dataType", "volumetric") != "volumetric":
-            raise GacelleError(GX_EUNSUPPORTED, "surface data are not accelerated")
+        surface = fitting is not None and str(fitting.get("dataType", "volumetric")).lower() == "surface"
+        if surface:
+            ex = self._prepare_surface(data, mask, ex, fitting)
         nsl = lmax // 2 + 1
         if data.shape[-1] / nsl > len(self.b):
             for k in ("bval", "bvec", "BDELTA"):
@@ -592,6 +643,8 @@ class gpuNEXI(_ModelBase):
         elif data.shape[-1] < len(self.b) * nsl:
             raise GacelleError(GX_EINVAL, f"Input has {data.shape[-1]} volumes but model expects "
                                           f"{len(self.b) * nsl}. Check lmax or input data.")
+        if surface:
+            return data, mask, ex
         ns = len(self.b)
         sl0 = data[..., :ns]
         with np.errstate(invalid="ignore"):
@@ -639,10 +692,16 @@ class gpuNEXI(_ModelBase):
             fitting["ub"] = self.ub[: len(self.modelParams)]
         if not len(fitting["lb"]):
             fitting["lb"] = self.lb[: len(self.modelParams)]
-        if fitting.get("dataType", "volumetric") != "volumetric":
-            raise GacelleError(GX_EUNSUPPORTED, "surface data are not accelerated")
+        surface = str(fitting.get("dataType", "volumetric")).lower() == "surface"
         prior = fitting["solver"] == "askadam" and str(fitting.get("regularisationType", "TV")).lower() == "prior" \
             and np.atleast_1d(fitting["lambda"])[0] > 0
+        surface_tv = fitting["solver"] == "askadam" and surface and not prior \
+            and np.atleast_1d(fitting["lambda"])[0] > 0
+        if surface_tv and (not extradata or "neighbours" not in extradata or "dr" not in extradata):
+            raise GacelleError(GX_EINVAL, "fitting.dataType is 'surface' and fitting.lambda > 0, but "
+                                          "extradata.neighbours/extradata.dr were not provided to fit(). This is "
+                                          "normally populated by estimate() - if calling fit() directly, supply "
+                                          "extradata.neighbours and extradata.dr yourself.")
         if prior:
             # NEXI/gpuNEXI.m:382-410: mu / sigma structs with a field per regmap name
             ex = extradata or {}
@@ -670,6 +729,13 @@ class gpuNEXI(_ModelBase):
         w = None
         if not np.all(wv == 1):
             w = np.broadcast_to(wv, utils.dims3(mask) + (wv.size,)).copy()
+        if surface_tv:
+            from .askadam_solver import askadam
+            userFcn = [self.FWD, self.surface_total_variation]
+            userInput = [[fitting["lmax"], fitting["solver"]],
+                         [mask, extradata["neighbours"], fitting["lambda"], fitting["regmap"], extradata["dr"]]]
+            return askadam(self.context, fitting.get("path", "fused")).optimisation(
+                dwi, mask, w, pars0, fitting, userFcn, userInput)
         if prior:
             from .askadam_solver import askadam
             ex = extradata or {}
@@ -679,6 +745,36 @@ class gpuNEXI(_ModelBase):
             return askadam(self.context, fitting.get("path", "fused")).optimisation(
                 dwi, mask, w, pars0, fitting, userFcn, userInput)
         return self._solve(dwi, mask, w, pars0, fitting, extradata=extradata)
+
+    @staticmethod
+    def surface_total_variation(parameters, mask, neighbours, lambda_, regmap, edgeLength):
+        """gpuNEXI.surface_total_variation (NEXI/gpuNEXI.m:1165-1254): sum_r
+        lambda_r / Nmask * sum |theta(v) - theta(nb)| / edgeLength over every
+        neighbour slot of every masked vertex, theta being the parameter image
+        [1, Nvertex, Nhemi] (0 off the mask) and non-finite quotients dropped.
+        As a userFcn entry it selects the engine's surface TV; called directly
+        it evaluates the loss of [1, Nvox] parameter rows on the host."""
+        lam = [float(x) for x in np.atleast_1d(lambda_)]
+        if not lam or lam[0] <= 0:
+            return 0.0
+        mask = np.asarray(mask)
+        d3 = utils.dims3(mask)
+        nmask = int(np.count_nonzero(mask))
+        nb = np.asarray(neighbours)
+        maxnb = nb.shape[3]
+        glob = (nb.reshape((-1, maxnb), order="F").astype(np.int64) - 1
+                + (np.arange(d3[0] * d3[1] * d3[2]) // (d3[0] * d3[1]) * d3[1])[:, None])
+        ln = np.asarray(edgeLength, dtype=np.float32).reshape((-1, maxnb), order="F")
+        sel = mask.ravel(order="F") > 0
+        loss = 0.0
+        for name, l in zip(np.atleast_1d(regmap), lam):
+            th = utils.reshape_GD2ND(np.asarray(parameters[name], dtype=np.float32).reshape(1, -1), mask)
+            th = np.asarray(th, dtype=np.float32).ravel(order="F")
+            with np.errstate(divide="ignore", invalid="ignore"):
+                q = (th[:, None] - th[glob]) / ln
+            q = q[sel]
+            loss += float(np.sum(np.abs(q[np.isfinite(q)]), dtype=np.float64)) / nmask * l
+        return loss
 
     @staticmethod
     def prior_distribution_normal(parameters, mask, lambda_, regmap, mu, sigma):

@@ -89,9 +89,12 @@ typedef enum {
 typedef enum { GX_MCMC_MH = 0, GX_MCMC_ENSEMBLE = 1 } gx_mcmc_algorithm;
 typedef enum { GX_GW_SIMULTANEOUS = 0, GX_GW_REDBLACK = 1 } gx_gw_update;
 typedef enum { GX_MEM_HOST = 0, GX_MEM_DEVICE = 1 } gx_memory;
-/* fitting.regularisationType: the spatial TV of utils/spatial_total_variation.m,
- * or gpuNEXI.prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307) */
-typedef enum { GX_REG_TV = 0, GX_REG_PRIOR = 1 } gx_reg_type;
+/* The regulariser of the lambda / regmap entries: the spatial TV of
+ * utils/spatial_total_variation.m; gpuNEXI.prior_distribution_normal
+ * (NEXI/gpuNEXI.m:1256-1307, fitting.regularisationType 'prior'); or
+ * gpuNEXI.surface_total_variation (NEXI/gpuNEXI.m:1165-1254, fitting.dataType
+ * 'surface' with TV) over the mesh neighbours in gx_volume. */
+typedef enum { GX_REG_TV = 0, GX_REG_PRIOR = 1, GX_REG_SURFACE_TV = 2 } gx_reg_type;
 
 typedef struct gx_context gx_context;
 
@@ -129,6 +132,16 @@ typedef struct {
     const float* prior_mu;
     const float* prior_sd;
     double prior_offset;
+    /* GX_REG_SURFACE_TV: the vertices of the grid (dims, grid_index as for TV)
+     * and, per voxel, its mesh neighbours as [max_neighbours][nvox] grid
+     * indices with the edge lengths; a vertex with fewer neighbours repeats its
+     * own index.  The regulariser adds lambda_r / nvox * sum |theta_v -
+     * theta_nb| / length over the voxels' slots (theta = 0 off the mask,
+     * non-finite quotients dropped); the adjacency must be symmetric with equal
+     * lengths both ways, as a triangle mesh gives. */
+    int32_t max_neighbours;
+    const int32_t* neighbours;
+    const float* edge_length;
 } gx_volume;
 
 /* askAdam options: the `fitting` struct after askadam.check_set_default_basic

@@ -59,7 +59,8 @@ class OrcAdamOpts(C.Structure):
 class OrcVolume(C.Structure):
     _fields_ = [("dims", C.c_int * 3), ("nvox", C.c_int), ("grid_index", _ip),
                 ("data", _dp), ("weights", _dp), ("theta0", _dp), ("b1", _dp), ("sigma", _dp),
-                ("norm_nvox", C.c_double), ("prior_mu", _dp), ("prior_sd", _dp), ("prior_offset", C.c_double)]
+                ("norm_nvox", C.c_double), ("prior_mu", _dp), ("prior_sd", _dp), ("prior_offset", C.c_double),
+                ("max_neighbours", C.c_int), ("neighbours", _ip), ("edge_length", _dp)]
 
 
 class OrcAdamResult(C.Structure):
@@ -277,7 +278,8 @@ class Volume:
     """One masked volume in the oracle's SoA layout: arrays are [k][nvox]."""
 
     def __init__(self, data, dims=None, grid_index=None, weights=None, theta0=None, b1=None,
-                 sigma=None, norm_nvox=0.0, prior_mu=None, prior_sd=None, prior_offset=0.0):
+                 sigma=None, norm_nvox=0.0, prior_mu=None, prior_sd=None, prior_offset=0.0,
+                 neighbours=None, edge_length=None):
         self.data = _f64(data)
         nv = self.data.shape[1]
         self.grid_index = None if grid_index is None else np.ascontiguousarray(grid_index, np.int32)
@@ -295,6 +297,12 @@ class Volume:
         self.s.prior_mu = _d(self.prior_mu)
         self.s.prior_sd = _d(self.prior_sd)
         self.s.prior_offset = float(prior_offset)
+        self.neighbours = None if neighbours is None else np.ascontiguousarray(neighbours, np.int32)
+        self.edge_length = _f64(edge_length)
+        if self.neighbours is not None:
+            self.s.max_neighbours = self.neighbours.shape[0]
+            self.s.neighbours = self.neighbours.ctypes.data_as(_ip)
+            self.s.edge_length = _d(self.edge_length)
 
     @property
     def nvox(self):
@@ -353,6 +361,8 @@ def adam_opts(lb, ub, fitting: dict):
         o.reg_param[i] = k
         o.lambda_[i] = l
     o.reg_type = 1 if str(f.get("regularisationType", "TV")).lower() == "prior" else 0
+    if o.reg_type == 0 and str(f.get("dataType", "volumetric")).lower() == "surface":
+        o.reg_type = 2
     o.tv_3d = 1 if str(f.get("TVmode", "2D")).upper() == "3D" else 0
     vs = list(f.get("voxelSize", [2, 2, 2])) + [1.0] * 3
     for i in range(3):

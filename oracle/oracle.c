@@ -620,6 +620,34 @@ static double eval_z(adam_ctx* c, const double* z, double* gz, double* res, doub
             reg += sr / nmask * o->lambda[r];
         }
         reg += vol->prior_offset;
+    } else if (o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == 2) {
+        /* surface_total_variation (NEXI/gpuNEXI.m:1236-1251): theta on the vertex
+         * grid (0 off the mask), (theta_v - theta_nb) / length per neighbour slot
+         * of every masked vertex, non-finite entries zeroed, sum |.| / Nmask *
+         * lambda.  The gradient is the exact adjoint, scattered to both ends. */
+        double nmask = (double)nv;
+        int* inv = (int*)malloc(sizeof(int) * c->ngrid);
+        for (size_t q = 0; q < c->ngrid; ++q) inv[q] = -1;
+        for (int v = 0; v < nv; ++v) inv[vol->grid_index[v]] = v;
+        for (int r = 0; r < o->n_reg; ++r) {
+            int k = o->reg_param[r];
+            memset(c->grid, 0, sizeof(double) * c->ngrid);
+            for (int v = 0; v < nv; ++v) c->grid[vol->grid_index[v]] = theta[(size_t)k * nv + v];
+            double sr = 0.0;
+            for (int v = 0; v < nv; ++v)
+                for (int j = 0; j < vol->max_neighbours; ++j) {
+                    int q = vol->neighbours[(size_t)j * nv + v];
+                    double len = vol->edge_length[(size_t)j * nv + v];
+                    double t = (c->grid[vol->grid_index[v]] - c->grid[q]) / len;
+                    if (!isfinite(t)) continue;
+                    sr += fabs(t);
+                    double d = (t > 0 ? 1.0 : (t < 0 ? -1.0 : 0.0)) / len * o->lambda[r] / nmask;
+                    gth[(size_t)k * nv + v] += d;
+                    if (inv[q] >= 0) gth[(size_t)k * nv + inv[q]] -= d;
+                }
+            reg += sr / nmask * o->lambda[r];
+        }
+        free(inv);
     } else if (o->n_reg > 0 && o->lambda[0] > 0) { /* spatial_total_variation.m:29 */
         double nmask = (double)nv;
         for (int r = 0; r < o->n_reg; ++r) {
@@ -656,6 +684,7 @@ static int setup_ctx(adam_ctx* c, const orc_model* m, const orc_volume* vol,
     if (o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == 1) {
         if (!vol->prior_mu || !vol->prior_sd) return -1;
     } else if (o->n_reg > 0 && o->lambda[0] > 0) {
+        if (o->reg_type == 2 && (!vol->neighbours || !vol->edge_length)) return -1;
         if (!vol->grid_index) return -1;
         c->ngrid = (size_t)vol->dims[0] * vol->dims[1] * vol->dims[2];
         c->mask = (unsigned char*)calloc(c->ngrid, 1);

@@ -112,7 +112,8 @@ typedef struct {
     double outlier_weight;
     int weight_update_interval, outlier_check_window;
     double outlier_voxel_thres, outlier_pop_thres, outlier_init_thres, outlier_init_pop_thres;
-    int reg_type;                /* 0: spatial TV; 1: prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307) */
+    int reg_type;                /* 0: spatial TV; 1: prior_distribution_normal (NEXI/gpuNEXI.m:1256-1307);
+                                  * 2: surface_total_variation (NEXI/gpuNEXI.m:1165-1254) */
 } orc_adam_opts;
 
 typedef struct {
@@ -128,6 +129,9 @@ typedef struct {
     const double* prior_mu;      /* [n_reg][nvox] prior mean (reg_type 1) */
     const double* prior_sd;      /* [n_reg][nvox] prior SD */
     double prior_offset;         /* prior loss of the grid points outside the mask */
+    int max_neighbours;          /* reg_type 2 (surface TV): mesh neighbours per voxel */
+    const int* neighbours;       /* [max_neighbours][nvox] grid indices */
+    const double* edge_length;   /* [max_neighbours][nvox] */
 } orc_volume;
 
 typedef struct {

@@ -89,7 +89,7 @@ def reg_fields(f, names):
 
 
 def run_engine(kind, y, theta0, f, names, path="fused", dims=None, gidx=None, b1=None, sigma=None,
-               weights=None, context=None, prior=None, **model_kw):
+               weights=None, context=None, prior=None, surface=None, **model_kw):
     gxm, _ = models(kind, **model_kw)
     lb, ub = bounds(kind)
     opts = gx_askadam.build_opts(f, names, lb, ub, path)
@@ -98,14 +98,15 @@ def run_engine(kind, y, theta0, f, names, path="fused", dims=None, gidx=None, b1
     d3 = dims if dims is not None else (nv, 1, 1)
     g = gidx if gidx is not None else np.arange(nv, dtype=np.int32)
     solver = gx_askadam.askadam(context, path)
-    res = solver._run(gxm, y, weights, theta0, b1, sigma, g, d3, opts, nm, len(names), prior)
+    res = solver._run(gxm, y, weights, theta0, b1, sigma, g, d3, opts, nm, len(names), prior, surface)
     res["timing"] = solver.last_timing
     return res
 
 
 def run_oracle(kind, y, theta0, f, names, dims=None, gidx=None, b1=None, sigma=None, weights=None,
-               norm_nvox=0.0, prior=None, **model_kw):
-    """prior: (mu [n_reg][nvox], sd [n_reg][nvox], offset) of the prior regulariser."""
+               norm_nvox=0.0, prior=None, surface=None, **model_kw):
+    """prior: (mu [n_reg][nvox], sd [n_reg][nvox], offset) of the prior regulariser;
+    surface: (neighbours, edge lengths), [maxNeighbours][nvox], of the surface TV."""
     _, om = models(kind, **model_kw)
     f = reg_fields(dict(f), names)
     o = _oracle_opts(kind, f)
@@ -119,7 +120,9 @@ def run_oracle(kind, y, theta0, f, names, dims=None, gidx=None, b1=None, sigma=N
                         norm_nvox=norm_nvox,
                         prior_mu=None if prior is None else np.asarray(prior[0], np.float64),
                         prior_sd=None if prior is None else np.asarray(prior[1], np.float64),
-                        prior_offset=0.0 if prior is None else float(prior[2]))
+                        prior_offset=0.0 if prior is None else float(prior[2]),
+                        neighbours=None if surface is None else surface[0],
+                        edge_length=None if surface is None else np.asarray(surface[1], np.float64))
     return oracle.askadam(om, vol, o, want_residual=True)
 
 

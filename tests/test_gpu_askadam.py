@@ -866,3 +866,135 @@ def test_gpuNEXI_fit_with_prior_distribution(ctx):
     assert abs(out["final"]["loss_reg"] - orc["final_reg"]) <= 1e-4 * orc["final_reg"]
     host = gpuNEXI.prior_distribution_normal({"fa": fa[None, :]}, mask, [1e-3], ["fa"], mu, sdm)
     assert out["final"]["loss_reg"] == pytest.approx(host, rel=1e-4)
+
+
+# ------------------------------------------------------------- surface TV ----
+def _surface_case(seed, lam=(3e-3,), regmap=("fa",)):
+    """NEXI data on two hemisphere sheets [1, Nvertex, 2] with a partial mask,
+    and the surface-TV neighbour tables of the masked vertices."""
+    from gacelle_b200 import utils
+    from gacelle_b200.askadam_solver import askadam
+    import test_surface
+    neighbours, edge, mask = test_surface._surface_problem(seed, nx=14, ny=12)
+    idx = utils.mask_index(mask)
+    n = idx.size
+    y, th0, th = _problem("nexi", n, seed + 100)
+    tables = askadam._surface_tables((neighbours, edge), mask, idx)
+    f = fitting(**{"lambda": list(lam), "regmap": list(regmap), "dataType": "surface"})
+    return neighbours, edge, mask, idx, y, th0, th, tables, f
+
+
+def test_surface_tv_model_gradient_matches_oracle(ctx):
+    """One evaluation through gx_model_gradient: the kernel's gradient uses
+    the symmetric adjacency (each masked neighbour holds the edge back), the
+    oracle scatters the exact adjoint; relative 1e-3 of the largest
+    component, the regularisation loss to 1e-5."""
+    import ctypes as C
+    neighbours, edge, mask, idx, y, _, th, tables, f = _surface_case(80, (3e-3, 1e-3), ("fa", "ra"))
+    lb, ub = bounds("nexi")
+    th = np.clip(th, np.array(lb)[:, None] + 1e-3, np.array(ub)[:, None] - 1e-3).astype(np.float32)
+    names = NAMES["nexi"]
+    opts = gx_askadam.build_opts(f, names, lb, ub)
+    assert opts.reg_type == _lib.REG_SURFACE_TV
+    gxm, om = models("nexi")
+    n = y.shape[1]
+    vol = _lib.GxVolume()
+    for i in range(3):
+        vol.dims[i] = mask.shape[i]
+    vol.nvox = n
+    gi = idx.astype(np.int32)
+    vol.grid_index = gi.ctypes.data_as(_lib._i32p)
+    vol.data = y.ctypes.data_as(_lib._fp)
+    nbt = np.ascontiguousarray(tables[0], np.int32)
+    lnt = np.ascontiguousarray(tables[1], np.float32)
+    vol.max_neighbours = nbt.shape[0]
+    vol.neighbours = nbt.ctypes.data_as(_lib._i32p)
+    vol.edge_length = lnt.ctypes.data_as(_lib._fp)
+    g = np.zeros_like(th)
+    L = C.c_double(); Lf = C.c_double(); Lr = C.c_double()
+    _lib.check(_lib.lib().gx_model_gradient(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, C.byref(vol), C.byref(opts),
+                                            th.ctypes.data, g.ctypes.data, None, C.byref(L), C.byref(Lf),
+                                            C.byref(Lr)))
+    from helpers import reg_fields
+    o = oracle.adam_opts(lb, ub, reg_fields(dict(f), names))
+    ov = oracle.Volume(y.astype(np.float64), dims=mask.shape, grid_index=gi, neighbours=nbt,
+                       edge_length=lnt.astype(np.float64))
+    Lo, go, _, fo, ro = oracle.model_gradient(om, ov, o, th.astype(np.float64))
+    assert ro > 0 and abs(Lr.value - ro) <= 1e-5 * ro
+    for k in range(4):
+        scale = np.max(np.abs(go[k]))
+        assert np.max(np.abs(g[k] - go[k])) <= 1e-3 * scale + 1e-12, k
+    # a neighbour index outside the grid is rejected on the device
+    bad = nbt.copy()
+    bad[0, 5] = mask.size
+    vol.neighbours = bad.ctypes.data_as(_lib._i32p)
+    with pytest.raises(_lib.GacelleError):
+        _lib.check(_lib.lib().gx_model_gradient(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, C.byref(vol),
+                                                C.byref(opts), th.ctypes.data, g.ctypes.data, None, C.byref(L),
+                                                C.byref(Lf), C.byref(Lr)))
+
+
+@pytest.mark.parametrize("lam", [1e-5, 3e-3])
+@pytest.mark.parametrize("path", ["fused", "plain"])
+def test_askadam_surface_tv_matches_oracle(ctx, path, lam):
+    """askAdam with the surface TV (one launch per epoch on the fused path,
+    op-by-op on the plain one) against the FP64 oracle.  The TV is L1-like:
+    where it flattens the map, neighbouring values sit at the kink and the
+    exact path depends on rounding (the FP64 oracle itself moves fa by ~1e-3
+    relative RMSE at lambda 3e-3 when the data are perturbed at 1e-5, the FP32
+    forward's error).  The maps are held to three times that band, measured
+    here, plus 1e-4; the regularisation loss to 1e-3."""
+    neighbours, edge, mask, idx, y, th0, _, tables, f = _surface_case(81, (lam,))
+    f = dict(f, iteration=200)
+    kw = dict(dims=mask.shape, gidx=idx.astype(np.int32), surface=tables)
+    eng = run_engine("nexi", y, th0, f, NAMES["nexi"], path=path, **kw)
+    orc = run_oracle("nexi", y, th0, f, NAMES["nexi"], **kw)
+    rng = np.random.default_rng(84)
+    opt = run_oracle("nexi", y.astype(np.float64) * (1 + 1e-5 * rng.standard_normal(y.shape)), th0, f,
+                     NAMES["nexi"], **kw)
+    for k in range(4):
+        band = rel_rmse(opt["final"][k], orc["final"][k])
+        assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 3 * band + 1e-4, (k, band)
+    assert abs(eng["final_loss_reg"] - orc["final_reg"]) <= 1e-3 * orc["final_reg"]
+    np.testing.assert_allclose(eng["loss_history"], orc["loss_history"], rtol=1e-3)
+    assert eng["timing"]["tv_path"] == 0         # never the cooperative grid-TV kernel
+
+
+def test_gpuNEXI_estimate_on_surface(ctx, tmp_path):
+    """gpuNEXI.estimate with fitting.dataType = 'surface' from FreeSurfer
+    surfaces on disk: the geometry is read, the surface TV runs on the
+    engine, and the fit equals the solver run on the same tables; TV makes
+    the fa map smoother along the mesh than the unregularised fit."""
+    import test_surface
+    from gacelle_b200 import gpuNEXI, utils
+    from gacelle_b200.askadam_solver import askadam
+    nv = test_surface.write_subject(str(tmp_path), nx=14, ny=12)
+    rng = np.random.default_rng(82)
+    mask = rng.random((1, nv, 2)) > 0.2
+    idx = utils.mask_index(mask)
+    y, th0, th = _problem("nexi", idx.size, 83, sigma=0.03)
+    b = np.tile([1.0, 2.5, 4.0, 6.0, 8.0, 10.0], 4)
+    d = np.repeat([20.0, 27.0, 35.0, 49.0], 6)
+    m = gpuNEXI(b, d)
+    m.context = ctx
+    data = utils.reshape_GD2ND(y, mask).reshape((1, nv, 2, 24), order="F")
+    f = {"iteration": 200, "start": "default", "lossFunction": "mse", "lambda": [2e-3], "regmap": ["fa"],
+         "dataType": "surface", "tol": 0.0, "patienceConvergence": float("inf"), "convergenceStepTol": 0.0,
+         "convergenceGradTol": 0.0}
+    ex = {"surf_dir": str(tmp_path), "hemisphere": ["lh", "rh"]}
+    out = m.estimate(data, mask, ex, dict(f))
+    free = m.estimate(data, mask, ex, dict(f, **{"lambda": [0.0]}))
+    assert out["final"]["loss_reg"] > 0 and free["final"]["loss_reg"] == 0
+    nb, edge = m.get_surface_geometry(str(tmp_path), 0.5, ["lh", "rh"])
+    fa = utils.reshape_ND2GD(out["final"]["fa"][..., None], idx)[0]
+    fa0 = utils.reshape_ND2GD(free["final"]["fa"][..., None], idx)[0]
+    tv = gpuNEXI.surface_total_variation
+    assert tv({"fa": fa[None]}, mask, nb, [1.0], ["fa"], edge) < tv({"fa": fa0[None]}, mask, nb, [1.0], ["fa"], edge)
+    assert out["final"]["loss_reg"] == pytest.approx(tv({"fa": fa[None]}, mask, nb, [2e-3], ["fa"], edge), rel=1e-4)
+    # the same fit through the solver with the tables built by hand
+    fit = m.check_set_default(dict(f))
+    tables = askadam._surface_tables((nb, edge), mask, idx)
+    x0 = np.tile(np.array(m.startPoint[:4], np.float32)[:, None], (1, idx.size))
+    eng = run_engine("nexi", utils.reshape_ND2GD(data, idx).astype(np.float32), x0, dict(fit, lb=m.lb[:4],
+                     ub=m.ub[:4]), NAMES["nexi"], dims=mask.shape, gidx=idx.astype(np.int32), surface=tables)
+    np.testing.assert_array_equal(eng["final_theta"][0], fa)
