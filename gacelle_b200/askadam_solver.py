@@ -383,6 +383,12 @@ class askadam:
         out["lossHistory"] = res["loss_history"]
         return out
 
+    @staticmethod
+    def save_askadam_output(output_filename, out):
+        """utils/askadam.m:993-1009: save ``out`` to a MAT-file when a file
+        name is given."""
+        return utils.save_output(output_filename, out)
+
     # ----- static tools of the reference (utils/askadam.m:1063-1183) -----
     @staticmethod
     def unscale_parameters(parameters, lb, ub, modelParams, parameterTransform="linear"):

@@ -70,6 +70,12 @@ class mcmc:
     check_set_default_basic = staticmethod(check_set_default_basic)
     get_number_burnin = staticmethod(get_number_burnin)
 
+    @staticmethod
+    def save_mcmc_output(outputFilename, out):
+        """utils/mcmc.m:702-718: save ``out`` to a MAT-file when a file name
+        is given."""
+        return utils.save_output(outputFilename, out)
+
     def optimisation(self, data, mask, weights, pars0, fitting, FWDfunc, *varargin, extradata=None):
         """mcmc.optimisation (utils/mcmc.m:18-80)."""
         model = _model_of(FWDfunc)

@@ -21,6 +21,13 @@ from . import dwi as dwi_util
 from ._lib import GacelleError, GX_EINVAL, GX_EUNSUPPORTED
 
 
+def _save(fitting, out):
+    """The end of every model's estimate(): askadam.save_askadam_output or
+    mcmc.save_mcmc_output of fitting.outputFilename (e.g.
+    NEXI/gpuNEXI.m:243-249)."""
+    utils.save_output(fitting.get("outputFilename"), out)
+
+
 class _GxModelHandle:
     """A gx_model struct plus the arrays it points into."""
 
@@ -242,6 +249,7 @@ class gpuR2starMapping(_ModelBase):
                 out[which]["M0"] = out[which]["M0"] * scale
         if "mean" in out and "M0" in out["mean"]:
             out["mean"]["M0"] = out["mean"]["M0"] * scale
+        _save(fitting, out)
         return out
 
 
@@ -409,6 +417,7 @@ class gpuJointR1R2starMapping(_ModelBase):
         for which in ("final", "min", "mean"):
             if which in out and "M0" in out[which]:
                 out[which]["M0"] = out[which]["M0"] * scale
+        _save(fitting, out)
         return out
 
 
@@ -678,6 +687,7 @@ class gpuNEXI(_ModelBase):
         dwi, mask, ex = self.prepare_dwi_data(dwi, mask, extradata, int(fitting["lmax"]), fitting)
         out = self.fit(dwi.astype(np.float32), mask, fitting, pars0, ex)
         out["mask"] = mask
+        _save(fitting, out)
         return out
 
     def fit(self, dwi, mask=None, fitting=None, pars0=None, extradata=None):
@@ -948,4 +958,5 @@ class gpuNEXIrice(gpuNEXI):
         dwi, mask, ex = self.prepare_dwi_data(dwi, mask, extraData, int(fitting["lmax"]))
         out = self.fit(dwi, mask, fitting, ex, pars0)
         out["mask"] = mask
+        _save(fitting, out)
         return out

@@ -78,3 +78,34 @@ def set_nan_inf_zero(data):
 def initialise_x0(dims, model_params, start_point) -> dict:
     """utils.initialise_x0 (utils/utils.m:1586-1592): constant start maps."""
     return {p: np.full(dims, float(v), dtype=np.float32) for p, v in zip(model_params, start_point)}
+
+
+def _mat_value(v):
+    """A value scipy.io.savemat can write as MATLAB would hold it: nested dicts
+    become structs, None becomes [] and tuples of numbers arrays."""
+    if isinstance(v, dict):
+        return {k: _mat_value(x) for k, x in v.items()}
+    if v is None:
+        return np.zeros((0, 0))
+    if isinstance(v, (list, tuple)) and all(isinstance(x, str) for x in v):
+        return np.array(v, dtype=object)
+    return v
+
+
+def save_output(filename, out):
+    """askadam.save_askadam_output / mcmc.save_mcmc_output
+    (utils/askadam.m:993-1009, utils/mcmc.m:702-718): with a non-empty file
+    name, create its folder and save the output structure as the variable
+    ``out`` of a MAT-file (MATLAB's level-5 format).  Returns whether a file
+    was written."""
+    if filename is None or (not isinstance(filename, str) and np.size(filename) == 0) or filename == "":
+        return False
+    import os
+
+    import scipy.io
+    folder = os.path.dirname(str(filename))
+    if folder and not os.path.isdir(folder):
+        os.makedirs(folder)
+    scipy.io.savemat(str(filename), {"out": _mat_value(out)}, do_compression=True)
+    print(f"Estimation output is saved at {filename}")
+    return True

@@ -698,10 +698,11 @@ def test_batch_of_volumes_equals_separate_fits(ctx, tv):
         assert abs(b["final_loss"] - a["final_loss"]) <= 1e-6 * abs(a["final_loss"])
 
 
-def test_joint_r1r2s_estimate_with_prior_start(ctx):
+def test_joint_r1r2s_estimate_with_prior_start(ctx, tmp_path):
     """gpuJointR1R2starMapping.estimate with start='prior': DESPOT1 scaling
     and starting points (host), the fused R1-R2* fit (device), M0 scaled
-    back; the fit lands near the phantom's maps, closer than its start."""
+    back; the fit lands near the phantom's maps, closer than its start; the
+    output is saved to fitting.outputFilename."""
     from gacelle_b200 import models, phantoms
     y, gt = phantoms.r1r2s_volume(600, 77, sigma=0.002)
     img = y.T.reshape(10, 12, 5, y.shape[0], order="F").astype(np.float64)
@@ -709,7 +710,8 @@ def test_joint_r1r2s_estimate_with_prior_start(ctx):
     m = models.gpuJointR1R2starMapping(phantoms.R1R2S_TE, phantoms.R1R2S_TR, phantoms.R1R2S_FA)
     m.context = ctx
     f = {"iteration": 1500, "initialLearnRate": 0.01, "lossFunction": "mse", "start": "prior", "tol": 0.0,
-         "patienceConvergence": float("inf"), "convergenceStepTol": 0.0, "convergenceGradTol": 0.0}
+         "patienceConvergence": float("inf"), "convergenceStepTol": 0.0, "convergenceGradTol": 0.0,
+         "outputFilename": str(tmp_path / "out" / "r1r2s.mat")}
     _, mask2, scale = m.prepare_data(img, mask)
     p0 = m.estimate_prior(img / scale, mask2)
     out = m.estimate(img, mask, f)
@@ -720,6 +722,9 @@ def test_joint_r1r2s_estimate_with_prior_start(ctx):
         assert err_fit < 0.05 and err_fit < err_start, (k, err_fit, err_start)
     m0 = gt["M0"].reshape(10, 12, 5, order="F")
     assert np.median(np.abs(out["final"]["M0"] / m0 - 1)) < 0.05
+    import scipy.io
+    saved = scipy.io.loadmat(f["outputFilename"], squeeze_me=True, struct_as_record=False)["out"]
+    np.testing.assert_array_equal(saved.final.R2star, out["final"]["R2star"])
 
 
 # ------------------------------------- prior-distribution regulariser ----

@@ -178,3 +178,23 @@ def test_device_rician_polynomials_on_host(tmp_path):
     np.testing.assert_allclose(lg, np.log(sp.i0e(x)), atol=2e-6)
     ratio = sp.i1e(x) / sp.i0e(x)
     np.testing.assert_allclose(omr, 1 - ratio, rtol=5e-5, atol=5e-7)
+
+
+def test_save_output_writes_a_mat_file(tmp_path):
+    """askadam.save_askadam_output / mcmc.save_mcmc_output (utils/askadam.m:
+    993-1009, utils/mcmc.m:702-718): the folder is created, the structure is
+    the variable 'out'; an empty file name writes nothing."""
+    import scipy.io
+    from gacelle_b200.askadam_solver import askadam
+    from gacelle_b200.mcmc_solver import mcmc
+    out = {"final": {"M0": np.arange(6, dtype=np.float32).reshape(3, 2, 1), "loss": 0.25,
+                     "stopReason": "convergence"},
+           "lossHistory": np.linspace(1, 0, 5), "mask": np.ones((3, 2, 1), bool), "unused": None}
+    p = tmp_path / "sub" / "fit.mat"
+    assert askadam.save_askadam_output(str(p), out)
+    m = scipy.io.loadmat(str(p), squeeze_me=True, struct_as_record=False)["out"]
+    np.testing.assert_array_equal(m.final.M0, out["final"]["M0"][..., 0])
+    assert m.final.loss == 0.25 and m.final.stopReason == "convergence"
+    np.testing.assert_allclose(m.lossHistory, out["lossHistory"])
+    assert not askadam.save_askadam_output([], out) and not mcmc.save_mcmc_output("", out)
+    assert mcmc.save_mcmc_output(str(tmp_path / "m.mat"), {"mean": {"R2star": np.ones(4)}})
