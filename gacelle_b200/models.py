@@ -21,6 +21,27 @@ from . import dwi as dwi_util
 from ._lib import GacelleError, GX_EINVAL, GX_EUNSUPPORTED
 
 
+def _segmented(fitting, fit, data, mask, extradata=None, pars0=None):
+    """fit(data, mask, extradata, pars0) whole, or in fitting.NSegmentUser
+    slabs with fitting.segmentOverlap halo slices (segments.fit_segmented)."""
+    from . import segments
+    nseg = fitting.get("NSegmentUser")
+    nseg = int(np.atleast_1d(nseg)[0]) if nseg is not None and np.size(nseg) else 1
+    if nseg <= 1:
+        return fit(data, mask, extradata, pars0)
+    return segments.fit_segmented(fit, data, mask, nseg, int(fitting.get("segmentOverlap") or 0), extradata, pars0)
+
+
+def _rescale_m0(out, fitting, scale):
+    """Undo the data scaling on M0 (R2star/gpuR2starMapping.m:163-177): final
+    and min maps for askadam; every metric map and the posterior for mcmc."""
+    keys = ["final", "min"] if fitting.get("solver", "askadam") != "mcmc" else \
+        list(np.atleast_1d(fitting.get("metric", ["mean", "std"]))) + ["posterior"]
+    for k in keys:
+        if isinstance(out.get(k), dict) and "M0" in out[k]:
+            out[k]["M0"] = out[k]["M0"] * scale
+
+
 def _save(fitting, out):
     """The end of every model's estimate(): askadam.save_askadam_output or
     mcmc.save_mcmc_output of fitting.outputFilename (e.g.
@@ -239,16 +260,14 @@ class gpuR2starMapping(_ModelBase):
         return self._solve(data, mask, w, pars0, fitting)
 
     def estimate(self, data, mask, fitting=None):
-        """R2star/gpuR2starMapping.m:94-179 (one segment: the engine fits the
-        whole volume in one launch)."""
+        """R2star/gpuR2starMapping.m:94-179: scaled data, fit (in
+        fitting.NSegmentUser slabs with segmentOverlap halo slices when asked;
+        the engine needs no memory-driven split), M0 scaled back."""
         fitting = self.check_set_default(fitting)
         data, mask, scale = self.prepare_data(data, mask)
-        out = self.fit(data.astype(np.float32), mask, fitting)
-        for which in ("final", "min"):
-            if which in out and "M0" in out[which]:
-                out[which]["M0"] = out[which]["M0"] * scale
-        if "mean" in out and "M0" in out["mean"]:
-            out["mean"]["M0"] = out["mean"]["M0"] * scale
+        out = _segmented(fitting, lambda d, m, e, p: self.fit(d.astype(np.float32), m, fitting), data, mask)
+        out["mask"] = mask
+        _rescale_m0(out, fitting, scale)
         _save(fitting, out)
         return out
 
@@ -409,14 +428,15 @@ class gpuJointR1R2starMapping(_ModelBase):
         return img, mask, scale
 
     def estimate(self, data, mask, fitting=None, extraData=None):
-        """R1R2s/gpuJointR1R2starMapping.m:120-194 (one segment): scaled data,
-        fit, M0 scaled back."""
+        """R1R2s/gpuJointR1R2starMapping.m:120-194: scaled data, fit (in
+        fitting.NSegmentUser slabs when asked, extraData cut with them), M0
+        scaled back."""
         fitting = self.check_set_default(fitting)
         data, mask, scale = self.prepare_data(data, mask, extraData)
-        out = self.fit(data.astype(np.float32), mask, fitting, extraData)
-        for which in ("final", "min", "mean"):
-            if which in out and "M0" in out[which]:
-                out[which]["M0"] = out[which]["M0"] * scale
+        out = _segmented(fitting, lambda d, m, e, p: self.fit(d.astype(np.float32), m, fitting, e), data, mask,
+                         extraData)
+        out["mask"] = mask
+        _rescale_m0(out, fitting, scale)
         _save(fitting, out)
         return out
 
@@ -681,11 +701,13 @@ class gpuNEXI(_ModelBase):
         return data, valid, ex
 
     def estimate(self, dwi, mask, extradata=None, fitting=None, pars0=None):
-        """NEXI/gpuNEXI.m:148-252: data preparation, then fit (the engine
-        fits the whole volume in one call, no segmentation)."""
+        """NEXI/gpuNEXI.m:148-252: data preparation, then fit (in
+        fitting.NSegmentUser slabs / hemispheres when asked, extradata and
+        pars0 cut with them)."""
         fitting = self.check_set_default(fitting)
         dwi, mask, ex = self.prepare_dwi_data(dwi, mask, extradata, int(fitting["lmax"]), fitting)
-        out = self.fit(dwi.astype(np.float32), mask, fitting, pars0, ex)
+        out = _segmented(fitting, lambda d, m, e, p: self.fit(d.astype(np.float32), m, fitting, p, e), dwi, mask,
+                         ex, pars0)
         out["mask"] = mask
         _save(fitting, out)
         return out

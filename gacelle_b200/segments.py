@@ -108,6 +108,45 @@ def restore_segments(parts: list[dict], segs: list[dict], shape3) -> dict:
     return merge(parts, ())
 
 
+def slice_extradata_recursive(extradata, sl):
+    """gpuNEXI.slice_extradata_recursive (NEXI/gpuNEXI.m:884-897): arrays of
+    three or more dimensions are cut to the slices ``sl``, nested dicts (e.g.
+    the prior's mu / sigma maps) recursively, anything else is passed on."""
+    if extradata is None:
+        return None
+    out = {}
+    for k, v in extradata.items():
+        if isinstance(v, dict):
+            out[k] = slice_extradata_recursive(v, sl)
+        elif np.ndim(v) >= 3:
+            out[k] = _slab(v, sl)
+        else:
+            out[k] = v
+    return out
+
+
+def fit_segmented(fit: Callable, data, mask, nseg: int, overlap: int = 0, extradata: dict | None = None,
+                  pars0: dict | None = None) -> dict:
+    """The segment loop of the models' estimate() (e.g.
+    R2star/gpuR2starMapping.m:128-157, NEXI/gpuNEXI.m:209-236) on one GPU:
+    ``nseg`` slabs of about equal voxel counts (fitting.NSegmentUser; the
+    engine needs no memory-driven split), each fitted independently with
+    ``overlap`` halo slices (fitting.segmentOverlap), cropped to its owned
+    slices and written back (crop_segment_output,
+    restore_segment_structure).  ``fit(data_slab, mask_slab, extradata_slab,
+    pars0_slab) -> out``."""
+    mask = np.asarray(mask)
+    shape3 = mask.shape + (1,) * (3 - mask.ndim)
+    m3 = mask.reshape(shape3, order="F")
+    segs = rank_segments(m3, max(int(nseg), 1), int(overlap))
+    parts = []
+    for s in segs:
+        p0 = None if pars0 is None else {k: _slab(v, s["fit"]) if np.ndim(v) >= 3 else v for k, v in pars0.items()}
+        parts.append(fit(_slab(np.asarray(data), s["fit"]), _slab(m3, s["fit"]),
+                         slice_extradata_recursive(extradata, s["fit"]), p0))
+    return restore_segments(parts, segs, shape3)
+
+
 def fit_distributed(fit: Callable, data, mask, extradata: dict | None = None, pars0: dict | None = None,
                     overlap: int = 0, group=None) -> dict:
     """Fit one volume split into one slab per rank.
@@ -129,7 +168,7 @@ def fit_distributed(fit: Callable, data, mask, extradata: dict | None = None, pa
         raise ValueError(f"{world} ranks but only {len(segs)} non-empty slabs")
     s = segs[rank]
     sub = lambda a: None if a is None else (_slab(a, s["fit"]) if np.ndim(a) >= 3 else a)  # noqa: E731
-    ex = None if extradata is None else {k: sub(v) for k, v in extradata.items()}
+    ex = slice_extradata_recursive(extradata, s["fit"])
     p0 = None if pars0 is None else {k: sub(v) for k, v in pars0.items()}
     mine = fit(_slab(np.asarray(data), s["fit"]), _slab(mask.reshape(shape3, order="F"), s["fit"]), ex, p0)
     if world == 1:

@@ -167,3 +167,30 @@ def test_failing_rank_does_not_hang_the_other():
     res = _run("fail")
     assert "rank 1 failed" in res[1]
     assert res[0] != "no error"
+
+
+def test_fit_segmented_slices_fits_and_restores():
+    """The segment loop of estimate() (R2star/gpuR2starMapping.m:128-157,
+    NEXI/gpuNEXI.m:209-236): each slab sees its haloed slices of data, mask,
+    pars0 and (recursively) extradata; only owned slices are written back;
+    scalars become one value per segment."""
+    rng = np.random.default_rng(5)
+    shape = (4, 3, 9)
+    mask = rng.random(shape) > 0.3
+    data = rng.random(shape + (2,))
+    ex = {"b1": rng.random(shape), "mu": {"fa": rng.random(shape)}, "bval": np.arange(2.0), "dr": 0.5}
+    p0 = {"fa": rng.random(shape)}
+    seen = []
+
+    def fit(d, m, e, p):
+        seen.append(m.shape[2])
+        assert d.shape[:3] == m.shape == e["b1"].shape == e["mu"]["fa"].shape == p["fa"].shape
+        assert e["bval"].shape == (2,) and e["dr"] == 0.5
+        return {"final": {"x": (d[..., 0] + e["b1"] + e["mu"]["fa"] + p["fa"]) * m, "loss": float(m.sum())}}
+
+    out = segments.fit_segmented(fit, data, mask, 3, 1, ex, p0)
+    assert len(seen) == 3 and sum(seen) == 9 + 4            # three slabs, halos on the two internal faces
+    np.testing.assert_allclose(out["final"]["x"], (data[..., 0] + ex["b1"] + ex["mu"]["fa"] + p0["fa"]) * mask)
+    assert out["final"]["loss"].shape == (3,)
+    whole = segments.fit_segmented(fit, data, mask, 1, 0, ex, p0)
+    np.testing.assert_allclose(whole["final"]["x"], out["final"]["x"])

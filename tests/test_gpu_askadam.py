@@ -1003,3 +1003,40 @@ def test_gpuNEXI_estimate_on_surface(ctx, tmp_path):
     eng = run_engine("nexi", utils.reshape_ND2GD(data, idx).astype(np.float32), x0, dict(fit, lb=m.lb[:4],
                      ub=m.ub[:4]), NAMES["nexi"], dims=mask.shape, gidx=idx.astype(np.int32), surface=tables)
     np.testing.assert_array_equal(eng["final_theta"][0], fa)
+    # fitting.NSegmentUser = Nhemi: one exact fit per hemisphere (NEXI/gpuNEXI.m:537-546)
+    split = m.estimate(data, mask, ex, dict(f, NSegmentUser=2))
+    for h, hemi in enumerate(("lh", "rh")):
+        one = m.estimate(data[:, :, h:h + 1], mask[:, :, h:h + 1], {"surf_dir": str(tmp_path), "hemisphere": [hemi]},
+                         dict(f))
+        np.testing.assert_array_equal(split["final"]["fa"][:, :, h], one["final"]["fa"][:, :, 0])
+
+
+def test_r2s_estimate_in_segments(ctx):
+    """gpuR2starMapping.estimate with fitting.NSegmentUser = 2 and
+    segmentOverlap = 2 under 3-D TV (R2star/gpuR2starMapping.m:128-157): each
+    slab is fitted on the engine with its halo slices and only its owned
+    slices are kept, so the result equals the two slab fits restored by
+    hand.  (It is not the whole-volume fit: each slab's loss is a mean over
+    its own voxels, which shifts Adam's epsilon against the gradient; the
+    FP64 oracle gives the same few-percent difference, and the reference
+    warns that a segmented fit may differ from one segment,
+    utils/utils.m:798.)"""
+    from gacelle_b200 import models, phantoms, segments
+    mask = phantoms.ellipsoid_mask((24, 20, 16), 1.0)
+    data, _ = phantoms.r2s_phantom(mask, 31)
+    m = models.gpuR2starMapping(phantoms.R2S_TE)
+    m.context = ctx
+    f = {"iteration": 300, "initialLearnRate": 0.01, "lossFunction": "mse", "start": "default", "tol": 0.0,
+         "patienceConvergence": float("inf"), "convergenceStepTol": 0.0, "convergenceGradTol": 0.0,
+         "lambda": [1e-3], "regmap": ["R2star"], "TVmode": "3D"}
+    seg = m.estimate(data, mask, dict(f, NSegmentUser=2, segmentOverlap=2))
+    whole = m.estimate(data, mask, dict(f))
+    d2, m2, scale = m.prepare_data(data, mask)
+    fit = m.check_set_default(dict(f))
+    segs = segments.rank_segments(m2, 2, overlap=2)
+    parts = [m.fit(d2[:, :, s["fit"]].astype(np.float32), m2[:, :, s["fit"]], fit) for s in segs]
+    byhand = segments.restore_segments(parts, segs, m2.shape)
+    np.testing.assert_array_equal(seg["final"]["R2star"], byhand["final"]["R2star"])
+    np.testing.assert_array_equal(seg["final"]["M0"], byhand["final"]["M0"] * scale)
+    assert seg["final"]["loss"].shape == (2,) and np.array_equal(seg["mask"], m2)
+    assert np.isscalar(whole["final"]["loss"]) or np.ndim(whole["final"]["loss"]) == 0
