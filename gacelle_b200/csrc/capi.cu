@@ -850,7 +850,11 @@ static gx_status replay_volume(AdamJob& J, int i, int target, float* th_out, flo
     int e0 = slot * J.ckpt_every + 1;
     if (J.tv) CK(launch_tv_scatter(V.a, J.grid[(e0 - 1) & 1], J.B, V.nblocks, c->stream));  // e0 >= 1
     size_t o = J.hv[i].off;
-    TRY(run_epochs(J, V.a, V.nblocks, e0, target + 1, target, false, res_out ? res_out + o : nullptr));
+    // a job of one volume replays through the cooperative TV kernel (its plan
+    // covers exactly this view; it computes bit for bit what the per-epoch
+    // kernel does); a view of a larger job runs one launch per epoch
+    TRY(run_epochs(J, V.a, V.nblocks, e0, target + 1, target, false, res_out ? res_out + o : nullptr,
+                   J.nvol == 1));
     CK(launch_finalize(V.a, V.a.z, th_out + o, nullptr, nullptr, J.B, V.nblocks, c->stream));
     return GX_OK;
 }
