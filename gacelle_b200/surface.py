@@ -36,14 +36,19 @@ def read_surf(path):
     if magic != TRIANGLE_MAGIC:
         raise GacelleError(GX_EUNSUPPORTED, f"{path}: only FreeSurfer triangle surfaces are read "
                                             f"(magic {magic:#x})")
-    # creation line, then an empty line
-    p = raw.index(b"\n", 3) + 1
-    p = raw.index(b"\n", p) + 1
-    nv, nf = np.frombuffer(raw, dtype=">i4", count=2, offset=p)
-    p += 8
-    v = np.frombuffer(raw, dtype=">f4", count=3 * int(nv), offset=p).reshape(-1, 3)
-    p += 12 * int(nv)
-    f = np.frombuffer(raw, dtype=">i4", count=3 * int(nf), offset=p).reshape(-1, 3)
+    try:
+        # creation line, then an empty line
+        p = raw.index(b"\n", 3) + 1
+        p = raw.index(b"\n", p) + 1
+        nv, nf = (int(x) for x in np.frombuffer(raw, dtype=">i4", count=2, offset=p))
+        p += 8
+        v = np.frombuffer(raw, dtype=">f4", count=3 * nv, offset=p).reshape(-1, 3)
+        p += 12 * nv
+        f = np.frombuffer(raw, dtype=">i4", count=3 * nf, offset=p).reshape(-1, 3)
+    except ValueError as exc:
+        raise GacelleError(GX_EINVAL, f"{path}: truncated FreeSurfer surface file ({exc})") from None
+    if f.size and (f.min() < 0 or f.max() >= nv):
+        raise GacelleError(GX_EINVAL, f"{path}: face vertex index outside [0, {nv})")
     return v.astype(np.float64), f.astype(np.int64)
 
 

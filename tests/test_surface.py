@@ -56,8 +56,14 @@ def test_read_write_surf_roundtrip(tmp_path):
     v2, f2 = read_surf(p)
     np.testing.assert_array_equal(v2, v.astype(np.float32))
     np.testing.assert_array_equal(f2, f)
-    with open(p, "r+b") as fh:
-        fh.write(b"\xff\xff\xff")                     # quad-file magic
+    with open(p, "rb") as fh:
+        raw = fh.read()
+    with open(p, "wb") as fh:
+        fh.write(raw[:-10])                              # truncated
+    with pytest.raises(GacelleError):
+        read_surf(p)
+    with open(p, "wb") as fh:
+        fh.write(b"\xff\xff\xff" + raw[3:])             # quad-file magic
     with pytest.raises(GacelleError):
         read_surf(p)
 
