@@ -439,8 +439,9 @@ static bool copy_kind_host(int mem) { return mem == GX_MEM_HOST; }
 static gx_status upload_rows(gx_context* c, float* dst, size_t stride, size_t off, const float* src,
                              int rows, int n, int mem, long long* bytes) {
     cudaMemcpyKind kind = copy_kind_host(mem) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-    for (int r = 0; r < rows; ++r)
-        CK(cudaMemcpyAsync(dst + (size_t)r * stride + off, src + (size_t)r * n, sizeof(float) * n, kind, c->stream));
+    if (rows > 0 && n > 0)  // one strided copy of the whole matrix
+        CK(cudaMemcpy2DAsync(dst + off, sizeof(float) * stride, src, sizeof(float) * n, sizeof(float) * n, rows,
+                             kind, c->stream));
     if (copy_kind_host(mem)) *bytes += (long long)rows * n * sizeof(float);
     return GX_OK;
 }
@@ -449,8 +450,9 @@ static gx_status download_rows(gx_context* c, float* dst, const float* src, size
                                int rows, int n, int mem, long long* bytes) {
     if (!dst) return GX_OK;
     cudaMemcpyKind kind = copy_kind_host(mem) ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-    for (int r = 0; r < rows; ++r)
-        CK(cudaMemcpyAsync(dst + (size_t)r * n, src + (size_t)r * stride + off, sizeof(float) * n, kind, c->stream));
+    if (rows > 0 && n > 0)
+        CK(cudaMemcpy2DAsync(dst, sizeof(float) * n, src + off, sizeof(float) * stride, sizeof(float) * n, rows,
+                             kind, c->stream));
     if (copy_kind_host(mem)) *bytes += (long long)rows * n * sizeof(float);
     return GX_OK;
 }
