@@ -1040,3 +1040,58 @@ def test_r2s_estimate_in_segments(ctx):
     np.testing.assert_array_equal(seg["final"]["M0"], byhand["final"]["M0"] * scale)
     assert seg["final"]["loss"].shape == (2,) and np.array_equal(seg["mask"], m2)
     assert np.isscalar(whole["final"]["loss"]) or np.ndim(whole["final"]["loss"]) == 0
+
+
+@pytest.mark.parametrize("kind", ["prior", "surface"])
+def test_device_resident_prior_and_surface_match_host_call(ctx, kind):
+    """The prior's mu / SD rows and the surface TV's neighbour / length rows
+    given as device pointers (GX_MEM_DEVICE) give the same fit as the host
+    buffers: identical final and minimum-loss maps."""
+    import ctypes as C
+    import torch
+    from gacelle_b200.models import _GxModelHandle
+    if kind == "prior":
+        y, th0, _, mu, sd, f = _prior_case("nexi", 512, 90, crossing=False)
+        kw = dict(prior=(mu, sd, 0.5))
+        dims, gidx = (y.shape[1], 1, 1), np.arange(y.shape[1], dtype=np.int32)
+    else:
+        neighbours, edge, mask, idx, y, th0, _, tables, f = _surface_case(91)
+        kw = dict(surface=tables)
+        dims, gidx = mask.shape, idx.astype(np.int32)
+    f = dict(f, iteration=120)
+    ref = run_engine("nexi", y, th0, f, NAMES["nexi"], dims=dims, gidx=gidx, **kw)
+    lb, ub = bounds("nexi")
+    opts = gx_askadam.build_opts(f, NAMES["nexi"], lb, ub, "fused")
+    gxm, _ = models("nexi")
+    dev = torch.device("cuda", 0)
+    fp = lambda t: C.cast(C.c_void_p(t.data_ptr()), _lib._fp)  # noqa: E731
+    ip = lambda t: C.cast(C.c_void_p(t.data_ptr()), _lib._i32p)  # noqa: E731
+    nm, n = y.shape
+    d = {"y": torch.from_numpy(np.ascontiguousarray(y, np.float32)).to(dev),
+         "th0": torch.from_numpy(np.ascontiguousarray(th0, np.float32)).to(dev),
+         "gidx": torch.from_numpy(gidx).to(dev)}
+    v = _lib.GxVolume()
+    for i in range(3):
+        v.dims[i] = dims[i]
+    v.nvox = n
+    v.grid_index = ip(d["gidx"])
+    v.data = fp(d["y"])
+    v.theta0 = fp(d["th0"])
+    if kind == "prior":
+        d["mu"] = torch.from_numpy(np.ascontiguousarray(mu)).to(dev)
+        d["sd"] = torch.from_numpy(np.ascontiguousarray(sd)).to(dev)
+        v.prior_mu, v.prior_sd, v.prior_offset = fp(d["mu"]), fp(d["sd"]), 0.5
+    else:
+        d["nb"] = torch.from_numpy(np.ascontiguousarray(tables[0], np.int32)).to(dev)
+        d["len"] = torch.from_numpy(np.ascontiguousarray(tables[1], np.float32)).to(dev)
+        v.max_neighbours, v.neighbours, v.edge_length = tables[0].shape[0], ip(d["nb"]), fp(d["len"])
+    d_out = torch.full((2, 4, n), float("nan"), dtype=torch.float32, device=dev)
+    r = _lib.GxAskadamResult()
+    r.final_theta = fp(d_out[0])
+    r.min_theta = fp(d_out[1])
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(gxm.s), _lib.MEM_DEVICE, C.byref(v), 1, C.byref(opts),
+                                     C.byref(r)))
+    out = d_out.cpu().numpy()
+    np.testing.assert_array_equal(out[0], ref["final_theta"])
+    np.testing.assert_array_equal(out[1], ref["min_theta"])
