@@ -247,6 +247,7 @@ class gpuR2starMapping(_ModelBase):
         data = np.asarray(data)
         if mask is None:
             mask = np.ones(utils.dims3(data), dtype=bool)
+        extraData = self._with_b1(extraData)
         fitting = self.check_set_default(fitting)
         self.updateProperty(fitting)
         fitting["modelParams"] = list(self.modelParams)
@@ -340,11 +341,36 @@ class gpuJointR1R2starMapping(_ModelBase):
     def _gx_model(self):
         return _GxModelHandle(_lib.MODEL_R1R2S, te=self.te, fa_deg=self.fa, tr=self.tr)
 
+    def _with_b1(self, extraData):
+        """extraData with ``b1`` for the engine.  The reference takes the
+        flip angles as extraData.trueFlipAngle [..., 1, Nfa] in radians when
+        given, else b1 x the nominal angles (R1R2s/gpuJointR1R2starMapping.m:
+        387-391).  The engine scales the nominal angles by one b1 per voxel,
+        so trueFlipAngle becomes b1 = trueFlipAngle / nominal when that ratio
+        is the same for every flip angle (to 1e-6); otherwise it is rejected."""
+        if extraData is None or "trueFlipAngle" not in extraData:
+            return extraData
+        tfa = np.asarray(extraData["trueFlipAngle"], dtype=np.float64)
+        nfa = self.fa.size
+        if tfa.shape[-1] != nfa:
+            raise GacelleError(GX_EINVAL, f"extraData.trueFlipAngle needs {nfa} flip angles along its last axis")
+        ratio = tfa / np.deg2rad(self.fa)
+        b1 = ratio[..., :1]
+        if np.any(np.abs(ratio - b1) > 1e-6 * np.maximum(np.abs(b1), 1e-30)):
+            raise GacelleError(GX_EUNSUPPORTED, "extraData.trueFlipAngle with a flip-angle-dependent scale: the "
+                                                "engine takes one b1 per voxel")
+        b1 = b1[..., 0]
+        while b1.ndim > 3 and b1.shape[-1] == 1:   # the singleton TE axis of [x,y,z,1,Nfa]
+            b1 = b1[..., 0]
+        ex = dict(extraData)
+        del ex["trueFlipAngle"]
+        ex["b1"] = b1
+        return ex
+
     def FWD(self, pars, extraData=None, solver=None, fitting=None):
         """R1R2s/gpuJointR1R2starMapping.m:375-422 (measurements TE fastest, then FA)."""
         b1 = None
-        if extraData is not None and "trueFlipAngle" in extraData:
-            raise GacelleError(GX_EUNSUPPORTED, "extraData.trueFlipAngle: pass b1 instead")
+        extraData = self._with_b1(extraData)
         if extraData is not None and "b1" in extraData:
             b1 = extraData["b1"]
         return self._fwd_struct(pars, ["M0", "R1", "R2star"], b1)
@@ -365,6 +391,7 @@ class gpuJointR1R2starMapping(_ModelBase):
         data = np.asarray(data)
         if mask is None:
             mask = np.ones(utils.dims3(data), dtype=bool)
+        extraData = self._with_b1(extraData)
         fitting = self.check_set_default(fitting)
         self.updateProperty(fitting)
         fitting["modelParams"] = list(self.modelParams)
@@ -384,6 +411,7 @@ class gpuJointR1R2starMapping(_ModelBase):
         return self._solve(data, mask, None, pars0, fitting, extradata=extraData)
 
     def _b1(self, extraData, d3):
+        extraData = self._with_b1(extraData)
         if extraData is not None and "b1" in extraData and extraData["b1"] is not None:
             return np.asarray(extraData["b1"], dtype=np.float64).reshape(d3)
         return np.ones(d3)

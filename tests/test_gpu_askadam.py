@@ -1095,3 +1095,34 @@ def test_device_resident_prior_and_surface_match_host_call(ctx, kind):
     out = d_out.cpu().numpy()
     np.testing.assert_array_equal(out[0], ref["final_theta"])
     np.testing.assert_array_equal(out[1], ref["min_theta"])
+
+
+def test_r1r2s_fwd_and_fit_with_true_flip_angle(ctx):
+    """gpuJointR1R2starMapping.FWD / fit with extraData.trueFlipAngle
+    ([x,y,z,1,Nfa], radians): the same signal and fit as extraData.b1 with
+    trueFlipAngle = b1 x the nominal angles; the signal matches the FP64
+    oracle at those angles."""
+    from gacelle_b200 import models, phantoms
+    rng = np.random.default_rng(92)
+    shape = (6, 5, 4)
+    m = models.gpuJointR1R2starMapping(phantoms.R1R2S_TE, phantoms.R1R2S_TR, phantoms.R1R2S_FA)
+    m.context = ctx
+    pars = {"M0": rng.uniform(0.5, 1.5, shape), "R1": rng.uniform(0.5, 1.5, shape),
+            "R2star": rng.uniform(10, 50, shape)}
+    b1 = rng.uniform(0.8, 1.2, shape)
+    tfa = b1[..., None, None] * np.deg2rad(phantoms.R1R2S_FA)
+    s_t = m.FWD(pars, {"trueFlipAngle": tfa})
+    s_b = m.FWD(pars, {"b1": b1})
+    np.testing.assert_array_equal(s_t, s_b)
+    th = np.stack([pars[k].ravel(order="F") for k in ("M0", "R1", "R2star")])
+    ref = oracle.forward(oracle.r1r2s(phantoms.R1R2S_TE, phantoms.R1R2S_FA, phantoms.R1R2S_TR), th,
+                         b1.ravel(order="F"))
+    np.testing.assert_allclose(s_t.reshape(-1, s_t.shape[-1], order="F").T, ref, rtol=2e-5, atol=1e-7)
+    data = (s_b + 0.002 * rng.standard_normal(s_b.shape)).astype(np.float32)
+    f = {"iteration": 100, "lossFunction": "mse", "tol": 0.0, "patienceConvergence": float("inf"),
+         "convergenceStepTol": 0.0, "convergenceGradTol": 0.0}
+    mask = np.ones(shape, bool)
+    a = m.fit(data, mask, dict(f), {"trueFlipAngle": tfa})
+    b = m.fit(data, mask, dict(f), {"b1": b1})
+    for k in ("M0", "R1", "R2star"):
+        np.testing.assert_array_equal(a["final"][k], b["final"][k])

@@ -198,3 +198,25 @@ def test_save_output_writes_a_mat_file(tmp_path):
     np.testing.assert_allclose(m.lossHistory, out["lossHistory"])
     assert not askadam.save_askadam_output([], out) and not mcmc.save_mcmc_output("", out)
     assert mcmc.save_mcmc_output(str(tmp_path / "m.mat"), {"mean": {"R2star": np.ones(4)}})
+
+
+def test_r1r2s_true_flip_angle_becomes_b1():
+    """extraData.trueFlipAngle (R1R2s/gpuJointR1R2starMapping.m:387-391),
+    [x,y,z,1,Nfa] in radians: a per-voxel scale of the nominal angles becomes
+    b1; a scale that differs between flip angles is rejected."""
+    from gacelle_b200 import GacelleError, gpuJointR1R2starMapping
+    m = gpuJointR1R2starMapping(np.linspace(2, 40, 12) * 1e-3, 0.03, [5.0, 20.0])
+    b1 = np.random.default_rng(0).uniform(0.8, 1.2, (3, 4, 2))
+    tfa = b1[..., None, None] * np.deg2rad([5.0, 20.0])
+    ex = m._with_b1({"trueFlipAngle": tfa, "other": 1})
+    np.testing.assert_allclose(ex["b1"], b1, rtol=1e-12)
+    assert "trueFlipAngle" not in ex and ex["other"] == 1
+    row = m._with_b1({"trueFlipAngle": b1.reshape(1, -1, 1) * np.deg2rad([5.0, 20.0])})
+    np.testing.assert_allclose(row["b1"], b1.reshape(1, -1), rtol=1e-12)
+    bad = tfa.copy()
+    bad[0, 0, 0, 0, 1] *= 1.01
+    with pytest.raises(GacelleError):
+        m._with_b1({"trueFlipAngle": bad})
+    with pytest.raises(GacelleError):
+        m._with_b1({"trueFlipAngle": tfa[..., :1]})
+    assert m._with_b1({"b1": b1})["b1"] is b1 and m._with_b1(None) is None
