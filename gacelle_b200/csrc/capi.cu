@@ -404,8 +404,6 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
     const bool prior = reg && o->reg_type == GX_REG_PRIOR;
     const bool surf = reg && o->reg_type == GX_REG_SURFACE_TV;
     const bool tv = reg && !prior && !surf;
-    if (prior && o->robust_convergence)
-        return fail(GX_EUNSUPPORTED, "robustConvergence with the prior regulariser");
     if (tv)
         for (int d = 0; d < (o->tv_3d ? 3 : 2); ++d)
             if (!(o->voxel_size[d] > 0)) return fail(GX_EINVAL, "voxel_size must be positive");

@@ -1126,3 +1126,31 @@ def test_r1r2s_fwd_and_fit_with_true_flip_angle(ctx):
     b = m.fit(data, mask, dict(f), {"b1": b1})
     for k in ("M0", "R1", "R2star"):
         np.testing.assert_array_equal(a["final"][k], b["final"][k])
+
+
+def test_robust_convergence_with_prior_matches_oracle(ctx):
+    """robustConvergence together with the prior regulariser (both on the
+    op-by-op path): the flagged voxels equal the FP64 oracle's and the maps
+    stay within the FP32-state band (L1 loss; the prior means lie above ub,
+    so their z-scores never change sign)."""
+    import test_oracle
+    om, y, th0, out = test_oracle._robust_problem(n_out=20, seed=62)
+    y32, th0 = y.astype(np.float32), th0.astype(np.float32)
+    n = y.shape[1]
+    mu = np.vstack([np.full(n, 3.0), np.full(n, 250.0)]).astype(np.float32)
+    sd = np.vstack([np.full(n, 0.5), np.full(n, 50.0)]).astype(np.float32)
+    f = fitting(iteration=300, lossFunction="l1", regularisationType="prior",
+                **{"lambda": [1e-4, 1e-4], "regmap": ["M0", "R2star"]})
+    fr = dict(f, robustConvergence=True)
+    pr = (mu, sd, 0.0)
+    eng = run_engine("r2s", y32, th0, fr, NAMES["r2s"], prior=pr)
+    orc = run_oracle("r2s", y32, th0, fr, NAMES["r2s"], prior=pr)
+    o32 = run_oracle("r2s", y32, th0, dict(fr, _state_f32=True), NAMES["r2s"], prior=pr)
+    plain = run_engine("r2s", y32, th0, f, NAMES["r2s"], path="plain", prior=pr)
+    changed = np.flatnonzero(np.any(eng["final_theta"] != plain["final_theta"], axis=0))
+    np.testing.assert_array_equal(changed, np.flatnonzero(orc["ever_flagged"]))
+    assert orc["ever_flagged"].sum() >= 3
+    for k in range(2):
+        band = rel_rmse(o32["final"][k], orc["final"][k])
+        assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 2 * band + 1e-4, (k, band)
+    assert abs(eng["final_loss_reg"] - orc["final_reg"]) <= 1e-4 * orc["final_reg"]
