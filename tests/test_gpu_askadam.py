@@ -1154,3 +1154,74 @@ def test_robust_convergence_with_prior_matches_oracle(ctx):
         band = rel_rmse(o32["final"][k], orc["final"][k])
         assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 2 * band + 1e-4, (k, band)
     assert abs(eng["final_loss_reg"] - orc["final_reg"]) <= 1e-4 * orc["final_reg"]
+
+
+def _fit_batch_nexi(ctx, vols, f):
+    """One gx_askadam call of the NEXI model over several volumes, each a dict
+    with y, th0, dims, gidx and either prior (mu, sd, offset) or surface
+    (neighbours, lengths) rows; per volume the final parameters and loss."""
+    import ctypes as C
+    gxm, _ = models("nexi")
+    lb, ub = bounds("nexi")
+    opts = gx_askadam.build_opts(f, NAMES["nexi"], lb, ub, "fused")
+    keep, outs = [], []
+    cv = (_lib.GxVolume * len(vols))()
+    cr = (_lib.GxAskadamResult * len(vols))()
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        return a
+
+    for i, v in enumerate(vols):
+        n = v["y"].shape[1]
+        for d in range(3):
+            cv[i].dims[d] = v["dims"][d]
+        cv[i].nvox = n
+        cv[i].data = arr(v["y"], np.float32).ctypes.data_as(_lib._fp)
+        cv[i].theta0 = arr(v["th0"], np.float32).ctypes.data_as(_lib._fp)
+        cv[i].grid_index = arr(v["gidx"], np.int32).ctypes.data_as(_lib._i32p)
+        if "prior" in v:
+            cv[i].prior_mu = arr(v["prior"][0], np.float32).ctypes.data_as(_lib._fp)
+            cv[i].prior_sd = arr(v["prior"][1], np.float32).ctypes.data_as(_lib._fp)
+            cv[i].prior_offset = v["prior"][2]
+        if "surface" in v:
+            nb = arr(v["surface"][0], np.int32)
+            cv[i].max_neighbours = nb.shape[0]
+            cv[i].neighbours = nb.ctypes.data_as(_lib._i32p)
+            cv[i].edge_length = arr(v["surface"][1], np.float32).ctypes.data_as(_lib._fp)
+        o = {"final_theta": np.zeros((4, n), np.float32)}
+        cr[i].final_theta = o["final_theta"].ctypes.data_as(_lib._fp)
+        outs.append(o)
+    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, cv, len(vols), C.byref(opts), cr))
+    for o, r in zip(outs, cr):
+        o["final_loss"], o["final_loss_reg"] = r.final_loss, r.final_loss_reg
+    return outs
+
+
+@pytest.mark.parametrize("kind", ["prior", "surface"])
+def test_batch_with_prior_or_surface_tv_equals_separate_fits(ctx, kind):
+    """Two volumes in one call with the prior regulariser (per-volume mu / SD
+    rows and grid offset) or the surface TV (per-volume neighbour tables of
+    different widths: the narrower one is padded with its own index) give
+    each volume the fit of a call that fits it alone."""
+    vols = []
+    for seed in (93, 94):
+        if kind == "prior":
+            y, th0, _, mu, sd, f = _prior_case("nexi", 320 + 64 * (seed - 93), seed, crossing=False)
+            n = y.shape[1]
+            vols.append({"y": y, "th0": th0, "dims": (n, 1, 1), "gidx": np.arange(n), "prior": (mu, sd, 0.25 * seed)})
+        else:
+            neighbours, edge, mask, idx, y, th0, _, tables, f = _surface_case(seed)
+            nb, ln = tables
+            if seed == 94:  # one more (padding) slot than the other volume
+                nb = np.vstack([nb, idx[None, :].astype(np.int32)])
+                ln = np.vstack([ln, np.full((1, ln.shape[1]), 1e6, np.float32)])
+            vols.append({"y": y, "th0": th0, "dims": mask.shape, "gidx": idx, "surface": (nb, ln)})
+    f = dict(f, iteration=120)
+    both = _fit_batch_nexi(ctx, vols, f)
+    for v, b in zip(vols, both):
+        a = _fit_batch_nexi(ctx, [v], f)[0]
+        for k in range(4):
+            assert rel_rmse(b["final_theta"][k], a["final_theta"][k]) <= 1e-5, k
+        assert abs(b["final_loss_reg"] - a["final_loss_reg"]) <= 1e-6 * abs(a["final_loss_reg"])
