@@ -991,6 +991,10 @@ class gpuNEXIrice(gpuNEXI):
         if extraData is None or "sigma" not in extraData:
             raise GacelleError(GX_EINVAL, "gpuNEXIrice.fit needs extraData['sigma']")
         fitting = self.check_set_default(fitting)
+        # the reference calls askadam with its FWD alone (NEXI/gpuNEXIrice.m:303):
+        # volumetric data and the default spatial TV, whatever else is set
+        fitting["regularisationType"] = "TV"
+        fitting["dataType"] = "volumetric"
         if mask is None:
             mask = np.ones(utils.dims3(np.asarray(dwi)), dtype=bool)
         start = fitting.get("start")
