@@ -247,7 +247,6 @@ class gpuR2starMapping(_ModelBase):
         data = np.asarray(data)
         if mask is None:
             mask = np.ones(utils.dims3(data), dtype=bool)
-        extraData = self._with_b1(extraData)
         fitting = self.check_set_default(fitting)
         self.updateProperty(fitting)
         fitting["modelParams"] = list(self.modelParams)
