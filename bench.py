@@ -439,6 +439,7 @@ def extras(ctx, W, opts, model, stream, args):
     out["mcmc_ms_per_step"] = t["main_kernel_ms"] / steps
     out.update(extra_r1r2s_batch(ctx, args))
     out.update(extra_nexi_rician(ctx, args))
+    out.update(extra_nexi_surface(ctx, args))
     return out
 
 
@@ -543,6 +544,64 @@ def extra_nexi_rician(ctx, args):
     r["dictionary_ms"] = t["main_kernel_ms"]
     r["dictionary_pairs_per_s"] = nv * x_train.shape[1] / (t["main_kernel_ms"] / 1000.0)
     return r
+
+
+def extra_nexi_surface(ctx, args):
+    """NEXI fits on cortical-surface data at fsaverage scale: two hemisphere
+    meshes of 405 x 405 vertices (164,025 each; a triangulated sheet stands in
+    for the subject's surface), 24 shells, Nx 14, MSE, the same start and
+    iteration count three times: no regulariser, surface TV on fa (mesh
+    neighbour tables, one launch per epoch) and the prior distribution on fa
+    and ra (fused).  Reports each fit's voxel-iterations/s."""
+    from gacelle_b200 import askadam_solver as gxa
+    from gacelle_b200 import phantoms, surface, utils
+    from gacelle_b200.models import _GxModelHandle
+    _lib = _lib_mod()
+    side, iters = 405, args.c3_iters // 5
+    nvh = side * side
+    idx = np.arange(side * side).reshape(side, side)
+    faces = np.concatenate([np.stack([idx[:-1, :-1], idx[1:, :-1], idx[1:, 1:]], -1).reshape(-1, 3),
+                            np.stack([idx[:-1, :-1], idx[1:, 1:], idx[:-1, 1:]], -1).reshape(-1, 3)])
+    nb, _ = surface.mesh_neighbours(faces, nvh)
+    nbs = np.concatenate([nb, nb + nvh]).T                                   # [maxnb][2 nvh], grid indices
+    lens = np.where(nbs == np.arange(2 * nvh)[None, :], 1e6, 1.0).astype(np.float32)  # edge lengths 1
+    nv = 2 * nvh
+    y, gt = phantoms.nexi_volume(nv, 1006, sigma=0.02, rician=False, nx=14)
+    b, d = phantoms.nexi_shells()
+    model = _GxModelHandle(_lib.MODEL_NEXI, bval=b, delta=d, lmax=0, nx=14)
+    lb, ub = [2.2e-16, 2.2e-16, 2.2e-16, 1 / 250], [1.0, 3.0, 3.0, 1.0]
+    th0 = np.ascontiguousarray(np.tile(np.array([[0.4], [2.0], [1.0], [0.05]], np.float32), (1, nv)))
+    y = np.ascontiguousarray(y, np.float32)
+    gidx = np.arange(nv, dtype=np.int32)
+    nbs = np.ascontiguousarray(nbs, np.int32)
+    mu = np.ascontiguousarray(np.vstack([gt["fa"], gt["ra"]]), np.float32)
+    sd = np.ascontiguousarray(np.vstack([np.full(nv, 0.1), np.full(nv, 0.02)]), np.float32)
+    out = {"surface_workload": f"NEXI lmax 0, MSE, Nx 14, 24 shells, 2 x {nvh} surface vertices, {iters} iterations"}
+    for tag, reg in (("none", {}), ("surface_tv", {"lambda": [1e-3], "regmap": ["fa"], "dataType": "surface"}),
+                     ("prior", {"lambda": [1e-3, 1e-3], "regmap": ["fa", "ra"], "regularisationType": "prior"})):
+        f = gxa.check_set_default_basic(dict({"iteration": iters, "initialLearnRate": 0.01, "lossFunction": "mse",
+                                              "tol": 0.0, "patienceConvergence": float("inf"),
+                                              "convergenceStepTol": 0.0, "convergenceGradTol": 0.0}, **reg))
+        opts = gxa.build_opts(f, ["fa", "Da", "De", "ra"], lb, ub, "fused")
+        vol = _gx_volume(y, th0)
+        vol.dims[0], vol.dims[1], vol.dims[2] = 1, nvh, 2
+        vol.grid_index = gidx.ctypes.data_as(_lib._i32p)
+        if tag == "surface_tv":
+            vol.max_neighbours = nbs.shape[0]
+            vol.neighbours = nbs.ctypes.data_as(_lib._i32p)
+            vol.edge_length = lens.ctypes.data_as(_lib._fp)
+        if tag == "prior":
+            vol.prior_mu = mu.ctypes.data_as(_lib._fp)
+            vol.prior_sd = sd.ctypes.data_as(_lib._fp)
+        th = np.zeros((4, nv), np.float32)
+        res = _lib.GxAskadamResult()
+        res.final_theta = th.ctypes.data_as(_lib._fp)
+        _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, C.byref(vol), 1,
+                                         C.byref(opts), C.byref(res)))
+        t = ctx.timing()
+        out[f"surface_{tag}_voxel_iterations_per_s"] = nv * iters / (t["main_kernel_ms"] / 1000.0)
+        out[f"surface_{tag}_ms_per_iteration"] = t["main_kernel_ms"] / iters
+    return out
 
 
 def main():
