@@ -16,8 +16,10 @@ is the spherical mean.  The norm over m does not depend on which orthonormal
 real basis spans degree l, so the basis here is built from its own
 associated-Legendre recursion.
 
-Everything is float64 numpy on the host: a one-off pass over the input, not
-part of the iterated fit.  Images follow MATLAB's column-major voxel order.
+Everything is numpy on the host, in the input's float type (float32 stays
+float32, as MATLAB keeps single data single): a one-off pass over the input,
+not part of the iterated fit.  Images follow MATLAB's column-major voxel
+order.
 """
 from __future__ import annotations
 
@@ -40,8 +42,12 @@ def _as_vec(v, n, empty_value):
 
 
 def _vox_by_vol(dwi):
-    """[x, y, z, vol] -> ([Nvox, vol] in column-major voxel order, dims)."""
-    dwi = np.asarray(dwi, dtype=np.float64)
+    """[x, y, z, vol] -> ([Nvox, vol] in column-major voxel order, dims); a
+    float32 or float64 input keeps its type (MATLAB computes in the input's
+    class), anything else becomes float64."""
+    dwi = np.asarray(dwi)
+    if dwi.dtype not in (np.float32, np.float64):
+        dwi = dwi.astype(np.float64)
     if dwi.ndim < 4:
         dwi = dwi.reshape(dwi.shape + (1,) * (4 - dwi.ndim))
     dims = dwi.shape[:3]
@@ -171,13 +177,17 @@ class DWIutility:
         [Ndir, 3] directions; returns [lmax/2+1, Nvox] invariants S_0, S_2, ...
         The least-squares fit is the pseudo-inverse (leastSquaresSHT.m:33,
         unweighted) of the basis up to ``lmax`` at the doubled directions."""
-        S = np.asarray(S, dtype=np.float64)
+        S = np.asarray(S)
+        if S.dtype not in (np.float32, np.float64):
+            S = S.astype(np.float64)
         g = np.asarray(g, dtype=np.float64)
-        S2 = np.concatenate([S, S], axis=0)
+        n = g.shape[0]
         g2 = np.concatenate([g, -g], axis=0)
         Y = self.getSH(int(lmax), self.cart2sph_incl(g2))
-        F = np.linalg.pinv(Y) @ S2
-        out = np.zeros((int(lmax) // 2 + 1, S.shape[1]))
+        P = np.linalg.pinv(Y)
+        # the samples are doubled ([S; S]), so P [S; S] = (P[:, :n] + P[:, n:]) S
+        F = (P[:, :n] + P[:, n:]).astype(S.dtype) @ S
+        out = np.zeros((int(lmax) // 2 + 1, S.shape[1]), dtype=S.dtype)
         for l in range(0, int(lmax) + 1, 2):
             out[l // 2] = np.sqrt(np.sum(F[l * l:(l + 1) ** 2] ** 2, axis=0)) / math.sqrt(4 * math.pi * (2 * l + 1))
         return out
@@ -203,7 +213,7 @@ class DWIutility:
         bu = np.unique(bval)
         bu = bu[bu != 0]
         nsh = int(lmax) // 2 + 1
-        out = np.zeros((flat.shape[0], nsh * bu.size))
+        out = np.zeros((flat.shape[0], nsh * bu.size), dtype=flat.dtype)
         with np.errstate(divide="ignore", invalid="ignore"):
             for k, b in enumerate(bu):
                 ind = bval == b
@@ -219,7 +229,7 @@ class DWIutility:
         g = self._bvec_rows(bvec)
         bu = np.unique(bval)
         nsh = int(lmax) // 2 + 1
-        out = np.zeros((flat.shape[0], nsh * bu.size))
+        out = np.zeros((flat.shape[0], nsh * bu.size), dtype=flat.dtype)
         for k, b in enumerate(bu):
             ind = bval == b
             out[:, k::bu.size] = self.SHrotinv(flat[:, ind].T, g[ind], lmax).T
@@ -275,7 +285,7 @@ class DWIutility:
             it = te == tv
             ib0 = it & (bval == 0)
             if ib0.any():
-                blk = np.zeros((flat.shape[0], nsh, 1))
+                blk = np.zeros((flat.shape[0], nsh, 1), dtype=flat.dtype)
                 blk[:, 0, 0] = flat[:, ib0].mean(axis=1)
                 blocks.append(blk)
                 b_out.append(0.0)

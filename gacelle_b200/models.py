@@ -42,6 +42,12 @@ def _rescale_m0(out, fitting, scale):
             out[k]["M0"] = out[k]["M0"] * scale
 
 
+def _float_data(a):
+    """float32 / float64 arrays as they are; anything else as float64."""
+    a = np.asarray(a)
+    return a if a.dtype in (np.float32, np.float64) else a.astype(np.float64)
+
+
 def _save(fitting, out):
     """The end of every model's estimate(): askadam.save_askadam_output or
     mcmc.save_mcmc_output of fitting.outputFilename (e.g.
@@ -683,7 +689,7 @@ class gpuNEXI(_ModelBase):
         below 0.01, whose S_0 decay correlates below 0.1 with the median
         decay of the voxels that passed the two tests (a flat decay counts as
         0), or that hold NaN/Inf (set to 0 in the returned data)."""
-        data = np.asarray(data, dtype=np.float64)
+        data = _float_data(data)  # single stays single, as in the reference
         mask = np.asarray(mask) > 0
         ex = dict(extradata or {})
         surface = fitting is not None and str(fitting.get("dataType", "volumetric")).lower() == "surface"
@@ -917,7 +923,7 @@ class gpuNEXIrice(gpuNEXI):
         normalised by the mean b0 signal and floored at epsilon; voxels with
         NaN/Inf, a signal above 1.01, sigma > 1 (SNR < 1) or a signal whose
         correlation with the mean signal shape is below 0.1 leave the mask."""
-        dwi = np.asarray(dwi, dtype=np.float64)
+        dwi = _float_data(dwi)  # single stays single, as in the reference
         mask = np.asarray(mask) > 0
         ex = dict(extradata)
         bval = np.asarray(ex.get("bval", np.ones(dwi.shape[-1])), dtype=np.float64).ravel()
