@@ -86,10 +86,13 @@ def _slab(a, sl):
 
 
 def restore_segments(parts: list[dict], segs: list[dict], shape3) -> dict:
-    """restore_segment_structure (utils/utils.m:1348-1470) over whole segments:
-    arrays whose third dimension spans a segment's fitted slices contribute
-    their owned slices at the owned positions; scalars become one value per
-    segment; other values are kept from the first segment."""
+    """restore_segment_structure / restore_field (utils/utils.m:1348-1484)
+    over whole segments: arrays whose third dimension spans a segment's
+    fitted slices contribute their owned slices at the owned positions;
+    scalars become one value per segment; voxel-indexed matrices [Nm, Nv]
+    (second dimension above 1) are concatenated along voxels, vectors along
+    their length and 3-D arrays with equal trailing dimensions along the
+    first; anything else is kept from the first segment."""
     def merge(vals, path):
         first = vals[0]
         if isinstance(first, dict):
@@ -104,6 +107,13 @@ def restore_segments(parts: list[dict], segs: list[dict], shape3) -> dict:
             for v, s in zip(vals, segs):
                 out[:, :, s["owned"], ...] = v[:, :, s["local"], ...]
             return out
+        if isinstance(first, np.ndarray) and len(vals) > 1:
+            if first.ndim == 2 and first.shape[1] > 1 and all(v.ndim == 2 for v in vals):
+                return np.concatenate(vals, axis=1)
+            if first.ndim == 1 or (first.ndim == 2 and first.shape[1] == 1):
+                return np.concatenate([np.asarray(v).reshape(-1, *first.shape[1:]) for v in vals], axis=0)
+            if first.ndim == 3 and all(v.shape[1:] == first.shape[1:] for v in vals):
+                return np.concatenate(vals, axis=0)
         return first
     return merge(parts, ())
 

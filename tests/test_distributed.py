@@ -189,6 +189,14 @@ def test_fit_segmented_slices_fits_and_restores():
         return {"final": {"x": (d[..., 0] + e["b1"] + e["mu"]["fa"] + p["fa"]) * m, "loss": float(m.sum())}}
 
     out = segments.fit_segmented(fit, data, mask, 3, 1, ex, p0)
+    # the other merge rules of restore_field (utils/utils.m:1446-1474)
+    parts = [{"res": np.full((2, 3), k), "hist": np.arange(4.0) + k, "post": np.full((2, 5, 6), k),
+              "other": np.full((2, 2, 2, 2), k)} for k in range(2)]
+    segs2 = segments.rank_segments(mask, 2, 0)
+    r = segments.restore_segments(parts, segs2, mask.shape)
+    assert r["res"].shape == (2, 6) and r["res"][0, 3] == 1         # concatenated along voxels
+    assert r["hist"].shape == (8,) and r["post"].shape == (4, 5, 6)
+    assert r["other"].max() == 0                                     # kept from the first segment
     assert len(seen) == 3 and sum(seen) == 9 + 4            # three slabs, halos on the two internal faces
     np.testing.assert_allclose(out["final"]["x"], (data[..., 0] + ex["b1"] + ex["mu"]["fa"] + p0["fa"]) * mask)
     assert out["final"]["loss"].shape == (3,)
