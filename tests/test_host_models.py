@@ -75,6 +75,14 @@ def test_r1r2s_b1_and_true_flip_angle(engine):
     np.testing.assert_allclose(a, b1.ravel(order="F"), rtol=1e-6)
     out = m.estimate(data, mask, {"iteration": 5, "start": "prior"}, {"trueFlipAngle": tfa})
     assert out["final"]["M0"].shape == (6, 5, 4) and engine[-1]["theta0"].shape == (3, 120)
+    # mcmc receives the same b1, and estimate rescales M0 in every metric
+    m2 = gpuJointR1R2starMapping(phantoms.R1R2S_TE, phantoms.R1R2S_TR, phantoms.R1R2S_FA)
+    est = m2.estimate(data, mask, {"solver": "mcmc", "iteration": 20, "algorithm": "ensemble",
+                                   "metric": ["mean", "std"]}, {"trueFlipAngle": tfa})
+    c = engine[-1]
+    assert c["kind"] == "mcmc" and c["names"] == ["M0", "R1", "R2star", "noise"]
+    np.testing.assert_allclose(np.asarray(c["b1"]).ravel(), b1.ravel(order="F"), rtol=1e-6)
+    assert est["mean"]["M0"].shape == (6, 5, 4)
 
 
 def test_nexi_paths(engine, tmp_path):
