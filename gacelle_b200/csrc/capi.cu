@@ -72,7 +72,33 @@ struct gx_context {
     void* buf[S_NSLOTS] = {};
     size_t cap[S_NSLOTS] = {};
     cudaEvent_t ev[4] = {};
+    // pinned staging of the small per-call tables, so that their copies are
+    // queued without draining the stream (every call ends with a sync, so the
+    // next call may refill it)
+    void* pin = nullptr;
+    size_t pin_cap = 0;
+    cudaEvent_t pin_ev = nullptr;  // recorded after the copies out of `pin`
 };
+
+// The context's pinned staging buffer, once the copies queued from it by an
+// earlier call (which may have failed before its final sync) have run.
+static gx_status pinned(gx_context* c, size_t bytes, void** out) {
+    if (c->pin_ev) CK(cudaEventSynchronize(c->pin_ev));
+    else CK(cudaEventCreateWithFlags(&c->pin_ev, cudaEventDisableTiming));
+    if (c->pin_cap < bytes) {
+        if (c->pin) {
+            cudaStreamSynchronize(c->stream);
+            cudaFreeHost(c->pin);
+            c->pin = nullptr;
+            c->pin_cap = 0;
+        }
+        size_t b = bytes + bytes / 8 + 256;
+        CK(cudaMallocHost(&c->pin, b));
+        c->pin_cap = b;
+    }
+    *out = c->pin;
+    return GX_OK;
+}
 
 static gx_status ws(gx_context* c, Slot s, size_t bytes, void** out) {
     if (bytes == 0) bytes = 16;
@@ -189,6 +215,8 @@ gx_status gx_context_destroy(gx_context* c) {
     cudaStreamSynchronize(c->stream);
     for (int s = 0; s < S_NSLOTS; ++s)
         if (c->buf[s]) cudaFree(c->buf[s]);
+    if (c->pin) cudaFreeHost(c->pin);
+    if (c->pin_ev) cudaEventDestroy(c->pin_ev);
     for (auto& ev : c->ev) cudaEventDestroy(ev);
     cudaStreamDestroy(c->own);
     delete c;
@@ -660,20 +688,28 @@ static gx_status adam_setup(AdamJob& J) {
     DevVol* dvols;
     TRY(wsT(c, S_BLK, J.hblk.size(), &blk));
     TRY(wsT(c, S_VOLS, 2 * J.hv.size(), &dvols));
-    std::vector<DevVol> both(J.hv);
-    for (const DevVol& d : J.hv) {
-        DevVol l = d;
-        l.off = 0;
-        both.push_back(l);
+    // block map, volume table (+ per-volume copies with off = 0) and the
+    // optimiser schedule staged in the context's pinned buffer: three queued copies
+    const size_t nblk = J.hblk.size(), nvt = 2 * J.hv.size();
+    const size_t o_vols = (sizeof(int) * nblk + 15) / 16 * 16;
+    const size_t o_sched = o_vols + (sizeof(DevVol) * nvt + 15) / 16 * 16;
+    unsigned char* stage;
+    TRY(pinned(c, o_sched + sizeof(float2) * ((size_t)N + 1), (void**)&stage));
+    memcpy(stage, J.hblk.data(), sizeof(int) * nblk);
+    DevVol* sv = reinterpret_cast<DevVol*>(stage + o_vols);
+    for (size_t i = 0; i < J.hv.size(); ++i) {
+        sv[i] = J.hv[i];
+        sv[J.hv.size() + i] = J.hv[i];
+        sv[J.hv.size() + i].off = 0;
     }
-    CK(cudaMemcpyAsync(blk, J.hblk.data(), sizeof(int) * J.hblk.size(), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(dvols, both.data(), sizeof(DevVol) * both.size(), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpyAsync(blk, stage, sizeof(int) * nblk, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dvols, sv, sizeof(DevVol) * nvt, cudaMemcpyHostToDevice, c->stream));
     J.local_vols = dvols + J.hv.size();
     a.blk_vol = blk;
     a.vols = dvols;
     // optimiser schedule per epoch (update_learn_rate :1180-1183, adamupdate bias correction)
-    std::vector<float2> sched((size_t)N + 1, float2{0.f, 0.f});
+    float2* sched = reinterpret_cast<float2*>(stage + o_sched);
+    sched[0] = float2{0.f, 0.f};
     for (int e = 1; e <= N; ++e) {
         double lr = o->initial_learn_rate / (1.0 + o->decay_rate * (e - 1));
         if (o->optimiser == GX_OPT_ADAM)
@@ -682,8 +718,9 @@ static gx_status adam_setup(AdamJob& J) {
             sched[e] = float2{(float)lr, 0.f};
     }
     float2* dsched;
-    TRY(wsT(c, S_SCHED, sched.size(), &dsched));
-    CK(cudaMemcpyAsync(dsched, sched.data(), sizeof(float2) * sched.size(), cudaMemcpyHostToDevice, c->stream));
+    TRY(wsT(c, S_SCHED, (size_t)N + 1, &dsched));
+    CK(cudaMemcpyAsync(dsched, sched, sizeof(float2) * ((size_t)N + 1), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->pin_ev, c->stream));
     a.sched = dsched;
     TRY(wsT(c, S_HIST, (size_t)J.nvol * (N + 1) * kHistW, &a.hist));
     CK(cudaMemsetAsync(a.hist, 0, sizeof(double) * J.nvol * (N + 1) * kHistW, c->stream));
