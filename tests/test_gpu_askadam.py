@@ -1225,3 +1225,45 @@ def test_batch_with_prior_or_surface_tv_equals_separate_fits(ctx, kind):
         for k in range(4):
             assert rel_rmse(b["final_theta"][k], a["final_theta"][k]) <= 1e-5, k
         assert abs(b["final_loss_reg"] - a["final_loss_reg"]) <= 1e-6 * abs(a["final_loss_reg"])
+
+
+def test_nexi_lmax2_estimate_from_full_acquisition(ctx):
+    """gpuNEXI.estimate with lmax 2 on a full acquisition: each shell's
+    directional signal Sl0 + 5 Sl2 P2(g.n) is band-limited to degree 2, so its
+    invariants are exactly (Sl0, Sl2) (the degree-2 norm of b P2(g.n) is
+    b / 5 after the 1/sqrt(4 pi 5) scaling), and the fit equals the fit of the
+    per-shell [Sl0; Sl2] signal bit for bit."""
+    from gacelle_b200 import gpuNEXI
+    rng = np.random.default_rng(95)
+    dims = (4, 4, 3)
+    n = int(np.prod(dims))
+    bs, D = [1.0, 2.5, 4.0, 6.0], 30.0
+    m = gpuNEXI(bs, [D] * 4)
+    m.context = ctx
+    th = random_theta("nexi2", n, rng)
+    pars = {k: th[i][None, :] for i, k in enumerate(["fa", "Da", "De", "ra", "p2"])}
+    sl = m.FWD(pars, 2).astype(np.float32)                                   # [8, n]: Sl0 x 4, Sl2 x 4
+    sl_img = sl.T.reshape(dims + (8,), order="F").astype(np.float64)
+    axis = np.array([0.3, -0.5, 0.81])
+    axis /= np.linalg.norm(axis)
+    vols, bval, bvec = [np.ones(dims)] * 2, [0.0, 0.0], [[0.0, 0.0, 0.0]] * 2
+    for i, b in enumerate(bs):
+        g = rng.standard_normal((30, 3))
+        g /= np.linalg.norm(g, axis=1, keepdims=True)
+        for gi in g:
+            p2 = 1.5 * float(gi @ axis) ** 2 - 0.5
+            vols.append(sl_img[..., i] + 5.0 * sl_img[..., 4 + i] * p2)
+            bval.append(b)
+            bvec.append(gi)
+    dwi = np.stack(vols, axis=-1)
+    ex = {"bval": np.array(bval), "bvec": np.array(bvec).T, "BDELTA": D}
+    f = {"iteration": 80, "start": "default", "lossFunction": "mse", "lmax": 2}
+    mask = np.ones(dims, dtype=bool)
+    full = gpuNEXI(bs, [D] * 4)
+    full.context = ctx
+    prep, valid, _ = full.prepare_dwi_data(dwi, mask, ex, 2, full.check_set_default(dict(f)))
+    assert np.array_equal(prep.astype(np.float32), sl_img.astype(np.float32))
+    out = full.estimate(dwi, mask, ex, dict(f))
+    ref = m.fit(sl_img.astype(np.float32), out["mask"], dict(f))
+    for p in ["fa", "Da", "De", "ra", "p2"]:
+        np.testing.assert_array_equal(out["final"][p], ref["final"][p])
