@@ -122,6 +122,13 @@ def test_nexi_paths(engine, tmp_path):
     n0 = len(engine)
     m.estimate(sdata, smask, ex, dict(base, dataType="surface", NSegmentUser=2, **{"lambda": [1e-3]}))
     assert len(engine) - n0 == 2 and engine[-1]["dims"] == (1, nv, 1)
+    # the prior on surface data (geometry-agnostic, NEXI/gpuNEXI.m:382-415): no mesh needed
+    smu = {"fa": np.full((1, nv, 2), 0.5)}
+    ssd = {"fa": np.full((1, nv, 2), 0.1)}
+    m.estimate(sdata, smask, {"mu": smu, "sigma": ssd},
+               dict(base, dataType="surface", regularisationType="prior", regmap=["fa"], **{"lambda": [1e-3]}))
+    c = engine[-1]
+    assert c["opts"].reg_type == _lib.REG_PRIOR and c["surface"] is None and c["prior"][0].shape == (1, 2 * nv)
 
 
 def test_nexi_rice_fit_keeps_spatial_tv(engine):
