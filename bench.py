@@ -49,6 +49,7 @@ def parse_args():
     p.add_argument("--iters", type=int, default=NITER, help="askAdam iterations per fit (profiling runs)")
     p.add_argument("--c3-iters", type=int, default=1000, help="iterations of the batched joint R1R2* side run")
     p.add_argument("--c4-iters", type=int, default=100, help="iterations of the NEXI Rician side run")
+    p.add_argument("--surf-iters", type=int, default=200, help="iterations of the cortical-surface NEXI side run")
     p.add_argument("--grid", default="128x128x64", help="phantom grid (profiling runs)")
     p.add_argument("--mcmc-steps", type=int, default=200, help="GW steps of the MCMC side measurement")
     return p.parse_args()
@@ -557,7 +558,7 @@ def extra_nexi_surface(ctx, args):
     from gacelle_b200 import phantoms, surface, utils
     from gacelle_b200.models import _GxModelHandle
     _lib = _lib_mod()
-    side, iters = 405, args.c3_iters // 5
+    side, iters = 405, args.surf_iters
     nvh = side * side
     idx = np.arange(side * side).reshape(side, side)
     faces = np.concatenate([np.stack([idx[:-1, :-1], idx[1:, :-1], idx[1:, 1:]], -1).reshape(-1, 3),
