@@ -36,6 +36,16 @@ ALG_BYTES_PER_VOXEL_ITER = 100.0   # 12 echoes x 4 B data + (z, m, v) x 2 params
 SFU_OPS_PER_VOXEL_ITER = 22.0
 FP32_FLOP_PER_VOXEL_ITER = 190.0
 METRIC = "askAdam voxel-fits/s & MCMC samples/s, fused vs plain GPU, equal FP64 error"
+WORKLOAD = ("askAdam R2* MSE + 3-D TV (lambda 1e-3 on R2*), 128x128x64 ellipsoid mask (629,432 voxels), "
+            "12 echoes TE=2:3.5:40.5 ms, Adam lr 0.01, 4000 iterations")
+
+
+def bench_config(nvox_total, world, grid="128x128x64", iters=NITER):
+    """The config object both arms print (the same workload, the same keys)."""
+    return {"workload": WORKLOAD if grid == "128x128x64" and iters == NITER else
+            f"askAdam R2* MSE + 3-D TV, grid {grid}, {iters} iterations",
+            "global_batch": nvox_total, "seq_len": iters, "parallelism": f"replicas{world}",
+            "l2": "GPU: flushed between steps (256 MB write); CPU: the working set exceeds the host caches"}
 
 
 def parse_args():
@@ -52,6 +62,10 @@ def parse_args():
     p.add_argument("--surf-iters", type=int, default=200, help="iterations of the cortical-surface NEXI side run")
     p.add_argument("--grid", default="128x128x64", help="phantom grid (profiling runs)")
     p.add_argument("--mcmc-steps", type=int, default=200, help="GW steps of the MCMC side measurement")
+    p.add_argument("--parity-iters", type=int, default=400, help="epochs of the fused/plain vs FP64 parity leg")
+    p.add_argument("--mcmc-cpu-voxels", type=int, default=256, help="voxels of the MCMC CPU baseline sample")
+    p.add_argument("--mcmc-cpu-steps", type=int, default=100, help="GW steps of the MCMC CPU baseline sample")
+    p.add_argument("--no-parity", action="store_true", help="skip the fused/plain vs FP64 parity leg")
     return p.parse_args()
 
 
@@ -71,19 +85,15 @@ def dist_setup(args):
 
 
 def workload(seed=1002, grid="128x128x64", iters=NITER):
-    from gacelle_b200 import phantoms, utils
+    from gacelle_b200 import phantoms
     dims = tuple(int(x) for x in grid.split("x"))
-    mask = phantoms.ellipsoid_mask(dims, 1.05)
-    data, _ = phantoms.r2s_phantom(mask, seed)
-    idx = utils.mask_index(mask)
-    y = utils.reshape_ND2GD(data, idx)
-    n = y.shape[1]
-    th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, n))
+    P = phantoms.r2s_tv_volume(seed, dims)
+    mask, y, idx, th0, n = P["mask"], P["y"], P["idx"], P["th0"], P["nvox"]
     fitting = {"iteration": iters, "initialLearnRate": 0.01, "decayRate": 0.0, "lossFunction": "mse",
                "tol": 0.0, "convergenceValue": 1e-6, "patienceConvergence": float("inf"),
                "convergenceStepTol": 0.0, "convergenceGradTol": 0.0, "lambda": [1e-3], "regmap": ["R2star"],
                "TVmode": "3D", "voxelSize": [2, 2, 2], "parameterTransform": "sigmoid"}
-    return {"mask": mask, "y": y, "idx": idx.astype(np.int32), "th0": th0, "fitting": fitting, "nvox": n,
+    return {"mask": mask, "y": y, "idx": idx, "th0": th0, "fitting": fitting, "nvox": n,
             "te": phantoms.R2S_TE, "lb": [0.0, 0.1], "ub": [2.0, 200.0]}
 
 
@@ -209,9 +219,7 @@ def reference_arm(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded phantom, seed 1002)",
-            "config": {"workload": "askAdam R2* MSE + 3-D TV, 128x128x64 ellipsoid mask (629,432 voxels), "
-                                   "12 echoes, 4000 iterations", "global_batch": W["nvox"], "seq_len": NITER,
-                       "parallelism": f"replicas{args.gpus}", "l2": "working set per step exceeds L2 on CPU"},
+            "config": bench_config(W["nvox"] * args.gpus, args.gpus),
             "cpu_baseline": {"value": value, "unit": "voxel-fits/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "voxel-fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -343,47 +351,50 @@ def engine_arm(args, world, rank, local):
     th = d_out[0].cpu().numpy()
     assert np.all(np.isfinite(th)) and th[1].min() >= 0.1 and th[1].max() <= 200.0
 
-    peak, peak_kind = measured_peaks()
     # one launch of the hot kernel covers iters / (launches per fit) epochs: all of them for the
     # persistent kernel, one for the per-epoch kernel (GACELLE_B200_TV_KERNEL=step)
     avg_launch_ms = main_ms / max(main_n, 1)
     launches_per_fit = main_n / args.steps
     epochs_per_launch = args.iters / max(launches_per_fit, 1.0)
     persistent = launches_per_fit < args.iters
-    kname = "tv_persistent" if persistent else "tv_step"
-    alg_bytes = ALG_BYTES_PER_VOXEL_ITER * n * epochs_per_launch
-    achieved = alg_bytes / (avg_launch_ms / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind,
-                "kernel": ("tv_persistent_kernel<MSE,12> (every epoch of the fit in one cooperative launch: "
-                           "forward, loss, adjoint, TV, Adam)") if persistent else
-                          "tv_step_kernel<R2S,MSE> (one epoch: forward, loss, adjoint, TV, Adam)",
-                "epochs_per_launch": epochs_per_launch,
-                "algorithmic_bytes_per_launch": alg_bytes,
-                "avg_launch_ms": avg_launch_ms,
-                "voxel_iterations_per_s": n * epochs_per_launch / (avg_launch_ms / 1000.0),
-                "traffic": profile_traffic(kname)}
-    # the compute roofs of the same launch (the kernel keeps its state on chip, so the HBM figure
-    # is a streaming-equivalent rate): MUFU 16 ops/clk/SM, FP32 128 FMA/clk/SM at the sampled clock
-    vit = roofline["voxel_iterations_per_s"]
+    vit = n * epochs_per_launch / (avg_launch_ms / 1000.0)   # voxel-iterations/s of the hot kernel
+    # The binding roof is the SFU (MUFU) pipe: the kernel keeps its optimiser state on chip and moves
+    # 1.5 % of a streaming implementation's bytes through DRAM, so the HBM figure below is a
+    # streaming-equivalent rate, not a bound.  SFU peak: 16 MUFU ops/clk/SM x SMs x sampled SM clock
+    # (the measured peaks file holds copy bandwidth and GEMM rates only).
     ghz = (clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0) / 1000.0
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
     sfu_peak, fp32_peak = 16 * nsm * ghz * 1e9, 2 * 128 * nsm * ghz * 1e9
-    roofline["compute"] = {"sfu_ops_per_voxel_iter": SFU_OPS_PER_VOXEL_ITER,
-                           "sfu_achieved_per_s": vit * SFU_OPS_PER_VOXEL_ITER, "sfu_peak_per_s": sfu_peak,
-                           "sfu_frac": vit * SFU_OPS_PER_VOXEL_ITER / sfu_peak,
-                           "fp32_flop_per_voxel_iter": FP32_FLOP_PER_VOXEL_ITER,
-                           "fp32_achieved_tflops": vit * FP32_FLOP_PER_VOXEL_ITER / 1e12,
-                           "fp32_peak_tflops": fp32_peak / 1e12,
-                           "fp32_frac": vit * FP32_FLOP_PER_VOXEL_ITER / fp32_peak,
-                           "peak_kind": "nominal per-SM rates x SM count x sampled SM clock"}
+    sfu_achieved = vit * SFU_OPS_PER_VOXEL_ITER
+    hbm_peak, hbm_kind = measured_peaks()
+    stream_bytes = ALG_BYTES_PER_VOXEL_ITER * n * epochs_per_launch
+    kname = "tv_persistent" if persistent else "tv_step"
+    roofline = {"bound": "sfu", "achieved": sfu_achieved / 1e9, "peak": sfu_peak / 1e9, "unit": "G MUFU op/s",
+                "frac": sfu_achieved / sfu_peak,
+                "peak_kind": "nominal 16 MUFU op/clk/SM x %d SMs x sampled %.3f GHz (no measured SFU peak)" % (nsm, ghz),
+                "traffic": profile_traffic(kname),
+                "traffic_source": f"ncu capture committed under profiles/ ({kname}_r2s_c2_traffic.json), "
+                                  "DRAM bytes read + written per launch; not measured in this run",
+                "kernel": ("tv_persistent_kernel<MSE,12> (every epoch of the fit in one cooperative launch: "
+                           "forward, loss, adjoint, TV, Adam)") if persistent else
+                          "tv_step_kernel<R2S,MSE> (one epoch: forward, loss, adjoint, TV, Adam)",
+                "units_per_launch": f"{n} voxels x {epochs_per_launch:.0f} epochs",
+                "sfu_ops_per_voxel_iter": SFU_OPS_PER_VOXEL_ITER,
+                "epochs_per_launch": epochs_per_launch,
+                "avg_launch_ms": avg_launch_ms,
+                "voxel_iterations_per_s": vit,
+                "fp32": {"flop_per_voxel_iter": FP32_FLOP_PER_VOXEL_ITER,
+                         "achieved_tflops": vit * FP32_FLOP_PER_VOXEL_ITER / 1e12,
+                         "peak_tflops": fp32_peak / 1e12, "frac": vit * FP32_FLOP_PER_VOXEL_ITER / fp32_peak},
+                "hbm_streaming_equivalent": {
+                    "bytes_per_voxel_iter": ALG_BYTES_PER_VOXEL_ITER, "bytes_per_launch": stream_bytes,
+                    "gbs": stream_bytes / (avg_launch_ms / 1000.0) / 1e9, "peak_gbs": hbm_peak,
+                    "peak_kind": hbm_kind,
+                    "note": "bytes a streaming (state in HBM) implementation would move; this kernel does not"}}
     line = {"metric": METRIC, "value": value, "unit": "voxel-fits/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom, seed 1002+rank)",
-            "config": {"workload": "askAdam R2* MSE + 3-D TV (lambda 1e-3 on R2*), 128x128x64 ellipsoid mask "
-                                   "(629,432 voxels), 12 echoes TE=2:3.5:40.5 ms, Adam lr 0.01, 4000 iterations",
-                       "global_batch": world * n, "seq_len": NITER, "parallelism": f"replicas{world}",
-                       "l2": "flushed between steps (256 MB write)", "path": "fused"},
+            "config": bench_config(world * n, world, args.grid, args.iters),
             "gpu_launches": launches, "clocks": clk, "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": "voxel-fits/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h}}
@@ -405,15 +416,18 @@ def extras(ctx, W, opts, model, stream, args):
     from gacelle_b200 import mcmc_solver, phantoms
     from gacelle_b200.models import gpuNEXI
     out = {}
-    f = gxa.check_set_default_basic(dict(W["fitting"], iteration=200))
     n = W["nvox"]
+    # the op-by-op (plain) path on the same volume, the full 4000 iterations
+    f = gxa.check_set_default_basic(dict(W["fitting"], iteration=NITER))
     solver = gxa.askadam(ctx, "plain")
     o2 = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], "plain")
     solver._run(model, W["y"], None, W["th0"], None, None, W["idx"], W["mask"].shape, o2, 12, 2)
     t = solver.last_timing
-    plain_ms_iter = t["main_kernel_ms"] / 200.0
-    out["plain_voxel_fits_per_s"] = n / (plain_ms_iter * NITER / 1000.0)
-    out["plain_ms_per_iteration"] = plain_ms_iter
+    out["plain_voxel_fits_per_s"] = n / (t["main_kernel_ms"] / 1000.0)
+    out["plain_ms_per_iteration"] = t["main_kernel_ms"] / NITER
+    out["plain_iterations_timed"] = NITER
+    if not args.no_parity:
+        out.update(parity_leg(ctx, W, model, args.parity_iters))
     # MCMC
     nv, steps = 200_000, args.mcmc_steps
     y, gt = phantoms.nexi_volume(nv, 1005, sigma=0.02, rician=False, nx=14)
@@ -438,9 +452,112 @@ def extras(ctx, W, opts, model, stream, args):
     out["mcmc_accepted_samples_per_s"] = st["n_accepted"] / sec
     out["mcmc_acceptance"] = st["n_accepted"] / st["n_proposals"]
     out["mcmc_ms_per_step"] = t["main_kernel_ms"] / steps
+    out.update(mcmc_cpu_leg(args))
+    out.update(extra_c1(ctx, args))
     out.update(extra_r1r2s_batch(ctx, args))
     out.update(extra_nexi_rician(ctx, args))
     out.update(extra_nexi_surface(ctx, args))
+    return out
+
+
+def mcmc_cpu_leg(args):
+    """CPU baseline of the Goodman-Weare side run: the FP64 oracle's sampler on
+    a voxel subset of the same phantom (same protocol, walkers and stretch
+    scale) on all host threads, proposals/s extrapolated per voxel-walker-step."""
+    import oracle
+    from gacelle_b200 import phantoms
+    nv, steps, W = args.mcmc_cpu_voxels, args.mcmc_cpu_steps, 64
+    y, gt = phantoms.nexi_volume(nv, 1005, sigma=0.02, rician=False, nx=14)
+    b, d = phantoms.nexi_shells()
+    x0 = np.vstack([gt["fa"], gt["Da"], gt["De"], gt["ra"], np.full(nv, 0.02)])
+    lb = [2.220446049250313e-16] * 3 + [1 / 250, 0.02]
+    ub = [1.0, 3.0, 3.0, 1.0, 0.02]
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    r = oracle.mcmc(oracle.nexi(b, d, nx=14), oracle.Volume(y.astype(np.float64)), x0, lb, ub,
+                    iteration=steps, thinning=10, burnin=0.2, nwalker=W, step_size=2.0, seed=1005, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"mcmc_cpu_baseline": {"value": r["n_proposals"] / dt, "unit": "proposals/s", "cores": cores,
+                                  "kind": "port", "accepted_samples_per_s": r["n_accepted"] / dt,
+                                  "sample": f"{nv} voxels x {W} walkers x {steps} steps of a phantom with the "
+                                            f"same distributions and protocol ({dt:.1f} s)"}}
+
+
+def extra_c1(ctx, args):
+    """The CPU-baseline configuration: mono-exponential R2*, 64x64x1 voxels
+    (full mask, 4096), 12 echoes, MSE, Adam lr 0.01, 2000 iterations, start
+    (1, 30), seed 1001: the FP64 oracle on one host thread and on all of
+    them, the plain and the fused GPU paths (host buffers, whole calls)."""
+    import oracle
+    from gacelle_b200 import askadam_solver as gxa, phantoms, utils
+    from gacelle_b200.models import _GxModelHandle
+    from gacelle_b200 import _lib
+    mask = np.ones((64, 64, 1), bool)
+    data, _ = phantoms.r2s_phantom(mask, 1001)
+    idx = utils.mask_index(mask).astype(np.int32)
+    y = utils.reshape_ND2GD(data, idx)
+    n = y.shape[1]
+    th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, n))
+    iters = 2000
+    f = gxa.check_set_default_basic({"iteration": iters, "initialLearnRate": 0.01, "decayRate": 0.0,
+                                     "lossFunction": "mse", "tol": 0.0, "patienceConvergence": float("inf"),
+                                     "convergenceStepTol": 0.0, "convergenceGradTol": 0.0})
+    lb, ub = [0.0, 0.1], [2.0, 200.0]
+    out = {"c1_workload": f"R2* MSE, 64x64x1 voxels ({n}), 12 echoes, {iters} iterations, no TV"}
+    model = _GxModelHandle(_lib.MODEL_R2S, te=phantoms.R2S_TE)
+    for path in ("plain", "fused"):
+        o = gxa.build_opts(f, ["M0", "R2star"], lb, ub, path)
+        solver = gxa.askadam(ctx, path)
+        solver._run(model, y, None, th0, None, None, idx, mask.shape, o, 12, 2)
+        t = solver.last_timing
+        out[f"c1_{path}_voxel_fits_per_s"] = n / (t["total_ms"] / 1000.0)
+        out[f"c1_{path}_call_ms"] = t["total_ms"]
+    vol = oracle.Volume(y.astype(np.float64), theta0=th0.astype(np.float64))
+    for tag, thr in (("1thread", 1), ("allcores", os.cpu_count() or 1)):
+        t0 = time.perf_counter()
+        oracle.askadam(oracle.r2s(phantoms.R2S_TE), vol, oracle.adam_opts(lb, ub, dict(f, nthreads=thr)),
+                       want_min=False, want_history=False)
+        dt = time.perf_counter() - t0
+        out[f"c1_cpu_{tag}_voxel_fits_per_s"] = n / dt
+        out[f"c1_cpu_{tag}_threads"] = thr
+    return out
+
+
+def parity_leg(ctx, W, model, iters):
+    """The "equal FP64 error" half of the metric on the benchmark volume: the
+    fused and the plain path run `iters` epochs of the same fit, the FP64
+    oracle (the checker) runs it in double precision and once more with its
+    parameter state rounded to FP32 after every update; per parameter map the
+    relative RMSE of each GPU path against FP64, and the FP32-state band."""
+    import oracle
+    from gacelle_b200 import askadam_solver as gxa
+    f = gxa.check_set_default_basic(dict(W["fitting"], iteration=iters))
+    res = {}
+    for path in ("fused", "plain"):
+        o = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], path)
+        r = gxa.askadam(ctx, path)._run(model, W["y"], None, W["th0"], None, None, W["idx"], W["mask"].shape,
+                                        o, 12, 2)
+        res[path] = r["final_theta"].astype(np.float64)
+    fo = dict(f, _reg_index=[1], _reg_lambda=[1e-3], nthreads=os.cpu_count() or 1)
+    vol = oracle.Volume(W["y"].astype(np.float64), dims=W["mask"].shape, grid_index=W["idx"],
+                        theta0=W["th0"].astype(np.float64))
+    t0 = time.perf_counter()
+    o64 = oracle.askadam(oracle.r2s(W["te"]), vol, oracle.adam_opts(W["lb"], W["ub"], fo), want_min=False)
+    o32 = oracle.askadam(oracle.r2s(W["te"]), vol, oracle.adam_opts(W["lb"], W["ub"], dict(fo, _state_f32=True)),
+                         want_min=False)
+    dt = time.perf_counter() - t0
+
+    def rr(a, b):
+        return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
+    out = {"parity_workload": f"the benchmark volume, {iters} epochs, final parameter maps vs the FP64 oracle",
+           "parity_oracle_s": dt}
+    for k, p in enumerate(("M0", "R2star")):
+        band = rr(o32["final"][k], o64["final"][k])
+        out[f"parity_{p}_fused_rel_rmse"] = rr(res["fused"][k], o64["final"][k])
+        out[f"parity_{p}_plain_rel_rmse"] = rr(res["plain"][k], o64["final"][k])
+        out[f"parity_{p}_fp32_state_band"] = band
+        out[f"parity_{p}_within_2x_band"] = bool(max(out[f"parity_{p}_fused_rel_rmse"],
+                                                     out[f"parity_{p}_plain_rel_rmse"]) <= 2 * band + 1e-5)
     return out
 
 

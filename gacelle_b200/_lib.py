@@ -106,12 +106,17 @@ class GxTiming(C.Structure):
                 ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("tv_path", C.c_int32)]
 
 
+class GxTestHooks(C.Structure):
+    _fields_ = [("fail_alloc_at", C.c_int32), ("wait_limit_cycles", C.c_int64),
+                ("barrier_extra_arrivals", C.c_int32)]
+
+
 TV_PERSISTENT, TV_PAIRS, TV_DATA_SMEM, TV_DATA_QUADS = 1, 2, 4, 8
 
 
 STRUCTS = {"gx_model": GxModel, "gx_volume": GxVolume, "gx_askadam_opts": GxAskadamOpts,
            "gx_askadam_result": GxAskadamResult, "gx_mcmc_opts": GxMcmcOpts,
-           "gx_mcmc_result": GxMcmcResult, "gx_timing": GxTiming}
+           "gx_mcmc_result": GxMcmcResult, "gx_timing": GxTiming, "gx_test_hooks": GxTestHooks}
 
 # name -> (restype, argtypes) for every entry point declared in the header
 SIGNATURES = {
@@ -126,6 +131,7 @@ SIGNATURES = {
     "gx_dictionary_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
                                       C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gx_set_cancel_flag": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "gx_context_set_test_hooks": (C.c_int, [C.c_void_p, C.POINTER(GxTestHooks)]),
     "gx_model_sizes": (C.c_int, [C.POINTER(GxModel), _i32p, _i32p]),
     "gx_forward": (C.c_int, [C.c_void_p, C.POINTER(GxModel), C.c_int32, C.c_void_p, C.c_void_p,
                              C.c_int32, C.c_void_p]),

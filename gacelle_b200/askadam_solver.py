@@ -354,12 +354,19 @@ class askadam:
         r = _lib.GxAskadamResult()
         for k, a in out.items():
             setattr(r, k, a.ctypes.data_as(_lib._dp if a.dtype == np.float64 else _lib._fp))
-        _lib.check(_lib.lib().gx_askadam(ctx.ptr, _lib.C.byref(gxm.s), _lib.MEM_HOST, _lib.C.byref(vol), 1,
-                                         _lib.C.byref(opts), _lib.C.byref(r)))
+        st = _lib.lib().gx_askadam(ctx.ptr, _lib.C.byref(gxm.s), _lib.MEM_HOST, _lib.C.byref(vol), 1,
+                                   _lib.C.byref(opts), _lib.C.byref(r))
         self.last_timing = ctx.timing()
         for f in ("final_loss", "final_loss_fidelity", "final_loss_reg", "min_loss", "min_loss_fidelity",
                   "min_loss_reg", "final_niteration", "min_niteration", "stop_reason"):
             out[f] = getattr(r, f)
+        try:
+            _lib.check(st)
+        except _lib.GacelleError as e:
+            # a non-finite loss still returns the fit's (partial) result
+            if st == _lib.GX_ENUMERIC:
+                e.partial = out
+            raise
         return out
 
     @staticmethod

@@ -110,11 +110,11 @@ __device__ __forceinline__ void grid_arrive_one(PersistBarrier* gb) {
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&gb->count) : "memory");
 }
 
-__device__ __forceinline__ bool grid_wait_one(PersistBarrier* gb, unsigned int target) {
+__device__ __forceinline__ bool grid_wait_one(PersistBarrier* gb, unsigned int target, long long limit) {
     const long long t0 = clock64();
     while (ld_acquire_gpu(&gb->count) < target) {
         if (*(volatile int*)&gb->error) return false;
-        if (clock64() - t0 > kBarrierSpinCycles) {
+        if (clock64() - t0 > limit) {
             atomicExch(&gb->error, 1);
             return false;
         }
@@ -151,12 +151,14 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 }
 
 // Wait for the completion of the barrier's phase with the given parity
-// (the barrier is never more than one phase ahead of the waiter).  Bounded:
-// false, with the grid's error flag raised, once the wait has expired.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned int parity, PersistBarrier* gb) {
+// (the barrier is never more than one phase ahead of the waiter).  Bounded
+// by `limit` SM clock cycles: false, with the grid's error flag raised, once
+// the wait has expired.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned int parity, PersistBarrier* gb,
+                                          long long limit) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kBarrierSpinCycles) {
+        if (clock64() - t0 > limit) {
             atomicExch(&gb->error, 1);
             return false;
         }
@@ -309,7 +311,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const int vol = a.blk_vol[base / p.pad_block];
         for (int e = p.e_begin; e <= p.e_end; ++e) {
             const unsigned int ph = (unsigned int)(e - p.e_begin) & 1u;
-            if (!mbar_wait(&bar_arrive, ph, p.barrier)) {
+            if (!mbar_wait(&bar_arrive, ph, p.barrier, p.spin_cycles)) {
                 if (lane == 31) {
                     *(volatile int*)&s_err = 1;
                     mbar_arrive(&bar_open);
@@ -321,7 +323,8 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             int ok = 1;
             if (e < p.e_end && lane == 31) {
                 grid_arrive_one(p.barrier);
-                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x);
+                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x + p.extra_arrivals,
+                                   p.spin_cycles);
                 if (!ok) *(volatile int*)&s_err = 1;
             }
             if (p.record && a.hist && lane < NQ) {
@@ -418,7 +421,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         }
         // every CTA's map of the previous epoch (written before its arrival)
         if (e > p.e_begin)
-            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier) ||
+            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, p.spin_cycles) ||
                 *(volatile int*)&s_err)
                 return;
         const bool ckpt = upd && a.ckpt_every > 0 && (e % a.ckpt_every) == 0;
@@ -540,7 +543,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         }
         // every CTA's map of the previous epoch (written before its arrival)
         if (e > p.e_begin)
-            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier) ||
+            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, p.spin_cycles) ||
                 *(volatile int*)&s_err)
                 return;
         // pass 2: TV subgradient, chain rule, optimiser, new map values

@@ -78,6 +78,8 @@ struct gx_context {
     void* pin = nullptr;
     size_t pin_cap = 0;
     cudaEvent_t pin_ev = nullptr;  // recorded after the copies out of `pin`
+    gx_test_hooks hooks{};         // fault injection (tests); all zero = off
+    int ws_requests = 0;           // workspace requests of the current call
 };
 
 // The context's pinned staging buffer, once the copies queued from it by an
@@ -102,6 +104,9 @@ static gx_status pinned(gx_context* c, size_t bytes, void** out) {
 
 static gx_status ws(gx_context* c, Slot s, size_t bytes, void** out) {
     if (bytes == 0) bytes = 16;
+    if (c->hooks.fail_alloc_at > 0 && ++c->ws_requests == c->hooks.fail_alloc_at)
+        return fail(GX_ENOMEM, "device workspace request %d (%zu bytes): allocation failure injected by the "
+                               "context's test hooks", c->ws_requests, bytes);
     if (c->cap[s] < bytes) {
         if (c->buf[s]) {
             cudaStreamSynchronize(c->stream);
@@ -166,6 +171,7 @@ struct CallScope {
     explicit CallScope(gx_context* ctx) : c(ctx), lk(ctx->mu), launches0(g_kernel_launches) {
         cudaSetDevice(ctx->device);
         c->timing = gx_timing{};
+        c->ws_requests = 0;
     }
 };
 
@@ -185,6 +191,7 @@ size_t gx_struct_size(const char* name) {
     if (n == "gx_mcmc_opts") return sizeof(gx_mcmc_opts);
     if (n == "gx_mcmc_result") return sizeof(gx_mcmc_result);
     if (n == "gx_timing") return sizeof(gx_timing);
+    if (n == "gx_test_hooks") return sizeof(gx_test_hooks);
     return 0;
 }
 
@@ -239,6 +246,15 @@ gx_status gx_last_timing(gx_context* c, gx_timing* out) {
 gx_status gx_set_cancel_flag(gx_context* c, volatile int32_t* flag) {
     if (!c) return fail(GX_EINVAL, "context is NULL");
     c->cancel = flag;
+    return GX_OK;
+}
+
+gx_status gx_context_set_test_hooks(gx_context* c, const gx_test_hooks* h) {
+    if (!c) return fail(GX_EINVAL, "context is NULL");
+    if (h && (h->fail_alloc_at < 0 || h->wait_limit_cycles < 0 || h->barrier_extra_arrivals < 0))
+        return fail(GX_EINVAL, "gx_context_set_test_hooks: negative setting");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->hooks = h ? *h : gx_test_hooks{};
     return GX_OK;
 }
 
@@ -407,10 +423,10 @@ struct Tracker {
 // ---------------------------------------------------------------------------
 // askAdam
 // ---------------------------------------------------------------------------
-static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume* vols, int nvol,
-                               int nm) {
+// Checks of the options every askAdam entry point makes: iteration count,
+// bounds, and the loss / optimiser / transform enumerations.
+static gx_status validate_adam_common(const gx_askadam_opts* o, int np) {
     if (!o) return fail(GX_EINVAL, "opts is NULL");
-    if (!vols || nvol < 1) return fail(GX_EINVAL, "need at least one volume");
     if (o->iteration < 0) return fail(GX_EINVAL, "iteration must be >= 0");
     if (!o->lb || !o->ub) return fail(GX_EINVAL, "lb/ub are required");
     for (int k = 0; k < np; ++k)
@@ -419,6 +435,14 @@ static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume
     if (o->optimiser < GX_OPT_ADAM || o->optimiser > GX_OPT_RMSPROP) return fail(GX_EINVAL, "unknown optimiser %d", o->optimiser);
     if (o->transform != GX_TRANSFORM_SIGMOID && o->transform != GX_TRANSFORM_LINEAR)
         return fail(GX_EINVAL, "unknown parameterTransform %d", o->transform);
+    return GX_OK;
+}
+
+static gx_status validate_adam(const gx_askadam_opts* o, int np, const gx_volume* vols, int nvol,
+                               int nm) {
+    if (!o) return fail(GX_EINVAL, "opts is NULL");
+    if (!vols || nvol < 1) return fail(GX_EINVAL, "need at least one volume");
+    TRY(validate_adam_common(o, np));
     if (o->n_reg < 0 || o->n_reg > kMaxReg) return fail(GX_EINVAL, "n_reg must be in [0, %d]", kMaxReg);
     for (int r = 0; r < o->n_reg; ++r)
         if (o->reg_param[r] < 0 || o->reg_param[r] >= np) return fail(GX_EINVAL, "regmap index %d out of range", o->reg_param[r]);
@@ -693,6 +717,10 @@ static gx_status adam_setup(AdamJob& J) {
     const size_t nblk = J.hblk.size(), nvt = 2 * J.hv.size();
     const size_t o_vols = (sizeof(int) * nblk + 15) / 16 * 16;
     const size_t o_sched = o_vols + (sizeof(DevVol) * nvt + 15) / 16 * 16;
+    // every destination exists before the stage is filled, so that no return
+    // path leaves copies out of the stage queued without pin_ev behind them
+    float2* dsched;
+    TRY(wsT(c, S_SCHED, (size_t)N + 1, &dsched));
     unsigned char* stage;
     TRY(pinned(c, o_sched + sizeof(float2) * ((size_t)N + 1), (void**)&stage));
     memcpy(stage, J.hblk.data(), sizeof(int) * nblk);
@@ -702,8 +730,6 @@ static gx_status adam_setup(AdamJob& J) {
         sv[J.hv.size() + i] = J.hv[i];
         sv[J.hv.size() + i].off = 0;
     }
-    CK(cudaMemcpyAsync(blk, stage, sizeof(int) * nblk, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(dvols, sv, sizeof(DevVol) * nvt, cudaMemcpyHostToDevice, c->stream));
     J.local_vols = dvols + J.hv.size();
     a.blk_vol = blk;
     a.vols = dvols;
@@ -717,10 +743,22 @@ static gx_status adam_setup(AdamJob& J) {
         else
             sched[e] = float2{(float)lr, 0.f};
     }
-    float2* dsched;
-    TRY(wsT(c, S_SCHED, (size_t)N + 1, &dsched));
-    CK(cudaMemcpyAsync(dsched, sched, sizeof(float2) * ((size_t)N + 1), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaEventRecord(c->pin_ev, c->stream));
+    {
+        // the three copies out of the stage; pin_ev is recorded behind them
+        // even when one fails, so the next call's pinned() waits for the
+        // copies that were queued
+        cudaError_t e = cudaMemcpyAsync(blk, stage, sizeof(int) * nblk, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dvols, sv, sizeof(DevVol) * nvt, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dsched, sched, sizeof(float2) * ((size_t)N + 1), cudaMemcpyHostToDevice, c->stream);
+        const cudaError_t er = cudaEventRecord(c->pin_ev, c->stream);
+        if (e == cudaSuccess && er != cudaSuccess) e = er;
+        if (e != cudaSuccess) {
+            if (er != cudaSuccess) cudaStreamSynchronize(c->stream);  // no event: drain instead
+            CK(e);
+        }
+    }
     a.sched = dsched;
     TRY(wsT(c, S_HIST, (size_t)J.nvol * (N + 1) * kHistW, &a.hist));
     CK(cudaMemsetAsync(a.hist, 0, sizeof(double) * J.nvol * (N + 1) * kHistW, c->stream));
@@ -854,6 +892,8 @@ static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e
         p.barrier = J.barrier;
         p.pad_block = J.B;
         p.data_quads = J.data_quads;
+        p.spin_cycles = c->hooks.wait_limit_cycles > 0 ? c->hooks.wait_limit_cycles : kBarrierSpinCycles;
+        p.extra_arrivals = (unsigned int)c->hooks.barrier_extra_arrivals;
         CK(cudaMemsetAsync(J.barrier, 0, sizeof(PersistBarrier), c->stream));
         CK(launch_tv_persistent(a, J.plan, p, c->stream));
         return GX_OK;
@@ -1632,4 +1672,6 @@ gx_status internal_model(const gx_model* m, const double* lb, const double* ub, 
 }
 
 bool internal_can_stop(const gx_askadam_opts* o) { return can_stop(o); }
+
+gx_status internal_validate_opts(const gx_askadam_opts* o, int np) { return validate_adam_common(o, np); }
 }  // namespace gx

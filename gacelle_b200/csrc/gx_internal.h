@@ -205,7 +205,8 @@ extern long long g_kernel_launches;  // launches of this library's kernels (proc
 
 // Persistent cooperative TV kernel (askadam_persistent.cu).
 constexpr int kPersistMaxThreads = 1024;
-constexpr long long kBarrierSpinCycles = 4000000000LL;  // about 2 s at B200 clocks
+// default bound of the persistent kernel's waits: about 2 s at B200 clocks
+constexpr long long kBarrierSpinCycles = 4000000000LL;
 
 struct PersistBarrier {
     unsigned int count;  // CTA arrivals since the launch (zeroed before it)
@@ -223,6 +224,8 @@ struct PersistArgs {
     int data_in_smem;
     int pad_block;           // block size of the work-list padding (blk_vol granularity)
     const float4* data_quads; // [quad_width/4][nvtot] echo quads of the measurements, or nullptr
+    long long spin_cycles;   // bound of every wait, SM clock cycles (kBarrierSpinCycles unless a test sets it)
+    unsigned int extra_arrivals; // 0; a test's count of arrivals the grid barrier waits for beyond the grid's
 };
 
 struct PersistPlan {
@@ -250,5 +253,7 @@ gx_status internal_fail(gx_status s, const char* msg);
 gx_status internal_model(const gx_model* m, const double* lb, const double* ub, DevProtocol* P,
                          int* np, int* nm, int* id);
 bool internal_can_stop(const gx_askadam_opts* o);
+// iteration count, bounds and the loss / optimiser / transform enumerations
+gx_status internal_validate_opts(const gx_askadam_opts* o, int np);
 
 }  // namespace gx

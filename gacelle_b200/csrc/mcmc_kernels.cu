@@ -67,15 +67,19 @@ __global__ void gw_partner_kernel(McmcParams p, int* partner, int nsteps, int gl
     else rb_anchors_dev(p.seed, k, (global_block ? kTagGwGRbPart : kTagGwRbPart) | bits, p.nwalker, out);
 }
 
-template <int MODEL>
-__device__ __forceinline__ double log_prob(const McmcParams& p, const DevProtocol& P, const float* x,
-                                           const float* y, const float* w, const VoxAux& va) {
+// logP_Gaussian (utils/logP_Gaussian.m:18-20) of the model's parameters and
+// the noise sigma (the last of the NV variables, a compile-time index so that
+// the caller's parameter vector stays in registers); y / w with strides.
+template <int MODEL, int NV>
+__device__ __forceinline__ double log_prob_t(int nm, const DevProtocol& P, const float (&x)[NV], const float* y,
+                                             int ys, const float* w, int ws, const VoxAux& va) {
     constexpr int NP = ModelNP<MODEL>::value;
-    SosSink<NP> sink{y, 1, w, 1, 0.0};
+    static_assert(NV == NP + 1, "the variables are the model's parameters and the noise sigma");
+    SosSink<NP> sink{y, ys, w, ws, 0.0};
     model_eval<MODEL>(P, x, va, sink);
-    double noise = (double)x[p.nvar - 1];
-    double n2 = noise * noise;
-    return -sink.sos / (2.0 * n2) - 0.5 * p.nm * log(6.283185307179586 * n2);
+    const double noise = (double)x[NV - 1];
+    const double n2 = noise * noise;
+    return -sink.sos / (2.0 * n2) - 0.5 * nm * log(6.283185307179586 * n2);
 }
 
 __device__ __forceinline__ int kept_index(const McmcParams& p, int k) {
@@ -86,15 +90,36 @@ __device__ __forceinline__ int kept_index(const McmcParams& p, int k) {
     return c < p.ns ? c : -1;
 }
 
+// Walker start (mcmc.m:267-275): x0 + (ub-lb)*startRange*randn, clamped; the
+// normal draws of walker w of voxel v come four at a time from the Philox
+// stream (v, w, j, kTagGwInit).
+template <int NV>
+__device__ __forceinline__ void gw_walker_start(const McmcParams& p, int v, int w, float (&x)[NV]) {
+    float nrm[(NV + 3) / 4 * 4];
+#pragma unroll
+    for (int j = 0; j * 4 < NV; ++j) {
+        U4 u = philox((uint32_t)v, (uint32_t)w, (uint32_t)j, kTagGwInit, p.seed);
+        box_muller(u.x, u.y, nrm[4 * j], nrm[4 * j + 1]);
+        box_muller(u.z, u.w, nrm[4 * j + 2], nrm[4 * j + 3]);
+    }
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        float val = p.x0[(size_t)q * p.nvox + v] + (p.ub[q] - p.lb[q]) * p.start_range * nrm[q];
+        x[q] = fminf(fmaxf(val, p.lb[q]), p.ub[q]);
+    }
+}
+
 // Goodman-Weare, steps [k0, k1] of repetition rr.  State between launches:
-// xstate [nvar][nvox][W], lpstate [nvox][W].
-template <int MODEL>
+// xstate [nvar][nvox][W], lpstate [nvox][W].  NV = parameters + noise, fixed
+// at compile time: every per-walker vector (state, proposal, running sums)
+// is indexed by constants and lives in registers.
+template <int MODEL, int NV>
 __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float* xstate,
                           double* lpstate, double* sum, double* sumsq) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ DevProtocol s_P;
     stage_protocol(p.P, &s_P);
-    const int W = p.nwalker, nvar = p.nvar, nm = p.nm;
+    const int W = p.nwalker, nm = p.nm;
     const int h = W / 2;
     const int tpv = p.update == 0 ? W : (W - h);
     const int vpb = blockDim.x / tpv;
@@ -102,10 +127,10 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
     const int v = blockIdx.x * vpb + vl;
     const bool in_block = vl < vpb;
     const bool live = in_block && v < p.nvox;
-    float* xs = reinterpret_cast<float*>(smem_raw);               // [vpb][W][nvar]
-    float* ys = xs + vpb * W * nvar;                              // [vpb][nm]
+    float* xs = reinterpret_cast<float*>(smem_raw);               // [vpb][W][NV]
+    float* ys = xs + vpb * W * NV;                                // [vpb][nm]
     float* ws = ys + vpb * nm;                                    // [vpb][nm]
-    float* xv = xs + (in_block ? vl : 0) * W * nvar;
+    float* xv = xs + (in_block ? vl : 0) * W * NV;
     const float* yv = ys + (in_block ? vl : 0) * nm;
     const float* wv = p.weights ? ws + (in_block ? vl : 0) * nm : nullptr;
     if (live)
@@ -119,142 +144,126 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
         for (int f = 0; f < p.P.n_fa; ++f) sincosf(b1 * p.P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
 
-    // walkers owned by this thread
-    int wown[2];
-    int nown;
-    if (p.update == 0) { wown[0] = a; nown = 1; }
-    else { wown[0] = a < h ? a : -1; wown[1] = h + a; nown = 2; }
-    float x[2][kMaxParam];
-    double lp[2];
-    double s1[kMaxParam], s2[kMaxParam];
-    for (int q = 0; q < kMaxParam; ++q) { s1[q] = 0.0; s2[q] = 0.0; }
+    // walkers owned by this thread: slot 0 (simultaneous: walker a; red-black:
+    // walker a of the first half, if any) and slot 1 (red-black: walker h + a)
+    const bool rb = p.update != 0;
+    const int wown0 = rb ? (a < h ? a : -1) : a, wown1 = rb ? h + a : -1;
+    const bool own0 = live && wown0 >= 0 && wown0 < W, own1 = live && wown1 >= 0 && wown1 < W;
+    float x0s[NV], x1s[NV];
+    double lp0 = 0.0, lp1 = 0.0;
+    double s1[NV], s2[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) { s1[q] = 0.0; s2[q] = 0.0; x0s[q] = 0.0f; x1s[q] = 0.0f; }
     __syncthreads();
-    for (int o = 0; o < nown; ++o) {
-        int w = wown[o];
-        if (!live || w < 0 || w >= W) continue;
-        if (init) {
-            // walker start: x0 + (ub-lb)*startRange*randn, clamped (mcmc.m:267-275)
-            float nrm[8];
-            for (int j = 0; j * 4 < nvar; ++j) {
-                U4 u = philox((uint32_t)v, (uint32_t)w, (uint32_t)j, kTagGwInit, p.seed);
-                float n0, n1, n2, n3;
-                box_muller(u.x, u.y, n0, n1);
-                box_muller(u.z, u.w, n2, n3);
-                nrm[4 * j] = n0; nrm[4 * j + 1] = n1; nrm[4 * j + 2] = n2; nrm[4 * j + 3] = n3;
-            }
-            for (int q = 0; q < nvar; ++q) {
-                float val = p.x0[(size_t)q * p.nvox + v] + (p.ub[q] - p.lb[q]) * p.start_range * nrm[q];
-                x[o][q] = fminf(fmaxf(val, p.lb[q]), p.ub[q]);
-            }
-        } else {
-            for (int q = 0; q < nvar; ++q) x[o][q] = xstate[((size_t)q * p.nvox + v) * W + w];
-        }
-        for (int q = 0; q < nvar; ++q) xv[w * nvar + q] = x[o][q];
+    if (own0) {
+        if (init) gw_walker_start<NV>(p, v, wown0, x0s);
+        else
+#pragma unroll
+            for (int q = 0; q < NV; ++q) x0s[q] = xstate[((size_t)q * p.nvox + v) * W + wown0];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) xv[wown0 * NV + q] = x0s[q];
+    }
+    if (own1) {
+        if (init) gw_walker_start<NV>(p, v, wown1, x1s);
+        else
+#pragma unroll
+            for (int q = 0; q < NV; ++q) x1s[q] = xstate[((size_t)q * p.nvox + v) * W + wown1];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) xv[wown1 * NV + q] = x1s[q];
     }
     __syncthreads();
-    for (int o = 0; o < nown; ++o) {
-        int w = wown[o];
-        if (!live || w < 0 || w >= W) continue;
-        lp[o] = init ? log_prob<MODEL>(p, s_P, x[o], yv, wv, va) : lpstate[(size_t)v * W + w];
-    }
-    if (!init && live)
-        for (int q = 0; q < nvar; ++q) {
-            s1[q] = 0.0;
-            s2[q] = 0.0;
-        }
+    if (own0) lp0 = init ? log_prob_t<MODEL, NV>(nm, s_P, x0s, yv, 1, wv, 1, va) : lpstate[(size_t)v * W + wown0];
+    if (own1) lp1 = init ? log_prob_t<MODEL, NV>(nm, s_P, x1s, yv, 1, wv, 1, va) : lpstate[(size_t)v * W + wown1];
     unsigned int nacc = 0;
     const float amin1 = p.a - 1.0f;
 
-    for (int k = k0; k <= k1; ++k) {
+    // stretch proposal of walker w (state xw, log-likelihood lpw) about its
+    // partner: xn and its log-likelihood lpp, and whether it is accepted
+    auto propose = [&](int w, int k, uint32_t flags, const float (&xw)[NV], double lpw, float (&xn)[NV],
+                       double& lpp) -> bool {
         const int* pt = p.partner + ((size_t)rr * p.iteration + (k - 1)) * W;
-        if (p.update == 0) {
-            float xn[kMaxParam];
-            bool acc = false;
+        const int q = pt[w];
+        U4 u = philox((uint32_t)v, (uint32_t)w, (uint32_t)k, kTagGwMove | ((uint32_t)rr << 16) | flags, p.seed);
+        float t = amin1 * u01(u.x) + 1.0f;
+        float zz = t * t / p.a;
+        bool oob = false;
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            float xq = xv[q * NV + j];
+            float xp = xq + (xw[j] - xq) * zz;
+            oob |= (xp < p.lb[j]) || (xp > p.ub[j]);
+            xn[j] = fminf(fmaxf(xp, p.lb[j]), p.ub[j]);
+        }
+        lpp = log_prob_t<MODEL, NV>(nm, s_P, xn, yv, 1, wv, 1, va);
+        double lr = (double)(NV - 1) * (double)logf(zz) + (lpp - lpw);
+        return !oob && lr > (double)logf(u01(u.y));
+    };
+    auto commit = [&](int w, const float (&xn)[NV], double lpp, float (&xw)[NV], double& lpw) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            xw[j] = xn[j];
+            xv[w * NV + j] = xn[j];
+        }
+        lpw = lpp;
+        ++nacc;
+    };
+
+    for (int k = k0; k <= k1; ++k) {
+        if (!rb) {
+            float xn[NV];
             double lpp = 0.0;
-            int w = wown[0];
-            if (live) {
-                int q = pt[w];
-                U4 u = philox((uint32_t)v, (uint32_t)w, (uint32_t)k, kTagGwMove | ((uint32_t)rr << 16), p.seed);
-                float t = amin1 * u01(u.x) + 1.0f;
-                float zz = t * t / p.a;
-                bool oob = false;
-                for (int j = 0; j < nvar; ++j) {
-                    float xq = xv[q * nvar + j];
-                    float xp = xq + (xv[w * nvar + j] - xq) * zz;
-                    oob |= (xp < p.lb[j]) || (xp > p.ub[j]);
-                    xn[j] = fminf(fmaxf(xp, p.lb[j]), p.ub[j]);
-                }
-                lpp = log_prob<MODEL>(p, s_P, xn, yv, wv, va);
-                double lr = (double)(nvar - 1) * (double)logf(zz) + (lpp - lp[0]);
-                acc = !oob && lr > (double)logf(u01(u.y));
-            }
+            const bool acc = own0 && propose(wown0, k, 0u, x0s, lp0, xn, lpp);
             __syncthreads();  // every walker has read the old ensemble
-            if (live && acc) {
-                for (int j = 0; j < nvar; ++j) {
-                    x[0][j] = xn[j];
-                    xv[w * nvar + j] = xn[j];
-                }
-                lp[0] = lpp;
-                ++nacc;
-            }
+            if (acc) commit(wown0, xn, lpp, x0s, lp0);
             __syncthreads();
         } else {
-            for (int s = 0; s < 2; ++s) {
-                int o = s;  // slot 0: first half, slot 1: second half
-                int w = wown[o];
-                bool act = live && w >= 0 && w < W;
-                if (act) {
-                    int q = pt[w];
-                    U4 u = philox((uint32_t)v, (uint32_t)w, (uint32_t)k,
-                                  kTagGwMove | ((uint32_t)rr << 16) | (1u << 8), p.seed);
-                    float t = amin1 * u01(u.x) + 1.0f;
-                    float zz = t * t / p.a;
-                    float xn[kMaxParam];
-                    bool oob = false;
-                    for (int j = 0; j < nvar; ++j) {
-                        float xq = xv[q * nvar + j];
-                        float xp = xq + (x[o][j] - xq) * zz;
-                        oob |= (xp < p.lb[j]) || (xp > p.ub[j]);
-                        xn[j] = fminf(fmaxf(xp, p.lb[j]), p.ub[j]);
-                    }
-                    double lpp = log_prob<MODEL>(p, s_P, xn, yv, wv, va);
-                    double lr = (double)(nvar - 1) * (double)logf(zz) + (lpp - lp[o]);
-                    if (!oob && lr > (double)logf(u01(u.y))) {
-                        for (int j = 0; j < nvar; ++j) {
-                            x[o][j] = xn[j];
-                            xv[w * nvar + j] = xn[j];
-                        }
-                        lp[o] = lpp;
-                        ++nacc;
-                    }
-                }
-                __syncthreads();  // the moved half is visible before the other half anchors on it
+            // the active half moves about anchors in the frozen half
+            if (own0) {
+                float xn[NV];
+                double lpp = 0.0;
+                if (propose(wown0, k, 1u << 8, x0s, lp0, xn, lpp)) commit(wown0, xn, lpp, x0s, lp0);
             }
+            __syncthreads();  // the moved half is visible before the other half anchors on it
+            if (own1) {
+                float xn[NV];
+                double lpp = 0.0;
+                if (propose(wown1, k, 1u << 8, x1s, lp1, xn, lpp)) commit(wown1, xn, lpp, x1s, lp1);
+            }
+            __syncthreads();
         }
         int c = kept_index(p, k);
-        if (c >= 0 && live) {
-            for (int o = 0; o < nown; ++o) {
-                int w = wown[o];
-                if (w < 0 || w >= W) continue;
-                for (int j = 0; j < nvar; ++j) {
-                    double d = (double)x[o][j] - (double)p.shift[(size_t)j * p.nvox + v];
+        if (c >= 0) {
+#pragma unroll
+            for (int o = 0; o < 2; ++o) {
+                const bool own = o == 0 ? own0 : own1;
+                if (!own) continue;
+                const int w = o == 0 ? wown0 : wown1;
+                const float (&xw)[NV] = o == 0 ? x0s : x1s;
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    double d = (double)xw[j] - (double)p.shift[(size_t)j * p.nvox + v];
                     s1[j] += d;
                     s2[j] += d * d;
                     if (p.posterior)
-                        p.posterior[((((size_t)j * p.repetition + rr) * p.ns + c) * W + w) * p.nvox + v] = x[o][j];
+                        p.posterior[((((size_t)j * p.repetition + rr) * p.ns + c) * W + w) * p.nvox + v] = xw[j];
                 }
             }
         }
     }
     // persist walker state, fold the kept-sample sums of this launch
+    if (own0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) xstate[((size_t)q * p.nvox + v) * W + wown0] = x0s[q];
+        lpstate[(size_t)v * W + wown0] = lp0;
+    }
+    if (own1) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) xstate[((size_t)q * p.nvox + v) * W + wown1] = x1s[q];
+        lpstate[(size_t)v * W + wown1] = lp1;
+    }
     if (live) {
-        for (int o = 0; o < nown; ++o) {
-            int w = wown[o];
-            if (w < 0 || w >= W) continue;
-            for (int q = 0; q < nvar; ++q) xstate[((size_t)q * p.nvox + v) * W + w] = x[o][q];
-            lpstate[(size_t)v * W + w] = lp[o];
-        }
-        for (int j = 0; j < nvar; ++j) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
             if (s1[j] != 0.0) atomicAdd(&sum[(size_t)j * p.nvox + v], s1[j]);
             if (s2[j] != 0.0) atomicAdd(&sumsq[(size_t)j * p.nvox + v], s2[j]);
         }
@@ -264,8 +273,10 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
     if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(p.n_acc, (unsigned long long)wsum);
 }
 
-// Metropolis-Hastings, one thread per voxel (mcmc.m:144-167).
-template <int MODEL>
+// Metropolis-Hastings, one thread per voxel (mcmc.m:144-167).  NV =
+// parameters + noise at compile time (the state in registers); the voxel's
+// measurements are read from [nm][nvox] with coalesced loads.
+template <int MODEL, int NV>
 __global__ void mh_kernel(McmcParams p, int rr, int k0, int k1, int init, float* xstate,
                           double* lpstate, double* sum, double* sumsq) {
     __shared__ DevProtocol s_P;
@@ -273,59 +284,60 @@ __global__ void mh_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
     __syncthreads();
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     bool live = v < p.nvox;
-    const int nvar = p.nvar, nm = p.nm;
-    float yv[kMaxMeas], wv[kMaxMeas];
-    if (live)
-        for (int m = 0; m < nm; ++m) {
-            yv[m] = p.data[(size_t)m * p.nvox + v];
-            wv[m] = p.weights ? p.weights[(size_t)m * p.nvox + v] : 1.0f;
-        }
+    const int nm = p.nm;
+    const float* yv = p.data + (live ? v : 0);
+    const float* wv = p.weights ? p.weights + (live ? v : 0) : nullptr;
     float b1 = (live && p.b1) ? p.b1[v] : 1.0f;
     float sa[MODEL == kR1R2S ? kMaxFA : 1], ca[MODEL == kR1R2S ? kMaxFA : 1];
     if (MODEL == kR1R2S)
         for (int f = 0; f < p.P.n_fa; ++f) sincosf(b1 * p.P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
-    float x[kMaxParam];
+    float x[NV];
     double lp = 0.0;
-    double s1[kMaxParam], s2[kMaxParam];
-    for (int q = 0; q < kMaxParam; ++q) { s1[q] = 0.0; s2[q] = 0.0; x[q] = 0.0f; }
+    double s1[NV], s2[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) { s1[q] = 0.0; s2[q] = 0.0; x[q] = 0.0f; }
     unsigned int nacc = 0;
     if (live) {
         if (init) {
-            for (int q = 0; q < nvar; ++q)
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
                 x[q] = fminf(fmaxf(p.x0[(size_t)q * p.nvox + v], p.lb[q]), p.ub[q]);
-            lp = log_prob<MODEL>(p, s_P, x, yv, wv, va);
+            lp = log_prob_t<MODEL, NV>(nm, s_P, x, yv, p.nvox, wv, p.nvox, va);
         } else {
-            for (int q = 0; q < nvar; ++q) x[q] = xstate[(size_t)q * p.nvox + v];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) x[q] = xstate[(size_t)q * p.nvox + v];
             lp = lpstate[v];
         }
         for (int k = k0; k <= k1; ++k) {
-            float nrm[8];
+            float nrm[(NV + 3) / 4 * 4];
             uint32_t tag = kTagMhMove | ((uint32_t)rr << 16);
-            for (int j = 0; j * 4 < nvar; ++j) {
+#pragma unroll
+            for (int j = 0; j * 4 < NV; ++j) {
                 U4 u = philox((uint32_t)v, (uint32_t)k, (uint32_t)j, tag, p.seed);
-                float n0, n1, n2, n3;
-                box_muller(u.x, u.y, n0, n1);
-                box_muller(u.z, u.w, n2, n3);
-                nrm[4 * j] = n0; nrm[4 * j + 1] = n1; nrm[4 * j + 2] = n2; nrm[4 * j + 3] = n3;
+                box_muller(u.x, u.y, nrm[4 * j], nrm[4 * j + 1]);
+                box_muller(u.z, u.w, nrm[4 * j + 2], nrm[4 * j + 3]);
             }
             U4 ua = philox((uint32_t)v, (uint32_t)k, 8u, tag, p.seed);
-            float xp[kMaxParam];
+            float xp[NV];
             bool oob = false;
-            for (int q = 0; q < nvar; ++q) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
                 float t = x[q] + p.xstep[q] * nrm[q];
                 oob |= (t < p.lb[q]) || (t > p.ub[q]);
                 xp[q] = fminf(fmaxf(t, p.lb[q]), p.ub[q]);
             }
-            double lpp = log_prob<MODEL>(p, s_P, xp, yv, wv, va);
+            double lpp = log_prob_t<MODEL, NV>(nm, s_P, xp, yv, p.nvox, wv, p.nvox, va);
             if (!oob && (lpp - lp) > (double)logf(u01(ua.x))) {
-                for (int q = 0; q < nvar; ++q) x[q] = xp[q];
+#pragma unroll
+                for (int q = 0; q < NV; ++q) x[q] = xp[q];
                 lp = lpp;
                 ++nacc;
             }
             int c = kept_index(p, k);
             if (c >= 0)
-                for (int j = 0; j < nvar; ++j) {
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
                     double d = (double)x[j] - (double)p.shift[(size_t)j * p.nvox + v];
                     s1[j] += d;
                     s2[j] += d * d;
@@ -333,9 +345,11 @@ __global__ void mh_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
                         p.posterior[(((size_t)j * p.repetition + rr) * p.ns + c) * p.nvox + v] = x[j];
                 }
         }
-        for (int q = 0; q < nvar; ++q) xstate[(size_t)q * p.nvox + v] = x[q];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) xstate[(size_t)q * p.nvox + v] = x[q];
         lpstate[v] = lp;
-        for (int j = 0; j < nvar; ++j) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
             sum[(size_t)j * p.nvox + v] += s1[j];
             sumsq[(size_t)j * p.nvox + v] += s2[j];
         }
@@ -401,14 +415,16 @@ __device__ __forceinline__ float gwg_global_init(const McmcParams& p, int w, int
     return p.lb[q] + (p.ub[q] - p.lb[q]) * u01(r);
 }
 
-// One thread per (voxel, walker); blockDim = vpb * W.
-template <int MODEL>
+// One thread per (voxel, walker); blockDim = vpb * W.  NV = parameters +
+// noise at compile time (per-thread vectors in registers).
+template <int MODEL, int NV>
 __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags, int half, float* xstate,
                                 double* lpstate) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ DevProtocol s_P;
     stage_protocol(p.P, &s_P);
-    const int W = p.nwalker, nvar = p.nvar, nm = p.nm, h = W / 2;
+    constexpr int nvar = NV;
+    const int W = p.nwalker, nm = p.nm, h = W / 2;
     const int vpb = blockDim.x / W;
     const int vl = threadIdx.x / W, w = threadIdx.x % W;
     const int v = blockIdx.x * vpb + vl;
@@ -439,41 +455,37 @@ __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags
     if (MODEL == kR1R2S)
         for (int f = 0; f < p.P.n_fa; ++f) sincosf(b1 * p.P.fa_rad[f], &sa[f], &ca[f]);
     VoxAux va{b1, sa, ca, 1};
-    float x[kMaxParam];
-    for (int q = 0; q < kMaxParam; ++q) x[q] = 0.0f;
+    float x[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) x[q] = 0.0f;
     if (live) {
         if (flags & kGwgInit) {
             // locals: x0 + (ub-lb)*startRange*randn, clamped (mcmc.m:483-484), goodman_weare's stream
-            float nrm[8];
-            for (int j = 0; j * 4 < nvar; ++j) {
-                U4 u = philox((uint32_t)v, (uint32_t)w, (uint32_t)j, kTagGwInit, p.seed);
-                float n0, n1, n2, n3;
-                box_muller(u.x, u.y, n0, n1);
-                box_muller(u.z, u.w, n2, n3);
-                nrm[4 * j] = n0; nrm[4 * j + 1] = n1; nrm[4 * j + 2] = n2; nrm[4 * j + 3] = n3;
-            }
-            for (int q = 0; q < nvar; ++q)
-                if (!p.is_global[q]) {
-                    float val = p.x0[(size_t)q * p.nvox + v] + (p.ub[q] - p.lb[q]) * p.start_range * nrm[q];
-                    x[q] = fminf(fmaxf(val, p.lb[q]), p.ub[q]);
-                }
+            float xi[NV];
+            gw_walker_start<NV>(p, v, w, xi);
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+                if (!p.is_global[q]) x[q] = xi[q];
         } else {
-            for (int q = 0; q < nvar; ++q)
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
                 if (!p.is_global[q]) x[q] = xstate[((size_t)q * p.nvox + v) * W + w];
         }
-        for (int q = 0; q < nvar; ++q) xv[w * nvar + q] = x[q];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) xv[w * NV + q] = x[q];
     }
     __syncthreads();
     // parameter vector of (this voxel, walker ww) with globals gsrc
-    auto compose = [&](const float* loc, const float* gsrc, float* out) {
-        for (int q = 0; q < nvar; ++q) out[q] = p.is_global[q] ? gsrc[q] : loc[q];
+    auto compose = [&](const float (&loc)[NV], const float* gsrc, float (&out)[NV]) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) out[q] = p.is_global[q] ? gsrc[q] : loc[q];
     };
     double lp = 0.0;
     if (live) {
         if (flags & kGwgInit) {
-            float xx[kMaxParam];
+            float xx[NV];
             compose(x, s_g + w * nvar, xx);
-            lp = log_prob<MODEL>(p, s_P, xx, yv, wv, va);
+            lp = log_prob_t<MODEL, NV>(nm, s_P, xx, yv, 1, wv, 1, va);
         } else {
             lp = lpstate[(size_t)v * W + w];
             if ((flags & kGwgApply) && p.gacc[w]) lp = p.lpg[(size_t)v * W + w];
@@ -485,7 +497,9 @@ __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags
         const float expo = (float)(p.nnd - 1);
         for (int s = 0; s < (p.update == 0 ? 1 : 2); ++s) {
             const bool act = live && (p.update == 0 || (s == 0 ? w < h : w >= h));
-            float xn[kMaxParam];
+            float xn[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) xn[q] = 0.0f;
             bool acc = false;
             double lpp = 0.0;
             if (act) {
@@ -495,24 +509,26 @@ __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags
                 float t = (p.a - 1.0f) * u01(u.x) + 1.0f;
                 float zz = t * t / p.a;
                 bool oob = false;
-                for (int q = 0; q < nvar; ++q) {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
                     if (p.is_global[q]) { xn[q] = 0.0f; continue; }
                     float xq = xv[q0 * nvar + q];
                     float xp = xq + (xv[w * nvar + q] - xq) * zz;
                     oob |= (xp < p.lb[q]) || (xp > p.ub[q]);
                     xn[q] = fminf(fmaxf(xp, p.lb[q]), p.ub[q]);
                 }
-                float xx[kMaxParam];
+                float xx[NV];
                 compose(xn, s_g + w * nvar, xx);
-                lpp = log_prob<MODEL>(p, s_P, xx, yv, wv, va);
+                lpp = log_prob_t<MODEL, NV>(nm, s_P, xx, yv, 1, wv, 1, va);
                 double lr = (double)expo * (double)logf(zz) + (lpp - lp);
                 acc = !oob && lr > (double)logf(u01(u.y));
             }
             __syncthreads();  // the (half-)ensemble was read before any walker moves
             if (act && acc) {
-                for (int q = 0; q < nvar; ++q) {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
                     x[q] = xn[q];
-                    xv[w * nvar + q] = xn[q];
+                    xv[w * NV + q] = xn[q];
                 }
                 lp = lpp;
                 ++nacc;
@@ -534,7 +550,8 @@ __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags
                 p.sumsq[(size_t)q * p.nvox + v] += s2;
             }
             if (p.posterior)
-                for (int q = 0; q < nvar; ++q)
+#pragma unroll
+                for (int q = 0; q < NV; ++q)
                     if (!p.is_global[q])
                         p.posterior[((((size_t)q * p.repetition + rr) * p.ns + c) * W + w) * p.nvox + v] = x[q];
         }
@@ -555,9 +572,9 @@ __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags
         const bool act = gwg_active(half, w, W);
         double d = 0.0;
         if (live && act) {
-            float xx[kMaxParam];
+            float xx[NV];
             compose(x, s_gp + w * nvar, xx);
-            double lpg = log_prob<MODEL>(p, s_P, xx, yv, wv, va);
+            double lpg = log_prob_t<MODEL, NV>(nm, s_P, xx, yv, 1, wv, 1, va);
             p.lpg[(size_t)v * W + w] = lpg;
             d = lpg - lp;
         }
@@ -570,7 +587,8 @@ __global__ void gwg_step_kernel(McmcParams p, int rr, int k, int warm, int flags
         }
     }
     if (live) {
-        for (int q = 0; q < nvar; ++q)
+#pragma unroll
+        for (int q = 0; q < NV; ++q)
             if (!p.is_global[q]) xstate[((size_t)q * p.nvox + v) * W + w] = x[q];
         lpstate[(size_t)v * W + w] = lp;
     }
@@ -696,6 +714,8 @@ cudaError_t launch_mcmc_partners(const McmcParams& p, int* partner, cudaStream_t
 template <int MODEL>
 static cudaError_t mcmc_run_model(const McmcParams& p, int block_hint, cudaStream_t s,
                                   float* xstate, double* lpstate) {
+    constexpr int NV = ModelNP<MODEL>::value + 1;  // the model's parameters and the noise sigma
+    if (p.nvar != NV) return cudaErrorInvalidValue;
     const int chunk = 250;  // steps per launch: bounded kernel duration
     if (p.algorithm == 1) {
         int W = p.nwalker, h = W / 2;
@@ -706,13 +726,14 @@ static cudaError_t mcmc_run_model(const McmcParams& p, int block_hint, cudaStrea
         size_t smem = sizeof(float) * ((size_t)vpb * W * p.nvar + 2 * (size_t)vpb * p.nm);
         int nb = (p.nvox + vpb - 1) / vpb;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(gw_kernel<MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(gw_kernel<MODEL, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
         for (int rr = 0; rr < p.repetition; ++rr)
             for (int k0 = 1; k0 <= p.iteration; k0 += chunk) {
                 int k1 = k0 + chunk - 1 < p.iteration ? k0 + chunk - 1 : p.iteration;
-                gw_kernel<MODEL><<<nb, block, smem, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, p.sum, p.sumsq);
+                gw_kernel<MODEL, NV><<<nb, block, smem, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, p.sum,
+                                                             p.sumsq);
                 ++g_kernel_launches;
                 cudaError_t e = cudaGetLastError();
                 if (e != cudaSuccess) return e;
@@ -723,7 +744,8 @@ static cudaError_t mcmc_run_model(const McmcParams& p, int block_hint, cudaStrea
         for (int rr = 0; rr < p.repetition; ++rr)
             for (int k0 = 1; k0 <= p.iteration; k0 += chunk) {
                 int k1 = k0 + chunk - 1 < p.iteration ? k0 + chunk - 1 : p.iteration;
-                mh_kernel<MODEL><<<nb, block, 0, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, p.sum, p.sumsq);
+                mh_kernel<MODEL, NV><<<nb, block, 0, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, p.sum,
+                                                          p.sumsq);
                 ++g_kernel_launches;
                 cudaError_t e = cudaGetLastError();
                 if (e != cudaSuccess) return e;
@@ -753,15 +775,18 @@ void gwg_launch_shape(const McmcParams& p, int block_hint, int* vpb, int* block,
 template <int MODEL>
 static cudaError_t mcmc_run_global(const McmcParams& p, int block_hint, cudaStream_t s, float* xstate,
                                    double* lpstate) {
+    if (p.nvar != ModelNP<MODEL>::value + 1) return cudaErrorInvalidValue;
     int vpb, block, nb;
     size_t smem;
     gwg_launch_shape(p, block_hint, &vpb, &block, &nb, &smem);
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(gwg_step_kernel<MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(gwg_step_kernel<MODEL, ModelNP<MODEL>::value + 1>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     auto A = [&](int rr, int k, int warm, int flags, int half) {
-        gwg_step_kernel<MODEL><<<nb, block, smem, s>>>(p, rr, k, warm, flags, half, xstate, lpstate);
+        gwg_step_kernel<MODEL, ModelNP<MODEL>::value + 1><<<nb, block, smem, s>>>(p, rr, k, warm, flags, half,
+                                                                                  xstate, lpstate);
         ++g_kernel_launches;
     };
     auto B = [&](int rr, int k, int warm, int half, int c) {

@@ -68,6 +68,46 @@ gx_status scratch_address(unsigned char** out) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
+// Byte offsets of the working arrays inside the fixed array for nvox voxels
+// (padded to whole blocks of B), nm measurements, np parameters and N
+// iterations; `total` is the bytes the layout needs.
+struct Layout {
+    size_t nvtot, nblocks;
+    size_t vol, blk, sched, hist, data, th, z, m1, m2, total;
+};
+
+Layout layout(size_t nvox, int B, int nm, int np, int N) {
+    Layout L;
+    L.nvtot = (nvox + B - 1) / B * B;
+    L.nblocks = L.nvtot / B;
+    size_t off = 0;
+    L.vol = off;   off += align256(sizeof(DevVol));
+    L.blk = off;   off += align256(sizeof(int) * L.nblocks);
+    L.sched = off; off += align256(sizeof(float2) * ((size_t)N + 1));
+    L.hist = off;  off += align256(sizeof(double) * ((size_t)N + 1) * kHistW);
+    L.data = off;  off += align256(sizeof(float) * nm * L.nvtot);
+    L.th = off;    off += align256(sizeof(float) * np * L.nvtot);
+    L.z = off;     off += align256(sizeof(float) * np * L.nvtot);
+    L.m1 = off;    off += align256(sizeof(float) * np * L.nvtot);
+    L.m2 = off;    off += align256(sizeof(float) * np * L.nvtot);
+    L.total = off;
+    return L;
+}
+
+// The largest voxel count whose layout fits the fixed array (0 if none does):
+// the layout grows with nvox, so a binary search over the same function
+// gives a figure that a retry is certain to pass.
+size_t max_voxels(int B, int nm, int np, int N) {
+    if (layout(1, B, nm, np, N).total > kScratchBytes) return 0;
+    size_t lo = 1, hi = kScratchBytes / sizeof(float) + 1;  // layout(hi) cannot fit
+    while (hi - lo > 1) {
+        const size_t mid = lo + (hi - lo) / 2;
+        if (layout(mid, B, nm, np, N).total <= kScratchBytes) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 }  // namespace
 
 extern "C" gx_status gx_askadam_noalloc(const gx_model* model, const float* data, const float* theta0,
@@ -76,48 +116,38 @@ extern "C" gx_status gx_askadam_noalloc(const gx_model* model, const float* data
     if (!model || !data || !theta0 || !o || !theta_out)
         return internal_fail(GX_EINVAL, "gx_askadam_noalloc: NULL argument");
     if (nvox < 1) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: nvox must be >= 1");
-    if (o->iteration < 0) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: iteration must be >= 0");
-    if (!o->lb || !o->ub) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: lb/ub are required");
     if (o->n_reg > 0 && o->lambda[0] > 0)
         return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: regularisation (TV or prior) needs gx_askadam");
     if (o->path != GX_PATH_FUSED) return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: fused path only");
+    if (o->robust_convergence)
+        return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: robustConvergence runs on gx_askadam's "
+                                              "op-by-op path; this entry point has the fused path only");
     if (internal_can_stop(o))
         return internal_fail(GX_EUNSUPPORTED, "gx_askadam_noalloc: runs every iteration; disable the stopping "
                                               "criteria (tol, patienceConvergence, step/grad tolerances)");
-    if (o->loss == GX_LOSS_GAUSS_LOGP || o->loss == GX_LOSS_RICIAN_LOGP)
-        if (!(o->sigma > 0)) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: likelihood loss needs sigma > 0");
     DevProtocol P;
     int np = 0, nm = 0, id = 0;
     gx_status st = internal_model(model, o->lb, o->ub, &P, &np, &nm, &id);
     if (st != GX_OK) return st;
-    for (int k = 0; k < np; ++k)
-        if (!(o->ub[k] > o->lb[k])) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: ub must exceed lb");
+    st = internal_validate_opts(o, np);  // iteration, bounds, loss / optimiser / transform kinds
+    if (st != GX_OK) return st;
+    if (o->loss == GX_LOSS_GAUSS_LOGP || o->loss == GX_LOSS_RICIAN_LOGP)
+        if (!(o->sigma > 0)) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: likelihood loss needs sigma > 0");
     const int B = o->block_size > 0 ? o->block_size : 128;
     if (B % 32 || B > 1024) return internal_fail(GX_EINVAL, "gx_askadam_noalloc: bad block_size");
     const int N = o->iteration;
 
     // layout of the fixed working memory
-    const size_t nvtot = ((size_t)nvox + B - 1) / B * B;
-    const size_t nblocks = nvtot / B;
-    size_t off = 0;
-    const size_t off_vol = off;   off += align256(sizeof(DevVol));
-    const size_t off_blk = off;   off += align256(sizeof(int) * nblocks);
-    const size_t off_sched = off; off += align256(sizeof(float2) * ((size_t)N + 1));
-    const size_t off_hist = off;  off += align256(sizeof(double) * ((size_t)N + 1) * kHistW);
-    const size_t off_data = off;  off += align256(sizeof(float) * nm * nvtot);
-    const size_t off_th = off;    off += align256(sizeof(float) * np * nvtot);
-    const size_t off_z = off;     off += align256(sizeof(float) * np * nvtot);
-    const size_t off_m1 = off;    off += align256(sizeof(float) * np * nvtot);
-    const size_t off_m2 = off;    off += align256(sizeof(float) * np * nvtot);
-    if (off > kScratchBytes) {
-        size_t fixed = align256(sizeof(DevVol)) + align256(sizeof(float2) * ((size_t)N + 1)) +
-                       align256(sizeof(double) * ((size_t)N + 1) * kHistW);
-        size_t per = sizeof(float) * (nm + 4 * (size_t)np) + sizeof(int) / B + 1;
+    const Layout Lo = layout((size_t)nvox, B, nm, np, N);
+    const size_t nvtot = Lo.nvtot, nblocks = Lo.nblocks;
+    const size_t off_vol = Lo.vol, off_blk = Lo.blk, off_sched = Lo.sched, off_hist = Lo.hist;
+    const size_t off_data = Lo.data, off_th = Lo.th, off_z = Lo.z, off_m1 = Lo.m1, off_m2 = Lo.m2;
+    if (Lo.total > kScratchBytes) {
         char msg[256];
         snprintf(msg, sizeof(msg),
                  "gx_askadam_noalloc: %d voxels x %d iterations need %zu bytes of working memory; the fixed "
-                 "array holds %zu (at most about %zu voxels at this iteration count)",
-                 nvox, N, off, kScratchBytes, fixed < kScratchBytes ? (kScratchBytes - fixed) / per : (size_t)0);
+                 "array holds %zu (at most %zu voxels at this iteration count)",
+                 nvox, N, Lo.total, kScratchBytes, max_voxels(B, nm, np, N));
         return internal_fail(GX_EINVAL, msg);
     }
     unsigned char* base = nullptr;
@@ -151,9 +181,10 @@ extern "C" gx_status gx_askadam_noalloc(const gx_model* model, const float* data
                     chunk[i] = float2{(float)lr, 0.f};
             }
         }
+        // a copy from pageable host memory has staged its source when the call
+        // returns, so the stack buffer can be refilled at once
         NA_CK(cudaMemcpyAsync(base + off_sched + sizeof(float2) * e0, chunk, sizeof(float2) * n,
                               cudaMemcpyHostToDevice, s));
-        NA_CK(cudaStreamSynchronize(s));  // the stack buffer is reused by the next chunk
     }
     NA_CK(cudaMemsetAsync(base + off_hist, 0, sizeof(double) * ((size_t)N + 1) * kHistW, s));
     float* d_data = reinterpret_cast<float*>(base + off_data);

@@ -118,3 +118,16 @@ def nexi_volume(nvox: int, seed: int, sigma=0.02, rician=True, nx=100):
     else:
         y = S + sigma * n1
     return np.ascontiguousarray(y.T.astype(np.float32)), {"fa": fa, "Da": Da, "De": De, "ra": ra}
+
+
+def r2s_tv_volume(seed: int = 1002, dims=(128, 128, 64)):
+    """The mono-exponential + 3-D TV workload: ellipsoid mask (629,432 voxels
+    on 128x128x64), 12 echoes, seeded phantom; masked data [12, nvox], grid
+    indices, and the start (M0, R2*) = (1, 30) of every voxel."""
+    from . import utils
+    mask = ellipsoid_mask(tuple(dims), 1.05)
+    data, gt = r2s_phantom(mask, seed)
+    idx = utils.mask_index(mask)
+    y = utils.reshape_ND2GD(data, idx)
+    th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, y.shape[1]))
+    return {"mask": mask, "y": y, "idx": idx.astype(np.int32), "th0": th0, "nvox": y.shape[1], "gt": gt}

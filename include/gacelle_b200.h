@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define GX_ABI_VERSION 5
+#define GX_ABI_VERSION 6
 
 typedef enum {
     GX_OK = 0,
@@ -282,6 +282,24 @@ gx_status gx_last_timing(gx_context* ctx, gx_timing* out);
 /* Host-side cancel flag polled between launches; nonzero stops the call
  * with GX_ECANCELLED.  NULL clears it. */
 gx_status gx_set_cancel_flag(gx_context* ctx, volatile int32_t* flag);
+
+/* Fault injection for tests of the error paths (the reference's counterparts
+ * are its error() identifiers and the out-of-memory catch of
+ * utils/utils.m:698-706).  The settings hold for the context's following
+ * calls until cleared (NULL or all zero). */
+typedef struct {
+    /* > 0: the n-th device workspace request of every following call fails as
+     * an allocation failure would (GX_ENOMEM), without touching the device. */
+    int32_t fail_alloc_at;
+    /* > 0: bound, in SM clock cycles, of every wait in the persistent TV
+     * kernel (default about 2 s). */
+    int64_t wait_limit_cycles;
+    /* > 0: the persistent kernel's grid barrier waits for this many arrivals
+     * more than the grid makes, so its bounded wait runs out: every CTA then
+     * returns and the call reports GX_ETIMEOUT, with the context usable. */
+    int32_t barrier_extra_arrivals;
+} gx_test_hooks;
+gx_status gx_context_set_test_hooks(gx_context* ctx, const gx_test_hooks* hooks);
 
 gx_status gx_model_sizes(const gx_model* model, int32_t* nparam, int32_t* nmeas);
 

@@ -46,7 +46,7 @@ def test_struct_layouts_match_binding(lib):
     for name, cls in _lib.STRUCTS.items():
         assert lib.gx_struct_size(name.encode()) == C.sizeof(cls), name
     assert lib.gx_struct_size(b"nope") == 0
-    assert lib.gx_abi_version() == 5
+    assert lib.gx_abi_version() == 6
     assert b"sm_100a" in lib.gx_version()
 
 

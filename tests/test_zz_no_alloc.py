@@ -8,11 +8,13 @@ engine works in a fixed array inside the library.
 The entry point must give the same parameters as gx_askadam (the existing
 entry point) within the parity tolerance of the other tests (relative RMSE
 1e-4; in practice identical), on two calls in a row, because every call
-reuses the same fixed working array.  This file is collected last so that a
+reuses the same fixed working array; and the device's free memory must not
+change across a call.  This file is collected last so that a
 run stopping at the first failure has already run every other test; it also
 passes alone in a fresh process.
 """
 import ctypes as C
+import re
 
 import numpy as np
 import pytest
@@ -73,9 +75,16 @@ def test_noalloc_matches_askadam_on_two_calls(kind, nvox, iters):
     for call in range(2):
         d_out.fill_(float("nan"))
         loss = C.c_double(0.0)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(dev)[0]
         st = L.gx_askadam_noalloc(C.byref(model.s), d_y.data_ptr(), d_th0.data_ptr(), nvox, C.byref(opts),
                                   C.c_void_p(stream.cuda_stream), d_out.data_ptr(), C.byref(loss))
         assert st == _lib.GX_OK, L.gx_last_error()
+        free1 = torch.cuda.mem_get_info(dev)[0]
+        if call == 1:
+            # the first call may load the library's kernels onto the device; the
+            # second one finds everything in place and allocates nothing
+            assert free1 == free0, (free0, free1)
         out = d_out.cpu().numpy()
         assert np.all(np.isfinite(out)), call
         for k in range(len(names)):
@@ -101,10 +110,38 @@ def test_noalloc_rejects_problems_beyond_its_fixed_memory():
                               d.data_ptr(), None)
     assert st == _lib.GX_EINVAL
     msg = L.gx_last_error().decode()
-    assert "at most about" in msg and "voxels" in msg
+    m = re.search(r"at most (\d+) voxels", msg)
+    assert m, msg
+    nmax = int(m.group(1))
+    assert 100_000 < nmax < 50_000_000
+    # the reported maximum is accepted, one voxel more is not
+    big_y = torch.zeros((y.shape[0], nmax + 1), dtype=torch.float32, device="cuda")
+    big_th = torch.ones((2, nmax + 1), dtype=torch.float32, device="cuda")
+    big_th[1] = 30.0
+    big_out = torch.empty((2, nmax + 1), dtype=torch.float32, device="cuda")
+    st = L.gx_askadam_noalloc(C.byref(model.s), big_y.data_ptr(), big_th.data_ptr(), nmax + 1, C.byref(opts),
+                              None, big_out.data_ptr(), None)
+    assert st == _lib.GX_EINVAL
+    st = L.gx_askadam_noalloc(C.byref(model.s), big_y.data_ptr(), big_th.data_ptr(), nmax, C.byref(opts), None,
+                              big_out.data_ptr(), None)
+    assert st == _lib.GX_OK, L.gx_last_error()
+    assert torch.isfinite(big_out[:, :nmax]).all()
     # stopping criteria cannot be honoured without the host-driven path
     f2 = dict(f, tol=1e-3)
     o2 = askadam_solver.build_opts(f2, names, lb, ub)
     st = L.gx_askadam_noalloc(C.byref(model.s), d.data_ptr(), d.data_ptr(), 64, C.byref(o2), None,
                               d.data_ptr(), None)
     assert st == _lib.GX_EUNSUPPORTED
+    # robustConvergence belongs to gx_askadam's op-by-op path: refused, not silently ignored
+    o3 = askadam_solver.build_opts(f, names, lb, ub)
+    o3.robust_convergence = 1
+    st = L.gx_askadam_noalloc(C.byref(model.s), d.data_ptr(), d.data_ptr(), 64, C.byref(o3), None,
+                              d.data_ptr(), None)
+    assert st == _lib.GX_EUNSUPPORTED
+    # unknown loss / optimiser / transform kinds are rejected as gx_askadam rejects them
+    for field, bad in (("loss", 17), ("optimiser", 9), ("transform", 5)):
+        o4 = askadam_solver.build_opts(f, names, lb, ub)
+        setattr(o4, field, bad)
+        st = L.gx_askadam_noalloc(C.byref(model.s), d.data_ptr(), d.data_ptr(), 64, C.byref(o4), None,
+                                  d.data_ptr(), None)
+        assert st == _lib.GX_EINVAL, field
