@@ -91,13 +91,13 @@ class GxMcmcOpts(C.Structure):
                 ("step_size", C.c_double), ("start_range", C.c_double),
                 ("ensemble_update", C.c_int32), ("x_step", _dp), ("lb", _dp), ("ub", _dp),
                 ("seed", C.c_uint64), ("block_size", C.c_int32), ("is_global", _i32p),
-                ("global_warmup", C.c_int32)]
+                ("global_warmup", C.c_int32), ("nbin", C.c_int32)]
 
 
 class GxMcmcResult(C.Structure):
     _fields_ = [("mean", _fp), ("std", _fp), ("posterior", _fp), ("n_accepted", C.c_int64),
                 ("n_proposals", C.c_int64), ("ns", C.c_int32), ("n_global_accepted", C.c_int64),
-                ("n_global_proposals", C.c_int64)]
+                ("n_global_proposals", C.c_int64), ("median", _fp), ("iqr", _fp), ("mode", _fp)]
 
 
 class GxTiming(C.Structure):

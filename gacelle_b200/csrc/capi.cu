@@ -59,7 +59,8 @@ enum Slot {
     S_GRID1, S_P_TH, S_P_DTH, S_P_SIG, S_P_DSIG, S_P_RES, S_P_GTH, S_P_GZ, S_P_ACC, S_ZMIN,
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
-    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_SURF_NB, S_SURF_LEN, S_NSLOTS
+    S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_SURF_NB, S_SURF_LEN,
+    S_MC_STATS, S_NSLOTS
 };
 
 struct gx_context {
@@ -1454,6 +1455,7 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     } else if (!o->x_step) {
         return fail(GX_EINVAL, "MH needs x_step (xStepSize)");
     }
+    if (o->nbin < 0 || o->nbin == 1 || o->nbin > (1 << 15)) return fail(GX_EINVAL, "Nbin must be in [2, 32768] (0 = 1001)");
     int ng = 0;
     if (o->is_global)
         for (int q = 0; q < nvar; ++q) ng += o->is_global[q] != 0;
@@ -1506,9 +1508,13 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
         CK(cudaMemsetAsync(sum, 0, sizeof(double) * nvar * nv, c->stream));
         CK(cudaMemsetAsync(sumsq, 0, sizeof(double) * nvar * nv, c->stream));
         CK(cudaMemsetAsync(nacc, 0, sizeof(unsigned long long), c->stream));
-        if (r.posterior) {
-            if (mem == GX_MEM_DEVICE) post = r.posterior;
-            else TRY(wsT(c, S_MC_POST, (size_t)nvar * o->repetition * ns * W * nv, &post));
+        // the kept samples stay on the device when the posterior is returned or
+        // summarised there (median / iqr / mode)
+        const bool want_stats = r.median || r.iqr || r.mode;
+        const size_t npost = (size_t)nvar * o->repetition * ns * W * nv;
+        if (r.posterior || want_stats) {
+            if (mem == GX_MEM_DEVICE && r.posterior) post = r.posterior;
+            else TRY(wsT(c, S_MC_POST, npost, &post));
         }
         if (o->algorithm == GX_MCMC_ENSEMBLE) TRY(wsT(c, S_MC_PART, (size_t)o->repetition * o->iteration * W, &partner));
         p.data = data; p.weights = w; p.b1 = b1; p.x0 = x0; p.shift = shift; p.sum = sum; p.sumsq = sumsq;
@@ -1553,6 +1559,8 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
             p.partial = reinterpret_cast<double*>(gb + o_part);
             CK(cudaMemsetAsync(gb, 0, o_gp, c->stream));  // state, decisions, sums, counter
         }
+        // slots that no step fills stay zero (res2out counts them)
+        if (post && mcmc_missing_slots(p) > 0) CK(cudaMemsetAsync(post, 0, sizeof(float) * npost, c->stream));
         if (partner) CK(launch_mcmc_partners(p, partner, c->stream));
         CK(cudaEventRecord(c->ev[2], c->stream));
         CK(launch_mcmc(p, id, o->block_size, c->stream));
@@ -1567,13 +1575,42 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
             TRY(wsT(c, S_MC_STD, (size_t)nvar * nv, &stdv));
         }
         CK(launch_mcmc_finalize(p, mean, stdv, c->stream));
+        float *dmed = nullptr, *diqr = nullptr, *dmode = nullptr;
+        if (want_stats) {
+            const int nbin = o->nbin > 0 ? o->nbin : 1001;
+            // [3][nvar][nv] outputs (host calls) and the bounds [nvar][2] in one buffer
+            const size_t nst = (size_t)nvar * nv;
+            const size_t o_lb = (sizeof(float) * 3 * nst + 15) / 16 * 16;
+            unsigned char* sb;
+            TRY(wsT(c, S_MC_STATS, o_lb + sizeof(double) * 2 * nvar, &sb));
+            float* st = reinterpret_cast<float*>(sb);
+            double* lbub = reinterpret_cast<double*>(sb + o_lb);
+            double hb[2 * kMaxParam];
+            for (int q = 0; q < nvar; ++q) { hb[2 * q] = o->lb[q]; hb[2 * q + 1] = o->ub[q]; }
+            CK(cudaMemcpyAsync(lbub, hb, sizeof(double) * 2 * nvar, cudaMemcpyHostToDevice, c->stream));
+            if (mem == GX_MEM_DEVICE) { dmed = r.median; diqr = r.iqr; dmode = r.mode; }
+            else {
+                dmed = r.median ? st : nullptr;
+                diqr = r.iqr ? st + nst : nullptr;
+                dmode = r.mode ? st + 2 * nst : nullptr;
+            }
+            CK(launch_posterior_stats(post, nvar, nv, o->repetition * ns * W, nbin, lbub, dmed, diqr, dmode,
+                                      c->stream));
+        }
         if (mem == GX_MEM_HOST) {
+            const size_t nst = (size_t)nvar * nv;
+            float* hs[3] = {r.median, r.iqr, r.mode};
+            float* ds[3] = {dmed, diqr, dmode};
+            for (int j = 0; j < 3; ++j)
+                if (hs[j]) {
+                    CK(cudaMemcpyAsync(hs[j], ds[j], sizeof(float) * nst, cudaMemcpyDeviceToHost, c->stream));
+                    d2h += sizeof(float) * nst;
+                }
             if (r.mean) { CK(cudaMemcpyAsync(r.mean, mean, sizeof(float) * nvar * nv, cudaMemcpyDeviceToHost, c->stream)); d2h += sizeof(float) * nvar * nv; }
             if (r.std) { CK(cudaMemcpyAsync(r.std, stdv, sizeof(float) * nvar * nv, cudaMemcpyDeviceToHost, c->stream)); d2h += sizeof(float) * nvar * nv; }
             if (r.posterior) {
-                size_t n = (size_t)nvar * o->repetition * ns * W * nv;
-                CK(cudaMemcpyAsync(r.posterior, post, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
-                d2h += sizeof(float) * n;
+                CK(cudaMemcpyAsync(r.posterior, post, sizeof(float) * npost, cudaMemcpyDeviceToHost, c->stream));
+                d2h += sizeof(float) * npost;
             }
         }
         unsigned long long acc = 0, gacc = 0;

@@ -200,6 +200,14 @@ cudaError_t launch_mcmc_partners(const McmcParams& p, int* partner, cudaStream_t
 void gwg_launch_shape(const McmcParams& p, int block_hint, int* vpb, int* block, int* nblocks, size_t* smem);
 cudaError_t launch_mcmc(const McmcParams& p, int model, int block, cudaStream_t s);
 cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, cudaStream_t s);
+// Kept slots the reference preallocates but never fills: numel(Nburnin+1:thinning:iteration)
+// minus the steps k with mod(k - Nburnin + 1, thinning) == 0.
+int mcmc_missing_slots(const McmcParams& p);
+// Posterior median / iqr / mode (posterior_stats.cu) of post [nvar][N][nvox],
+// N = rep * ns * W; lbub [nvar][2] (lb, ub) on the device; outputs
+// [nvar][nvox] or nullptr.
+cudaError_t launch_posterior_stats(const float* post, int nvar, int nvox, int N, int nbin, const double* lbub,
+                                   float* median, float* iqr, float* mode, cudaStream_t s);
 
 extern long long g_kernel_launches;  // launches of this library's kernels (process-wide)
 

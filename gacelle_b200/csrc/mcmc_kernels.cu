@@ -863,13 +863,17 @@ cudaError_t launch_mcmc(const McmcParams& p, int model, int block, cudaStream_t 
     return e;
 }
 
-cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, cudaStream_t s) {
+int mcmc_missing_slots(const McmcParams& p) {
     // kept = #k in (nburnin, iteration] with (k - nburnin + 1) % thinning == 0
     int kept = 0;
     for (int k = p.nburnin + 1; k <= p.iteration; ++k)
         if ((k - p.nburnin + 1) % p.thinning == 0) ++kept;
     int missing = p.ns - kept;
-    if (missing < 0) missing = 0;
+    return missing < 0 ? 0 : missing;
+}
+
+cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, cudaStream_t s) {
+    const int missing = mcmc_missing_slots(p);
     mcmc_finalize_kernel<<<(p.nvox + 127) / 128, 128, 0, s>>>(p, missing, mean, stdv);
     ++g_kernel_launches;
     if (p.ng > 0) {

@@ -114,12 +114,13 @@ class mcmc:
         ns = number_of_samples(fitting)
         W = int(fitting["Nwalker"]) if fitting["algorithm"].lower() == "ensemble" else 1
         post_bytes = 4 * len(names) * nv * W * ns * int(fitting["repetition"])
-        need_post = any(m in metrics for m in ("median", "iqr", "mode"))
-        want_post = fitting.get("returnPosterior", post_bytes <= POSTERIOR_LIMIT_BYTES) or need_post
-        res = self._run(model, y, w, x0, b1, names, fitting, want_post, is_global)
+        want_post = fitting.get("returnPosterior", post_bytes <= POSTERIOR_LIMIT_BYTES)
+        res = self._run(model, y, w, x0, b1, names, fitting, want_post, is_global,
+                        stats=[m for m in ("median", "iqr", "mode") if m in metrics])
         return self.res2out(res, fitting, mask, names)
 
-    def _run(self, model, y, w, x0, b1, names, fitting, want_post, is_global=None):
+    def _run(self, model, y, w, x0, b1, names, fitting, want_post, is_global=None, stats=()):
+        """stats: any of 'median', 'iqr', 'mode', computed on the device."""
         ctx = self.ctx or _lib.Context.default()
         nvar = len(names)
         nm, nv = y.shape
@@ -145,6 +146,7 @@ class mcmc:
         o.ub = ub.ctypes.data_as(_lib._dp)
         o.seed = int(fitting.get("seed", model.seed))
         o.block_size = int(fitting.get("blockSize", 0))
+        o.nbin = int(fitting.get("Nbin", 1001))
         keep = [y, x0]
         if is_global is not None:
             ig = np.ascontiguousarray(is_global, dtype=np.int32)
@@ -172,12 +174,16 @@ class mcmc:
         r.std = std.ctypes.data_as(_lib._fp)
         if post is not None:
             r.posterior = post.ctypes.data_as(_lib._fp)
+        summaries = {}
+        for m in stats:
+            summaries[m] = np.zeros((nvar, nv), np.float32)
+            setattr(r, m, summaries[m].ctypes.data_as(_lib._fp))
         _lib.check(_lib.lib().gx_mcmc(ctx.ptr, C.byref(model._gx_model().s), _lib.MEM_HOST, C.byref(vol), 1,
                                       C.byref(o), C.byref(r)))
         self.last_timing = ctx.timing()
         self.last_stats = {"n_accepted": r.n_accepted, "n_proposals": r.n_proposals, "ns": r.ns,
                            "n_global_accepted": r.n_global_accepted, "n_global_proposals": r.n_global_proposals}
-        return {"mean": mean, "std": std, "posterior": post, "W": W, "ns": ns, "rep": rep,
+        return {"mean": mean, "std": std, "posterior": post, "W": W, "ns": ns, "rep": rep, **summaries,
                 "is_global": list(is_global) if is_global is not None else [0] * nvar}
 
     @staticmethod
@@ -200,26 +206,10 @@ class mcmc:
         for m in [m.lower() for m in fitting["metric"]]:
             out[m] = {}
             for k, p in enumerate(names):
-                if m == "mean":
-                    v = res["mean"][k]
-                elif m == "std":
-                    v = res["std"][k]
+                if m in ("mean", "std", "median", "iqr", "mode") and m in res:
+                    v = res[m][k]   # computed on the device
                 else:
-                    samples = post[k].reshape(-1, nv).T.astype(np.float64)  # [nv, W*ns*rep]
-                    if m == "median":
-                        v = np.median(samples, axis=1)
-                    elif m == "iqr":
-                        q = np.percentile(samples, [25, 75], axis=1, method="hazen")
-                        v = q[1] - q[0]
-                    elif m == "mode":
-                        nb = int(fitting.get("Nbin", 1001))
-                        edges = np.linspace(fitting["lb"][k] - 1e-8, fitting["ub"][k] + 1e-8, nb)
-                        bins = np.clip(np.searchsorted(edges, samples, side="right") - 1, 0, nb - 2)
-                        counts = np.apply_along_axis(lambda r: np.bincount(r, minlength=nb - 1), 1, bins)
-                        mi = np.argmax(counts, axis=1)
-                        v = (edges[mi] + edges[mi + 1]) / 2
-                    else:
-                        raise GacelleError(GX_EINVAL, f"unknown metric {m}")
+                    raise GacelleError(GX_EINVAL, f"unknown metric {m}")
                 if isg[k]:
                     # one value for all voxels: a scalar, as reshape_ND2image passes it
                     out[m][p] = float(np.asarray(v).ravel()[0])

@@ -233,6 +233,7 @@ typedef struct {
      * NULL: every parameter is per voxel. */
     const int32_t* is_global;   /* [nvar] or NULL */
     int32_t global_warmup;      /* global-only iterations before the joint loop */
+    int32_t nbin;               /* mode: edges linspace(lb - 1e-8, ub + 1e-8, nbin); 0 = 1001 */
 } gx_mcmc_opts;
 
 typedef struct {
@@ -245,6 +246,15 @@ typedef struct {
      * statistics and posterior of a global parameter repeat its value for
      * every voxel */
     int64_t n_global_accepted, n_global_proposals;
+    /* res2out's order and histogram summaries (utils/mcmc.m:806-862), each
+     * [nvar][nvox] or NULL, computed on the device from the kept samples (the
+     * posterior need not be returned): median (mean of the two middle values
+     * for an even count), iqr (prctile midpoint rule), mode (centre of the most
+     * populated of the nbin - 1 bins, the lowest on ties; samples outside the
+     * edges ignored, NaN when none is inside) */
+    float* median;
+    float* iqr;
+    float* mode;
 } gx_mcmc_result;
 
 /* Device-side timing of the last compute call on a context (CUDA events on

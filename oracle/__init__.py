@@ -442,3 +442,35 @@ def mcmc(model: Model, vol: Volume, x0, lb, ub, algorithm="ensemble", iteration=
         # [nvar][rep][ns][W][nv] in C order == MATLAB [Nv, W, Ns, rep] per parameter
         out["posterior"] = post.reshape(nvar, repetition, ns, W, nv)
     return out
+
+
+def res2out_summaries(samples, lb, ub, nbin=1001):
+    """The order and histogram summaries of mcmc.res2out (utils/mcmc.m:806-862)
+    restated in numpy for one parameter: samples [nvox, N].  median: mean of
+    the two middle values for an even count; iqr: prctile(x, 75) - prctile(x,
+    25) with the midpoint rule (numpy's 'hazen'); mode: discretize over
+    linspace(lb - 1e-8, ub + 1e-8, nbin) (MATLAB's linspace d1 + ((0:n-1)
+    (d2 - d1)) / (n - 1), last element d2; bins closed on the left, the last
+    one on both sides, samples outside ignored), most populated bin with the
+    lowest index on ties, returned as the bin centre (NaN if no sample is
+    inside).  Returns float32 arrays [nvox]."""
+    x = np.asarray(samples, dtype=np.float64)
+    med = np.median(x, axis=1)
+    q = np.percentile(x, [25, 75], axis=1, method="hazen")
+    iqr = q[1] - q[0]
+    d1, d2 = float(lb) - 1e-8, float(ub) + 1e-8
+    n1 = nbin - 1
+    edges = d1 + (np.arange(nbin, dtype=np.float64) * (d2 - d1)) / n1
+    edges[-1] = d2
+    mode = np.full(x.shape[0], np.nan)
+    for v in range(x.shape[0]):
+        xv = x[v]
+        inside = (xv >= d1) & (xv <= d2)
+        if not inside.any():
+            continue
+        b = np.searchsorted(edges, xv[inside], side="right") - 1
+        b = np.minimum(b, n1 - 1)       # x == d2 falls in the last bin
+        cnt = np.bincount(b, minlength=n1)
+        k = int(np.argmax(cnt))         # first maximum: the lowest bin
+        mode[v] = (edges[k] + edges[k + 1]) / 2
+    return med.astype(np.float32), iqr.astype(np.float32), mode.astype(np.float32)

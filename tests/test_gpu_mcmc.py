@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="ensemble", iteration=1000, thinning=10, burnin=0.1,
                  repetition=1, nwalker=16, step_size=2.0, start_range=0.001, update="simultaneous",
-                 x_step=None, seed=7, posterior=True, weights=None, is_global=None, global_warmup=0):
+                 x_step=None, seed=7, posterior=True, weights=None, is_global=None, global_warmup=0, _hook=None):
     nvar, nv = x0.shape
     y = np.ascontiguousarray(y, np.float32)
     x0 = np.ascontiguousarray(x0, np.float32)
@@ -57,6 +57,8 @@ def _engine_mcmc(ctx, gxm, y, x0, lb, ub, algorithm="ensemble", iteration=1000, 
     r.std = std.ctypes.data_as(_lib._fp)
     if post is not None:
         r.posterior = post.ctypes.data_as(_lib._fp)
+    if _hook is not None:
+        _hook(r, o)
     _lib.check(_lib.lib().gx_mcmc(ctx.ptr, C.byref(gxm.s), _lib.MEM_HOST, C.byref(vol), 1, C.byref(o), C.byref(r)))
     return {"mean": mean, "std": std, "posterior": post, "n_accepted": r.n_accepted,
             "n_proposals": r.n_proposals, "ns": r.ns, "n_global_accepted": r.n_global_accepted,
@@ -229,3 +231,79 @@ def test_gw_global_through_mirror_returns_scalars(ctx):
     assert out["mean"]["M0"].shape == (50, 1, 1)
     assert out["posterior"]["R2star"].shape[0] == 1 and out["posterior"]["M0"].shape[0] == 50
     assert 25.0 < out["mean"]["R2star"] < 45.0
+
+
+# --------------------------------------------------------- res2out summaries on the device
+def _engine_summaries(ctx, gxm, y, x0, lb, ub, nbin=1001, posterior=True, **kw):
+    """_engine_mcmc plus the device's median / iqr / mode."""
+    nvar, nv = x0.shape
+    out = {}
+    arrays = {m: np.zeros((nvar, nv), np.float32) for m in ("median", "iqr", "mode")}
+
+    def hook(r, o):
+        for m, a in arrays.items():
+            setattr(r, m, a.ctypes.data_as(_lib._fp))
+        o.nbin = nbin
+    res = _engine_mcmc(ctx, gxm, y, x0, lb, ub, posterior=posterior, _hook=hook, **kw)
+    out.update(res)
+    out.update(arrays)
+    return out
+
+
+@pytest.mark.parametrize("case", ["gw_even", "gw_odd_redblack", "mh", "unfilled_slots", "beyond_smem"])
+def test_posterior_median_iqr_mode_on_device(ctx, case):
+    """median / iqr / mode computed on the device from the kept samples equal
+    the res2out restatement (utils/mcmc.m:806-862) applied to the returned
+    posterior: the sampler's N = W x ns x rep samples per voxel and parameter,
+    with an even and an odd count, Metropolis-Hastings (W = 1), slots that no
+    step fills (zeros, counted), a pinned parameter (all samples equal) and a
+    sample count too large for shared memory (read from HBM each pass)."""
+    gxm, om, y, x0, lb, ub = _r2s_problem(48 if case != "beyond_smem" else 6, 20)
+    kw = {"gw_even": dict(iteration=600, thinning=2, burnin=0.25, nwalker=16, seed=3),
+          "gw_odd_redblack": dict(iteration=601, thinning=4, burnin=0.2, nwalker=15, seed=4, update="redblack"),
+          "mh": dict(iteration=3001, thinning=3, burnin=0.1, seed=5, algorithm="mh", x_step=[0.01, 1.0, 0.0]),
+          "unfilled_slots": dict(iteration=5, thinning=10, burnin=0.0, nwalker=16, seed=6),
+          "beyond_smem": dict(iteration=1000, thinning=1, burnin=0.0, nwalker=64, seed=7)}[case]
+    eng = _engine_summaries(ctx, gxm, y, x0, lb, ub, nbin=501, **kw)
+    post = eng["posterior"]
+    nvar, nv = x0.shape
+    if case == "unfilled_slots":
+        assert eng["ns"] == 1 and np.all(post == 0)   # numel(1:10:5) = 1 slot, no step fills it
+    if case == "beyond_smem":
+        assert post.shape[1] * post.shape[2] * post.shape[3] == 64000
+    for k in range(nvar):
+        samples = post[k].reshape(-1, nv).T
+        med, iqr, mode = oracle.res2out_summaries(samples, lb[k], ub[k], nbin=501)
+        np.testing.assert_array_equal(eng["median"][k], med, err_msg=f"median {k}")
+        np.testing.assert_allclose(eng["iqr"][k], iqr, rtol=1e-6, atol=1e-7, err_msg=f"iqr {k}")
+        np.testing.assert_array_equal(eng["mode"][k], mode, err_msg=f"mode {k}")
+    # the pinned noise parameter: every sample equal
+    if case != "unfilled_slots":
+        assert np.all(eng["iqr"][2] == 0) and np.all(eng["median"][2] == np.float32(lb[2]))
+    if case in ("mh", "gw_odd_redblack"):
+        assert (post.shape[1] * post.shape[2] * post.shape[3]) % 2 == 1
+
+
+def test_posterior_summaries_without_returning_the_posterior(ctx):
+    """The summaries need no posterior output: the same run with and without
+    the posterior returned gives identical median / iqr / mode; and the host
+    mirror's optimisation() returns them as images."""
+    gxm, om, y, x0, lb, ub = _r2s_problem(32, 21)
+    kw = dict(iteration=400, thinning=2, burnin=0.2, nwalker=16, seed=9)
+    a = _engine_summaries(ctx, gxm, y, x0, lb, ub, posterior=True, **kw)
+    b = _engine_summaries(ctx, gxm, y, x0, lb, ub, posterior=False, **kw)
+    for m in ("median", "iqr", "mode"):
+        np.testing.assert_array_equal(a[m], b[m])
+    from gacelle_b200 import gpuR2starMapping, mcmc_solver
+    te = np.arange(2.0, 40.6, 3.5) * 1e-3
+    mask = np.ones((32, 1, 1), dtype=bool)
+    data = y.T.reshape(32, 1, 1, 12)
+    pars0 = {"M0": x0[0].reshape(32, 1, 1), "R2star": x0[1].reshape(32, 1, 1), "noise": x0[2].reshape(32, 1, 1)}
+    fit = {"algorithm": "GW", "iteration": 400, "thinning": 2, "burnin": 0.2, "Nwalker": 16, "lb": lb, "ub": ub,
+           "modelParams": ["M0", "R2star", "noise"], "metric": ["mean", "median", "iqr", "mode"], "seed": 9,
+           "returnPosterior": False}
+    out = mcmc_solver.mcmc(ctx).optimisation(data, mask, None, pars0, fit, gpuR2starMapping(te))
+    assert "posterior" not in out
+    np.testing.assert_array_equal(out["median"]["R2star"].ravel(), a["median"][1])
+    np.testing.assert_array_equal(out["mode"]["M0"].ravel(), a["mode"][0])
+    np.testing.assert_array_equal(out["iqr"]["R2star"].ravel(), a["iqr"][1])

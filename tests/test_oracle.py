@@ -600,3 +600,25 @@ def test_robust_convergence_judges_the_main_population():
     assert b["ever_flagged"].any() and np.all(np.isin(np.flatnonzero(b["ever_flagged"]), out))
     assert a["stop_reason"] == b["stop_reason"] == "convergence"
     assert b["final_niter"] < 0.6 * a["final_niter"], (b["final_niter"], a["final_niter"])
+
+
+def test_res2out_summaries_restate_matlab_semantics():
+    """Known answers of the res2out restatement: even/odd medians, the
+    prctile midpoint rule, the histogram mode with its lowest-bin tie rule and
+    samples outside the edges ignored."""
+    import oracle
+    x = np.array([[4.0, 1.0, 3.0, 2.0], [5.0, 1.0, 2.0, 2.0]])
+    med, iqr, mode = oracle.res2out_summaries(x, 0.0, 10.0, nbin=11)
+    assert med.tolist() == [2.5, 2.0]
+    # n = 4: the 25th percentile sits at position 0.5 (0-based), the 75th at 2.5
+    assert iqr[0] == pytest.approx((3.5 - 1.5), abs=1e-6)
+    assert iqr[1] == pytest.approx((3.5 - 1.5), abs=1e-6)
+    # bins of width 1 (+ 2e-9): row 0 has one sample per bin -> the lowest (x = 1) wins
+    assert mode[0] == pytest.approx(1.5, abs=1e-6)
+    assert mode[1] == pytest.approx(2.5, abs=1e-6)
+    med, iqr, mode = oracle.res2out_summaries(np.array([[1.0, 2.0, 9.0]]), 0.0, 10.0, nbin=11)
+    assert med[0] == 2.0
+    # n = 3: 25th at position 0.25 -> 1.25; 75th at 1.75 -> 2 + 0.75 * 7 = 7.25
+    assert iqr[0] == pytest.approx(7.25 - 1.25, abs=1e-6)
+    _, _, mode = oracle.res2out_summaries(np.array([[20.0, 30.0]]), 0.0, 10.0, nbin=11)
+    assert np.isnan(mode[0])
