@@ -904,6 +904,47 @@ static cudaError_t fused_dispatch2(const AdamParams& a, int loss, int e_begin, i
     }
 }
 
+// Largest launch block of fused_kernel<MODEL, LOSS, STATS> for this job:
+// the kernel's thread limit and the dynamic shared memory it takes per block.
+template <int MODEL, int LOSS, bool STATS>
+static int fused_limit3(const AdamParams& a) {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fused_kernel<MODEL, LOSS, STATS>) != cudaSuccess) return 0;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return 0;
+    constexpr int NQ = STATS ? kHistW : 1;
+    const size_t per = sizeof(float) * (size_t)(a.nm * (a.weights ? 2 : 1) + 2 * a.P.n_fa);
+    const size_t fixed = sizeof(double) * 2 * 32 * NQ + fa.sharedSizeBytes;
+    int b = fa.maxThreadsPerBlock / 32 * 32;
+    while (b > 0 && fixed + per * b > (size_t)optin) b -= 32;
+    return b;
+}
+
+template <int MODEL, bool STATS>
+static int fused_limit2(const AdamParams& a, int loss) {
+    switch (loss) {
+    case kL1: return fused_limit3<MODEL, kL1, STATS>(a);
+    case kL2: return fused_limit3<MODEL, kL2, STATS>(a);
+    case kHuber: return fused_limit3<MODEL, kHuber, STATS>(a);
+    case kMSE: return fused_limit3<MODEL, kMSE, STATS>(a);
+    case kGauss: return fused_limit3<MODEL, kGauss, STATS>(a);
+    default: return fused_limit3<MODEL, kRician, STATS>(a);
+    }
+}
+
+int fused_block_limit(const AdamParams& a, int model, int loss, bool stats) {
+#define GX_L(M) return stats ? fused_limit2<M, true>(a, loss) : fused_limit2<M, false>(a, loss)
+    switch (model) {
+    case kR2S: GX_L(kR2S);
+    case kR1R2S: GX_L(kR1R2S);
+    case kNEXI: GX_L(kNEXI);
+    default: GX_L(kNEXI2);
+    }
+#undef GX_L
+}
+
 cudaError_t launch_fused(const AdamParams& a, int model, int loss, bool stats, int e_begin,
                          int e_end, int update_last, bool record, int block, int nblocks,
                          cudaStream_t s) {

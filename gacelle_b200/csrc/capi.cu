@@ -18,6 +18,8 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <map>
+#include <array>
 
 #include "../../include/gacelle_b200.h"
 #include "gx_internal.h"
@@ -51,6 +53,35 @@ static gx_status fail(gx_status s, const char* fmt, ...) {
     } while (0)
 
 // ---------------------------------------------------------------------------
+// Autotuner cache: launch shapes chosen by trial runs, per key, for the
+// process (GACELLE_B200_AUTOTUNE=0 turns tuning off: the defaults are used).
+// ---------------------------------------------------------------------------
+struct TuneKey {
+    std::array<long long, 13> k;
+    bool operator<(const TuneKey& o) const { return k < o.k; }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, int> g_tune;
+
+static bool autotune_enabled() {
+    const char* e = getenv("GACELLE_B200_AUTOTUNE");
+    return !(e && strcmp(e, "0") == 0);
+}
+
+static int tune_lookup(const TuneKey& key) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    return it == g_tune.end() ? 0 : it->second;
+}
+
+static void tune_store(const TuneKey& key, int v) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = v;
+}
+
+constexpr int kTuneLayoutBlock = 512;  // layout block of tuned fused jobs: every candidate divides it
+
+// ---------------------------------------------------------------------------
 // Context and workspace
 // ---------------------------------------------------------------------------
 enum Slot {
@@ -60,7 +91,7 @@ enum Slot {
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
     S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_SURF_NB, S_SURF_LEN,
-    S_MC_STATS, S_NSLOTS
+    S_MC_STATS, S_TUNE, S_TUNE_HIST, S_BLK_L, S_NSLOTS
 };
 
 struct gx_context {
@@ -538,6 +569,11 @@ struct AdamJob {
     PersistPlan plan{};
     PersistBarrier* barrier = nullptr;
     float4* data_quads = nullptr;         // echo quads of the measurements for the persistent kernel
+    bool allow_tune = false;              // gx_askadam with block_size 0: the fused kernel's block is tuned
+    bool autotune = false;                // ... and this job tunes it (fused path, no TV)
+    int Bl = 0;                           // launch block of the fused kernel's main pass (0: B)
+    int* blk_l = nullptr;                 // block -> volume table for Bl
+    bool tuned_now = false;               // a trial ran in this call
 };
 
 static double sched_pow(double b, int e) { return std::pow(b, (double)e); }
@@ -587,12 +623,17 @@ static gx_status adam_setup(AdamJob& J) {
     gx_context* c = J.c;
     const gx_askadam_opts* o = J.o;
     int N = o->iteration;
-    J.B = o->block_size > 0 ? o->block_size : 128;
-    if (J.B % 32 || J.B < 32 || J.B > 1024) return fail(GX_EINVAL, "block_size must be a multiple of 32 in [32,1024]");
     J.prior = o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == GX_REG_PRIOR;
     J.surf = o->n_reg > 0 && o->lambda[0] > 0 && o->reg_type == GX_REG_SURFACE_TV;
     J.tv = o->n_reg > 0 && o->lambda[0] > 0 && !J.prior;   // grid TV or surface TV
     J.stats = o->step_tol > 0 || o->grad_tol > 0;
+    // the fused (no TV) path with block_size 0 tunes its launch block among
+    // the divisors of a 512-voxel layout block; every other path lays out and
+    // launches with block_size (default 128)
+    J.autotune = J.allow_tune && o->block_size == 0 && autotune_enabled() && o->path == GX_PATH_FUSED &&
+                 !o->robust_convergence && !J.tv;
+    J.B = o->block_size > 0 ? o->block_size : (J.autotune ? kTuneLayoutBlock : 128);
+    if (J.B % 32 || J.B < 32 || J.B > 1024) return fail(GX_EINVAL, "block_size must be a multiple of 32 in [32,1024]");
     // work-list layout
     J.hv.resize(J.nvol);
     int off = 0;
@@ -873,8 +914,15 @@ static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e
     a.res_out = res_out;
     if (!record) a.hist = nullptr;
     if (!J.tv) {
+        // the main pass (the whole work-list) launches with the tuned block
+        int B = J.B;
+        if (J.Bl > 0 && a.blk_vol == J.a.blk_vol && nblocks == J.nblocks) {
+            B = J.Bl;
+            nblocks = J.nvtot / J.Bl;
+            a.blk_vol = J.blk_l;
+        }
         // the prior's loss is recorded in the statistics columns of the history
-        CK(launch_fused(a, J.id, J.o->loss, (J.stats || J.prior) && record, e0, e1, update_last, record, J.B,
+        CK(launch_fused(a, J.id, J.o->loss, (J.stats || J.prior) && record, e0, e1, update_last, record, B,
                         nblocks, c->stream));
         return GX_OK;
     }
@@ -962,6 +1010,77 @@ static bool can_stop(const gx_askadam_opts* o) {
            o->tol > 0 || (signed_loss && o->tol > -INFINITY);
 }
 
+// Block -> volume table of launch block Bl (a divisor of the layout block B).
+static gx_status upload_blk_table(AdamJob& J, int Bl, int** out) {
+    const int k = J.B / Bl;
+    std::vector<int> t(J.hblk.size() * (size_t)k);
+    for (size_t b = 0; b < J.hblk.size(); ++b)
+        for (int j = 0; j < k; ++j) t[b * k + j] = J.hblk[b];
+    TRY(wsT(J.c, S_BLK_L, t.size(), out));
+    CK(cudaMemcpyAsync(*out, t.data(), sizeof(int) * t.size(), cudaMemcpyHostToDevice, J.c->stream));
+    CK(cudaStreamSynchronize(J.c->stream));  // t is freed on return
+    return GX_OK;
+}
+
+// Autotuner of the fused kernel's launch block.  Key: device, model, loss,
+// measurements, statistics / prior / weights / b1 / sigma-map variants,
+// optimiser, transform and the voxel-count class (log2 of the work-list).
+// On a miss every candidate (64, 128, 256, 512 threads, within the kernel's
+// thread and shared-memory limits) runs a few epochs of this job's own
+// kernel on its own data from a scratch copy of the start state (the job's
+// state and history untouched); the fastest is cached for the process.
+static gx_status tune_fused(AdamJob& J) {
+    gx_context* c = J.c;
+    const gx_askadam_opts* o = J.o;
+    const bool stats = J.stats || J.prior;
+    int cls = 0;
+    while ((1LL << (cls + 1)) <= (long long)J.nvtot) ++cls;
+    const TuneKey key{{1, c->device, J.id, o->loss, J.nm, stats ? 1 : 0, J.prior ? 1 : 0, J.a.weights ? 1 : 0,
+                       J.a.b1 ? 1 : 0, J.a.sigma ? 1 : 0, o->optimiser, o->transform, cls}};
+    int Bl = tune_lookup(key);
+    if (Bl <= 0) {
+        const int N = o->iteration;
+        const int E = std::max(1, std::min({8, N, (int)(2000000LL / std::max(J.nvtot, 1))}));
+        AdamParams t = J.a;
+        const size_t pn = (size_t)J.np * J.nvtot;
+        float* sc;
+        TRY(wsT(c, S_TUNE, 4 * pn, &sc));
+        t.z = sc; t.m1 = sc + pn; t.m2 = sc + 2 * pn; t.zprev = J.a.zprev ? sc + 3 * pn : nullptr;
+        CK(cudaMemcpyAsync(t.z, J.a.z, sizeof(float) * pn, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(t.m1, J.a.m1, sizeof(float) * pn, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(t.m2, J.a.m2, sizeof(float) * pn, cudaMemcpyDeviceToDevice, c->stream));
+        if (t.zprev) CK(cudaMemcpyAsync(t.zprev, J.a.zprev, sizeof(float) * pn, cudaMemcpyDeviceToDevice, c->stream));
+        TRY(wsT(c, S_TUNE_HIST, (size_t)J.nvol * (N + 1) * kHistW, &t.hist));
+        t.ckpt = nullptr;
+        t.ckpt_every = 0;
+        t.res_out = nullptr;
+        float best = 0.f;
+        for (int cand : {64, 128, 256, 512}) {
+            if (J.B % cand || fused_block_limit(t, J.id, o->loss, stats) < cand) continue;
+            int* blk;
+            TRY(upload_blk_table(J, cand, &blk));
+            t.blk_vol = blk;
+            float ms = 0.f;
+            for (int rep = 0; rep < 3; ++rep) {  // the first run warms the code and caches
+                CK(cudaEventRecord(c->ev[2], c->stream));
+                CK(launch_fused(t, J.id, o->loss, stats, 1, E, E - 1, true, cand, J.nvtot / cand, c->stream));
+                CK(cudaEventRecord(c->ev[3], c->stream));
+                CK(cudaEventSynchronize(c->ev[3]));
+                float m = 0.f;
+                cudaEventElapsedTime(&m, c->ev[2], c->ev[3]);
+                if (rep == 1 || (rep > 1 && m < ms)) ms = m;
+            }
+            if (Bl <= 0 || ms < best) { best = ms; Bl = cand; }
+        }
+        if (Bl <= 0) return fail(GX_ECUDA, "autotuner: no launch block fits the fused kernel");
+        tune_store(key, Bl);
+        J.tuned_now = true;
+    }
+    J.Bl = Bl;
+    TRY(upload_blk_table(J, Bl, &J.blk_l));
+    return GX_OK;
+}
+
 static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     gx_context* c = J.c;
     const gx_askadam_opts* o = J.o;
@@ -969,6 +1088,7 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     const bool stop_possible = can_stop(o);
     const int chunk = stop_possible ? (o->chunk > 0 ? o->chunk : 200) : (N > 0 ? N : 1);
     TRY(alloc_outputs(J, out));
+    if (J.autotune) TRY(tune_fused(J));
     if (J.tv) {
         CK(launch_tv_scatter(J.a, J.grid[0], J.B, J.nblocks, c->stream));
         const char* env = getenv("GACELLE_B200_TV_KERNEL");
@@ -1046,6 +1166,8 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
     c->timing.main_kernel_ms = ms;
     c->timing.main_launches = n_main;
+    c->timing.block_size = J.Bl > 0 ? J.Bl : (J.use_persist ? J.plan.threads : J.B);
+    c->timing.autotuned = J.tuned_now ? 1 : 0;
     c->timing.tv_path = !J.use_persist ? 0
                         : GX_TV_PERSISTENT | (J.plan.quad_pairs ? GX_TV_PAIRS : 0) |
                               (J.plan.data_in_smem ? GX_TV_DATA_SMEM : 0) | (J.data_quads ? GX_TV_DATA_QUADS : 0);
@@ -1299,6 +1421,7 @@ extern "C" gx_status gx_askadam(gx_context* c, const gx_model* model, int32_t me
     CallScope scope(c);
     AdamJob J;
     J.c = c; J.model = model; J.o = opts; J.mem = mem; J.vols = vols; J.nvol = nvol;
+    J.allow_tune = true;
     TRY(model_sizes(model, &J.np, &J.nm, &J.id));
     TRY(validate_adam(opts, J.np, vols, nvol, J.nm));
     for (int i = 0; i < nvol; ++i)
@@ -1431,6 +1554,67 @@ static int mcmc_nsamples(int iteration, int nb, int thinning) {
     return (iteration - nb - 1) / thinning + 1;  // numel(Nburnin+1:thinning:iteration)
 }
 
+// Autotuner of the MCMC kernels' block shape (Goodman-Weare: voxels per CTA;
+// MH: threads per CTA).  Key: device, model, algorithm, walkers, update
+// scheme, variables, measurements, weights / b1 variants and the voxel-count
+// class.  On a miss each candidate runs a few steps from the start on the
+// first voxels of this job (scratch walker state and sums; the job's buffers
+// untouched) and the fastest is cached for the process.
+static gx_status tune_mcmc(gx_context* c, const McmcParams& p, int model, int* block, bool* tuned) {
+    int cls = 0;
+    while ((1LL << (cls + 1)) <= (long long)p.nvox) ++cls;
+    const int W = p.algorithm == 1 ? p.nwalker : 1;
+    const TuneKey key{{2, c->device, model, p.algorithm, W, p.update, p.nvar, p.nm, p.weights ? 1 : 0,
+                       p.b1 ? 1 : 0, cls, 0, 0}};
+    int b = tune_lookup(key);
+    if (b <= 0) {
+        McmcParams t = p;
+        t.nvox = std::min(p.nvox, std::max(256, (1 << 19) / W));
+        t.posterior = nullptr;
+        const int k1 = std::min(p.iteration, 8);
+        const size_t nx = (size_t)t.nvar * t.nvox * W, nl = (size_t)t.nvox * W, ns = (size_t)t.nvar * t.nvox;
+        const size_t o_lp = (sizeof(float) * nx + 255) / 256 * 256;
+        const size_t o_s1 = o_lp + (sizeof(double) * nl + 255) / 256 * 256;
+        const size_t o_s2 = o_s1 + sizeof(double) * ns;
+        const size_t o_acc = o_s2 + sizeof(double) * ns;
+        unsigned char* sc;
+        TRY(wsT(c, S_TUNE, o_acc + sizeof(unsigned long long), &sc));
+        float* xs = reinterpret_cast<float*>(sc);
+        double* lps = reinterpret_cast<double*>(sc + o_lp);
+        double* s1 = reinterpret_cast<double*>(sc + o_s1);
+        double* s2 = reinterpret_cast<double*>(sc + o_s2);
+        t.n_acc = reinterpret_cast<unsigned long long*>(sc + o_acc);
+        int cand[8];
+        const int nc = mcmc_block_candidates(t, cand, 8);
+        float best = 0.f;
+        for (int j = 0; j < nc; ++j) {
+            float ms = 0.f;
+            bool ok = true;
+            for (int rep = 0; rep < 3 && ok; ++rep) {  // the first run warms the code and caches
+                CK(cudaEventRecord(c->ev[2], c->stream));
+                cudaError_t e = launch_mcmc_trial(t, model, cand[j], k1, xs, lps, s1, s2, c->stream);
+                if (e == cudaErrorInvalidConfiguration || e == cudaErrorLaunchOutOfResources) {
+                    cudaGetLastError();  // a shape this kernel cannot take: skipped
+                    ok = false;
+                    break;
+                }
+                CK(e);
+                CK(cudaEventRecord(c->ev[3], c->stream));
+                CK(cudaEventSynchronize(c->ev[3]));
+                float m = 0.f;
+                cudaEventElapsedTime(&m, c->ev[2], c->ev[3]);
+                if (rep == 1 || (rep > 1 && m < ms)) ms = m;
+            }
+            if (ok && (b <= 0 || ms < best)) { best = ms; b = cand[j]; }
+        }
+        if (b <= 0) return fail(GX_ECUDA, "autotuner: no block shape fits the MCMC kernel");
+        tune_store(key, b);
+        *tuned = true;
+    }
+    *block = b;
+    return GX_OK;
+}
+
 extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, const gx_volume* vols,
                              int32_t nvol, const gx_mcmc_opts* o, gx_mcmc_result* results) {
     if (!c || !o || !vols || !results || nvol < 1) return fail(GX_EINVAL, "NULL argument");
@@ -1473,6 +1657,8 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     long long h2d = 0, d2h = 0;
     double kernel_ms = 0.0;
     int launches = 0;
+    bool tuned_now = false;
+    int block_used = 0;
     CK(cudaEventRecord(c->ev[0], c->stream));
     for (int i = 0; i < nvol; ++i) {
         const gx_volume& v = vols[i];
@@ -1562,8 +1748,11 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
         // slots that no step fills stay zero (res2out counts them)
         if (post && mcmc_missing_slots(p) > 0) CK(cudaMemsetAsync(post, 0, sizeof(float) * npost, c->stream));
         if (partner) CK(launch_mcmc_partners(p, partner, c->stream));
+        int block = o->block_size;
+        if (block == 0 && ng == 0 && autotune_enabled()) TRY(tune_mcmc(c, p, id, &block, &tuned_now));
+        block_used = block > 0 ? block : 128;
         CK(cudaEventRecord(c->ev[2], c->stream));
-        CK(launch_mcmc(p, id, o->block_size, c->stream));
+        CK(launch_mcmc(p, id, block, c->stream));
         CK(cudaEventRecord(c->ev[3], c->stream));
         launches += ng > 0 ? (o->ensemble_update == GX_GW_REDBLACK ? 4 : 2) * (o->iteration + o->global_warmup) *
                                  o->repetition
@@ -1633,6 +1822,8 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     c->timing.total_ms = ms;
     c->timing.main_kernel_ms = kernel_ms;
     c->timing.main_launches = launches;
+    c->timing.block_size = block_used;
+    c->timing.autotuned = tuned_now ? 1 : 0;
     c->timing.kernel_launches = g_kernel_launches - scope.launches0;
     c->timing.h2d_bytes = h2d;
     c->timing.d2h_bytes = d2h;

@@ -75,6 +75,9 @@ cudaError_t launch_init_state(const AdamParams& a, const float* theta0, double r
 cudaError_t launch_fused(const AdamParams& a, int model, int loss, bool stats, int e_begin,
                          int e_end, int update_last, bool record, int block, int nblocks,
                          cudaStream_t s);
+// Largest launch block (multiple of 32) the fused kernel variant of this job
+// accepts: its thread limit and its per-block shared memory; 0 on error.
+int fused_block_limit(const AdamParams& a, int model, int loss, bool stats);
 cudaError_t launch_tv_step(const AdamParams& a, int model, int loss, bool stats, int e,
                            bool update, bool record, bool want_res, int block, int nblocks,
                            cudaStream_t s);
@@ -199,6 +202,11 @@ cudaError_t launch_mcmc_partners(const McmcParams& p, int* partner, cudaStream_t
 // (= rows of the partial-sum table) and dynamic shared memory.
 void gwg_launch_shape(const McmcParams& p, int block_hint, int* vpb, int* block, int* nblocks, size_t* smem);
 cudaError_t launch_mcmc(const McmcParams& p, int model, int block, cudaStream_t s);
+// Launch shapes the MCMC autotuner tries (threads per block), and one trial
+// launch of steps 1..k1 from the start into scratch state and sums.
+int mcmc_block_candidates(const McmcParams& p, int* out, int maxn);
+cudaError_t launch_mcmc_trial(const McmcParams& p, int model, int block_hint, int k1, float* xstate,
+                              double* lpstate, double* sum, double* sumsq, cudaStream_t s);
 cudaError_t launch_mcmc_finalize(const McmcParams& p, float* mean, float* stdv, cudaStream_t s);
 // Kept slots the reference preallocates but never fills: numel(Nburnin+1:thinning:iteration)
 // minus the steps k with mod(k - Nburnin + 1, thinning) == 0.

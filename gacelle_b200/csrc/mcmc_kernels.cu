@@ -711,47 +711,80 @@ cudaError_t launch_mcmc_partners(const McmcParams& p, int* partner, cudaStream_t
     return cudaGetLastError();
 }
 
+// Goodman-Weare launch shape for a block hint (threads): whole voxels of
+// tpv threads (one walker, or one walker of each half) per CTA.
+static void gw_shape(const McmcParams& p, int block_hint, int* vpb, int* block, size_t* smem) {
+    const int W = p.nwalker, h = W / 2;
+    const int tpv = p.update == 0 ? W : W - h;
+    const int target = block_hint > 0 ? block_hint : 128;
+    *vpb = target / tpv > 0 ? target / tpv : 1;
+    *block = *vpb * tpv;
+    *smem = sizeof(float) * ((size_t)(*vpb) * W * p.nvar + 2 * (size_t)(*vpb) * p.nm);
+}
+
+// Steps [k0, k1] of repetition rr as one launch (init: the walkers start at k0 == 1).
+template <int MODEL>
+static cudaError_t mcmc_launch_steps(const McmcParams& p, int block_hint, int rr, int k0, int k1, float* xstate,
+                                     double* lpstate, double* sum, double* sumsq, cudaStream_t s) {
+    constexpr int NV = ModelNP<MODEL>::value + 1;  // the model's parameters and the noise sigma
+    if (p.nvar != NV) return cudaErrorInvalidValue;
+    if (p.algorithm == 1) {
+        int vpb, block;
+        size_t smem;
+        gw_shape(p, block_hint, &vpb, &block, &smem);
+        const int nb = (p.nvox + vpb - 1) / vpb;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(gw_kernel<MODEL, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        gw_kernel<MODEL, NV><<<nb, block, smem, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, sum, sumsq);
+    } else {
+        const int block = block_hint > 0 ? block_hint : 128;
+        const int nb = (p.nvox + block - 1) / block;
+        mh_kernel<MODEL, NV><<<nb, block, 0, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, sum, sumsq);
+    }
+    ++g_kernel_launches;
+    return cudaGetLastError();
+}
+
 template <int MODEL>
 static cudaError_t mcmc_run_model(const McmcParams& p, int block_hint, cudaStream_t s,
                                   float* xstate, double* lpstate) {
-    constexpr int NV = ModelNP<MODEL>::value + 1;  // the model's parameters and the noise sigma
-    if (p.nvar != NV) return cudaErrorInvalidValue;
     const int chunk = 250;  // steps per launch: bounded kernel duration
-    if (p.algorithm == 1) {
-        int W = p.nwalker, h = W / 2;
-        int tpv = p.update == 0 ? W : W - h;
-        int target = block_hint > 0 ? block_hint : 128;
-        int vpb = target / tpv > 0 ? target / tpv : 1;
-        int block = vpb * tpv;
-        size_t smem = sizeof(float) * ((size_t)vpb * W * p.nvar + 2 * (size_t)vpb * p.nm);
-        int nb = (p.nvox + vpb - 1) / vpb;
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(gw_kernel<MODEL, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (int rr = 0; rr < p.repetition; ++rr)
+        for (int k0 = 1; k0 <= p.iteration; k0 += chunk) {
+            int k1 = k0 + chunk - 1 < p.iteration ? k0 + chunk - 1 : p.iteration;
+            cudaError_t e = mcmc_launch_steps<MODEL>(p, block_hint, rr, k0, k1, xstate, lpstate, p.sum, p.sumsq, s);
             if (e != cudaSuccess) return e;
         }
-        for (int rr = 0; rr < p.repetition; ++rr)
-            for (int k0 = 1; k0 <= p.iteration; k0 += chunk) {
-                int k1 = k0 + chunk - 1 < p.iteration ? k0 + chunk - 1 : p.iteration;
-                gw_kernel<MODEL, NV><<<nb, block, smem, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, p.sum,
-                                                             p.sumsq);
-                ++g_kernel_launches;
-                cudaError_t e = cudaGetLastError();
-                if (e != cudaSuccess) return e;
-            }
-    } else {
-        int block = block_hint > 0 ? block_hint : 128;
-        int nb = (p.nvox + block - 1) / block;
-        for (int rr = 0; rr < p.repetition; ++rr)
-            for (int k0 = 1; k0 <= p.iteration; k0 += chunk) {
-                int k1 = k0 + chunk - 1 < p.iteration ? k0 + chunk - 1 : p.iteration;
-                mh_kernel<MODEL, NV><<<nb, block, 0, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, p.sum,
-                                                          p.sumsq);
-                ++g_kernel_launches;
-                cudaError_t e = cudaGetLastError();
-                if (e != cudaSuccess) return e;
-            }
-    }
     return cudaSuccess;
+}
+
+int mcmc_block_candidates(const McmcParams& p, int* out, int maxn) {
+    int n = 0;
+    if (p.algorithm == 1) {
+        const int W = p.nwalker, tpv = p.update == 0 ? W : W - W / 2;
+        for (int vpb = 1; vpb <= 32 && n < maxn; vpb *= 2) {
+            const int block = vpb * tpv;
+            if (block > 1024) break;
+            if (block < 32 && vpb < 32) continue;  // at least one warp
+            out[n++] = block;
+        }
+    } else {
+        for (int b = 64; b <= 512 && n < maxn; b *= 2) out[n++] = b;
+    }
+    return n;
+}
+
+cudaError_t launch_mcmc_trial(const McmcParams& p, int model, int block_hint, int k1, float* xstate,
+                              double* lpstate, double* sum, double* sumsq, cudaStream_t s) {
+    switch (model) {
+    case kR2S: return mcmc_launch_steps<kR2S>(p, block_hint, 0, 1, k1, xstate, lpstate, sum, sumsq, s);
+    case kR1R2S: return mcmc_launch_steps<kR1R2S>(p, block_hint, 0, 1, k1, xstate, lpstate, sum, sumsq, s);
+    case kNEXI: return mcmc_launch_steps<kNEXI>(p, block_hint, 0, 1, k1, xstate, lpstate, sum, sumsq, s);
+    default: return mcmc_launch_steps<kNEXI2>(p, block_hint, 0, 1, k1, xstate, lpstate, sum, sumsq, s);
+    }
 }
 
 int kept_index_host(const McmcParams& p, int k) {

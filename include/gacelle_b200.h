@@ -175,7 +175,13 @@ typedef struct {
     double voxel_size[3];
     int32_t path;               /* gx_path */
     int32_t chunk;              /* fused path: iterations per launch if stopping may trigger; 0 = auto */
-    int32_t block_size;         /* 0 = auto-tuned */
+    /* threads per block; 0 = the default (128), or on the fused path without
+     * TV the block chosen by the project's autotuner: the first call of a key
+     * (model, loss, measurement count, variant, optimiser, transform, voxel-
+     * count class) times 64 / 128 / 256 / 512 threads on a few epochs of its own
+     * data and the fastest is kept for the process; GACELLE_B200_AUTOTUNE=0
+     * turns tuning off */
+    int32_t block_size;
     /* robustConvergence (update_outlier_mask, utils/askadam.m:448-510, and the
      * main-population convergence signal of :530-581): every
      * weight_update_interval epochs, voxels that improve less than
@@ -224,7 +230,9 @@ typedef struct {
     const double* lb;           /* [nvar] */
     const double* ub;           /* [nvar] */
     uint64_t seed;
-    int32_t block_size;         /* 0 = auto */
+    int32_t block_size;         /* threads per block (Goodman-Weare: a multiple of the walkers of one
+                                 * update); 0 = chosen by the autotuner (MH and Goodman-Weare without
+                                 * global parameters: trial steps per block shape, cached per key) */
     /* goodman_weare_wglobal_constant (utils/mcmc.m:385-626), chosen by the
      * reference when a start field has one value for all voxels: nonzero
      * entries mark parameters shared by all voxels of a volume (one value per
@@ -266,6 +274,9 @@ typedef struct {
     int64_t kernel_launches;    /* launches of this library's kernels in the call */
     int64_t h2d_bytes, d2h_bytes;
     int32_t tv_path;            /* askAdam with TV: GX_TV_* flags of the main pass, else 0 */
+    int32_t block_size;         /* threads per block of the main kernel's launches */
+    int32_t autotuned;          /* 1: the autotuner ran its trials in this call (block_size 0,
+                                 * first call of its key in the process) */
 } gx_timing;
 
 /* gx_timing.tv_path flags */

@@ -26,12 +26,12 @@ def engine(monkeypatch):
                 "min_loss_fidelity": 1.0, "min_loss_reg": 0.0, "final_niteration": opts.iteration,
                 "min_niteration": opts.iteration, "stop_reason": 0}
 
-    def mcmc_run(self, model, y, w, x0, b1, names, fitting, want_post, is_global=None):
-        calls.append(dict(kind="mcmc", y=y, w=w, x0=x0, b1=b1, names=names, fitting=fitting))
+    def mcmc_run(self, model, y, w, x0, b1, names, fitting, want_post, is_global=None, stats=()):
+        calls.append(dict(kind="mcmc", y=y, w=w, x0=x0, b1=b1, names=names, fitting=fitting, stats=list(stats)))
         nvar, nv = len(names), y.shape[1]
         x = np.asarray(x0, np.float32).reshape(nvar, -1)[:, :nv]
         return {"mean": x, "std": np.zeros_like(x), "posterior": None, "W": int(fitting.get("Nwalker", 1)),
-                "ns": 1, "rep": 1, "is_global": [0] * nvar}
+                "ns": 1, "rep": 1, "is_global": [0] * nvar, **{m: x for m in stats}}
 
     monkeypatch.setattr(askadam_solver.askadam, "_run", adam_run)
     monkeypatch.setattr(mcmc_solver.mcmc, "_run", mcmc_run)
