@@ -111,26 +111,32 @@ __device__ __forceinline__ void gw_walker_start(const McmcParams& p, int v, int 
 
 // Goodman-Weare, steps [k0, k1] of repetition rr.  State between launches:
 // xstate [nvar][nvox][W], lpstate [nvox][W].  NV = parameters + noise, fixed
-// at compile time: every per-walker vector (state, proposal, running sums)
-// is indexed by constants and lives in registers.
-template <int MODEL, int NV>
-__global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float* xstate,
-                          double* lpstate, double* sum, double* sumsq) {
+// at compile time, and RB (red-black: a thread owns a walker of each half)
+// keep every per-walker vector in registers; the running sums of the kept
+// samples live in shared memory (each thread its own walkers' slots) and are
+// folded into the per-voxel sums at the end of the launch.
+template <int MODEL, int NV, bool RB>
+__global__ void __launch_bounds__(1024, 1)
+gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float* xstate, double* lpstate, double* sum,
+          double* sumsq) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ DevProtocol s_P;
     stage_protocol(p.P, &s_P);
     const int W = p.nwalker, nm = p.nm;
     const int h = W / 2;
-    const int tpv = p.update == 0 ? W : (W - h);
+    const int tpv = RB ? (W - h) : W;
     const int vpb = blockDim.x / tpv;
     const int vl = threadIdx.x / tpv, a = threadIdx.x % tpv;
     const int v = blockIdx.x * vpb + vl;
     const bool in_block = vl < vpb;
     const bool live = in_block && v < p.nvox;
-    float* xs = reinterpret_cast<float*>(smem_raw);               // [vpb][W][NV]
+    double* ssum = reinterpret_cast<double*>(smem_raw);           // [2][vpb][W][NV] kept-sample sums
+    float* xs = reinterpret_cast<float*>(ssum + 2 * vpb * W * NV); // [vpb][W][NV]
     float* ys = xs + vpb * W * NV;                                // [vpb][nm]
     float* ws = ys + vpb * nm;                                    // [vpb][nm]
     float* xv = xs + (in_block ? vl : 0) * W * NV;
+    double* sv1 = ssum + (in_block ? vl : 0) * W * NV;
+    double* sv2 = sv1 + vpb * W * NV;
     const float* yv = ys + (in_block ? vl : 0) * nm;
     const float* wv = p.weights ? ws + (in_block ? vl : 0) * nm : nullptr;
     if (live)
@@ -145,15 +151,21 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
     VoxAux va{b1, sa, ca, 1};
 
     // walkers owned by this thread: slot 0 (simultaneous: walker a; red-black:
-    // walker a of the first half, if any) and slot 1 (red-black: walker h + a)
-    const bool rb = p.update != 0;
-    const int wown0 = rb ? (a < h ? a : -1) : a, wown1 = rb ? h + a : -1;
-    const bool own0 = live && wown0 >= 0 && wown0 < W, own1 = live && wown1 >= 0 && wown1 < W;
-    float x0s[NV], x1s[NV];
+    // walker a of the first half, if any) and, red-black, slot 1 (walker h + a)
+    const int wown0 = RB ? (a < h ? a : -1) : a, wown1 = RB ? h + a : -1;
+    const bool own0 = live && wown0 >= 0 && wown0 < W, own1 = RB && live && wown1 >= 0 && wown1 < W;
+    float x0s[NV], x1s[RB ? NV : 1];
     double lp0 = 0.0, lp1 = 0.0;
-    double s1[NV], s2[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) { s1[q] = 0.0; s2[q] = 0.0; x0s[q] = 0.0f; x1s[q] = 0.0f; }
+    for (int q = 0; q < NV; ++q) x0s[q] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < (RB ? NV : 1); ++q) x1s[q] = 0.0f;
+    if (own0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) { sv1[wown0 * NV + q] = 0.0; sv2[wown0 * NV + q] = 0.0; }
+    if (own1)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) { sv1[wown1 * NV + q] = 0.0; sv2[wown1 * NV + q] = 0.0; }
     __syncthreads();
     if (own0) {
         if (init) gw_walker_start<NV>(p, v, wown0, x0s);
@@ -163,17 +175,20 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
 #pragma unroll
         for (int q = 0; q < NV; ++q) xv[wown0 * NV + q] = x0s[q];
     }
-    if (own1) {
-        if (init) gw_walker_start<NV>(p, v, wown1, x1s);
-        else
+    if constexpr (RB) {
+        if (own1) {
+            if (init) gw_walker_start<NV>(p, v, wown1, x1s);
+            else
 #pragma unroll
-            for (int q = 0; q < NV; ++q) x1s[q] = xstate[((size_t)q * p.nvox + v) * W + wown1];
+                for (int q = 0; q < NV; ++q) x1s[q] = xstate[((size_t)q * p.nvox + v) * W + wown1];
 #pragma unroll
-        for (int q = 0; q < NV; ++q) xv[wown1 * NV + q] = x1s[q];
+            for (int q = 0; q < NV; ++q) xv[wown1 * NV + q] = x1s[q];
+        }
     }
     __syncthreads();
     if (own0) lp0 = init ? log_prob_t<MODEL, NV>(nm, s_P, x0s, yv, 1, wv, 1, va) : lpstate[(size_t)v * W + wown0];
-    if (own1) lp1 = init ? log_prob_t<MODEL, NV>(nm, s_P, x1s, yv, 1, wv, 1, va) : lpstate[(size_t)v * W + wown1];
+    if constexpr (RB)
+        if (own1) lp1 = init ? log_prob_t<MODEL, NV>(nm, s_P, x1s, yv, 1, wv, 1, va) : lpstate[(size_t)v * W + wown1];
     unsigned int nacc = 0;
     const float amin1 = p.a - 1.0f;
 
@@ -207,9 +222,19 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
         lpw = lpp;
         ++nacc;
     };
+    auto keep = [&](int w, int c, const float (&xw)[NV]) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            double d = (double)xw[j] - (double)p.shift[(size_t)j * p.nvox + v];
+            sv1[w * NV + j] += d;
+            sv2[w * NV + j] += d * d;
+            if (p.posterior)
+                p.posterior[((((size_t)j * p.repetition + rr) * p.ns + c) * W + w) * p.nvox + v] = xw[j];
+        }
+    };
 
     for (int k = k0; k <= k1; ++k) {
-        if (!rb) {
+        if constexpr (!RB) {
             float xn[NV];
             double lpp = 0.0;
             const bool acc = own0 && propose(wown0, k, 0u, x0s, lp0, xn, lpp);
@@ -231,23 +256,11 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
             }
             __syncthreads();
         }
-        int c = kept_index(p, k);
+        const int c = kept_index(p, k);
         if (c >= 0) {
-#pragma unroll
-            for (int o = 0; o < 2; ++o) {
-                const bool own = o == 0 ? own0 : own1;
-                if (!own) continue;
-                const int w = o == 0 ? wown0 : wown1;
-                const float (&xw)[NV] = o == 0 ? x0s : x1s;
-#pragma unroll
-                for (int j = 0; j < NV; ++j) {
-                    double d = (double)xw[j] - (double)p.shift[(size_t)j * p.nvox + v];
-                    s1[j] += d;
-                    s2[j] += d * d;
-                    if (p.posterior)
-                        p.posterior[((((size_t)j * p.repetition + rr) * p.ns + c) * W + w) * p.nvox + v] = xw[j];
-                }
-            }
+            if (own0) keep(wown0, c, x0s);
+            if constexpr (RB)
+                if (own1) keep(wown1, c, x1s);
         }
     }
     // persist walker state, fold the kept-sample sums of this launch
@@ -256,16 +269,20 @@ __global__ void gw_kernel(McmcParams p, int rr, int k0, int k1, int init, float*
         for (int q = 0; q < NV; ++q) xstate[((size_t)q * p.nvox + v) * W + wown0] = x0s[q];
         lpstate[(size_t)v * W + wown0] = lp0;
     }
-    if (own1) {
+    if constexpr (RB) {
+        if (own1) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) xstate[((size_t)q * p.nvox + v) * W + wown1] = x1s[q];
-        lpstate[(size_t)v * W + wown1] = lp1;
+            for (int q = 0; q < NV; ++q) xstate[((size_t)q * p.nvox + v) * W + wown1] = x1s[q];
+            lpstate[(size_t)v * W + wown1] = lp1;
+        }
     }
     if (live) {
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
-            if (s1[j] != 0.0) atomicAdd(&sum[(size_t)j * p.nvox + v], s1[j]);
-            if (s2[j] != 0.0) atomicAdd(&sumsq[(size_t)j * p.nvox + v], s2[j]);
+            double t1 = own0 ? sv1[wown0 * NV + j] : 0.0, t2 = own0 ? sv2[wown0 * NV + j] : 0.0;
+            if (own1) { t1 += sv1[wown1 * NV + j]; t2 += sv2[wown1 * NV + j]; }
+            if (t1 != 0.0) atomicAdd(&sum[(size_t)j * p.nvox + v], t1);
+            if (t2 != 0.0) atomicAdd(&sumsq[(size_t)j * p.nvox + v], t2);
         }
     }
     unsigned int wsum = nacc;
@@ -719,7 +736,8 @@ static void gw_shape(const McmcParams& p, int block_hint, int* vpb, int* block, 
     const int target = block_hint > 0 ? block_hint : 128;
     *vpb = target / tpv > 0 ? target / tpv : 1;
     *block = *vpb * tpv;
-    *smem = sizeof(float) * ((size_t)(*vpb) * W * p.nvar + 2 * (size_t)(*vpb) * p.nm);
+    *smem = sizeof(double) * 2 * (size_t)(*vpb) * W * p.nvar +
+            sizeof(float) * ((size_t)(*vpb) * W * p.nvar + 2 * (size_t)(*vpb) * p.nm);
 }
 
 // Steps [k0, k1] of repetition rr as one launch (init: the walkers start at k0 == 1).
@@ -733,12 +751,12 @@ static cudaError_t mcmc_launch_steps(const McmcParams& p, int block_hint, int rr
         size_t smem;
         gw_shape(p, block_hint, &vpb, &block, &smem);
         const int nb = (p.nvox + vpb - 1) / vpb;
+        auto k = p.update == 0 ? gw_kernel<MODEL, NV, false> : gw_kernel<MODEL, NV, true>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(gw_kernel<MODEL, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        gw_kernel<MODEL, NV><<<nb, block, smem, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, sum, sumsq);
+        k<<<nb, block, smem, s>>>(p, rr, k0, k1, k0 == 1 ? 1 : 0, xstate, lpstate, sum, sumsq);
     } else {
         const int block = block_hint > 0 ? block_hint : 128;
         const int nb = (p.nvox + block - 1) / block;
