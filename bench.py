@@ -66,6 +66,9 @@ def parse_args():
     p.add_argument("--mcmc-cpu-voxels", type=int, default=256, help="voxels of the MCMC CPU baseline sample")
     p.add_argument("--mcmc-cpu-steps", type=int, default=100, help="GW steps of the MCMC CPU baseline sample")
     p.add_argument("--no-parity", action="store_true", help="skip the fused/plain vs FP64 parity leg")
+    p.add_argument("--extras", default="", help="comma-separated side runs (default all): " + ",".join(EXTRAS))
+    p.add_argument("--path", default="fused", choices=["fused", "plain"],
+                   help="askAdam path of the main timed fit (plain: profiling runs of the op-by-op kernels)")
     return p.parse_args()
 
 
@@ -245,7 +248,7 @@ def engine_arm(args, world, rank, local):
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     f = gxa.check_set_default_basic(W["fitting"])
-    opts = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], "fused")
+    opts = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], args.path)
     model = _GxModelHandle(_lib.MODEL_R2S, te=W["te"])
     n, nm = W["nvox"], 12
     fp = lambda t: C.cast(C.c_void_p(t.data_ptr()), _lib._fp)  # noqa: E731
@@ -404,60 +407,172 @@ def engine_arm(args, world, rank, local):
                                 "sample": f"{n}-voxel volume, {args.cpu_iters} of {NITER} iterations "
                                           f"({dt:.1f} s on {cores} threads), extrapolated"}
         if not args.no_extra:
-            line["extra"] = extras(ctx, W, opts, model, stream, args)
+            line["extra"] = extras(ctx, W, opts, model, stream, args, ghz, nsm)
         print(json.dumps(line), flush=True)
 
 
-def extras(ctx, W, opts, model, stream, args):
-    """Side measurements: the plain (op-by-op) path on the same volume, and
-    Goodman-Weare MCMC on the NEXI model (200k voxels x 64 walkers, 24 shells,
-    14-node powder average, sigma fixed at 0.02) over a bounded number of steps."""
+# MUFU operations per Goodman-Weare proposal on NEXI (lmax 0, 24 shells x 14
+# nodes), counted from the kernel source: per node one rsqrt and two
+# exponentials; per proposal two logf (stretch factor, acceptance uniform)
+MCMC_SFU_PER_PROPOSAL = 24 * 14 * 3 + 2
+EXTRAS = ("plain", "parity", "mcmc", "mcmc_cpu", "c1", "c3", "c4", "surface", "autotune")
+
+
+def extras(ctx, W, opts, model, stream, args, ghz=1.965, nsm=148):
+    """Side measurements, each selectable with --extras: the plain (op-by-op)
+    path on the same volume; the fused/plain parity leg; Goodman-Weare MCMC on
+    the NEXI model (200k voxels x 64 walkers, 24 shells, 14-node powder
+    average, sigma fixed at 0.02) over a bounded number of steps, and its CPU
+    baseline; the C1, C3, C4 and cortical-surface configurations."""
     from gacelle_b200 import askadam_solver as gxa
     from gacelle_b200 import mcmc_solver, phantoms
     from gacelle_b200.models import gpuNEXI
+    want = set(args.extras.split(",")) if args.extras else set(EXTRAS)
     out = {}
     n = W["nvox"]
-    # the op-by-op (plain) path on the same volume, the full 4000 iterations
-    f = gxa.check_set_default_basic(dict(W["fitting"], iteration=NITER))
-    solver = gxa.askadam(ctx, "plain")
-    o2 = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], "plain")
-    solver._run(model, W["y"], None, W["th0"], None, None, W["idx"], W["mask"].shape, o2, 12, 2)
-    t = solver.last_timing
-    out["plain_voxel_fits_per_s"] = n / (t["main_kernel_ms"] / 1000.0)
-    out["plain_ms_per_iteration"] = t["main_kernel_ms"] / NITER
-    out["plain_iterations_timed"] = NITER
-    if not args.no_parity:
+    if "plain" in want:
+        # the op-by-op (plain) path on the same volume, the full 4000 iterations
+        f = gxa.check_set_default_basic(dict(W["fitting"], iteration=NITER))
+        solver = gxa.askadam(ctx, "plain")
+        o2 = gxa.build_opts(f, ["M0", "R2star"], W["lb"], W["ub"], "plain")
+        solver._run(model, W["y"], None, W["th0"], None, None, W["idx"], W["mask"].shape, o2, 12, 2)
+        t = solver.last_timing
+        out["plain_voxel_fits_per_s"] = n / (t["main_kernel_ms"] / 1000.0)
+        out["plain_ms_per_iteration"] = t["main_kernel_ms"] / NITER
+        out["plain_iterations_timed"] = NITER
+    if "parity" in want and not args.no_parity:
         out.update(parity_leg(ctx, W, model, args.parity_iters))
-    # MCMC
-    nv, steps = 200_000, args.mcmc_steps
+    if "mcmc" in want:
+        nv, steps = 200_000, args.mcmc_steps
+        y, gt = phantoms.nexi_volume(nv, 1005, sigma=0.02, rician=False, nx=14)
+        b, d = phantoms.nexi_shells()
+        m = gpuNEXI(b, d, nx=14)
+        m.updateProperty({"solver": "mcmc", "lmax": 0})
+        x0 = np.vstack([gt["fa"], gt["Da"], gt["De"], gt["ra"], np.full(nv, 0.02)]).astype(np.float32)
+        fit = mcmc_solver.check_set_default_basic({"algorithm": "ensemble", "iteration": steps, "burnin": 0.2,
+                                                   "thinning": 10, "Nwalker": 64, "StepSize": 2,
+                                                   "modelParams": m.modelParams,
+                                                   "lb": list(m.lb[:4]) + [0.02], "ub": list(m.ub[:4]) + [0.02],
+                                                   "returnPosterior": False})
+        mc = mcmc_solver.mcmc(ctx)
+        mask = np.ones((1, nv), bool)
+        pars0 = {p: x0[k] for k, p in enumerate(m.modelParams)}
+        mc.optimisation(y, mask, None, pars0, fit, m)   # first call of this key: the autotuner's trials
+        mc.optimisation(y, mask, None, pars0, fit, m)
+        t = mc.last_timing
+        st = mc.last_stats
+        sec = t["main_kernel_ms"] / 1000.0
+        out["mcmc_workload"] = (f"GW NEXI, {nv} voxels x 64 walkers, 24 shells, Nx 14, {steps} steps "
+                                f"(of the 5000-step run), simultaneous update")
+        out["mcmc_proposals_per_s"] = st["n_proposals"] / sec
+        out["mcmc_accepted_samples_per_s"] = st["n_accepted"] / sec
+        out["mcmc_acceptance"] = st["n_accepted"] / st["n_proposals"]
+        out["mcmc_ms_per_step"] = t["main_kernel_ms"] / steps
+        out["mcmc_block_size"] = t["block_size"]
+        sfu_peak = 16 * nsm * ghz * 1e9
+        out["mcmc_roofline"] = {"bound": "sfu", "mufu_per_proposal": MCMC_SFU_PER_PROPOSAL,
+                                "achieved": out["mcmc_proposals_per_s"] * MCMC_SFU_PER_PROPOSAL / 1e9,
+                                "peak": sfu_peak / 1e9, "unit": "G MUFU op/s",
+                                "frac": out["mcmc_proposals_per_s"] * MCMC_SFU_PER_PROPOSAL / sfu_peak,
+                                "kernel": "gw_kernel<NEXI,5,simultaneous>"}
+    if "mcmc_cpu" in want:
+        out.update(mcmc_cpu_leg(args))
+    if "c1" in want:
+        out.update(extra_c1(ctx, args))
+    if "c3" in want:
+        out.update(extra_r1r2s_batch(ctx, args))
+    if "c4" in want:
+        out.update(extra_nexi_rician(ctx, args))
+    if "surface" in want:
+        out.update(extra_nexi_surface(ctx, args))
+    if "autotune" in want:
+        out["autotune"] = autotune_leg(ctx)
+    return out
+
+
+def autotune_leg(ctx):
+    """Every launch shape the autotuner chooses from, timed explicitly, next
+    to its choice (block_size 0): the joint R1-R2* batch (1.26M voxels, 200
+    iterations), NEXI Rician Nx 100 (500k voxels, 10 iterations) and
+    Goodman-Weare NEXI (200k voxels x 64 walkers, 20 steps).  Device time of
+    the main kernel, ms."""
+    from gacelle_b200 import askadam_solver as gxa, mcmc_solver, phantoms
+    from gacelle_b200.models import _GxModelHandle, gpuNEXI
+    _lib = _lib_mod()
+    res = {}
+    # joint R1-R2* batch
+    sizes = [50_000, 110_000, 170_000, 230_000, 300_000, 400_000]
+    ys = [phantoms.r1r2s_volume(n, 1003 + i)[0] for i, n in enumerate(sizes)]
+    th0s = [np.ascontiguousarray(np.tile(np.array([[1.0], [1.0], [30.0]], np.float32), (1, n))) for n in sizes]
+    model = _GxModelHandle(_lib.MODEL_R1R2S, te=phantoms.R1R2S_TE, fa_deg=phantoms.R1R2S_FA, tr=phantoms.R1R2S_TR)
+    vols = (_lib.GxVolume * 6)(*[_gx_volume(y, t) for y, t in zip(ys, th0s)])
+    outs = [np.zeros((3, n), np.float32) for n in sizes]
+    rr = (_lib.GxAskadamResult * 6)()
+    for r, o in zip(rr, outs):
+        r.final_theta = o.ctypes.data_as(_lib._fp)
+
+    def fit_ms(model, vols, nvol, res_arr, f, names, lb, ub, block):
+        opts = gxa.build_opts(dict(f, blockSize=block), names, lb, ub, "fused")
+        ms = []
+        for _ in range(3):
+            _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, vols, nvol, C.byref(opts),
+                                             res_arr))
+            t = ctx.timing()
+            ms.append(t["main_kernel_ms"])
+        return min(ms[1:]), t["block_size"]
+    base = {"initialLearnRate": 0.01, "decayRate": 0.0, "lossFunction": "mse", "tol": 0.0,
+            "patienceConvergence": float("inf"), "convergenceStepTol": 0.0, "convergenceGradTol": 0.0}
+    f = gxa.check_set_default_basic(dict(base, iteration=200))
+    row = {}
+    for b in (64, 128, 256, 512, 0):
+        ms, used = fit_ms(model, vols, 6, rr, f, ["M0", "R1", "R2star"], [0.0, 0.1, 0.1], [2.0, 10.0, 200.0], b)
+        row["auto" if b == 0 else str(b)] = ms
+        if b == 0:
+            row["auto_block"] = used
+    res["joint_r1r2s_batch_200_iterations"] = row
+    # NEXI Rician, Nx 100
+    nv = 500_000
+    y, _ = phantoms.nexi_volume(nv, 1004, sigma=0.02, rician=True, nx=14)
+    b_, d_ = phantoms.nexi_shells()
+    model = _GxModelHandle(_lib.MODEL_NEXI, bval=b_, delta=d_, lmax=0, nx=100)
+    th0 = np.ascontiguousarray(np.tile(np.array([[0.4], [2.0], [1.0], [0.05]], np.float32), (1, nv)))
+    vol = _gx_volume(np.ascontiguousarray(y), th0)
+    out = np.zeros((4, nv), np.float32)
+    r1 = _lib.GxAskadamResult()
+    r1.final_theta = out.ctypes.data_as(_lib._fp)
+    f = gxa.check_set_default_basic(dict(base, iteration=10, lossFunction="rician", noiseSigma=0.02,
+                                         tol=-float("inf")))
+    row = {}
+    lb, ub = [2.2e-16, 2.2e-16, 2.2e-16, 1 / 250], [1.0, 3.0, 3.0, 1.0]
+    for b in (64, 128, 256, 512, 0):
+        ms, used = fit_ms(model, C.byref(vol), 1, C.byref(r1), f, ["fa", "Da", "De", "ra"], lb, ub, b)
+        row["auto" if b == 0 else str(b)] = ms
+        if b == 0:
+            row["auto_block"] = used
+    res["nexi_rician_nx100_10_iterations"] = row
+    # Goodman-Weare NEXI
+    nv = 200_000
     y, gt = phantoms.nexi_volume(nv, 1005, sigma=0.02, rician=False, nx=14)
-    b, d = phantoms.nexi_shells()
-    m = gpuNEXI(b, d, nx=14)
+    m = gpuNEXI(b_, d_, nx=14)
     m.updateProperty({"solver": "mcmc", "lmax": 0})
     x0 = np.vstack([gt["fa"], gt["Da"], gt["De"], gt["ra"], np.full(nv, 0.02)]).astype(np.float32)
-    fit = mcmc_solver.check_set_default_basic({"algorithm": "ensemble", "iteration": steps, "burnin": 0.2,
-                                               "thinning": 10, "Nwalker": 64, "StepSize": 2,
-                                               "modelParams": m.modelParams,
-                                               "lb": list(m.lb[:4]) + [0.02], "ub": list(m.ub[:4]) + [0.02],
-                                               "returnPosterior": False})
-    mc = mcmc_solver.mcmc(ctx)
-    mask = np.ones((1, nv), bool)
-    mc.optimisation(y, mask, None, {p: x0[k] for k, p in enumerate(m.modelParams)}, fit, m)
-    t = mc.last_timing
-    st = mc.last_stats
-    sec = t["main_kernel_ms"] / 1000.0
-    out["mcmc_workload"] = (f"GW NEXI, {nv} voxels x 64 walkers, 24 shells, Nx 14, {steps} steps "
-                            f"(of the 5000-step run), simultaneous update")
-    out["mcmc_proposals_per_s"] = st["n_proposals"] / sec
-    out["mcmc_accepted_samples_per_s"] = st["n_accepted"] / sec
-    out["mcmc_acceptance"] = st["n_accepted"] / st["n_proposals"]
-    out["mcmc_ms_per_step"] = t["main_kernel_ms"] / steps
-    out.update(mcmc_cpu_leg(args))
-    out.update(extra_c1(ctx, args))
-    out.update(extra_r1r2s_batch(ctx, args))
-    out.update(extra_nexi_rician(ctx, args))
-    out.update(extra_nexi_surface(ctx, args))
-    return out
+    row = {}
+    for b in (64, 128, 256, 512, 1024, 0):
+        fit = mcmc_solver.check_set_default_basic({"algorithm": "ensemble", "iteration": 20, "burnin": 0.2,
+                                                   "thinning": 10, "Nwalker": 64, "StepSize": 2,
+                                                   "modelParams": m.modelParams, "blockSize": b,
+                                                   "lb": list(m.lb[:4]) + [0.02], "ub": list(m.ub[:4]) + [0.02],
+                                                   "returnPosterior": False})
+        mc = mcmc_solver.mcmc(ctx)
+        ms = []
+        for _ in range(3):
+            mc.optimisation(y, np.ones((1, nv), bool), None, {p: x0[k] for k, p in enumerate(m.modelParams)}, fit, m)
+            ms.append(mc.last_timing["main_kernel_ms"])
+        row["auto" if b == 0 else str(b)] = min(ms[1:])
+        if b == 0:
+            row["auto_block"] = mc.last_timing["block_size"]
+    res["gw_nexi_20_steps"] = row
+    return res
 
 
 def mcmc_cpu_leg(args):
@@ -508,7 +623,8 @@ def extra_c1(ctx, args):
     for path in ("plain", "fused"):
         o = gxa.build_opts(f, ["M0", "R2star"], lb, ub, path)
         solver = gxa.askadam(ctx, path)
-        solver._run(model, y, None, th0, None, None, idx, mask.shape, o, 12, 2)
+        for _ in range(2):  # the first fused call of this configuration runs the autotuner's trials
+            solver._run(model, y, None, th0, None, None, idx, mask.shape, o, 12, 2)
         t = solver.last_timing
         out[f"c1_{path}_voxel_fits_per_s"] = n / (t["total_ms"] / 1000.0)
         out[f"c1_{path}_call_ms"] = t["total_ms"]
@@ -598,14 +714,15 @@ def extra_r1r2s_batch(ctx, args):
     res = (_lib.GxAskadamResult * 6)()
     for r, o in zip(res, outs):
         r.final_theta = o.ctypes.data_as(_lib._fp)
-    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, vols, 6, C.byref(opts), res))
+    for _ in range(2):  # the first call of this configuration runs the autotuner's trials
+        _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, vols, 6, C.byref(opts), res))
     t = ctx.timing()
     nv = sum(sizes)
     sec = t["main_kernel_ms"] / 1000.0
     return {"c3_workload": f"joint R1R2* batch of 6 volumes ({nv} voxels), 24 measurements, MSE, "
                            f"{args.c3_iters} iterations, one call",
             "c3_voxel_fits_per_s": nv / sec, "c3_voxel_iterations_per_s": nv * args.c3_iters / sec,
-            "c3_call_ms": t["total_ms"]}
+            "c3_call_ms": t["total_ms"], "c3_block_size": t["block_size"]}
 
 
 def extra_nexi_rician(ctx, args):
@@ -638,7 +755,7 @@ def extra_nexi_rician(ctx, args):
     lb, ub = [2.2e-16, 2.2e-16, 2.2e-16, 1 / 250], [1.0, 3.0, 3.0, 1.0]
     th0 = np.ascontiguousarray(np.tile(np.array([[0.4], [2.0], [1.0], [0.05]], np.float32), (1, nv)))
     f = gxa.check_set_default_basic({"iteration": args.c4_iters, "initialLearnRate": 0.01, "decayRate": 0.0,
-                                     "lossFunction": "rician", "noiseSigma": sig, "tol": 0.0,
+                                     "lossFunction": "rician", "noiseSigma": sig, "tol": -float("inf"),
                                      "patienceConvergence": float("inf"), "convergenceStepTol": 0.0,
                                      "convergenceGradTol": 0.0})
     opts = gxa.build_opts(f, ["fa", "Da", "De", "ra"], lb, ub, "fused")
@@ -646,12 +763,15 @@ def extra_nexi_rician(ctx, args):
     vol = _gx_volume(y, th0)
     res = _lib.GxAskadamResult()
     res.final_theta = out.ctypes.data_as(_lib._fp)
-    _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, C.byref(vol), 1, C.byref(opts),
-                                     C.byref(res)))
+    for _ in range(2):  # the first call of this configuration runs the autotuner's trials
+        _lib.check(_lib.lib().gx_askadam(ctx.ptr, C.byref(model.s), _lib.MEM_HOST, C.byref(vol), 1, C.byref(opts),
+                                         C.byref(res)))
+    assert res.final_niteration == args.c4_iters
     t = ctx.timing()
     sec = t["main_kernel_ms"] / 1000.0
     r = {"c4_workload": f"NEXI lmax 0, Rician loss, Nx {nx}, {nv} voxels, {args.c4_iters} iterations",
-         "c4_voxel_iterations_per_s": nv * args.c4_iters / sec, "c4_ms_per_iteration": t["main_kernel_ms"] / args.c4_iters}
+         "c4_voxel_iterations_per_s": nv * args.c4_iters / sec, "c4_ms_per_iteration": t["main_kernel_ms"] / args.c4_iters,
+         "c4_block_size": t["block_size"]}
     # dictionary starting points of the same voxels
     m = gpuNEXI(b, d)
     m.context = ctx

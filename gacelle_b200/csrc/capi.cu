@@ -1037,10 +1037,9 @@ static gx_status tune_fused(AdamJob& J) {
     while ((1LL << (cls + 1)) <= (long long)J.nvtot) ++cls;
     const TuneKey key{{1, c->device, J.id, o->loss, J.nm, stats ? 1 : 0, J.prior ? 1 : 0, J.a.weights ? 1 : 0,
                        J.a.b1 ? 1 : 0, J.a.sigma ? 1 : 0, o->optimiser, o->transform, cls}};
-    int Bl = tune_lookup(key);
+    int Bl = o->iteration < 2 ? 128 : tune_lookup(key);  // trials need two epochs of history rows
     if (Bl <= 0) {
         const int N = o->iteration;
-        const int E = std::max(1, std::min({8, N, (int)(2000000LL / std::max(J.nvtot, 1))}));
         AdamParams t = J.a;
         const size_t pn = (size_t)J.np * J.nvtot;
         float* sc;
@@ -1054,6 +1053,24 @@ static gx_status tune_fused(AdamJob& J) {
         t.ckpt = nullptr;
         t.ckpt_every = 0;
         t.res_out = nullptr;
+        // epochs per trial: about 1 ms of work (at least 2), so that the
+        // kernel's one-time staging of the measurements is amortised as in a fit
+        int E = 1;
+        {
+            int* blk;
+            TRY(upload_blk_table(J, 128, &blk));
+            t.blk_vol = blk;
+            float m = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {
+                CK(cudaEventRecord(c->ev[2], c->stream));
+                CK(launch_fused(t, J.id, o->loss, stats, 1, 1, 0, true, 128, J.nvtot / 128, c->stream));
+                CK(cudaEventRecord(c->ev[3], c->stream));
+                CK(cudaEventSynchronize(c->ev[3]));
+                cudaEventElapsedTime(&m, c->ev[2], c->ev[3]);
+            }
+            E = (int)std::min(64.0, std::max(2.0, 1.0 / std::max((double)m, 1e-3)));
+            E = std::max(1, std::min(E, N));
+        }
         float best = 0.f;
         for (int cand : {64, 128, 256, 512}) {
             if (J.B % cand || fused_block_limit(t, J.id, o->loss, stats) < cand) continue;
