@@ -162,9 +162,17 @@ def test_weighted_loss_with_nexi_weights_matches_oracle(ctx, loss, path):
     _, gu, _, _, _ = oracle.model_gradient(om, oracle.Volume(y.astype(np.float64)), o, th0.astype(np.float64))
     assert rel_rmse(gw, gu) > 1e-2
     if loss == "l1":
+        # the band of an FP32 run: the FP64 oracle with its state rounded to
+        # FP32 each epoch, and with the measurements perturbed at the FP32
+        # forward model's relative precision (2e-6; the 14-node trapezoid of
+        # fast exponentials is held to 2e-5 by test_forward_matches_oracle):
+        # the sign subgradient flips for residuals inside that precision, which
+        # the state rounding alone does not provoke
         o32 = run_oracle("nexi", y, th0, dict(f, _state_f32=True), NAMES["nexi"], weights=w)
+        yp = (y.astype(np.float64) * (1 + 2e-6 * np.random.default_rng(43).standard_normal(y.shape)))
+        opert = run_oracle("nexi", yp, th0, f, NAMES["nexi"], weights=w)
         for k in range(4):
-            band = rel_rmse(o32["final"][k], orc["final"][k])
+            band = max(rel_rmse(o32["final"][k], orc["final"][k]), rel_rmse(opert["final"][k], orc["final"][k]))
             assert rel_rmse(eng["final_theta"][k], orc["final"][k]) <= 2 * band + 1e-4, (k, band)
         return
     for k in range(4):

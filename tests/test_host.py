@@ -220,3 +220,43 @@ def test_r1r2s_true_flip_angle_becomes_b1():
     with pytest.raises(GacelleError):
         m._with_b1({"trueFlipAngle": tfa[..., :1]})
     assert m._with_b1({"b1": b1})["b1"] is b1 and m._with_b1(None) is None
+
+
+_MEX_API = """
+/* Declarations of the MATLAB C matrix / MEX API functions the gateway uses,
+   as documented by MathWorks (names and signatures only), for a compile check */
+#include <stddef.h>
+#include <stdbool.h>
+typedef struct mxArray_tag mxArray;
+typedef size_t mwSize;
+typedef size_t mwIndex;
+typedef enum { mxUNKNOWN_CLASS, mxCELL_CLASS, mxSTRUCT_CLASS, mxLOGICAL_CLASS, mxCHAR_CLASS, mxVOID_CLASS,
+               mxDOUBLE_CLASS, mxSINGLE_CLASS, mxINT8_CLASS, mxUINT8_CLASS, mxINT16_CLASS, mxUINT16_CLASS,
+               mxINT32_CLASS, mxUINT32_CLASS, mxINT64_CLASS, mxUINT64_CLASS } mxClassID;
+typedef enum { mxREAL, mxCOMPLEX } mxComplexity;
+bool mxIsStruct(const mxArray*); bool mxIsEmpty(const mxArray*); bool mxIsChar(const mxArray*);
+bool mxIsDouble(const mxArray*); bool mxIsSingle(const mxArray*); bool mxIsComplex(const mxArray*);
+bool mxIsUint64(const mxArray*); bool mxIsInt32(const mxArray*); bool mxIsCell(const mxArray*);
+mxArray* mxGetField(const mxArray*, mwIndex, const char*);
+void mxSetField(mxArray*, mwIndex, const char*, mxArray*);
+double mxGetScalar(const mxArray*); int mxGetString(const mxArray*, char*, mwSize);
+size_t mxGetNumberOfElements(const mxArray*); size_t mxGetM(const mxArray*); size_t mxGetN(const mxArray*);
+double* mxGetPr(const mxArray*); void* mxGetData(const mxArray*); mxArray* mxGetCell(const mxArray*, mwIndex);
+mxArray* mxCreateNumericMatrix(mwSize, mwSize, mxClassID, mxComplexity);
+mxArray* mxCreateDoubleMatrix(mwSize, mwSize, mxComplexity); mxArray* mxCreateDoubleScalar(double);
+mxArray* mxCreateStructMatrix(mwSize, mwSize, int, const char**); void mxDestroyArray(mxArray*);
+void mexErrMsgIdAndTxt(const char*, const char*, ...); void mexWarnMsgIdAndTxt(const char*, const char*, ...);
+"""
+
+
+def test_mex_gateway_compiles_against_the_mex_api(tmp_path):
+    """The MATLAB gateway (gacelle_b200/matlab/gacelle_b200_mex.c) is built only
+    where MATLAB is installed; here it is compiled against declarations of the
+    documented MEX API functions it calls and the C-ABI header, with warnings
+    as errors, so that a signature it passes to the engine cannot drift."""
+    (tmp_path / "mex.h").write_text(_MEX_API)
+    src = os.path.join(ROOT, "gacelle_b200", "matlab", "gacelle_b200_mex.c")
+    r = subprocess.run(["gcc", "-std=c11", "-fsyntax-only", "-Wall", "-Wextra", "-Werror", "-Wno-unused-parameter",
+                        "-I", str(tmp_path), "-I", os.path.join(ROOT, "include"), src],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
