@@ -164,6 +164,20 @@ def profile_traffic(kernel: str):
     return None
 
 
+def host_cpu() -> str:
+    """The host's CPU model and logical CPU count (the CPU baselines' cores)."""
+    model = "unknown CPU"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return f"{model}, {os.cpu_count()} logical CPUs"
+
+
 def max_over_ranks(x: float, world: int) -> float:
     if world == 1:
         return x
@@ -224,7 +238,7 @@ def reference_arm(args, world, rank):
             "data": "synthetic (seeded phantom, seed 1002)",
             "config": bench_config(W["nvox"] * args.gpus, args.gpus),
             "cpu_baseline": {"value": value, "unit": "voxel-fits/s", "cores": cores, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "host": host_cpu()},
             "e2e": {"value": value, "unit": "voxel-fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -403,7 +417,7 @@ def engine_arm(args, world, rank, local):
                     "d2h_bytes_per_step": d2h}}
     if rank == 0:
         cv, cores, dt = cpu_sample(W, args.cpu_iters)
-        line["cpu_baseline"] = {"value": cv, "unit": "voxel-fits/s", "cores": cores, "kind": "port",
+        line["cpu_baseline"] = {"value": cv, "unit": "voxel-fits/s", "cores": cores, "kind": "port", "host": host_cpu(),
                                 "sample": f"{n}-voxel volume, {args.cpu_iters} of {NITER} iterations "
                                           f"({dt:.1f} s on {cores} threads), extrapolated"}
         if not args.no_extra:

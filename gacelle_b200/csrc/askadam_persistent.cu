@@ -170,36 +170,9 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned int 
 // flags fl: bits 0-2 on the last x/y/z plane, 3-5 on the first, where the
 // neighbour wraps around periodically).  Interior voxels, almost all of a
 // masked volume, take the plain offsets.
-// Flag bits of the pair variant (bits 0-5: on the last / first x, y, z plane)
-constexpr unsigned int kFlXfIn = 64, kFlXbIn = 128;       // x+1 / x-1 is the slice's next / previous voxel
-constexpr unsigned int kFlXfZero = 256, kFlXbZero = 512;  // x+1 / x-1 outside the mask
-constexpr unsigned int kFlZfZero = 1024, kFlZbZero = 2048; // z+1 / z-1 outside the mask
-constexpr short kNbGlobal = -1, kNbZero = -2;             // y neighbour codes beside slice positions
-
 struct Neighbours {
     int sy, sz, wx, wy, wz;
     bool tv3;
-    // Pair variant: x and y neighbours inside the slice come from the
-    // slice's map values of the epoch in shared memory (cb, at the slice
-    // positions jxf / jxb / nyf / nyb), neighbours outside the mask are 0,
-    // the others are read from the map G in L2.
-    __device__ __forceinline__ void load_pair(const float* G, const float* cb, int pidx, unsigned int fl, short nyf,
-                                              short nyb, int jxf, int jxb, float (&f)[3], float (&b)[3]) const {
-        const int qxf = (fl & 1) ? pidx - wx : pidx + 1, qxb = (fl & 8) ? pidx + wx : pidx - 1;
-        f[0] = (fl & kFlXfIn) ? cb[jxf] : (fl & kFlXfZero) ? 0.0f : __ldcg(G + qxf);
-        b[0] = (fl & kFlXbIn) ? cb[jxb] : (fl & kFlXbZero) ? 0.0f : __ldcg(G + qxb);
-        const int qyf = (fl & 2) ? pidx - wy : pidx + sy, qyb = (fl & 16) ? pidx + wy : pidx - sy;
-        f[1] = nyf >= 0 ? cb[nyf] : nyf == kNbZero ? 0.0f : __ldcg(G + qyf);
-        b[1] = nyb >= 0 ? cb[nyb] : nyb == kNbZero ? 0.0f : __ldcg(G + qyb);
-        if (tv3) {
-            const int qzf = (fl & 4) ? pidx - wz : pidx + sz, qzb = (fl & 32) ? pidx + wz : pidx - sz;
-            f[2] = (fl & kFlZfZero) ? 0.0f : __ldcg(G + qzf);
-            b[2] = (fl & kFlZbZero) ? 0.0f : __ldcg(G + qzb);
-        } else {
-            f[2] = 0.0f;
-            b[2] = 0.0f;
-        }
-    }
     __device__ __forceinline__ void load(const float* G, int pidx, unsigned int fl, float (&f)[3],
                                          float (&b)[3]) const {
         if (!(fl & (tv3 ? 63u : 27u))) {
@@ -253,22 +226,13 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     // pass does not evaluate the transform again; same operations, same order.
     // PAIR (up to 16 measurements, without statistics): two voxels per
     // thread, pair instructions, with the fidelity-pass cache (CACHE)
-    // PAIR: slots 0 and 1 hold the unregularised parameter's z-gradient and the
-    // regularised one's fidelity gradient; slots 2 and 3 the regularised map
-    // value theta of every slice voxel for even and odd epochs, which the
-    // TV/update pass reads for the voxel itself and for its x and y
-    // neighbours inside the slice (dtheta/dz is recomputed there from z)
     constexpr bool PAIR = persist_pairs(MAXM, STATS);
     constexpr bool CACHE = PAIR;
     constexpr int NAUX = CACHE ? 4 : NP;
     float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NAUX][slice] fidelity pass results
     int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NAUX * p.slice);        // [slice] grid index
     unsigned short* s_fl = reinterpret_cast<unsigned short*>(s_p + p.slice); // [slice] boundary/mask flags
-    // PAIR: [2][slice] slice position of the +y and -y neighbour (kNbGlobal:
-    // read from the map in L2, kNbZero: outside the mask, 0)
-    short* s_ny = reinterpret_cast<short*>(s_fl + ((p.slice + 1) & ~1));
-    float* s_y = reinterpret_cast<float*>(PAIR ? reinterpret_cast<unsigned short*>(s_ny + 2 * p.slice)
-                                               : s_fl + ((p.slice + 1) & ~1));  // [nm][slice] if staged
+    float* s_y = reinterpret_cast<float*>(s_fl + ((p.slice + 1) & ~1));       // [nm][slice] if staged
     const int BT = blockDim.x, tid = threadIdx.x;
     const int base = blockIdx.x * p.slice;
     const int n = min(base + p.slice, a.nvtot) - base;  // voxels of this slice
@@ -319,65 +283,16 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         if (p.data_in_smem)
             for (int m = 0; m < a.nm; ++m) s_y[m * S + j] = a.data[(size_t)m * a.nvtot + base + i];
     }
-    if constexpr (PAIR) {
-        // neighbour codes of the pair variant, from the whole slice's grid
-        // indices: x+1 / x-1 is the work-list successor / predecessor in the
-        // slice, or outside the mask (its map value is 0); z+1 / z-1 outside
-        // the mask; the +y / -y neighbour's slice position (binary search over
-        // the slice's grid indices, kept only when it matches, so an unsorted
-        // work-list merely reads more neighbours from L2)
-        __syncthreads();
-        const int nval = max(0, min(n, V.nvox - (base - V.off)));  // voxels of the volume, not padding
-        auto find = [&](int q) -> short {
-            int lo = 0, hi = nval - 1;
-            while (lo <= hi) {
-                const int mid = (lo + hi) >> 1;
-                const int v = s_p[sidx(mid)];
-                if (v == q) return (short)sidx(mid);
-                if (v < q) lo = mid + 1;
-                else hi = mid - 1;
-            }
-            return kNbGlobal;
-        };
-        const bool tv3s = a.tv_3d != 0;
-        for (int i = tid; i < n; i += BT) {
-            const int j = sidx(i);
-            unsigned short fl = s_fl[j] & 63u;
-            short nyf = kNbGlobal, nyb = kNbGlobal;
-            if (i < nval && a.n_reg > 0) {
-                const int pp = s_p[j];
-                const int x = pp % dx, yz = pp / dx, y = yz % dy, zc = yz / dy;
-                const int qxf = x < dx - 1 ? pp + 1 : pp - wx, qxb = x > 0 ? pp - 1 : pp + wx;
-                const int qyf = y < dy - 1 ? pp + sy : pp - wy, qyb = y > 0 ? pp - sy : pp + wy;
-                const int qzf = zc < dz - 1 ? pp + sz : pp - wz, qzb = zc > 0 ? pp - sz : pp + wz;
-                if (i + 1 < nval && s_p[sidx(i + 1)] == qxf) fl |= kFlXfIn;
-                if (i >= 1 && s_p[sidx(i - 1)] == qxb) fl |= kFlXbIn;
-                if (!mk[qxf]) fl |= kFlXfZero;
-                if (!mk[qxb]) fl |= kFlXbZero;
-                if (tv3s && !mk[qzf]) fl |= kFlZfZero;
-                if (tv3s && !mk[qzb]) fl |= kFlZbZero;
-                nyf = mk[qyf] ? find(qyf) : kNbZero;
-                nyb = mk[qyb] ? find(qyb) : kNbZero;
-            }
-            s_fl[j] = fl;
-            s_ny[j] = nyf;
-            s_ny[S + j] = nyb;
-        }
-    }
     __shared__ DevProtocol s_P;
     stage_protocol(a.P, &s_P);
     // bar_arrive: one arrival per worker warp and epoch; bar_open: one per
-    // epoch boundary (the grid barrier has passed, or s_err is set);
-    // bar_fid (pair variant): one arrival per worker warp after its fidelity
-    // pass, so that the TV/update pass reads every slice voxel's map value
-    // of the epoch
-    __shared__ unsigned long long bar_arrive, bar_open, bar_fid;
+    // epoch boundary (the grid barrier has passed, or s_err is set)
+    __shared__ unsigned long long bar_arrive, bar_open;
     __shared__ int s_err;
     const int NWT = BT - 32;  // worker threads; the last warp is the barrier warp
     if (tid == 0) {
         mbar_init(&bar_arrive, (unsigned int)(NWT >> 5));
         mbar_init(&bar_open, 1u);
-        mbar_init(&bar_fid, (unsigned int)(NWT >> 5));
         s_err = 0;
     }
     __syncthreads();
@@ -499,23 +414,16 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const float2 gr = mul2(kr == 0 ? g[0] : g[1], nrm), gn = mul2(kr == 0 ? g[1] : g[0], nrm);
             st2(s_gf + 0 * S, q, mul2(gn, kr == 0 ? dth[1] : dth[0]));
             st2(s_gf + 1 * S, q, gr);
-            st2(s_gf + (2 + (e & 1)) * S, q, kr == 0 ? th[0] : th[1]);
+            st2(s_gf + 2 * S, q, kr == 0 ? dth[0] : dth[1]);
+            st2(s_gf + 3 * S, q, kr == 0 ? th[0] : th[1]);
             if (ok0) q0 += tot.x;
             if (ok1) q0 += tot.y;
         }
-        // this warp's map values of the epoch are published to the CTA
-        __syncwarp();
-        if ((tid & 31) == 0) mbar_arrive(&bar_fid);
         // every CTA's map of the previous epoch (written before its arrival)
         if (e > p.e_begin)
             if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, p.spin_cycles) ||
                 *(volatile int*)&s_err)
                 return;
-        // every worker warp's map values of the epoch
-        if (!mbar_wait(&bar_fid, (unsigned int)(e - p.e_begin) & 1u, p.barrier, p.spin_cycles) ||
-            *(volatile int*)&s_err)
-            return;
-        const float* cb = s_gf + (2 + (e & 1)) * S;  // theta of the slice's voxels, this epoch
         const bool ckpt = upd && a.ckpt_every > 0 && (e % a.ckpt_every) == 0;
         float* cp = ckpt ? a.ckpt + (size_t)(e / a.ckpt_every) * 3 * NP * a.nvtot : nullptr;
         const float* G = gcur + V.grid_off;
@@ -527,21 +435,17 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const bool ok0 = (v0 - V.off) < V.nvox, ok1 = (v0 + 32 - V.off) < V.nvox;
             const float2 gn = ld2(s_gf + 0 * S, q);
             float2 grf = ld2(s_gf + 1 * S, q);
-            // the regularised parameter's theta and dtheta/dz, recomputed from
-            // its z exactly as the fidelity pass computed them
-            float2 dthr;
-            const float2 c = unscale_sig2(lbr, ubr, ld2(s_st + kr * S, q), dthr);
+            const float2 dthr = ld2(s_gf + 2 * S, q);
+            const float2 c = ld2(s_gf + 3 * S, q);
             const int2 pp = reinterpret_cast<const int2*>(s_p)[q];
             const int p0 = pp.x, p1 = pp.y;
             const unsigned int fl01 = reinterpret_cast<const unsigned int*>(s_fl)[q];
             const unsigned int fl0 = fl01 & 0xffffu, fl1 = fl01 >> 16;
-            const short2 nyf = reinterpret_cast<const short2*>(s_ny)[q];
-            const short2 nyb = reinterpret_cast<const short2*>(s_ny + S)[q];
             float f0[3] = {0.f, 0.f, 0.f}, b0[3] = {0.f, 0.f, 0.f}, f1[3] = {0.f, 0.f, 0.f}, b1[3] = {0.f, 0.f, 0.f};
-            if (ok0) nb.load_pair(G, cb, p0, fl0, nyf.x, nyb.x, sidx(i0 + 1), sidx(i0 - 1), f0, b0);
-            if (ok1) nb.load_pair(G, cb, p1, fl1, nyf.y, nyb.y, sidx(i0 + 33), sidx(i0 + 31), f1, b1);
-            const bool mb0[3] = {(fl0 & kFlXbZero) == 0, nyb.x != kNbZero, (fl0 & kFlZbZero) == 0};
-            const bool mb1[3] = {(fl1 & kFlXbZero) == 0, nyb.y != kNbZero, (fl1 & kFlZbZero) == 0};
+            if (ok0) nb.load(G, p0, fl0, f0, b0);
+            if (ok1) nb.load(G, p1, fl1, f1, b1);
+            const bool mb0[3] = {(fl0 & 64) != 0, (fl0 & 128) != 0, (fl0 & 256) != 0};
+            const bool mb1[3] = {(fl1 & 64) != 0, (fl1 & 128) != 0, (fl1 & 256) != 0};
             float2 cost, gt;
             tv_terms2(c, f0, b0, f1, b1, mb0, mb1, iv, tv3 ? 3 : 2, cost, gt);
             if (ok0) {
@@ -856,13 +760,9 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
     }
     const bool stats_any = true;  // size for the larger (statistics) variant
     const int NS = stats_any ? 4 : 3;
-    const int variant = persist_variant(a, loss, true);
-    // two voxels per thread; slice positions must fit the pair variant's int16 y-neighbour table
-    const bool pairs = persist_pairs(variant, stats) && pair_layout_ok(a.nvtot, slice) && slice <= 16384;
     size_t red = sizeof(double) * 2 * 32 * kHistW;
     size_t state = sizeof(float) * (size_t)(NS + 1) * 2 * slice + sizeof(int) * slice +
-                   sizeof(unsigned short) * ((slice + 1) & ~1) +  // + fidelity gradient [2][slice]
-                   (pairs ? sizeof(short) * 2 * (size_t)slice : 0);  // y-neighbour positions of the pair variant
+                   sizeof(unsigned short) * ((slice + 1) & ~1);  // + fidelity gradient [2][slice]
     size_t data = sizeof(float) * (size_t)a.nm * slice;
     const size_t budget = (size_t)smem_optin - 2048;  // static shared memory (staged protocol) and slack
     if (red + state > budget) return false;
@@ -871,6 +771,8 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
     // worker threads: as many as fit beside the barrier warp, spread so that
     // the last pass over the slice is full (every worker warp reaches the
     // grid barrier after the same number of voxels)
+    const int variant = persist_variant(a, loss, true);
+    const bool pairs = persist_pairs(variant, stats) && pair_layout_ok(a.nvtot, slice);  // two voxels per thread
     const int units = pairs ? slice / 2 : slice;
     // every variant that may run with this thread count must allow it
     const int maxw = std::min(persist_max_threads(variant, stats), persist_max_threads(variant, !stats)) - 32;
@@ -900,7 +802,7 @@ cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, P
     // the pair variant needs slices and a work-list of whole 64-voxel chunks;
     // otherwise the run-time variant takes the launch
     int var = variant;
-    if (persist_pairs(var, p.stats != 0) && (!pair_layout_ok(a.nvtot, plan.slice) || plan.slice > 16384)) var = 0;
+    if (persist_pairs(var, p.stats != 0) && !pair_layout_ok(a.nvtot, plan.slice)) var = 0;
     const int pairs = persist_pairs(var, p.stats != 0) ? 1 : 0;
     if (var != plan.quad_width || pairs != plan.quad_pairs) p.data_quads = nullptr;  // read [nm][nvtot]
     if (var == 8) return launch_persist_t<kMSE, 8>(a, p, plan.threads, plan.ctas, plan.smem, s);
