@@ -64,6 +64,8 @@ def parse_args():
     p.add_argument("--mcmc-steps", type=int, default=200, help="GW steps of the MCMC side measurement")
     p.add_argument("--parity-iters", type=int, default=400, help="epochs of the fused/plain vs FP64 parity leg")
     p.add_argument("--mcmc-cpu-voxels", type=int, default=256, help="voxels of the MCMC CPU baseline sample")
+    p.add_argument("--mcmc-summary-steps", type=int, default=200,
+                   help="GW steps of the on-device median/iqr/mode run (5000: the full 102 GB posterior in HBM)")
     p.add_argument("--mcmc-cpu-steps", type=int, default=100, help="GW steps of the MCMC CPU baseline sample")
     p.add_argument("--no-parity", action="store_true", help="skip the fused/plain vs FP64 parity leg")
     p.add_argument("--extras", default="", help="comma-separated side runs (default all): " + ",".join(EXTRAS))
@@ -429,7 +431,7 @@ def engine_arm(args, world, rank, local):
 # nodes), counted from the kernel source: per node one rsqrt and two
 # exponentials; per proposal two logf (stretch factor, acceptance uniform)
 MCMC_SFU_PER_PROPOSAL = 24 * 14 * 3 + 2
-EXTRAS = ("plain", "parity", "mcmc", "mcmc_cpu", "c1", "c3", "c4", "surface", "autotune")
+EXTRAS = ("plain", "parity", "mcmc", "mcmc_summaries", "mcmc_cpu", "c1", "c3", "c4", "surface", "autotune")
 
 
 def extras(ctx, W, opts, model, stream, args, ghz=1.965, nsm=148):
@@ -489,6 +491,8 @@ def extras(ctx, W, opts, model, stream, args, ghz=1.965, nsm=148):
                                 "peak": sfu_peak / 1e9, "unit": "G MUFU op/s",
                                 "frac": out["mcmc_proposals_per_s"] * MCMC_SFU_PER_PROPOSAL / sfu_peak,
                                 "kernel": "gw_kernel<NEXI,5,simultaneous>"}
+    if "mcmc_summaries" in want:
+        out.update(mcmc_summaries_leg(ctx, args))
     if "mcmc_cpu" in want:
         out.update(mcmc_cpu_leg(args))
     if "c1" in want:
@@ -587,6 +591,36 @@ def autotune_leg(ctx):
             row["auto_block"] = mc.last_timing["block_size"]
     res["gw_nexi_20_steps"] = row
     return res
+
+
+def mcmc_summaries_leg(ctx, args):
+    """res2out's median / iqr / mode of the Goodman-Weare NEXI run (200k voxels
+    x 64 walkers), computed on the device from the kept samples, which stay in
+    HBM (no posterior returned): the summaries' kernel time and the samples
+    per voxel it ranks."""
+    from gacelle_b200 import mcmc_solver, phantoms
+    from gacelle_b200.models import gpuNEXI
+    nv, steps = 200_000, args.mcmc_summary_steps
+    y, gt = phantoms.nexi_volume(nv, 1005, sigma=0.02, rician=False, nx=14)
+    b, d = phantoms.nexi_shells()
+    m = gpuNEXI(b, d, nx=14)
+    m.updateProperty({"solver": "mcmc", "lmax": 0})
+    x0 = np.vstack([gt["fa"], gt["Da"], gt["De"], gt["ra"], np.full(nv, 0.02)]).astype(np.float32)
+    fit = mcmc_solver.check_set_default_basic({"algorithm": "ensemble", "iteration": steps, "burnin": 0.2,
+                                               "thinning": 10, "Nwalker": 64, "StepSize": 2,
+                                               "modelParams": m.modelParams,
+                                               "metric": ["mean", "std", "median", "iqr", "mode"],
+                                               "lb": list(m.lb[:4]) + [0.02], "ub": list(m.ub[:4]) + [0.02],
+                                               "returnPosterior": False})
+    mc = mcmc_solver.mcmc(ctx)
+    out = mc.optimisation(y, np.ones((1, nv), bool), None, {p: x0[k] for k, p in enumerate(m.modelParams)}, fit, m)
+    t = mc.last_timing
+    ns = mcmc_solver.number_of_samples(fit)
+    assert np.all(np.isfinite(out["median"]["fa"])) and np.all(np.isfinite(out["mode"]["Da"]))
+    return {"mcmc_summaries_workload": f"GW NEXI, {nv} voxels x 64 walkers, {steps} steps, {ns} kept samples per "
+                                       f"walker: median, iqr, mode of 5 parameters over {64 * ns} samples per voxel",
+            "mcmc_summaries_ms": t["aux_kernel_ms"], "mcmc_summaries_posterior_bytes": 4 * 5 * nv * 64 * ns,
+            "mcmc_summaries_chain_ms": t["main_kernel_ms"]}
 
 
 def mcmc_cpu_leg(args):

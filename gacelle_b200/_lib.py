@@ -104,7 +104,7 @@ class GxTiming(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("main_kernel_ms", C.c_double),
                 ("main_launches", C.c_int32), ("kernel_launches", C.c_int64),
                 ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("tv_path", C.c_int32),
-                ("block_size", C.c_int32), ("autotuned", C.c_int32)]
+                ("block_size", C.c_int32), ("autotuned", C.c_int32), ("aux_kernel_ms", C.c_double)]
 
 
 class GxTestHooks(C.Structure):

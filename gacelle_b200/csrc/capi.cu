@@ -103,7 +103,7 @@ struct gx_context {
     gx_timing timing{};
     void* buf[S_NSLOTS] = {};
     size_t cap[S_NSLOTS] = {};
-    cudaEvent_t ev[4] = {};
+    cudaEvent_t ev[6] = {};  // call, main kernel, post-processing kernels
     // pinned staging of the small per-call tables, so that their copies are
     // queued without draining the stream (every call ends with a sync, so the
     // next call may refill it)
@@ -1676,6 +1676,8 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     int launches = 0;
     bool tuned_now = false;
     int block_used = 0;
+    bool aux_pending = false;
+    double aux_ms = 0.0;
     CK(cudaEventRecord(c->ev[0], c->stream));
     for (int i = 0; i < nvol; ++i) {
         const gx_volume& v = vols[i];
@@ -1800,8 +1802,11 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
                 diqr = r.iqr ? st + nst : nullptr;
                 dmode = r.mode ? st + 2 * nst : nullptr;
             }
+            CK(cudaEventRecord(c->ev[4], c->stream));
             CK(launch_posterior_stats(post, nvar, nv, o->repetition * ns * W, nbin, lbub, dmed, diqr, dmode,
                                       c->stream));
+            CK(cudaEventRecord(c->ev[5], c->stream));
+            aux_pending = true;
         }
         if (mem == GX_MEM_HOST) {
             const size_t nst = (size_t)nvar * nv;
@@ -1828,6 +1833,11 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
         kernel_ms += ms;
+        if (aux_pending) {
+            cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+            aux_ms += ms;
+            aux_pending = false;
+        }
         r.n_accepted = (int64_t)acc;
         r.n_proposals = (int64_t)nv * W * o->iteration * o->repetition;
         r.ns = ns;
@@ -1841,6 +1851,7 @@ extern "C" gx_status gx_mcmc(gx_context* c, const gx_model* model, int32_t mem, 
     c->timing.main_launches = launches;
     c->timing.block_size = block_used;
     c->timing.autotuned = tuned_now ? 1 : 0;
+    c->timing.aux_kernel_ms = aux_ms;
     c->timing.kernel_launches = g_kernel_launches - scope.launches0;
     c->timing.h2d_bytes = h2d;
     c->timing.d2h_bytes = d2h;

@@ -277,6 +277,8 @@ typedef struct {
     int32_t block_size;         /* threads per block of the main kernel's launches */
     int32_t autotuned;          /* 1: the autotuner ran its trials in this call (block_size 0,
                                  * first call of its key in the process) */
+    double aux_kernel_ms;       /* summed duration of the post-processing kernels (MCMC: the
+                                 * posterior median / iqr / mode) */
 } gx_timing;
 
 /* gx_timing.tv_path flags */
