@@ -211,9 +211,14 @@ __host__ __device__ constexpr int persist_max_threads(int maxm, bool stats) {
     return (maxm > 16 || persist_pairs(maxm, stats)) ? 768 : kPersistMaxThreads;
 }
 
-template <int LOSS, bool STATS, int MAXM>
+// HOOK: the bound of the waits and the grid barrier's arrival count come from
+// the launch arguments (the context's test hooks); otherwise they are the
+// compile-time default, which keeps the wait loops of the timed kernel lean.
+template <int LOSS, bool STATS, int MAXM, bool HOOK>
 __global__ void __launch_bounds__(persist_max_threads(MAXM, STATS), 1)
 tv_persistent_kernel(AdamParams a, PersistArgs p) {
+    const long long wait_limit = HOOK ? p.spin_cycles : kBarrierSpinCycles;
+    const unsigned int extra_arrivals = HOOK ? p.extra_arrivals : 0u;
     constexpr int NP = 2;  // R2*: M0, R2star
     constexpr int NS = STATS ? 4 : 3;  // z, m1, m2 [, z of the previous epoch]
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -311,7 +316,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const int vol = a.blk_vol[base / p.pad_block];
         for (int e = p.e_begin; e <= p.e_end; ++e) {
             const unsigned int ph = (unsigned int)(e - p.e_begin) & 1u;
-            if (!mbar_wait(&bar_arrive, ph, p.barrier, p.spin_cycles)) {
+            if (!mbar_wait(&bar_arrive, ph, p.barrier, wait_limit)) {
                 if (lane == 31) {
                     *(volatile int*)&s_err = 1;
                     mbar_arrive(&bar_open);
@@ -323,8 +328,8 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             int ok = 1;
             if (e < p.e_end && lane == 31) {
                 grid_arrive_one(p.barrier);
-                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x + p.extra_arrivals,
-                                   p.spin_cycles);
+                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x + extra_arrivals,
+                                   wait_limit);
                 if (!ok) *(volatile int*)&s_err = 1;
             }
             if (p.record && a.hist && lane < NQ) {
@@ -421,7 +426,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         }
         // every CTA's map of the previous epoch (written before its arrival)
         if (e > p.e_begin)
-            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, p.spin_cycles) ||
+            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, wait_limit) ||
                 *(volatile int*)&s_err)
                 return;
         const bool ckpt = upd && a.ckpt_every > 0 && (e % a.ckpt_every) == 0;
@@ -543,7 +548,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         }
         // every CTA's map of the previous epoch (written before its arrival)
         if (e > p.e_begin)
-            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, p.spin_cycles) ||
+            if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, wait_limit) ||
                 *(volatile int*)&s_err)
                 return;
         // pass 2: TV subgradient, chain rule, optimiser, new map values
@@ -700,7 +705,9 @@ int persist_variant(const AdamParams& a, int loss, bool res_after_loop) {
 template <int LOSS, int MAXM>
 cudaError_t launch_persist_t(const AdamParams& a, PersistArgs p, int bt, int nblocks, size_t smem,
                              cudaStream_t s) {
-    auto k = p.stats ? tv_persistent_kernel<LOSS, true, MAXM> : tv_persistent_kernel<LOSS, false, MAXM>;
+    const bool hook = p.spin_cycles != kBarrierSpinCycles || p.extra_arrivals != 0;
+    auto k = p.stats ? (hook ? tv_persistent_kernel<LOSS, true, MAXM, true> : tv_persistent_kernel<LOSS, true, MAXM, false>)
+                     : (hook ? tv_persistent_kernel<LOSS, false, MAXM, true> : tv_persistent_kernel<LOSS, false, MAXM, false>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {const_cast<void*>(static_cast<const void*>(&a)), static_cast<void*>(&p)};
@@ -712,8 +719,8 @@ cudaError_t launch_persist_t(const AdamParams& a, PersistArgs p, int bt, int nbl
 template <int LOSS, int MAXM>
 int occupancy_t(int bt, size_t smem) {
     int nb = 0, nb2 = 0;
-    auto k0 = tv_persistent_kernel<LOSS, false, MAXM>;
-    auto k1 = tv_persistent_kernel<LOSS, true, MAXM>;
+    auto k0 = tv_persistent_kernel<LOSS, false, MAXM, false>;
+    auto k1 = tv_persistent_kernel<LOSS, true, MAXM, false>;
     if (cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
         cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 0;
