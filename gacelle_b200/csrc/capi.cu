@@ -1025,8 +1025,9 @@ static gx_status upload_blk_table(AdamJob& J, int Bl, int** out) {
 // Autotuner of the fused kernel's launch block.  Key: device, model, loss,
 // measurements, statistics / prior / weights / b1 / sigma-map variants,
 // optimiser, transform and the voxel-count class (log2 of the work-list).
-// On a miss every candidate (64, 128, 256, 512 threads, within the kernel's
-// thread and shared-memory limits) runs a few epochs of this job's own
+// On a miss every candidate (64, 128, 256, 512 threads, and 32 for short
+// work-lists, within the kernel's thread and shared-memory limits) runs a
+// few epochs of this job's own
 // kernel on its own data from a scratch copy of the start state (the job's
 // state and history untouched); the fastest is cached for the process.
 static gx_status tune_fused(AdamJob& J) {
@@ -1072,7 +1073,9 @@ static gx_status tune_fused(AdamJob& J) {
             E = std::max(1, std::min(E, N));
         }
         float best = 0.f;
-        for (int cand : {64, 128, 256, 512}) {
+        for (int cand : {32, 64, 128, 256, 512}) {
+            // one-warp blocks only for work-lists that leave SMs idle with 64-thread blocks
+            if (cand == 32 && J.nvtot > 64 * 148) continue;
             if (J.B % cand || fused_block_limit(t, J.id, o->loss, stats) < cand) continue;
             int* blk;
             TRY(upload_blk_table(J, cand, &blk));

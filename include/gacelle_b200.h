@@ -178,8 +178,9 @@ typedef struct {
     /* threads per block; 0 = the default (128), or on the fused path without
      * TV the block chosen by the project's autotuner: the first call of a key
      * (model, loss, measurement count, variant, optimiser, transform, voxel-
-     * count class) times 64 / 128 / 256 / 512 threads on a few epochs of its own
-     * data and the fastest is kept for the process; GACELLE_B200_AUTOTUNE=0
+     * count class) times 64 / 128 / 256 / 512 threads (and 32 for work-lists
+     * of at most 64 x 148 voxels) on a few epochs of its own data and the
+     * fastest is kept for the process; GACELLE_B200_AUTOTUNE=0
      * turns tuning off */
     int32_t block_size;
     /* robustConvergence (update_outlier_mask, utils/askadam.m:448-510, and the

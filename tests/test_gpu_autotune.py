@@ -34,7 +34,7 @@ def test_fused_block_is_tuned_once_and_reused(ctx, monkeypatch):
     f = fitting(iteration=40, initialLearnRate=0.01, optimiser="rmsprop", lossFunction="huber")
     a = run_engine("nexi2", y, th0, f, NAMES["nexi2"], context=ctx)
     ta = a["timing"]
-    assert ta["autotuned"] == 1 and ta["block_size"] in (64, 128, 256, 512), ta
+    assert ta["autotuned"] == 1 and ta["block_size"] in (32, 64, 128, 256, 512), ta
     b = run_engine("nexi2", y, th0, f, NAMES["nexi2"], context=ctx)
     assert b["timing"]["autotuned"] == 0 and b["timing"]["block_size"] == ta["block_size"]
     c = run_engine("nexi2", y, th0, dict(f, blockSize=ta["block_size"]), NAMES["nexi2"], context=ctx)
