@@ -667,8 +667,12 @@ __device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const floa
         const float2 r2x4 = bcast2(4.0f * r2), r1x4 = bcast2(4.0f * r1);
         float2 S0p = z2, Sfp = z2, Sd1p = z2, Sd2p = z2, Sr1p = z2, Sr2p = z2;
         float2 T0p = z2, Tfp = z2, Td1p = z2, Td2p = z2, Tr1p = z2, Tr2p = z2;
-        for (int i = 0; i < nx; i += 2) {
-            const float2 x = make_float2((float)i * h, (float)(i + 1) * h);
+        // node indices (i, i+1) carried as exact floats (integers below 2^24),
+        // so the loop converts no integer to float: conversions share the
+        // SFU's issue rate with the rsqrt and the exponentials of the node
+        float2 fi = make_float2(0.0f, 1.0f);
+        for (int i = 0; i < nx; i += 2, fi = add2(fi, two)) {
+            const float2 x = mul2(fi, bcast2(h));
             const float2 x2 = mul2(x, x);
             const float2 d1 = mul2(bDa2, x2);
             const float2 s = add2(base2, d1);
