@@ -5,8 +5,11 @@
 // launch: the slice's Adam state lives in shared memory (and its measurements
 // too when they fit; otherwise they are read from L2, all of a voxel's echoes
 // in flight together), and only the regularised parameter map travels between
-// CTAs (the double-buffered full-grid TV map, read through L2 with
-// ld.global.cg since other CTAs wrote it in the same launch).
+// CTAs (the double-buffered full-grid TV map with a one-cell halo that holds
+// the periodic neighbours, read through L2 with ld.global.cg since other CTAs
+// wrote it in the same launch).  Each launch writes its start map from the
+// staged state and passes one grid barrier before the first epoch, so it
+// depends on no map left by another kernel.
 //
 // An epoch runs in two passes over the slice.  The fidelity pass (forward
 // model, loss, adjoint) needs only the CTA's own voxels; the TV/update pass
@@ -22,8 +25,9 @@
 // error flag that the host reports as GX_ETIMEOUT, and every CTA returns.
 //
 // The per-voxel arithmetic (forward model, loss, adjoint, TV subgradient,
-// sigmoid chain rule, optimiser) is the same code as tv_step_kernel, so the
-// two paths produce the same parameters.  Reference: utils/askadam.m:23-117,
+// sigmoid chain rule, optimiser) rounds as tv_step_kernel does, so the two
+// paths produce the same parameters (the two-voxel variant's TV signs come
+// from saturated products, tv_terms2m, equal to tv_terms' bit for bit).  Reference: utils/askadam.m:23-117,
 // 673-691; utils/spatial_total_variation.m:24-66.
 #include <algorithm>
 
@@ -32,6 +36,8 @@
 namespace gx {
 
 namespace {
+
+template <int V> struct IntC { static constexpr int value = V; };
 
 __device__ __forceinline__ float warp_sum_p(float v) {
 #pragma unroll
@@ -166,32 +172,38 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned int 
     return true;
 }
 
-// The six face neighbours' values in a TV map G (grid index pidx, staging
-// flags fl: bits 0-2 on the last x/y/z plane, 3-5 on the first, where the
-// neighbour wraps around periodically).  Interior voxels, almost all of a
-// masked volume, take the plain offsets.
-struct Neighbours {
-    int sy, sz, wx, wy, wz;
+// The persistent kernel's TV map of one volume, with a one-cell halo on
+// every face: grid point (x, y, z) sits at P = (x+1) + (y+1) sy + (z+1) sz,
+// and the halo cell beyond a face holds the value of the periodic neighbour
+// (the voxel on the opposite face), so the six face neighbours of every grid
+// point are at P +- 1, P +- sy, P +- sz (utils/spatial_total_variation.m:
+// 55-66 wraps around with circshift).  A voxel on a face writes its new value
+// also into the halo cell that mirrors it: on the last x plane at P - mx, on
+// the first at P + mx (likewise y, z).  Layout L > 0: the strides are 2^L
+// and 2^2L (dx + 2, dy + 2 <= 2^L), so the neighbour offsets are immediate
+// operands of the loads (L = 7, 8, 9); L = 0: sy = dx + 2, sz = (dx + 2)(dy + 2).
+struct HaloMap {
+    int sy, sz;      // strides
+    int mx, my, mz;  // mirror offsets dx, dy sy, dz sz
     bool tv3;
-    __device__ __forceinline__ void load(const float* G, int pidx, unsigned int fl, float (&f)[3],
-                                         float (&b)[3]) const {
-        if (!(fl & (tv3 ? 63u : 27u))) {
-            const float* g = G + pidx;
-            f[0] = __ldcg(g + 1); b[0] = __ldcg(g - 1);
-            f[1] = __ldcg(g + sy); b[1] = __ldcg(g - sy);
-            if (tv3) { f[2] = __ldcg(g + sz); b[2] = __ldcg(g - sz); }
-            else { f[2] = 0.0f; b[2] = 0.0f; }
-            return;
-        }
-        const int fw0 = (fl & 1) ? pidx - wx : pidx + 1, bw0 = (fl & 8) ? pidx + wx : pidx - 1;
-        const int fw1 = (fl & 2) ? pidx - wy : pidx + sy, bw1 = (fl & 16) ? pidx + wy : pidx - sy;
-        f[0] = __ldcg(G + fw0); b[0] = __ldcg(G + bw0);
-        f[1] = __ldcg(G + fw1); b[1] = __ldcg(G + bw1);
+    template <int L>
+    __device__ __forceinline__ void load(const float* G, int P, float (&f)[3], float (&b)[3]) const {
+        const int ty = L > 0 ? 1 << L : sy, tz = L > 0 ? 1 << (2 * L) : sz;
+        const float* g = G + P;
+        f[0] = __ldcg(g + 1); b[0] = __ldcg(g - 1);
+        f[1] = __ldcg(g + ty); b[1] = __ldcg(g - ty);
+        if (tv3) { f[2] = __ldcg(g + tz); b[2] = __ldcg(g - tz); }
+        else { f[2] = 0.0f; b[2] = 0.0f; }
+    }
+    // fl: the voxel's face flags (bits 0-2 last x/y/z plane, 3-5 first)
+    __device__ __forceinline__ void mirror(float* G, int P, unsigned int fl, float v) const {
+        if (fl & 1) G[P - mx] = v;
+        if (fl & 8) G[P + mx] = v;
+        if (fl & 2) G[P - my] = v;
+        if (fl & 16) G[P + my] = v;
         if (tv3) {
-            const int fw2 = (fl & 4) ? pidx - wz : pidx + sz, bw2 = (fl & 32) ? pidx + wz : pidx - sz;
-            f[2] = __ldcg(G + fw2); b[2] = __ldcg(G + bw2);
-        } else {
-            f[2] = 0.0f; b[2] = 0.0f;
+            if (fl & 4) G[P - mz] = v;
+            if (fl & 32) G[P + mz] = v;
         }
     }
 };
@@ -236,8 +248,8 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     constexpr int NAUX = CACHE ? 4 : NP;
     float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NAUX][slice] fidelity pass results
     int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NAUX * p.slice);        // [slice] grid index
-    unsigned short* s_fl = reinterpret_cast<unsigned short*>(s_p + p.slice); // [slice] boundary/mask flags
-    float* s_y = reinterpret_cast<float*>(s_fl + ((p.slice + 1) & ~1));       // [nm][slice] if staged
+    unsigned int* s_w = reinterpret_cast<unsigned int*>(s_p + p.slice);      // [slice] mask words (mask_scale)
+    float* s_y = reinterpret_cast<float*>(s_w + p.slice);                     // [nm][slice] if staged
     const int BT = blockDim.x, tid = threadIdx.x;
     const int base = blockIdx.x * p.slice;
     const int n = min(base + p.slice, a.nvtot) - base;  // voxels of this slice
@@ -251,32 +263,52 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         int off, nvox;
         float norm;
         double normd;
-        long long grid_off;
-    } V{Vg.off, Vg.nvox, Vg.norm, Vg.normd, Vg.grid_off};
+        long long grid_off, hgrid_off;
+    } V{Vg.off, Vg.nvox, Vg.norm, Vg.normd, Vg.grid_off, Vg.hgrid_off};
     const float tvs0 = Vg.tv_scale[0], tvs1 = Vg.tv_scale[1];
     const int dx = Vg.dims[0], dy = Vg.dims[1], dz = Vg.dims[2];
     const int sy = dx, sz = dx * dy;
     const int wx = dx - 1, wy = (dy - 1) * dx, wz = (dz - 1) * dx * dy;  // wrap offsets
-    const Neighbours nb{sy, sz, wx, wy, wz, a.tv_3d != 0};
+    const int hy = p.hlayout > 0 ? 1 << p.hlayout : dx + 2;
+    const int hz = p.hlayout > 0 ? 1 << (2 * p.hlayout) : (dx + 2) * (dy + 2);
+    const HaloMap hm{hy, hz, dx, dy * hy, dz * hz, a.tv_3d != 0};
     const unsigned char* mk = a.maskgrid + V.grid_off;
-    // stage the slice's state, TV neighbourhood (and measurements, if they fit) once
+    // the map of the launch's first epoch: written below from the staged state
+    float* const gstart = ((p.e_begin >= 1 && ((p.e_begin - 1) & 1)) ? p.grid1 : p.grid0) + V.hgrid_off;
+    // stage the slice's state, TV neighbourhood (and measurements, if they fit)
+    // once, and write the slice's values of the start map; a padding voxel
+    // takes the map position of the volume's first voxel (so that its
+    // neighbour loads stay inside the map), no mask and no map write
     for (int i = tid; i < n; i += BT) {
         const int v = base + i;
         int pp = 0;
-        unsigned short fl = 0;
-        if ((v - V.off) < V.nvox && a.n_reg > 0) {
-            pp = a.gidx[v];
-            const int x = pp % dx, yz = pp / dx, y = yz % dy, zc = yz / dy;
-            fl = (unsigned short)((x == dx - 1) | ((y == dy - 1) << 1) | ((zc == dz - 1) << 2) |
-                                  ((x == 0) << 3) | ((y == 0) << 4) | ((zc == 0) << 5));
-            const int bw0 = x > 0 ? pp - 1 : pp + wx;
-            const int bw1 = y > 0 ? pp - sy : pp + wy;
-            const int bw2 = zc > 0 ? pp - sz : pp + wz;
-            fl |= (unsigned short)((mk[bw0] ? 64 : 0) | (mk[bw1] ? 128 : 0) | (mk[bw2] ? 256 : 0));
+        unsigned int w = 0;
+        const bool real = (v - V.off) < V.nvox;
+        if (a.n_reg > 0) {
+            const int gp = a.gidx[real ? v : V.off];
+            const int x = gp % dx, yz = gp / dx, y = yz % dy, zc = yz / dy;
+            const unsigned int wrap = (x == dx - 1) | ((y == dy - 1) << 1) | ((zc == dz - 1) << 2) |
+                                      ((x == 0) << 3) | ((y == 0) << 4) | ((zc == 0) << 5);
+            const int bw0 = x > 0 ? gp - 1 : gp + wx;
+            const int bw1 = y > 0 ? gp - sy : gp + wy;
+            const int bw2 = zc > 0 ? gp - sz : gp + wz;
+            w = wrap << 24;
+            if (real)
+                w |= (mk[bw0] ? kMaskByte : 0u) | (mk[bw1] ? kMaskByte << 8 : 0u) | (mk[bw2] ? kMaskByte << 16 : 0u);
+            pp = (x + 1) + (y + 1) * hy + (zc + 1) * hz;
+            if (real)
+                for (int r = 0; r < min(a.n_reg, 2); ++r) {
+                    const int k = a.reg_param[r];
+                    float dd;
+                    const float th = unscale(a.transform, a.P.lb[k], a.P.ub[k], a.z[(size_t)k * a.nvtot + v], dd);
+                    float* G = gstart + (size_t)r * p.hgrid_total;
+                    G[pp] = th;
+                    hm.mirror(G, pp, wrap, th);
+                }
         }
         const int j = sidx(i);
         s_p[j] = pp;
-        s_fl[j] = fl;
+        s_w[j] = w;
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             size_t gi = (size_t)k * a.nvtot + base + i;
@@ -301,6 +333,14 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         s_err = 0;
     }
     __syncthreads();
+    // every CTA's part of the start map before the first TV pass (the grid
+    // barrier's first round; the epoch boundaries follow from the second)
+    if (tid == BT - 1) {
+        grid_arrive_one(p.barrier);
+        if (!grid_wait_one(p.barrier, gridDim.x + extra_arrivals, wait_limit)) s_err = 1;
+    }
+    __syncthreads();
+    if (s_err) return;
     constexpr bool STD = MAXM > 0;
     const bool tv3 = a.tv_3d != 0;
     const int nm = a.nm;
@@ -328,7 +368,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             int ok = 1;
             if (e < p.e_end && lane == 31) {
                 grid_arrive_one(p.barrier);
-                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 1) * gridDim.x + extra_arrivals,
+                ok = grid_wait_one(p.barrier, (unsigned int)(e - p.e_begin + 2) * gridDim.x + extra_arrivals,
                                    wait_limit);
                 if (!ok) *(volatile int*)&s_err = 1;
             }
@@ -358,9 +398,11 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         // + q % 32 and i1 = i0 + 32 of the slice (a warp covers 64
         // consecutive voxels, and each of its per-voxel accesses 32
         // consecutive ones); the parameter, gradient and optimiser arithmetic
-        // in pair instructions, lane .x on voxel i0 and .y on voxel i1
-        const int kr = a.reg_param[0];  // the regularised parameter
-        const float lbr = a.P.lb[kr], ubr = a.P.ub[kr];
+        // in pair instructions, lane .x on voxel i0 and .y on voxel i1; the
+        // regularised parameter kr is a compile-time constant of the epoch's
+        // code (false: a wait has failed, the kernel returns)
+        auto pair_epoch = [&](auto KR, auto HLC) -> bool {
+        constexpr int kr = decltype(KR)::value, HL = decltype(HLC)::value;
         const size_t half = (size_t)(a.nvtot >> 1);
         const int npair = n >> 1;  // n is a multiple of 64 in pair mode
         // shared memory: pair q at float2 position q; global: voxels v0, v0+32
@@ -393,28 +435,33 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             }
             float2 th[NP], dth[NP];
 #pragma unroll
-            for (int k = 0; k < NP; ++k) th[k] = unscale_sig2(a.P.lb[k], a.P.ub[k], ld2(s_st + k * S, q), dth[k]);
+            for (int k = 0; k < NP; ++k) th[k] = unscale_sig2c(p.k, k, ld2(s_st + k * S, q), dth[k]);
             // R2sMseSums on both lanes with the residual negated, y - M0 E:
             // every partial sum is the exact negative of the scalar one
             float2 sse = make_float2(0.f, 0.f), g0n = sse, g1n = sse;
             const float2 nM0 = make_float2(-th[0].x, -th[0].y), R2 = th[1];
+            auto echo = [&](int m) {
+                const float2 x = mul2(a.P.nl2e_pair[m], R2);
+                const float2 E = make_float2(ex2_ftz(x.x), ex2_ftz(x.y));
+                const float2 rn = fma2(nM0, E, y[m]);
+                sse = fma2(rn, rn, sse);
+                const float2 qn = mul2(rn, E);
+                g0n = add2(g0n, qn);
+                g1n = fma2(a.P.te_pair[m], qn, g1n);
+            };
+            if (nm == MAXM) {  // the full protocol: no per-echo test
 #pragma unroll
-            for (int m = 0; m < MAXM; ++m)
-                if (m < nm) {
-                    const float2 x = mul2(a.P.nl2e_pair[m], R2);
-                    const float2 E = make_float2(ex2_ftz(x.x), ex2_ftz(x.y));
-                    const float2 rn = fma2(nM0, E, y[m]);
-                    sse = fma2(rn, rn, sse);
-                    const float2 qn = mul2(rn, E);
-                    g0n = add2(g0n, qn);
-                    g1n = fma2(a.P.te_pair[m], qn, g1n);
-                }
+                for (int m = 0; m < MAXM; ++m) echo(m);
+            } else {
+#pragma unroll
+                for (int m = 0; m < MAXM; ++m)
+                    if (m < nm) echo(m);
+            }
             const float2 zero = make_float2(0.f, 0.f);
-            const float s2 = mul1(2.0f, a.mse_scale);
-            const float2 tot = mul2(add2(zero, sse), bcast2(a.mse_scale));
+            const float2 tot = mul2(add2(zero, sse), p.k.mse);
             float2 g[NP];
-            g[0] = mul2(sub2(zero, g0n), bcast2(s2));
-            g[1] = mul2(fma2(th[0], g1n, zero), bcast2(s2));
+            g[0] = mul2(sub2(zero, g0n), p.k.s2);
+            g[1] = mul2(fma2(th[0], g1n, zero), p.k.s2);
             const float2 nrm = bcast2(V.norm);
             const float2 gr = mul2(kr == 0 ? g[0] : g[1], nrm), gn = mul2(kr == 0 ? g[1] : g[0], nrm);
             st2(s_gf + 0 * S, q, mul2(gn, kr == 0 ? dth[1] : dth[0]));
@@ -428,12 +475,12 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         if (e > p.e_begin)
             if (!mbar_wait(&bar_open, (unsigned int)(e - 1 - p.e_begin) & 1u, p.barrier, wait_limit) ||
                 *(volatile int*)&s_err)
-                return;
+                return false;
         const bool ckpt = upd && a.ckpt_every > 0 && (e % a.ckpt_every) == 0;
         float* cp = ckpt ? a.ckpt + (size_t)(e / a.ckpt_every) * 3 * NP * a.nvtot : nullptr;
-        const float* G = gcur + V.grid_off;
-        float* Gn = gnext + V.grid_off;
-        const float iv[3] = {ivx, ivy, ivz};
+        const float* G = gcur + V.hgrid_off;
+        float* Gn = gnext + V.hgrid_off;
+        const float2 scx = bcast2(sc.x), scy = bcast2(sc.y);
         // pass 2: TV subgradient, chain rule, optimiser, new map values
         for (int q = tid; q < npair; q += NWT) {
             const int i0 = ((q >> 5) << 6) + (q & 31), v0 = base + i0;
@@ -444,15 +491,14 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const float2 c = ld2(s_gf + 3 * S, q);
             const int2 pp = reinterpret_cast<const int2*>(s_p)[q];
             const int p0 = pp.x, p1 = pp.y;
-            const unsigned int fl01 = reinterpret_cast<const unsigned int*>(s_fl)[q];
-            const unsigned int fl0 = fl01 & 0xffffu, fl1 = fl01 >> 16;
-            float f0[3] = {0.f, 0.f, 0.f}, b0[3] = {0.f, 0.f, 0.f}, f1[3] = {0.f, 0.f, 0.f}, b1[3] = {0.f, 0.f, 0.f};
-            if (ok0) nb.load(G, p0, fl0, f0, b0);
-            if (ok1) nb.load(G, p1, fl1, f1, b1);
-            const bool mb0[3] = {(fl0 & 64) != 0, (fl0 & 128) != 0, (fl0 & 256) != 0};
-            const bool mb1[3] = {(fl1 & 64) != 0, (fl1 & 128) != 0, (fl1 & 256) != 0};
+            const uint2 w01 = reinterpret_cast<const uint2*>(s_w)[q];
+            // every voxel loads (a padding voxel at a valid position), only
+            // real voxels add their terms
+            float f0[3], b0[3], f1[3], b1[3];
+            hm.load<HL>(G, p0, f0, b0);
+            hm.load<HL>(G, p1, f1, b1);
             float2 cost, gt;
-            tv_terms2(c, f0, b0, f1, b1, mb0, mb1, iv, tv3 ? 3 : 2, cost, gt);
+            tv_terms2m(c, f0, b0, f1, b1, w01.x, w01.y, p.k.iv, tv3 ? 3 : 2, cost, gt);
             if (ok0) {
                 q1 = __fmaf_rn(tvs0, cost.x, q1);
                 grf.x = fma1(tvs0, gt.x, grf.x);
@@ -471,7 +517,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     float* p1s = s_st + (1 * NP + k) * S;
                     float* p2s = s_st + (2 * NP + k) * S;
                     float2 zz = ld2(pz, q), mm1 = ld2(p1s, q), mm2 = ld2(p2s, q);
-                    adam_step2(oc, sc, zz, mm1, mm2, gz[k]);
+                    adam_step2c(p.k, scx, scy, zz, mm1, mm2, gz[k]);
                     st2(pz, q, zz);
                     st2(p1s, q, mm1);
                     st2(p2s, q, mm2);
@@ -483,11 +529,24 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     }
                 }
                 float2 dd;
-                const float2 thr = unscale_sig2(lbr, ubr, zr, dd);
+                const float2 thr = unscale_sig2c(p.k, kr, zr, dd);
                 if (ok0) Gn[p0] = thr.x;
                 if (ok1) Gn[p1] = thr.y;
+                const unsigned int fw0 = ok0 ? w01.x >> 24 : 0u, fw1 = ok1 ? w01.y >> 24 : 0u;
+                if (fw0 | fw1) {  // voxels on a face of the volume: the halo copies
+                    hm.mirror(Gn, p0, fw0, thr.x);
+                    hm.mirror(Gn, p1, fw1, thr.y);
+                }
             }
         }
+        return true;
+        };
+        bool go;
+        if (p.hlayout == 7) go = a.reg_param[0] == 0 ? pair_epoch(IntC<0>{}, IntC<7>{}) : pair_epoch(IntC<1>{}, IntC<7>{});
+        else if (p.hlayout == 8) go = a.reg_param[0] == 0 ? pair_epoch(IntC<0>{}, IntC<8>{}) : pair_epoch(IntC<1>{}, IntC<8>{});
+        else if (p.hlayout == 9) go = a.reg_param[0] == 0 ? pair_epoch(IntC<0>{}, IntC<9>{}) : pair_epoch(IntC<1>{}, IntC<9>{});
+        else go = a.reg_param[0] == 0 ? pair_epoch(IntC<0>{}, IntC<0>{}) : pair_epoch(IntC<1>{}, IntC<0>{});
+        if (!go) return;
         } else {
         // pass 1: data fidelity of the slice (own voxels only)
         for (int i = tid; i < n; i += NWT) {
@@ -566,14 +625,15 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 gth[k] = s_gf[k * S + i];
             }
             if (ok && nreg > 0) {
-                const unsigned int fl = s_fl[i];
-                const bool mb[3] = {(fl & 64) != 0, (fl & 128) != 0, (fl & 256) != 0};
+                const unsigned int w = s_w[i];
+                const unsigned int fl = w >> 24;
+                const bool mb[3] = {(w & 1u) != 0, (w & 0x100u) != 0, (w & 0x10000u) != 0};
                 const float iv[3] = {ivx, ivy, ivz};
                 for (int r = 0; r < nreg; ++r) {
                     const int k = a.reg_param[r];
                     const float c = k == 0 ? th[0] : th[1];
                     float f[3], b[3];
-                    nb.load(gcur + (size_t)r * a.grid_total + V.grid_off, pidx, fl, f, b);
+                    hm.load<0>(gcur + (size_t)r * p.hgrid_total + V.hgrid_off, pidx, f, b);
                     float cost, gr;
                     tv_terms(c, f, b, mb, iv, tv3 ? 3 : 2, cost, gr);
                     const float tvs = r == 0 ? tvs0 : tvs1;
@@ -617,8 +677,11 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 for (int r = 0; r < nreg; ++r) {
                     const int k = a.reg_param[r];
                     float dd;
-                    gnext[(size_t)r * a.grid_total + V.grid_off + pidx] =
-                        unscale(transform, a.P.lb[k], a.P.ub[k], k == 0 ? z[0] : z[1], dd);
+                    const float th = unscale(transform, a.P.lb[k], a.P.ub[k], k == 0 ? z[0] : z[1], dd);
+                    float* Gn = gnext + (size_t)r * p.hgrid_total + V.hgrid_off;
+                    Gn[pidx] = th;
+                    const unsigned int fl = s_w[i] >> 24;
+                    if (fl) hm.mirror(Gn, pidx, fl, th);
                 }
             }
         }
@@ -769,7 +832,7 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
     const int NS = stats_any ? 4 : 3;
     size_t red = sizeof(double) * 2 * 32 * kHistW;
     size_t state = sizeof(float) * (size_t)(NS + 1) * 2 * slice + sizeof(int) * slice +
-                   sizeof(unsigned short) * ((slice + 1) & ~1);  // + fidelity gradient [2][slice]
+                   sizeof(unsigned int) * slice;  // + fidelity gradient [2][slice], mask words
     size_t data = sizeof(float) * (size_t)a.nm * slice;
     const size_t budget = (size_t)smem_optin - 2048;  // static shared memory (staged protocol) and slack
     if (red + state > budget) return false;
@@ -802,6 +865,22 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
 
 cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s) {
     p.slice = plan.slice;
+    // the pair variant's constants, rounded as the kernels round them (FP32)
+    auto pr = [](float x) { return make_float2(x, x); };
+    p.k.nl2e = pr(-kLog2e);
+    p.k.one = pr(1.0f);
+    for (int i = 0; i < 2; ++i) {
+        p.k.rng[i] = pr(a.P.ub[i] - a.P.lb[i]);
+        p.k.lb[i] = pr(a.P.lb[i]);
+    }
+    p.k.b1 = pr(a.beta1);
+    p.k.omb1 = pr(1.0f - a.beta1);
+    p.k.b2 = pr(a.beta2);
+    p.k.omb2 = pr(1.0f - a.beta2);
+    p.k.eps = pr(a.eps);
+    p.k.mse = pr(a.mse_scale);
+    p.k.s2 = pr(2.0f * a.mse_scale);
+    for (int d = 0; d < 3; ++d) p.k.iv[d] = pr(a.inv_vs[d]);
     p.data_in_smem = plan.data_in_smem;
     // the register-prefetch variants write residuals after their epoch loop,
     // which needs a launch whose last epoch is not followed by an update

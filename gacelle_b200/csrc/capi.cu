@@ -91,7 +91,7 @@ enum Slot {
     S_MC_PART, S_MC_SUM, S_MC_SUMSQ, S_MC_SHIFT, S_MC_X0, S_MC_POST, S_MC_ACC, S_MC_MEAN,
     S_MC_STD, S_FWD_TH, S_FWD_SIG, S_FWD_B1, S_BAR, S_MC_GLOB, S_ROBUST, S_DICT_SIG, S_DICT_D,
     S_DICT_W, S_DICT_E, S_DICT_C, S_DICT_B, S_DICT_S, S_FLAGS, S_DATA_QUADS, S_PRIOR_MU, S_PRIOR_SD, S_SURF_NB, S_SURF_LEN,
-    S_MC_STATS, S_TUNE, S_TUNE_HIST, S_BLK_L, S_NSLOTS
+    S_MC_STATS, S_TUNE, S_TUNE_HIST, S_BLK_L, S_HGRID0, S_HGRID1, S_NSLOTS
 };
 
 struct gx_context {
@@ -557,6 +557,9 @@ struct AdamJob {
     std::vector<int> hblk;
     int nvtot = 0, nblocks = 0;
     long long grid_total = 0;
+    long long hgrid_total = 0;            // haloed maps of the persistent kernel (per map)
+    int hlayout = 0;                      // their strides (PersistArgs::hlayout)
+    float* hgrid[2] = {nullptr, nullptr};
     AdamParams a;
     int ckpt_every = 0, nslots = 0;
     std::vector<double> hist;   // [nvol][N+1][kHistW]
@@ -637,7 +640,19 @@ static gx_status adam_setup(AdamJob& J) {
     // work-list layout
     J.hv.resize(J.nvol);
     int off = 0;
-    long long goff = 0;
+    long long goff = 0, hgoff = 0;
+    // haloed map layout: power-of-two strides when every volume's x and y
+    // extents (with the halo) fit, so that the neighbour offsets are constants
+    if (J.tv) {
+        int dmax = 0, zmax = 0;
+        for (int i = 0; i < J.nvol; ++i) {
+            dmax = std::max(dmax, std::max(J.vols[i].dims[0], J.vols[i].dims[1]) + 2);
+            zmax = std::max(zmax, J.vols[i].dims[2] + 2);
+        }
+        J.hlayout = dmax <= 128 && zmax <= (1 << 16) ? 7
+                    : dmax <= 256 && zmax <= (1 << 14) ? 8
+                    : dmax <= 512 && zmax <= (1 << 12) ? 9 : 0;
+    }
     for (int i = 0; i < J.nvol; ++i) {
         const gx_volume& v = J.vols[i];
         DevVol& d = J.hv[i];
@@ -649,15 +664,21 @@ static gx_status adam_setup(AdamJob& J) {
         d.norm = (float)d.normd;
         for (int q = 0; q < 3; ++q) d.dims[q] = J.tv ? v.dims[q] : (q == 0 ? v.nvox : 1);
         d.grid_off = goff;
+        d.hgrid_off = hgoff;
         for (int r = 0; r < o->n_reg && r < kMaxReg; ++r) d.tv_scale[r] = (float)(o->lambda[r] / (double)v.nvox);
         d.prior_off = J.prior ? (float)v.prior_offset : 0.0f;
-        if (J.tv) goff += (long long)v.dims[0] * v.dims[1] * v.dims[2];
+        if (J.tv) {
+            goff += (long long)v.dims[0] * v.dims[1] * v.dims[2];
+            hgoff += J.hlayout > 0 ? (long long)(v.dims[2] + 2) << (2 * J.hlayout)
+                                   : (long long)(v.dims[0] + 2) * (v.dims[1] + 2) * (v.dims[2] + 2);
+        }
         for (int b = 0; b < d.npad / J.B; ++b) J.hblk.push_back(i);
         off += d.npad;
     }
     J.nvtot = off;
     J.nblocks = off / J.B;
     J.grid_total = goff;
+    J.hgrid_total = hgoff;
 
     AdamParams& a = J.a;
     memset(&a, 0, sizeof(a));
@@ -936,8 +957,10 @@ static gx_status run_epochs(AdamJob& J, AdamParams a, int nblocks, int e0, int e
         p.want_res = res_out != nullptr;
         p.stats = (J.stats && record) ? 1 : 0;
         p.loss = J.o->loss;
-        p.grid0 = J.grid[0];
-        p.grid1 = J.grid[1];
+        p.grid0 = J.hgrid[0];
+        p.grid1 = J.hgrid[1];
+        p.hgrid_total = J.hgrid_total;
+        p.hlayout = J.hlayout;
         p.barrier = J.barrier;
         p.pad_block = J.B;
         p.data_quads = J.data_quads;
@@ -1114,10 +1137,22 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
         const char* env = getenv("GACELLE_B200_TV_KERNEL");
         bool want = !(env && strcmp(env, "step") == 0);
         std::vector<int> npad(J.nvol);
-        for (int i = 0; i < J.nvol; ++i) npad[i] = J.hv[i].npad;
+        for (int i = 0; i < J.nvol; ++i) {
+            npad[i] = J.hv[i].npad;
+            const gx_volume& v = J.vols[i];
+            // map positions are 32-bit in the persistent kernel
+            if ((long long)(v.dims[0] + 2) * (v.dims[1] + 2) * (v.dims[2] + 2) >= (1LL << 31)) want = false;
+        }
         J.use_persist = want && !J.surf &&
                         plan_persistent(J.a, J.id, o->loss, J.stats, J.B, npad.data(), J.nvol, &J.plan);
-        if (J.use_persist) TRY(wsT(c, S_BAR, 1, &J.barrier));
+        if (J.use_persist) {
+            TRY(wsT(c, S_BAR, 1, &J.barrier));
+            const size_t hn = (size_t)J.a.n_reg * J.hgrid_total;
+            TRY(wsT(c, S_HGRID0, hn, &J.hgrid[0]));
+            TRY(wsT(c, S_HGRID1, hn, &J.hgrid[1]));
+            CK(cudaMemsetAsync(J.hgrid[0], 0, sizeof(float) * hn, c->stream));
+            CK(cudaMemsetAsync(J.hgrid[1], 0, sizeof(float) * hn, c->stream));
+        }
         if (J.use_persist && J.plan.quad_width > 0) {
             TRY(wsT(c, S_DATA_QUADS, (size_t)J.nvtot * (J.plan.quad_width / 4), &J.data_quads));
             CK(launch_echo_quads(J.a.data, J.nm, J.nvtot, J.plan.quad_width, J.plan.quad_pairs != 0, J.data_quads,

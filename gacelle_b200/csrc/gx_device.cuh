@@ -910,6 +910,56 @@ __device__ __forceinline__ void tv_terms2(float2 c, const float (&f0)[3], const 
     grad = gr;
 }
 
+// Saturated product (PTX mul.sat: the result clamped to [0, 1], NaN to 0).
+__device__ __forceinline__ float mul_sat1(float a, float b) {
+    float d;
+    asm("mul.rn.ftz.sat.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+
+// Backward-neighbour mask word of a voxel: byte d (d = 0, 1, 2 for x, y, z)
+// is kMaskByte when the backward neighbour along d lies inside the mask, else
+// 0; byte 3 holds the periodic-wrap flags (bit 0-2 last x/y/z plane, 3-5
+// first).  Broadcasting byte d to all four bytes gives the float kSignScale
+// (bits 0x7F7F7F7F, about 3.4e38) or 0.
+constexpr unsigned int kMaskByte = 0x7Fu;
+__device__ __forceinline__ float mask_scale(unsigned int w, int d) {
+    return __int_as_float((int)__byte_perm(w, 0u, (unsigned int)d * 0x1111u));
+}
+
+// tv_terms2 with the signs as saturated products and the mask as a scale
+// (w0 / w1: the two voxels' mask words).  With subnormals flushed every
+// nonzero x has |x| >= 2^-126, so sat(x K) - sat(-x K) = sgn0(x) exactly for
+// K >= 2^127 (and 0 for x = 0 or NaN), and sat(x 0) = 0 drops a backward
+// term outside the mask; -|df| = df (-sgn0(df)) exactly.  Every lane result
+// equals tv_terms' bit for bit: the costs add the same rounded |df iv|, and
+// the gradient terms are small integers times iv (exact products), so the
+// fused multiply-add rounds as the separate multiply and add.
+// ivp: the inverse voxel sizes as (iv, iv) pairs.
+__device__ __forceinline__ void tv_terms2m(float2 c, const float (&f0)[3], const float (&b0)[3],
+                                           const float (&f1)[3], const float (&b1)[3], unsigned int w0,
+                                           unsigned int w1, const float2* ivp, int nd, float2& cost, float2& grad) {
+    const float K = __int_as_float(0x7F7F7F7F);
+    float2 cs = make_float2(0.0f, 0.0f), gr = cs;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (d < nd) {
+            const float2 ivd = ivp[d];
+            const float2 df = sub2(make_float2(f0[d], f1[d]), c);
+            const float2 snf = sub2(make_float2(mul_sat1(-df.x, K), mul_sat1(-df.y, K)),
+                                    make_float2(mul_sat1(df.x, K), mul_sat1(df.y, K)));  // -sgn0(df)
+            cs = sub2(cs, mul2(mul2(df, snf), ivd));                                   // + |df iv|
+            const float2 cb = sub2(c, make_float2(b0[d], b1[d]));
+            const float k0 = mask_scale(w0, d), k1 = mask_scale(w1, d);
+            const float2 sb = sub2(make_float2(mul_sat1(cb.x, k0), mul_sat1(cb.y, k1)),
+                                   make_float2(mul_sat1(-cb.x, k0), mul_sat1(-cb.y, k1)));  // mb sgn0(cb)
+            gr = fma2(add2(snf, sb), ivd, gr);
+        }
+    }
+    cost = cs;
+    grad = gr;
+}
+
 // Optimiser step of one parameter (adamupdate / sgdmupdate / rmspropupdate,
 // called from utils/askadam.m:673-691).  sc = per-epoch schedule:
 // Adam (lr_e/(1-b1^e), 1/(1-b2^e)); others (lr_e, 0).  The square root is
@@ -952,6 +1002,39 @@ __device__ __forceinline__ float2 unscale_sig2(float lb, float ub, float2 z, flo
     const float2 d = bcast2(sub1(ub, lb));
     dth = mul2(mul2(d, s), sub2(bcast2(1.0f), s));
     return fma2(d, s, bcast2(lb));
+}
+
+// The constants of the pair transform and optimiser as (x, x) pairs, so that
+// the pair instructions take them as kernel-parameter operands.
+struct PairConsts {
+    float2 nl2e;      // -log2(e)
+    float2 one;
+    float2 rng[2];    // ub - lb of the two parameters
+    float2 lb[2];
+    float2 b1, omb1, b2, omb2, eps;  // Adam: beta1, 1 - beta1, beta2, 1 - beta2, epsilon
+    float2 mse, s2;   // mse_scale, 2 mse_scale
+    float2 iv[3];     // inverse voxel sizes
+};
+
+// unscale_sig2 with its constants from PairConsts (same operations).
+__device__ __forceinline__ float2 unscale_sig2c(const PairConsts& k, int i, float2 z, float2& dth) {
+    const float2 e = mul2(z, k.nl2e);
+    const float2 den = add2(k.one, make_float2(ex2_ftz(e.x), ex2_ftz(e.y)));
+    const float2 s = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
+    dth = mul2(mul2(k.rng[i], s), sub2(k.one, s));
+    return fma2(k.rng[i], s, k.lb[i]);
+}
+
+// adam_step2 with its constants from PairConsts and the epoch's schedule as
+// pairs scx = (sc.x, sc.x), scy = (sc.y, sc.y) (same operations).
+__device__ __forceinline__ void adam_step2c(const PairConsts& k, float2 scx, float2 scy, float2& z, float2& m1,
+                                            float2& m2, float2 g) {
+    m1 = fma2(k.b1, m1, mul2(k.omb1, g));
+    m2 = fma2(k.b2, m2, mul2(mul2(k.omb2, g), g));
+    const float2 v = mul2(m2, scy);
+    const float2 den = add2(make_float2(fast_sqrt0(v.x), fast_sqrt0(v.y)), k.eps);
+    const float2 num = mul2(scx, m1);
+    z = sub2(z, mul2(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y))));
 }
 
 __device__ __forceinline__ void adam_step2(const OptConst& o, float2 sc, float2& z, float2& m1, float2& m2,

@@ -23,6 +23,7 @@ struct DevVol {
     double normd;
     int dims[3];        // TV grid
     long long grid_off; // offset of the volume's grid in the TV grid buffers
+    long long hgrid_off; // offset of the volume's haloed map in the persistent kernel's map buffers
     float tv_scale[kMaxReg];  // lambda_k / Nmask (spatial_total_variation.m:40; also the prior's)
     float prior_off;    // prior regulariser loss of the grid points outside the mask
 };
@@ -233,8 +234,14 @@ struct PersistBarrier {
 struct PersistArgs {
     int e_begin, e_end, update_last;
     int record, want_res, stats, loss;
-    float* grid0;            // TV map of even epochs' input (parity 0)
+    // TV maps of the persistent kernel (input of even / odd epochs): per
+    // volume (dx+2) x (dy+2) x (dz+2) with a one-cell halo on every face that
+    // holds the periodic neighbour's value, so that every neighbour load has
+    // a fixed offset; [n_reg][hgrid_total], zero outside the mask
+    float* grid0;
     float* grid1;
+    long long hgrid_total;
+    int hlayout;             // L = 7, 8, 9: strides 2^L, 2^2L; 0: (dx+2), (dx+2)(dy+2) per volume
     PersistBarrier* barrier; // zeroed before the launch
     int slice;               // voxels per CTA
     int data_in_smem;
@@ -242,6 +249,7 @@ struct PersistArgs {
     const float4* data_quads; // [quad_width/4][nvtot] echo quads of the measurements, or nullptr
     long long spin_cycles;   // bound of every wait, SM clock cycles (kBarrierSpinCycles unless a test sets it)
     unsigned int extra_arrivals; // 0; a test's count of arrivals the grid barrier waits for beyond the grid's
+    PairConsts k;            // constants of the two-voxel variant (filled by launch_tv_persistent)
 };
 
 struct PersistPlan {
