@@ -238,9 +238,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     float* s_st = reinterpret_cast<float*>(s_red + 2 * 32 * kHistW);         // [NS][NP][slice]
     // CACHE: the standard configuration without statistics keeps, from the
     // fidelity pass, the unregularised parameter's z-gradient and the
-    // regularised one's fidelity gradient, dtheta/dz and theta (in the space
-    // the previous-epoch z takes when statistics are on), so the TV/update
-    // pass does not evaluate the transform again; same operations, same order.
+    // regularised one's fidelity gradient (in the space the previous-epoch z
+    // takes when statistics are on), and from the update pass the regularised
+    // parameter's theta and dtheta/dz, so that no pass evaluates a transform
+    // another pass has evaluated; same operations, same order.
     // PAIR (up to 16 measurements, without statistics): two voxels per
     // thread, pair instructions, with the fidelity-pass cache (CACHE)
     constexpr bool PAIR = persist_pairs(MAXM, STATS);
@@ -265,6 +266,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         double normd;
         long long grid_off, hgrid_off;
     } V{Vg.off, Vg.nvox, Vg.norm, Vg.normd, Vg.grid_off, Vg.hgrid_off};
+    const int nreal = V.off + V.nvox - base;  // slice voxels i < nreal are real (the padding follows)
     const float tvs0 = Vg.tv_scale[0], tvs1 = Vg.tv_scale[1];
     const int dx = Vg.dims[0], dy = Vg.dims[1], dz = Vg.dims[2];
     const int sy = dx, sz = dx * dy;
@@ -309,6 +311,13 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         const int j = sidx(i);
         s_p[j] = pp;
         s_w[j] = w;
+        if constexpr (CACHE) {  // theta and dtheta/dz of the regularised parameter (see pass 2)
+            const int k = a.reg_param[0];
+            float dd;
+            const float th = unscale(0, a.P.lb[k], a.P.ub[k], a.z[(size_t)k * a.nvtot + v], dd);
+            s_gf[2 * S + j] = dd;
+            s_gf[3 * S + j] = th;
+        }
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             size_t gi = (size_t)k * a.nvtot + base + i;
@@ -403,7 +412,6 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         // code (false: a wait has failed, the kernel returns)
         auto pair_epoch = [&](auto KR, auto HLC) -> bool {
         constexpr int kr = decltype(KR)::value, HL = decltype(HLC)::value;
-        const size_t half = (size_t)(a.nvtot >> 1);
         const int npair = n >> 1;  // n is a multiple of 64 in pair mode
         // shared memory: pair q at float2 position q; global: voxels v0, v0+32
         auto ld2 = [](const float* b, int q) { return reinterpret_cast<const float2*>(b)[q]; };
@@ -415,13 +423,15 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         // pass 1: data fidelity of the slice (own voxels only)
         for (int q = tid; q < npair; q += NWT) {
             const int i0 = ((q >> 5) << 6) + (q & 31), v0 = base + i0;
-            const bool ok0 = (v0 - V.off) < V.nvox, ok1 = (v0 + 32 - V.off) < V.nvox;
+            const bool ok0 = i0 < nreal, ok1 = i0 + 32 < nreal;
             float2 y[MAXM];  // measurement m of both voxels
             if (p.data_quads) {
-                const float4* pq = p.data_quads + (base >> 1) + q;
+                // chunk-interleaved pair quads: quad j of pair u at
+                // ((u / 32) (MAXM / 2) + j) 32 + u % 32 (constant offsets)
+                const float4* pq = p.data_quads + (size_t)((base >> 6) + (q >> 5)) * (MAXM / 2) * 32 + (q & 31);
 #pragma unroll
                 for (int j = 0; j < MAXM / 2; ++j) {
-                    const float4 t = __ldcg(pq + j * half);
+                    const float4 t = __ldcg(pq + j * 32);
                     y[2 * j] = make_float2(t.x, t.y);
                     y[2 * j + 1] = make_float2(t.z, t.w);
                 }
@@ -435,7 +445,13 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             }
             float2 th[NP], dth[NP];
 #pragma unroll
-            for (int k = 0; k < NP; ++k) th[k] = unscale_sig2c(p.k, k, ld2(s_st + k * S, q), dth[k]);
+            for (int k = 0; k < NP; ++k)
+                if (k == kr) {  // written by the previous update (or the staging)
+                    th[k] = ld2(s_gf + 3 * S, q);
+                    dth[k] = ld2(s_gf + 2 * S, q);
+                } else {
+                    th[k] = unscale_sig2c(p.k, k, ld2(s_st + k * S, q), dth[k]);
+                }
             // R2sMseSums on both lanes with the residual negated, y - M0 E:
             // every partial sum is the exact negative of the scalar one
             float2 sse = make_float2(0.f, 0.f), g0n = sse, g1n = sse;
@@ -466,8 +482,6 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             const float2 gr = mul2(kr == 0 ? g[0] : g[1], nrm), gn = mul2(kr == 0 ? g[1] : g[0], nrm);
             st2(s_gf + 0 * S, q, mul2(gn, kr == 0 ? dth[1] : dth[0]));
             st2(s_gf + 1 * S, q, gr);
-            st2(s_gf + 2 * S, q, kr == 0 ? dth[0] : dth[1]);
-            st2(s_gf + 3 * S, q, kr == 0 ? th[0] : th[1]);
             if (ok0) q0 += tot.x;
             if (ok1) q0 += tot.y;
         }
@@ -484,7 +498,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         // pass 2: TV subgradient, chain rule, optimiser, new map values
         for (int q = tid; q < npair; q += NWT) {
             const int i0 = ((q >> 5) << 6) + (q & 31), v0 = base + i0;
-            const bool ok0 = (v0 - V.off) < V.nvox, ok1 = (v0 + 32 - V.off) < V.nvox;
+            const bool ok0 = i0 < nreal, ok1 = i0 + 32 < nreal;
             const float2 gn = ld2(s_gf + 0 * S, q);
             float2 grf = ld2(s_gf + 1 * S, q);
             const float2 dthr = ld2(s_gf + 2 * S, q);
@@ -530,6 +544,10 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                 }
                 float2 dd;
                 const float2 thr = unscale_sig2c(p.k, kr, zr, dd);
+                // the new map value and its dtheta/dz serve the next
+                // fidelity pass too (the same transform of the same z)
+                st2(s_gf + 2 * S, q, dd);
+                st2(s_gf + 3 * S, q, thr);
                 if (ok0) Gn[p0] = thr.x;
                 if (ok1) Gn[p1] = thr.y;
                 const unsigned int fw0 = ok0 ? w01.x >> 24 : 0u, fw1 = ok1 ? w01.y >> 24 : 0u;
@@ -915,18 +933,21 @@ __global__ void echo_quads_kernel(const float* data, int nm, int nvtot, int widt
 }
 
 // Pair quads: with the voxel pairs (u0, u0 + 32), u0 = 64 (u / 32) + u % 32,
-// out[j][u] = (y_2j(u0), y_2j(u0+32), y_2j+1(u0), y_2j+1(u0+32)).
+// quad j of pair u = (y_2j(u0), y_2j(u0+32), y_2j+1(u0), y_2j+1(u0+32)) at
+// out[((u / 32) (width / 2) + j) 32 + u % 32]: the width / 2 quads of 32
+// consecutive pairs lie together, 512 bytes apart.
 __global__ void pair_quads_kernel(const float* data, int nm, int nvtot, int width, float4* out) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     const int npair = nvtot >> 1;
     if (u >= npair) return;
     const int u0 = ((u >> 5) << 6) + (u & 31);
+    float4* o = out + (size_t)(u >> 5) * (width / 2) * 32 + (u & 31);
     for (int j = 0; j < width / 2; ++j) {
         const int m0 = 2 * j, m1 = 2 * j + 1;
         const float* r0 = data + (size_t)m0 * nvtot + u0;
         const float* r1 = data + (size_t)m1 * nvtot + u0;
-        out[(size_t)j * npair + u] = make_float4(m0 < nm ? r0[0] : 0.f, m0 < nm ? r0[32] : 0.f,
-                                                 m1 < nm ? r1[0] : 0.f, m1 < nm ? r1[32] : 0.f);
+        o[j * 32] = make_float4(m0 < nm ? r0[0] : 0.f, m0 < nm ? r0[32] : 0.f, m1 < nm ? r1[0] : 0.f,
+                                m1 < nm ? r1[32] : 0.f);
     }
 }
 

@@ -246,7 +246,7 @@ struct PersistArgs {
     int slice;               // voxels per CTA
     int data_in_smem;
     int pad_block;           // block size of the work-list padding (blk_vol granularity)
-    const float4* data_quads; // [quad_width/4][nvtot] echo quads of the measurements, or nullptr
+    const float4* data_quads; // echo quads of the measurements (launch_echo_quads layout), or nullptr
     long long spin_cycles;   // bound of every wait, SM clock cycles (kBarrierSpinCycles unless a test sets it)
     unsigned int extra_arrivals; // 0; a test's count of arrivals the grid barrier waits for beyond the grid's
     PairConsts k;            // constants of the two-voxel variant (filled by launch_tv_persistent)
@@ -263,8 +263,10 @@ bool plan_persistent(const AdamParams& a, int model, int loss, bool stats, int p
                      int nvol, PersistPlan* plan);
 cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, PersistArgs p, cudaStream_t s);
 // Echo quads out[j][v] = (data[4j][v], .., data[4j+3][v]), or with pairs
-// out[j][u] = (data[2j][2u], data[2j][2u+1], data[2j+1][2u], data[2j+1][2u+1]);
-// 0 for nm <= m < width (width % 4 == 0, nvtot even)
+// (voxels u0 = 64 (u / 32) + u % 32 and u0 + 32) quad j of pair u =
+// (data[2j][u0], data[2j][u0+32], data[2j+1][u0], data[2j+1][u0+32]) at
+// out[((u / 32) (width / 2) + j) 32 + u % 32]; 0 for nm <= m < width
+// (width % 4 == 0; nvtot even, with pairs a multiple of 64)
 cudaError_t launch_echo_quads(const float* data, int nm, int nvtot, int width, bool pairs, float4* out,
                               cudaStream_t s);
 
