@@ -30,11 +30,12 @@ sys.path.insert(0, ROOT)
 NITER = 4000
 ALG_BYTES_PER_VOXEL_ITER = 100.0   # 12 echoes x 4 B data + (z, m, v) x 2 params read+write + 4 B TV map
 # compute per voxel-iteration of the standard R2* + TV step, counted from the kernel source:
-# MUFU ops = 12 ex2 (echoes) + 3 x (ex2 + rcp) (sigmoid, twice in the fidelity pass, once for the
-# map) + 2 x (sqrt + rcp) (Adam); FP32 FLOP (FMA = 2) = 12 x 9 (echoes) + 3 x 8 (sigmoid)
-# + 8 (loss / gradient scaling) + 24 (TV, 3 axes) + 2 x 13 (Adam)
-SFU_OPS_PER_VOXEL_ITER = 22.0
-FP32_FLOP_PER_VOXEL_ITER = 190.0
+# MUFU ops = 12 ex2 (echoes) + 2 x (ex2 + rcp) (sigmoid of each parameter once per iteration: the
+# regularised one's serves the map and the next fidelity pass) + 2 x (sqrt + rcp) (Adam);
+# FP32 FLOP (FMA = 2) = 12 x 9 (echoes) + 2 x 8 (sigmoid) + 8 (loss / gradient scaling)
+# + 24 (TV, 3 axes) + 2 x 13 (Adam)
+SFU_OPS_PER_VOXEL_ITER = 20.0
+FP32_FLOP_PER_VOXEL_ITER = 182.0
 METRIC = "askAdam voxel-fits/s & MCMC samples/s, fused vs plain GPU, equal FP64 error"
 WORKLOAD = ("askAdam R2* MSE + 3-D TV (lambda 1e-3 on R2*), 128x128x64 ellipsoid mask (629,432 voxels), "
             "12 echoes TE=2:3.5:40.5 ms, Adam lr 0.01, 4000 iterations")
