@@ -336,6 +336,41 @@ def test_tv_persistent_kernel_matches_per_epoch_kernel(ctx, case, monkeypatch):
         assert a["final_niteration"] == 151
 
 
+@pytest.mark.parametrize("shape,tv_mode", [((200, 30, 12), "3D"), ((300, 24, 10), "3D"), ((600, 12, 6), "3D"),
+                                           ((40, 40, 24), "2D"), ((300, 24, 10), "2D")])
+def test_tv_persistent_map_layouts_match_per_epoch_kernel(ctx, shape, tv_mode, monkeypatch):
+    """The persistent kernel keeps its TV map with a one-cell halo of the
+    periodic neighbours, laid out with strides 2^L / 2^2L when the volume's
+    x and y extents (plus the halo) fit 2^L (L = 7, 8, 9) and with strides
+    (dx+2), (dx+2)(dy+2) otherwise.  Volumes of 200, 300 and 600 voxels in x
+    take L = 8, 9 and the run-time strides; the ellipsoid mask touches every
+    face of the grid, so the halo copies (the wrap-around of
+    utils/spatial_total_variation.m:55-66) are exercised, in 3-D and in 2-D
+    TV.  Each fit equals the one-launch-per-epoch kernel's, which reads the
+    plain grid with explicit wrap-around."""
+    from gacelle_b200 import phantoms, utils
+    te = np.arange(2.0, 40.6, 3.5) * 1e-3
+    mask = phantoms.ellipsoid_mask(shape, 1.1)
+    for ax in range(3):
+        assert np.take(mask, 0, axis=ax).any() and np.take(mask, -1, axis=ax).any()
+    data, _ = phantoms.r2s_phantom(mask, 11, te=te)
+    idx = utils.mask_index(mask)
+    y = utils.reshape_ND2GD(data, idx)
+    th0 = np.tile(np.array([[1.0], [30.0]], np.float32), (1, y.shape[1]))
+    kw = dict(dims=mask.shape, gidx=idx.astype(np.int32), te=te)
+    f = fitting(iteration=200, initialLearnRate=0.01, **{"lambda": [1e-5], "regmap": ["R2star"], "TVmode": tv_mode})
+    monkeypatch.setenv("GACELLE_B200_TV_KERNEL", "step")
+    a = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
+    monkeypatch.setenv("GACELLE_B200_TV_KERNEL", "persistent")
+    b = run_engine("r2s", y, th0, f, NAMES["r2s"], **kw)
+    assert a["timing"]["tv_path"] == 0 and b["timing"]["tv_path"] & P_
+    for k in range(2):
+        assert rel_rmse(b["final_theta"][k], a["final_theta"][k]) <= 1e-5, k
+        assert rel_rmse(b["min_theta"][k], a["min_theta"][k]) <= 1e-5, k
+    assert a["min_niteration"] == b["min_niteration"]
+    np.testing.assert_allclose(a["loss_history"][:201], b["loss_history"][:201], rtol=1e-6)
+
+
 @pytest.mark.parametrize("stream_kind", ["side", "default"])
 def test_device_resident_call_on_torch_stream_matches_host_call(stream_kind):
     """gx_askadam with device pointers (GX_MEM_DEVICE) on a PyTorch stream --
