@@ -997,11 +997,13 @@ static gx_status replay_volume(AdamJob& J, int i, int target, float* th_out, flo
     V.a.ckpt = nullptr;
     CK(launch_copy_state(V.a, src, nullptr, nullptr, nullptr, false, J.B, V.nblocks, c->stream));
     int e0 = slot * J.ckpt_every + 1;
-    if (J.tv) CK(launch_tv_scatter(V.a, J.grid[(e0 - 1) & 1], J.B, V.nblocks, c->stream));  // e0 >= 1
-    size_t o = J.hv[i].off;
     // a job of one volume replays through the cooperative TV kernel (its plan
     // covers exactly this view; it computes bit for bit what the per-epoch
-    // kernel does); a view of a larger job runs one launch per epoch
+    // kernel does, and writes its own start map); a view of a larger job runs
+    // one launch per epoch, from the map of its start state
+    const bool persist = J.nvol == 1 && J.use_persist;
+    if (J.tv && !persist) CK(launch_tv_scatter(V.a, J.grid[(e0 - 1) & 1], J.B, V.nblocks, c->stream));  // e0 >= 1
+    size_t o = J.hv[i].off;
     TRY(run_epochs(J, V.a, V.nblocks, e0, target + 1, target, false, res_out ? res_out + o : nullptr,
                    J.nvol == 1));
     CK(launch_finalize(V.a, V.a.z, th_out + o, nullptr, nullptr, J.B, V.nblocks, c->stream));
@@ -1133,7 +1135,6 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
     TRY(alloc_outputs(J, out));
     if (J.autotune) TRY(tune_fused(J));
     if (J.tv) {
-        CK(launch_tv_scatter(J.a, J.grid[0], J.B, J.nblocks, c->stream));
         const char* env = getenv("GACELLE_B200_TV_KERNEL");
         bool want = !(env && strcmp(env, "step") == 0);
         std::vector<int> npad(J.nvol);
@@ -1158,6 +1159,9 @@ static gx_status adam_fused(AdamJob& J, AdamOut& out) {
             CK(launch_echo_quads(J.a.data, J.nm, J.nvtot, J.plan.quad_width, J.plan.quad_pairs != 0, J.data_quads,
                                  c->stream));
         }
+        // the per-epoch kernel reads the start map from the plain grid (the
+        // persistent kernel writes its own)
+        if (!J.use_persist) CK(launch_tv_scatter(J.a, J.grid[0], J.B, J.nblocks, c->stream));
     }
 
     out.tr.assign(J.nvol, Tracker());
