@@ -133,7 +133,7 @@ __global__ void init_state_kernel(AdamParams a, const float* theta0, float rando
 // Fused multi-epoch kernel (no spatial coupling).
 // ---------------------------------------------------------------------------
 template <int MODEL, int LOSS, bool STATS>
-__global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_last, int record) {
+__device__ __forceinline__ void fused_body(const AdamParams& a, int e_begin, int e_end, int update_last, int record) {
     constexpr int NP = ModelNP<MODEL>::value;
     constexpr int NQ = STATS ? kHistW : 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -189,7 +189,7 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
         acc.aux = aux; acc.mse_scale = a.mse_scale; acc.hd = a.huber_delta;
         acc.res = (a.res_out && e == e_end && valid) ? a.res_out + v : nullptr;
         acc.rs = a.nvtot;
-        model_eval<MODEL>(s_P, th, va, acc);
+        model_eval<MODEL, MODEL == kR1R2S>(s_P, th, va, acc);
         acc.finish();
         float gz[NP];
         float reg = 0.0f;
@@ -255,6 +255,26 @@ __global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_la
             if (STATS) a.zprev[i] = zp[k];
         }
     }
+}
+
+template <int MODEL, int LOSS, bool STATS>
+__global__ void fused_kernel(AdamParams a, int e_begin, int e_end, int update_last, int record) {
+    fused_body<MODEL, LOSS, STATS>(a, e_begin, e_end, update_last, record);
+}
+
+// The joint R1-R2* model's fused kernel: the two-angle, 12-echo protocol with
+// its echo loop unrolled, registers capped at 80 (unrolled and uncapped it
+// takes 128 and loses half of the resident warps).
+template <int LOSS, bool STATS>
+__global__ void __maxnreg__(80) fused_kernel_r1r2s(AdamParams a, int e_begin, int e_end, int update_last,
+                                                   int record) {
+    fused_body<kR1R2S, LOSS, STATS>(a, e_begin, e_end, update_last, record);
+}
+
+template <int MODEL, int LOSS, bool STATS>
+constexpr auto fused_kernel_fn() {
+    if constexpr (MODEL == kR1R2S) return &fused_kernel_r1r2s<LOSS, STATS>;
+    else return &fused_kernel<MODEL, LOSS, STATS>;
 }
 
 // ---------------------------------------------------------------------------
@@ -880,7 +900,7 @@ static cudaError_t fused_dispatch3(const AdamParams& a, int e_begin, int e_end, 
     constexpr int NQ = STATS ? kHistW : 1;
     size_t smem = sizeof(double) * 2 * 32 * NQ +
                   sizeof(float) * (size_t)block * (a.nm * (a.weights ? 2 : 1) + 2 * a.P.n_fa);
-    auto k = fused_kernel<MODEL, LOSS, STATS>;
+    auto k = fused_kernel_fn<MODEL, LOSS, STATS>();
     if (smem > 48 * 1024) {
         cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (err != cudaSuccess) return err;
@@ -909,7 +929,7 @@ static cudaError_t fused_dispatch2(const AdamParams& a, int loss, int e_begin, i
 template <int MODEL, int LOSS, bool STATS>
 static int fused_limit3(const AdamParams& a) {
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, fused_kernel<MODEL, LOSS, STATS>) != cudaSuccess) return 0;
+    if (cudaFuncGetAttributes(&fa, fused_kernel_fn<MODEL, LOSS, STATS>()) != cudaSuccess) return 0;
     int dev = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)

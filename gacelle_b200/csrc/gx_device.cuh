@@ -534,12 +534,15 @@ __device__ __forceinline__ void model_r2s_unrolled(const DevProtocol& P, int nm,
 // for R2*), r = (A M0) E2 - y, and per flip angle f the sums sum q and sum
 // te q with q = r E2, so that dS/dM0 = A E2, dS/dR1 = M0 E2 dA/dR1 and dS/dR2*
 // = -te A M0 E2 are applied once per voxel.  Explicit roundings; echo times
-// outer, flip angles inner.  RES: the residual output is written.
-template <int NFA, bool EXACT, bool RES, class Acc>
+// outer, flip angles inner.  RES: the residual output is written.  NTE > 0:
+// exactly NTE echo times, the loop unrolled (the echo constants become
+// constant-bank operands, no loop control); 0: any number.
+template <int NFA, bool EXACT, bool RES, int NTE, class Acc>
 __device__ __forceinline__ void r1r2s_mse_sums(const DevProtocol& P, float R2, int nfa, const float (&AM0)[NFA],
                                                float& sse, float (&Sq)[NFA], float (&Stq)[NFA], Acc& acc) {
-    const int nte = P.n_te;
-#pragma unroll 2
+    const int nte = NTE > 0 ? NTE : P.n_te;
+    constexpr int UNROLL = NTE > 0 ? NTE : 2;
+#pragma unroll UNROLL
     for (int t = 0; t < nte; ++t) {
         const float te = P.te[t];
         const float E2 = ex2_ftz(mul1(-P.te_l2e[t], R2));
@@ -557,7 +560,7 @@ __device__ __forceinline__ void r1r2s_mse_sums(const DevProtocol& P, float R2, i
     }
 }
 
-template <int NFA, bool EXACT, class Acc>
+template <int NFA, bool EXACT, int NTE, class Acc>
 __device__ __forceinline__ void r1r2s_mse(const DevProtocol& P, float M0, float R1, float R2, const VoxAux& va,
                                           Acc& acc) {
     const float E1 = __expf(-P.tr * R1);
@@ -577,8 +580,8 @@ __device__ __forceinline__ void r1r2s_mse(const DevProtocol& P, float M0, float 
         Stq[f] = 0.0f;
     }
     float sse = 0.0f;
-    if (acc.res) r1r2s_mse_sums<NFA, EXACT, true>(P, R2, nfa, AM0, sse, Sq, Stq, acc);
-    else r1r2s_mse_sums<NFA, EXACT, false>(P, R2, nfa, AM0, sse, Sq, Stq, acc);
+    if (acc.res) r1r2s_mse_sums<NFA, EXACT, true, NTE>(P, R2, nfa, AM0, sse, Sq, Stq, acc);
+    else r1r2s_mse_sums<NFA, EXACT, false, NTE>(P, R2, nfa, AM0, sse, Sq, Stq, acc);
     float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
 #pragma unroll
     for (int f = 0; f < NFA; ++f)
@@ -594,18 +597,21 @@ __device__ __forceinline__ void r1r2s_mse(const DevProtocol& P, float M0, float 
 }
 
 // S = M0 sin(a)(1-E1)/(1-cos(a)E1) exp(-TE R2*), E1 = exp(-TR R1), a = b1*FA;
-// measurement index TE fastest then FA (R1R2s/gpuJointR1R2starMapping.m:375-422,513-525)
-template <class Acc>
+// measurement index TE fastest then FA (R1R2s/gpuJointR1R2starMapping.m:375-422,513-525).
+// UNROLL (the register-capped fused kernel): the two-angle, 12-echo protocol
+// with its echo loop unrolled.
+template <bool UNROLL, class Acc>
 __device__ __forceinline__ void model_r1r2s(const DevProtocol& P, const float* th,
                                             const VoxAux& va, Acc& acc) {
     float M0 = th[0], R1 = th[1], R2 = th[2];
     if constexpr (AccMse<Acc>::value) {
         if (P.n_fa == 2) {
-            r1r2s_mse<2, true>(P, M0, R1, R2, va, acc);
+            if (UNROLL && P.n_te == 12) r1r2s_mse<2, true, 12>(P, M0, R1, R2, va, acc);
+            else r1r2s_mse<2, true, 0>(P, M0, R1, R2, va, acc);
             return;
         }
         if (P.n_fa <= 4) {
-            r1r2s_mse<4, false>(P, M0, R1, R2, va, acc);
+            r1r2s_mse<4, false, 0>(P, M0, R1, R2, va, acc);
             return;
         }
     }
@@ -774,11 +780,13 @@ __device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const floa
     }
 }
 
-template <int MODEL, class Acc>
+// UNROLL: unrolled protocol loops where a caller's register budget allows
+// (the fused kernel of the joint R1-R2* model).
+template <int MODEL, bool UNROLL = false, class Acc>
 __device__ __forceinline__ void model_eval(const DevProtocol& P, const float* th, const VoxAux& va,
                                            Acc& acc) {
     if constexpr (MODEL == kR2S) model_r2s(P, th, acc);
-    else if constexpr (MODEL == kR1R2S) model_r1r2s(P, th, va, acc);
+    else if constexpr (MODEL == kR1R2S) model_r1r2s<UNROLL>(P, th, va, acc);
     else if constexpr (MODEL == kNEXI) model_nexi_impl<false, Acc, 4>(P, th, va, acc);
     else model_nexi_impl<true, Acc, 5>(P, th, va, acc);
 }
