@@ -494,7 +494,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
         float* cp = ckpt ? a.ckpt + (size_t)(e / a.ckpt_every) * 3 * NP * a.nvtot : nullptr;
         const float* G = gcur + V.hgrid_off;
         float* Gn = gnext + V.hgrid_off;
-        const float2 scx = bcast2(sc.x), scy = bcast2(sc.y);
+        const float2 nscx = bcast2(-sc.x), scy = bcast2(sc.y);
         // pass 2: TV subgradient, chain rule, optimiser, new map values
         for (int q = tid; q < npair; q += NWT) {
             const int i0 = ((q >> 5) << 6) + (q & 31), v0 = base + i0;
@@ -512,7 +512,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
             hm.load<HL>(G, p0, f0, b0);
             hm.load<HL>(G, p1, f1, b1);
             float2 cost, gt;
-            tv_terms2m(c, f0, b0, f1, b1, w01.x, w01.y, p.k.iv, tv3 ? 3 : 2, cost, gt);
+            tv_terms2m(c, f0, b0, f1, b1, w01.x, w01.y, p.k.iv, p.k.niv, tv3 ? 3 : 2, cost, gt);
             if (ok0) {
                 q1 = __fmaf_rn(tvs0, cost.x, q1);
                 grf.x = fma1(tvs0, gt.x, grf.x);
@@ -531,7 +531,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
                     float* p1s = s_st + (1 * NP + k) * S;
                     float* p2s = s_st + (2 * NP + k) * S;
                     float2 zz = ld2(pz, q), mm1 = ld2(p1s, q), mm2 = ld2(p2s, q);
-                    adam_step2c(p.k, scx, scy, zz, mm1, mm2, gz[k]);
+                    adam_step2c(p.k, nscx, scy, zz, mm1, mm2, gz[k]);
                     st2(pz, q, zz);
                     st2(p1s, q, mm1);
                     st2(p2s, q, mm2);
@@ -898,7 +898,10 @@ cudaError_t launch_tv_persistent(const AdamParams& a, const PersistPlan& plan, P
     p.k.eps = pr(a.eps);
     p.k.mse = pr(a.mse_scale);
     p.k.s2 = pr(2.0f * a.mse_scale);
-    for (int d = 0; d < 3; ++d) p.k.iv[d] = pr(a.inv_vs[d]);
+    for (int d = 0; d < 3; ++d) {
+        p.k.iv[d] = pr(a.inv_vs[d]);
+        p.k.niv[d] = pr(-a.inv_vs[d]);
+    }
     p.data_in_smem = plan.data_in_smem;
     // the register-prefetch variants write residuals after their epoch loop,
     // which needs a launch whose last epoch is not followed by an update

@@ -842,7 +842,8 @@ __device__ __forceinline__ float unscale(int transform, float lb, float ub, floa
 // neighbour along axis d (periodic), mb[d] = backward neighbour inside the
 // mask, iv[d] = 1/voxel size.  cost = sum_d |f_d - c| iv_d;
 // d cost_total / d c = sum_d (-sgn(f_d - c) + mb_d sgn(c - b_d)) iv_d.
-// One function for every kernel so that all paths round identically.
+// One function for every one-voxel kernel (tv_terms2m restates it for two
+// voxels) so that all paths round identically.
 // sign(x) in {-1, 0, +1} (0 for +-0), as compare-and-select.
 __device__ __forceinline__ float sgn0(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
 
@@ -853,7 +854,7 @@ __device__ __forceinline__ void tv_terms(float c, const float* f, const float* b
     for (int d = 0; d < 3; ++d) {
         if (d < nd) {
             const float df = sub1(f[d], c);
-            cs = add1(cs, fabsf(mul1(df, iv[d])));
+            cs = fma1(fabsf(df), iv[d], cs);  // fused, as the two-voxel form
             const float t = -sgn0(df) + (mb[d] ? sgn0(sub1(c, b[d])) : 0.0f);  // small integers: exact
             gr = add1(gr, mul1(t, iv[d]));
         }
@@ -895,29 +896,6 @@ __device__ __forceinline__ void prior_terms(float th, float mu, float sd, float&
     grad = ok ? __fdiv_rn(sgn0(z), sd) : 0.0f;
 }
 
-// tv_terms for two voxels on the lanes of pair instructions (lane results
-// bit for bit those of tv_terms); mb0 / mb1 as in tv_terms.
-__device__ __forceinline__ void tv_terms2(float2 c, const float (&f0)[3], const float (&b0)[3], const float (&f1)[3],
-                                          const float (&b1)[3], const bool (&mb0)[3], const bool (&mb1)[3],
-                                          const float* iv, int nd, float2& cost, float2& grad) {
-    float2 cs = make_float2(0.0f, 0.0f), gr = cs;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        if (d < nd) {
-            const float2 ivd = make_float2(iv[d], iv[d]);
-            const float2 df = sub2(make_float2(f0[d], f1[d]), c);
-            const float2 m = mul2(df, ivd);
-            cs = add2(cs, make_float2(fabsf(m.x), fabsf(m.y)));
-            const float2 cb = sub2(c, make_float2(b0[d], b1[d]));
-            const float2 t = make_float2(-sgn0(df.x) + (mb0[d] ? sgn0(cb.x) : 0.0f),
-                                         -sgn0(df.y) + (mb1[d] ? sgn0(cb.y) : 0.0f));
-            gr = add2(gr, mul2(t, ivd));
-        }
-    }
-    cost = cs;
-    grad = gr;
-}
-
 // Saturated product (PTX mul.sat: the result clamped to [0, 1], NaN to 0).
 __device__ __forceinline__ float mul_sat1(float a, float b) {
     float d;
@@ -935,18 +913,20 @@ __device__ __forceinline__ float mask_scale(unsigned int w, int d) {
     return __int_as_float((int)__byte_perm(w, 0u, (unsigned int)d * 0x1111u));
 }
 
-// tv_terms2 with the signs as saturated products and the mask as a scale
-// (w0 / w1: the two voxels' mask words).  With subnormals flushed every
-// nonzero x has |x| >= 2^-126, so sat(x K) - sat(-x K) = sgn0(x) exactly for
-// K >= 2^127 (and 0 for x = 0 or NaN), and sat(x 0) = 0 drops a backward
-// term outside the mask; -|df| = df (-sgn0(df)) exactly.  Every lane result
-// equals tv_terms' bit for bit: the costs add the same rounded |df iv|, and
-// the gradient terms are small integers times iv (exact products), so the
-// fused multiply-add rounds as the separate multiply and add.
-// ivp: the inverse voxel sizes as (iv, iv) pairs.
+// tv_terms for two voxels on the lanes of pair instructions, with the signs
+// as saturated products and the mask as a scale (w0 / w1: the two voxels'
+// mask words).  With subnormals flushed every nonzero x has |x| >= 2^-126,
+// so sat(x K) - sat(-x K) = sgn0(x) exactly for K >= 2^127 (and 0 for x = 0
+// or NaN), and sat(x 0) = 0 drops a backward term outside the mask;
+// -|df| = df (-sgn0(df)) exactly.  Every lane result equals tv_terms' bit
+// for bit: the costs add |df| iv by the same fused multiply-add, and the
+// gradient terms are small integers times iv (exact products), so the fused
+// multiply-add rounds as the separate multiply and add.
+// ivp / nivp: the inverse voxel sizes and their negatives as (x, x) pairs.
 __device__ __forceinline__ void tv_terms2m(float2 c, const float (&f0)[3], const float (&b0)[3],
                                            const float (&f1)[3], const float (&b1)[3], unsigned int w0,
-                                           unsigned int w1, const float2* ivp, int nd, float2& cost, float2& grad) {
+                                           unsigned int w1, const float2* ivp, const float2* nivp, int nd,
+                                           float2& cost, float2& grad) {
     const float K = __int_as_float(0x7F7F7F7F);
     float2 cs = make_float2(0.0f, 0.0f), gr = cs;
 #pragma unroll
@@ -956,7 +936,7 @@ __device__ __forceinline__ void tv_terms2m(float2 c, const float (&f0)[3], const
             const float2 df = sub2(make_float2(f0[d], f1[d]), c);
             const float2 snf = sub2(make_float2(mul_sat1(-df.x, K), mul_sat1(-df.y, K)),
                                     make_float2(mul_sat1(df.x, K), mul_sat1(df.y, K)));  // -sgn0(df)
-            cs = sub2(cs, mul2(mul2(df, snf), ivd));                                   // + |df iv|
+            cs = fma2(mul2(df, snf), nivp[d], cs);                                      // + |df| iv
             const float2 cb = sub2(c, make_float2(b0[d], b1[d]));
             const float k0 = mask_scale(w0, d), k1 = mask_scale(w1, d);
             const float2 sb = sub2(make_float2(mul_sat1(cb.x, k0), mul_sat1(cb.y, k1)),
@@ -986,12 +966,16 @@ __device__ __forceinline__ float fast_sqrt0(float x) {
 }
 
 // Adam: m1 = b1 m1 + (1-b1) g, m2 = b2 m2 + ((1-b2) g) g,
-// z -= (lr_e m1) / (sqrt(m2 / (1-b2^e)) + eps).
+// z -= (lr_e m1) / (sqrt(m2 / (1-b2^e)) + eps), the last step as one fused
+// multiply-add z + (-(lr_e m1)) (1 / (...)).  (ptxas contracts an FP32x2
+// multiply followed by a subtraction into a fused multiply-add even with an
+// explicit .rn rounding, so the two-voxel form is fused; every form is
+// written fused so that all kernels round alike.)
 __device__ __forceinline__ void opt_step(const OptConst& o, float2 sc, float& z, float& m1, float& m2, float g) {
     if (o.optimiser == kAdam) {
         m1 = fma1(o.beta1, m1, mul1(sub1(1.0f, o.beta1), g));
         m2 = fma1(o.beta2, m2, mul1(mul1(sub1(1.0f, o.beta2), g), g));
-        z = sub1(z, mul1(mul1(sc.x, m1), rcp_ftz(add1(fast_sqrt0(mul1(m2, sc.y)), o.eps))));
+        z = fma1(mul1(-sc.x, m1), rcp_ftz(add1(fast_sqrt0(mul1(m2, sc.y)), o.eps)), z);
     } else if (o.optimiser == kSGDM) {
         m1 = o.momentum * m1 - sc.x * g;
         z += m1;
@@ -999,17 +983,6 @@ __device__ __forceinline__ void opt_step(const OptConst& o, float2 sc, float& z,
         m2 = o.rms_decay * m2 + (1.0f - o.rms_decay) * g * g;
         z -= __fdividef(sc.x * g, fast_sqrt0(m2) + o.rms_eps);
     }
-}
-
-// The same transform and Adam step on a pair of voxels (pair instructions;
-// bit for bit the scalar ones on each lane).
-__device__ __forceinline__ float2 unscale_sig2(float lb, float ub, float2 z, float2& dth) {
-    const float2 e = mul2(z, bcast2(-kLog2e));
-    const float2 den = add2(bcast2(1.0f), make_float2(ex2_ftz(e.x), ex2_ftz(e.y)));
-    const float2 s = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
-    const float2 d = bcast2(sub1(ub, lb));
-    dth = mul2(mul2(d, s), sub2(bcast2(1.0f), s));
-    return fma2(d, s, bcast2(lb));
 }
 
 // The constants of the pair transform and optimiser as (x, x) pairs, so that
@@ -1022,9 +995,11 @@ struct PairConsts {
     float2 b1, omb1, b2, omb2, eps;  // Adam: beta1, 1 - beta1, beta2, 1 - beta2, epsilon
     float2 mse, s2;   // mse_scale, 2 mse_scale
     float2 iv[3];     // inverse voxel sizes
+    float2 niv[3];    // their negatives
 };
 
-// unscale_sig2 with its constants from PairConsts (same operations).
+// The sigmoid transform of a pair of voxels with its constants from
+// PairConsts (on each lane bit for bit unscale's operations).
 __device__ __forceinline__ float2 unscale_sig2c(const PairConsts& k, int i, float2 z, float2& dth) {
     const float2 e = mul2(z, k.nl2e);
     const float2 den = add2(k.one, make_float2(ex2_ftz(e.x), ex2_ftz(e.y)));
@@ -1033,26 +1008,16 @@ __device__ __forceinline__ float2 unscale_sig2c(const PairConsts& k, int i, floa
     return fma2(k.rng[i], s, k.lb[i]);
 }
 
-// adam_step2 with its constants from PairConsts and the epoch's schedule as
-// pairs scx = (sc.x, sc.x), scy = (sc.y, sc.y) (same operations).
-__device__ __forceinline__ void adam_step2c(const PairConsts& k, float2 scx, float2 scy, float2& z, float2& m1,
+// The Adam step of opt_step on a pair of voxels, with its constants from
+// PairConsts and the epoch's schedule as pairs nscx = (-sc.x, -sc.x),
+// scy = (sc.y, sc.y) (on each lane bit for bit opt_step's operations).
+__device__ __forceinline__ void adam_step2c(const PairConsts& k, float2 nscx, float2 scy, float2& z, float2& m1,
                                             float2& m2, float2 g) {
     m1 = fma2(k.b1, m1, mul2(k.omb1, g));
     m2 = fma2(k.b2, m2, mul2(mul2(k.omb2, g), g));
     const float2 v = mul2(m2, scy);
     const float2 den = add2(make_float2(fast_sqrt0(v.x), fast_sqrt0(v.y)), k.eps);
-    const float2 num = mul2(scx, m1);
-    z = sub2(z, mul2(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y))));
-}
-
-__device__ __forceinline__ void adam_step2(const OptConst& o, float2 sc, float2& z, float2& m1, float2& m2,
-                                           float2 g) {
-    m1 = fma2(bcast2(o.beta1), m1, mul2(bcast2(sub1(1.0f, o.beta1)), g));
-    m2 = fma2(bcast2(o.beta2), m2, mul2(mul2(bcast2(sub1(1.0f, o.beta2)), g), g));
-    const float2 v = mul2(m2, bcast2(sc.y));
-    const float2 den = add2(make_float2(fast_sqrt0(v.x), fast_sqrt0(v.y)), bcast2(o.eps));
-    const float2 num = mul2(bcast2(sc.x), m1);
-    z = sub2(z, mul2(num, make_float2(rcp_ftz(den.x), rcp_ftz(den.y))));
+    z = fma2(mul2(nscx, m1), make_float2(rcp_ftz(den.x), rcp_ftz(den.y)), z);
 }
 
 #endif  // __CUDACC__
