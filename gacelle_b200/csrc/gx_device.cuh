@@ -664,9 +664,11 @@ __device__ __forceinline__ void model_nexi_impl(const DevProtocol& P, const floa
         float bDa = b * Da;
         float fd2 = omf * d2;
         // nodes in pairs (i, i+1) on the two lanes of pair instructions, an
-        // odd node count padded with a node of weight 0; per lane the same
-        // operations as a node at a time, the sums kept per lane and folded
-        // at the end
+        // odd node count padded with a node of weight 0; per lane the
+        // operations of a node at a time (ptxas may fuse a pair multiply
+        // into the following pair add; this is the model's only form, so
+        // every path rounds alike), the sums kept per lane and folded at
+        // the end
         const float2 z2 = make_float2(0.f, 0.f), half = bcast2(0.5f), one = bcast2(1.0f), two = bcast2(2.0f);
         const float2 bDa2 = bcast2(bDa), base2 = bcast2(base), q42 = bcast2(q4), c12 = bcast2(c1);
         const float2 f2 = bcast2(f), fd22 = bcast2(fd2), d22 = bcast2(d2), omf2 = bcast2(omf);
