@@ -248,7 +248,7 @@ tv_persistent_kernel(AdamParams a, PersistArgs p) {
     constexpr bool CACHE = PAIR;
     constexpr int NAUX = CACHE ? 4 : NP;
     float* s_gf = s_st + (size_t)NS * NP * p.slice;                          // [NAUX][slice] fidelity pass results
-    int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NAUX * p.slice);        // [slice] grid index
+    int* s_p = reinterpret_cast<int*>(s_gf + (size_t)NAUX * p.slice);        // [slice] position in the haloed map
     unsigned int* s_w = reinterpret_cast<unsigned int*>(s_p + p.slice);      // [slice] mask words (mask_scale)
     float* s_y = reinterpret_cast<float*>(s_w + p.slice);                     // [nm][slice] if staged
     const int BT = blockDim.x, tid = threadIdx.x;
